@@ -1,0 +1,346 @@
+// PyTorch extension over the dreamplace_b200 C ABI.
+//
+// Each function checks its tensors the way the reference's pybind ops do
+// (CHECK_FLAT_CUDA / CHECK_CONTIGUOUS / CHECK_EVEN, utility/src/torch.h:62-76),
+// allocates outputs through the caching allocator, launches on the current
+// stream and turns a non-zero C ABI status into a Python RuntimeError.
+// Function names and argument order follow the reference ops they replace:
+//   electric_potential_cuda.{density_map, fixed_density_map, electric_force}
+//   weighted_average_wirelength_cuda_merged.{forward, backward}
+//   pin_pos_cuda.{forward, backward}, hpwl_cuda.forward, move_boundary_cuda.forward,
+//   pws_cuda.forward
+#include <ATen/cuda/CUDAContext.h>
+#include <c10/cuda/CUDAGuard.h>
+#include <torch/extension.h>
+
+#include <cmath>
+
+#include "dreamplace_b200.h"
+
+namespace py = pybind11;
+
+#define CHECK_CUDA_T(x) TORCH_CHECK((x).is_cuda(), #x " must be a CUDA tensor")
+#define CHECK_CONTIG(x) TORCH_CHECK((x).is_contiguous(), #x " must be contiguous")
+#define CHECK_FLAT(x) TORCH_CHECK((x).is_cuda() && (x).is_contiguous() && (x).dim() == 1, #x " must be a flat contiguous CUDA tensor")
+#define CHECK_EVEN(x) TORCH_CHECK(((x).numel() & 1) == 0, #x " must have an even number of elements")
+#define CHECK_F32(x) TORCH_CHECK((x).scalar_type() == at::kFloat, #x " must be float32")
+#define CHECK_I32(x) TORCH_CHECK((x).scalar_type() == at::kInt, #x " must be int32")
+#define DP_CALL(expr)                                                        \
+  do {                                                                       \
+    int _rc = (expr);                                                        \
+    TORCH_CHECK(_rc == DP_OK, "dreamplace_b200: ", dp_last_error(), " (status ", _rc, ")"); \
+  } while (0)
+
+static dp_stream_t cur_stream() { return (dp_stream_t)at::cuda::getCurrentCUDAStream().stream(); }
+template <typename T>
+static T* ptr(const at::Tensor& t) { return t.data_ptr<T>(); }
+template <typename T>
+static T* optr(const c10::optional<at::Tensor>& t) {
+  return (t.has_value() && t->defined() && t->numel() > 0) ? t->data_ptr<T>() : nullptr;
+}
+
+// float reciprocal as the reference CPU op computes it: T(1.0 / (double)T(b))
+static float inv_f(double b) { return (float)(1.0 / (double)(float)b); }
+
+static int fraction_bits(double xl, double yl, double xh, double yh) {
+  double diearea = (xh - xl) * (yh - yl);
+  int integer_bits = std::max((int)std::ceil(std::log2(diearea)) + 1, 32);
+  return std::max(64 - integer_bits, 0);
+}
+
+// ---------------------------------------------------------------- density
+at::Tensor density_map(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy,
+                       at::Tensor ratio, at::Tensor bcx, at::Tensor bcy, at::Tensor init, double target_density,
+                       double xl, double yl, double xh, double yh, double bsx, double bsy, int num_movable,
+                       int num_filler, int padding, int nbx, int nby, int, int, int, int,
+                       int deterministic, c10::optional<at::Tensor> sorted_node_map) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos);
+  for (auto* t : {&sx, &sy, &ox, &oy, &ratio}) { CHECK_FLAT(*t); CHECK_F32(*t); }
+  CHECK_CUDA_T(init); CHECK_CONTIG(init); CHECK_F32(init);
+  TORCH_CHECK(init.numel() == (int64_t)nbx * nby, "initial_density_map has ", init.numel(), " elements, expected ", nbx * nby);
+  const int* snm = nullptr;
+  if (sorted_node_map.has_value() && sorted_node_map->defined()) {
+    CHECK_FLAT(*sorted_node_map); CHECK_I32(*sorted_node_map);
+    TORCH_CHECK(sorted_node_map->numel() >= num_movable, "sorted_node_map shorter than num_movable_nodes");
+    snm = ptr<int>(*sorted_node_map);
+  }
+  c10::cuda::CUDAGuard guard(pos.device());
+  int n = pos.numel() / 2;
+  auto out = at::empty({nbx, nby}, pos.options());
+  if (deterministic) {
+    auto scratch = at::empty({(int64_t)nbx * nby}, pos.options().dtype(at::kLong));
+    DP_CALL(dp_density_map_fx64(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                                ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
+                                num_movable, num_filler, nbx, nby, snm, fraction_bits(xl, yl, xh, yh),
+                                ptr<int64_t>(scratch), ptr<float>(out), cur_stream()));
+  } else {
+    DP_CALL(dp_density_map_f32(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                               ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
+                               num_movable, num_filler, nbx, nby, snm, ptr<float>(out), cur_stream()));
+  }
+  return out.view({-1});
+}
+
+// Integer fixed-point map of the deterministic scatter (for bit-exact checks).
+at::Tensor density_map_fixed_point(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy,
+                                   at::Tensor ratio, double xl, double yl, double xh, double yh, double bsx,
+                                   double bsy, int num_movable, int num_filler, int nbx, int nby,
+                                   c10::optional<at::Tensor> sorted_node_map) {
+  CHECK_FLAT(pos); CHECK_F32(pos);
+  c10::cuda::CUDAGuard guard(pos.device());
+  int n = pos.numel() / 2;
+  auto out = at::empty({nbx, nby}, pos.options());
+  auto scratch = at::empty({(int64_t)nbx * nby}, pos.options().dtype(at::kLong));
+  const int* snm = sorted_node_map.has_value() && sorted_node_map->defined() ? ptr<int>(*sorted_node_map) : nullptr;
+  DP_CALL(dp_density_map_fx64(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                              ptr<float>(ratio), nullptr, xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
+                              num_movable, num_filler, nbx, nby, snm, fraction_bits(xl, yl, xh, yh),
+                              ptr<int64_t>(scratch), ptr<float>(out), cur_stream()));
+  return scratch;
+}
+
+at::Tensor fixed_density_map(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor bcx, at::Tensor bcy, double xl,
+                             double yl, double xh, double yh, double bsx, double bsy, int num_movable,
+                             int num_terminals, int nbx, int nby, int, int, int deterministic) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos);
+  c10::cuda::CUDAGuard guard(pos.device());
+  int n = pos.numel() / 2;
+  auto out = at::empty({nbx, nby}, pos.options());
+  at::Tensor scratch;
+  if (deterministic) scratch = at::empty({(int64_t)nbx * nby}, pos.options().dtype(at::kLong));
+  DP_CALL(dp_fixed_density_map(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(bcx), ptr<float>(bcy),
+                               xl, yl, xh, yh, bsx, bsy, num_movable, num_terminals, nbx, nby, deterministic,
+                               fraction_bits(xl, yl, xh, yh), deterministic ? ptr<int64_t>(scratch) : nullptr,
+                               ptr<float>(out), cur_stream()));
+  return out;
+}
+
+at::Tensor density_map_exact(at::Tensor pos, at::Tensor sx, at::Tensor sy, std::vector<int64_t> range_list,
+                             at::Tensor initial, double xl, double yl, double xh, double yh, int nbx, int nby,
+                             int deterministic) {
+  CHECK_FLAT(pos); CHECK_F32(pos);
+  c10::cuda::CUDAGuard guard(pos.device());
+  int n = pos.numel() / 2;
+  auto out = initial.clone().contiguous();
+  std::vector<int> rb, re;
+  for (size_t i = 0; i + 1 < range_list.size(); i += 2) {
+    rb.push_back((int)range_list[i]);
+    re.push_back((int)range_list[i + 1]);
+  }
+  at::Tensor scratch;
+  if (deterministic) scratch = at::empty({(int64_t)nbx * nby}, pos.options().dtype(at::kLong));
+  DP_CALL(dp_density_map_exact(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), rb.data(), re.data(), (int)rb.size(),
+                               xl, yl, xh, yh, nbx, nby, deterministic, fraction_bits(xl, yl, xh, yh),
+                               deterministic ? ptr<int64_t>(scratch) : nullptr, ptr<float>(out), cur_stream()));
+  return out;
+}
+
+// overflow evaluation: returns fp64 [overflow, max_density]
+at::Tensor density_overflow(at::Tensor density_map, double target_area, double bin_area) {
+  CHECK_CUDA_T(density_map); CHECK_CONTIG(density_map); CHECK_F32(density_map);
+  c10::cuda::CUDAGuard guard(density_map.device());
+  auto out = at::empty({2}, density_map.options().dtype(at::kDouble));
+  DP_CALL(dp_density_overflow(ptr<float>(density_map), density_map.numel(), target_area, bin_area, ptr<double>(out),
+                              nullptr, cur_stream()));
+  return out;
+}
+
+at::Tensor electric_force(at::Tensor grad_pos, int nbx, int nby, int, int, int, int, at::Tensor ex, at::Tensor ey,
+                          at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio,
+                          at::Tensor bcx, at::Tensor bcy, double xl, double yl, double xh, double yh, double bsx,
+                          double bsy, int num_movable, int num_filler, int deterministic,
+                          c10::optional<at::Tensor> sorted_node_map, double scale) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos);
+  CHECK_CUDA_T(grad_pos); CHECK_F32(grad_pos);
+  CHECK_CUDA_T(ex); CHECK_CONTIG(ex); CHECK_CUDA_T(ey); CHECK_CONTIG(ey);
+  TORCH_CHECK(ex.numel() == (int64_t)nbx * nby && ey.numel() == (int64_t)nbx * nby, "field maps must be num_bins_x*num_bins_y");
+  c10::cuda::CUDAGuard guard(pos.device());
+  int n = pos.numel() / 2;
+  auto out = at::empty_like(pos);
+  auto g = grad_pos.contiguous();
+  const int* snm = sorted_node_map.has_value() && sorted_node_map->defined() ? ptr<int>(*sorted_node_map) : nullptr;
+  DP_CALL(dp_electric_force(ptr<float>(g), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(pos), n, ptr<float>(sx),
+                            ptr<float>(sy), ptr<float>(ox), ptr<float>(oy), ptr<float>(ratio), xl, yl, xh, yh, bsx, bsy,
+                            inv_f(bsx), inv_f(bsy), num_movable, num_filler, snm, (float)scale, ptr<float>(out),
+                            cur_stream()));
+  return out;
+}
+
+// ---------------------------------------------------------------- Poisson GEMMs
+static void* tensor_ptr(const py::dict& d, const char* key) {
+  if (!d.contains(key)) return nullptr;
+  py::object o = d[key];
+  if (o.is_none()) return nullptr;
+  at::Tensor t = o.cast<at::Tensor>();
+  TORCH_CHECK(t.is_cuda() && t.is_contiguous(), "transform_gemm: '", key, "' must be a contiguous CUDA tensor");
+  return t.data_ptr();
+}
+template <typename T>
+static T dict_get(const py::dict& d, const char* key, T dflt) {
+  return d.contains(key) ? d[key].cast<T>() : dflt;
+}
+
+void transform_gemm(int precision, int M, int N, int K, py::list problems) {
+  std::vector<dp_gemm_problem> probs;
+  for (auto item : problems) {
+    py::dict d = item.cast<py::dict>();
+    dp_gemm_problem q;
+    memset(&q, 0, sizeof(q));
+    q.a_hi = tensor_ptr(d, "a_hi"); q.a_lo = tensor_ptr(d, "a_lo");
+    q.b_hi = tensor_ptr(d, "b_hi"); q.b_lo = tensor_ptr(d, "b_lo");
+    q.lda = dict_get<int>(d, "lda", K); q.ldb = dict_get<int>(d, "ldb", K);
+    q.epilogue = dict_get<int>(d, "epilogue", DP_EPI_STORE);
+    q.alpha = dict_get<float>(d, "alpha", 1.0f);
+    q.ldc = dict_get<int>(d, "ldc", q.epilogue == DP_EPI_STORE_T ? M : N);
+    q.out_f32 = (float*)tensor_ptr(d, "out_f32");
+    q.out_hi = tensor_ptr(d, "out_hi"); q.out_lo = tensor_ptr(d, "out_lo");
+    const char* kf[3] = {"sp0_f32", "sp1_f32", "sp2_f32"};
+    const char* kh[3] = {"sp0_hi", "sp1_hi", "sp2_hi"};
+    const char* kl[3] = {"sp0_lo", "sp1_lo", "sp2_lo"};
+    for (int i = 0; i < 3; ++i) {
+      q.spec_out_f32[i] = (float*)tensor_ptr(d, kf[i]);
+      q.spec_out_hi[i] = tensor_ptr(d, kh[i]);
+      q.spec_out_lo[i] = tensor_ptr(d, kl[i]);
+    }
+    q.wv_scale = dict_get<float>(d, "wv_scale", 1.0f);
+    q.rho = (const float*)tensor_ptr(d, "rho");
+    q.energy_f64 = (double*)tensor_ptr(d, "energy");
+    probs.push_back(q);
+  }
+  DP_CALL(dp_transform_gemm(precision, M, N, K, probs.data(), (int)probs.size(), cur_stream()));
+}
+
+void prepare_operand(int precision, at::Tensor x, double scale, c10::optional<at::Tensor> out_f32,
+                     c10::optional<at::Tensor> out_hi, c10::optional<at::Tensor> out_lo) {
+  CHECK_CUDA_T(x); CHECK_CONTIG(x); CHECK_F32(x);
+  DP_CALL(dp_prepare_operand(precision, ptr<float>(x), x.numel(), (float)scale, optr<float>(out_f32),
+                             out_hi.has_value() ? out_hi->data_ptr() : nullptr,
+                             out_lo.has_value() ? out_lo->data_ptr() : nullptr, cur_stream()));
+}
+
+int tc_status() {
+  int s = 0;
+  DP_CALL(dp_tc_status(&s));
+  return s;
+}
+
+// ---------------------------------------------------------------- wirelength
+std::vector<at::Tensor> wa_merged_forward(at::Tensor pos, at::Tensor flat_netpin, at::Tensor netpin_start,
+                                          at::Tensor pin2net_map, at::Tensor net_weights, at::Tensor net_mask,
+                                          at::Tensor inv_gamma) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos);
+  CHECK_FLAT(flat_netpin); CHECK_I32(flat_netpin);
+  CHECK_FLAT(netpin_start); CHECK_I32(netpin_start);
+  CHECK_FLAT(net_mask);
+  CHECK_CUDA_T(inv_gamma); CHECK_F32(inv_gamma);
+  c10::cuda::CUDAGuard guard(pos.device());
+  int num_nets = netpin_start.numel() - 1;
+  int num_pins = pos.numel() / 2;
+  auto grad_intermediate = at::empty_like(pos);
+  auto wl = at::empty({}, pos.options());
+  auto wl64 = at::empty({1}, pos.options().dtype(at::kDouble));
+  auto ig = inv_gamma.contiguous();
+  DP_CALL(dp_wa_merged_forward(ptr<float>(pos), num_pins, ptr<int>(flat_netpin), ptr<int>(netpin_start), num_nets,
+                               net_weights.numel() ? ptr<float>(net_weights) : nullptr, net_mask.data_ptr<uint8_t>(),
+                               ptr<float>(ig), nullptr, ptr<double>(wl64), ptr<float>(wl), ptr<float>(grad_intermediate),
+                               cur_stream()));
+  return {wl, grad_intermediate};
+}
+
+at::Tensor wa_merged_backward(at::Tensor grad_pos, at::Tensor pos, at::Tensor grad_intermediate, at::Tensor flat_netpin,
+                              at::Tensor netpin_start, at::Tensor pin2net_map, at::Tensor net_weights,
+                              at::Tensor net_mask, at::Tensor inv_gamma, c10::optional<at::Tensor> pin_mask) {
+  CHECK_FLAT(grad_intermediate); CHECK_EVEN(grad_intermediate); CHECK_F32(grad_intermediate);
+  CHECK_CUDA_T(grad_pos); CHECK_F32(grad_pos);
+  CHECK_FLAT(pin2net_map); CHECK_I32(pin2net_map);
+  c10::cuda::CUDAGuard guard(grad_intermediate.device());
+  int num_pins = grad_intermediate.numel() / 2;
+  auto g = grad_pos.contiguous();
+  const uint8_t* pm = nullptr;
+  if (pin_mask.has_value() && pin_mask->defined()) {
+    CHECK_FLAT(*pin_mask);
+    TORCH_CHECK(pin_mask->element_size() == 1, "pin_mask must be bool or uint8");
+    pm = (const uint8_t*)pin_mask->data_ptr();
+  }
+  DP_CALL(dp_wa_merged_backward(ptr<float>(g), ptr<int>(pin2net_map),
+                                net_weights.numel() ? ptr<float>(net_weights) : nullptr, net_mask.data_ptr<uint8_t>(),
+                                pm, num_pins, ptr<float>(grad_intermediate), cur_stream()));
+  return grad_intermediate;
+}
+
+at::Tensor pin_pos_forward(at::Tensor pos, at::Tensor offx, at::Tensor offy, at::Tensor pin2node) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos); CHECK_I32(pin2node);
+  c10::cuda::CUDAGuard guard(pos.device());
+  int num_pins = offx.numel();
+  auto out = at::empty({2 * (int64_t)num_pins}, pos.options());
+  DP_CALL(dp_pin_pos_forward(ptr<float>(pos), pos.numel() / 2, ptr<float>(offx), ptr<float>(offy), ptr<int>(pin2node),
+                             num_pins, ptr<float>(out), cur_stream()));
+  return out;
+}
+
+at::Tensor pin_pos_backward(at::Tensor grad_out, at::Tensor pos, at::Tensor flat_node2pin, at::Tensor node2pin_start,
+                            int num_physical_nodes) {
+  CHECK_FLAT(grad_out); CHECK_EVEN(grad_out); CHECK_F32(grad_out);
+  CHECK_I32(flat_node2pin); CHECK_I32(node2pin_start);
+  c10::cuda::CUDAGuard guard(pos.device());
+  auto out = at::empty_like(pos);
+  DP_CALL(dp_pin_pos_backward(ptr<float>(grad_out), grad_out.numel() / 2, ptr<int>(flat_node2pin),
+                              ptr<int>(node2pin_start), num_physical_nodes, pos.numel() / 2, ptr<float>(out),
+                              cur_stream()));
+  return out;
+}
+
+// returns fp64 [1] total
+at::Tensor hpwl_forward(at::Tensor pin_pos, at::Tensor flat_netpin, at::Tensor netpin_start, at::Tensor net_weights,
+                        at::Tensor net_mask) {
+  CHECK_FLAT(pin_pos); CHECK_EVEN(pin_pos); CHECK_F32(pin_pos);
+  c10::cuda::CUDAGuard guard(pin_pos.device());
+  auto out = at::empty({1}, pin_pos.options().dtype(at::kDouble));
+  DP_CALL(dp_hpwl(ptr<float>(pin_pos), pin_pos.numel() / 2, ptr<int>(flat_netpin), ptr<int>(netpin_start),
+                  netpin_start.numel() - 1, net_weights.numel() ? ptr<float>(net_weights) : nullptr,
+                  net_mask.data_ptr<uint8_t>(), ptr<double>(out), nullptr, cur_stream()));
+  return out;
+}
+
+at::Tensor move_boundary_forward(at::Tensor pos, at::Tensor sx, at::Tensor sy, double xl, double yl, double xh,
+                                 double yh, int num_movable, int num_filler) {
+  CHECK_FLAT(pos); CHECK_EVEN(pos); CHECK_F32(pos);
+  c10::cuda::CUDAGuard guard(pos.device());
+  DP_CALL(dp_move_boundary(ptr<float>(pos), pos.numel() / 2, ptr<float>(sx), ptr<float>(sy), xl, yl, xh, yh,
+                           num_movable, num_filler, cur_stream()));
+  return pos;
+}
+
+at::Tensor pws_forward(at::Tensor net_weights, at::Tensor flat_nodepin, at::Tensor nodepin_start, at::Tensor pin2net,
+                       int num_nodes) {
+  CHECK_FLAT(net_weights); CHECK_F32(net_weights);
+  c10::cuda::CUDAGuard guard(net_weights.device());
+  auto out = at::empty({num_nodes}, net_weights.options());
+  DP_CALL(dp_pin_weight_sum(ptr<float>(net_weights), ptr<int>(flat_nodepin), ptr<int>(nodepin_start),
+                            ptr<int>(pin2net), nodepin_start.numel() - 1, num_nodes, ptr<float>(out), cur_stream()));
+  return out;
+}
+
+uint64_t launch_count() { return dp_launch_count(); }
+
+PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
+  m.doc() = "dreamplace_b200 native ops (sm_100a) over the C ABI";
+  m.def("density_map", &density_map);
+  m.def("density_map_fixed_point", &density_map_fixed_point);
+  m.def("fixed_density_map", &fixed_density_map);
+  m.def("density_map_exact", &density_map_exact);
+  m.def("density_overflow", &density_overflow);
+  m.def("electric_force", &electric_force);
+  m.def("transform_gemm", &transform_gemm);
+  m.def("prepare_operand", &prepare_operand);
+  m.def("tc_status", &tc_status);
+  m.def("wa_merged_forward", &wa_merged_forward);
+  m.def("wa_merged_backward", &wa_merged_backward);
+  m.def("pin_pos_forward", &pin_pos_forward);
+  m.def("pin_pos_backward", &pin_pos_backward);
+  m.def("hpwl_forward", &hpwl_forward);
+  m.def("move_boundary_forward", &move_boundary_forward);
+  m.def("pws_forward", &pws_forward);
+  m.def("launch_count", &launch_count);
+  m.def("version", &dp_version);
+}

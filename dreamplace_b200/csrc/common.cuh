@@ -1,0 +1,96 @@
+// Shared helpers for the dreamplace_b200 C ABI implementation (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <float.h>
+#include <math.h>
+#include <string.h>
+#include <stdio.h>
+#include <atomic>
+#include <string>
+
+#include "dreamplace_b200.h"
+
+namespace dpb {
+
+constexpr int kNumSMs = 148;  // B200
+
+void set_error(const char* fmt, ...);
+void count_launch(int n = 1);
+
+inline cudaStream_t as_stream(dp_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("%s: CUDA launch failed: %s", what, cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  count_launch();
+  return DP_OK;
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// grid size for a grid-stride elementwise kernel: a multiple of the SM count
+inline int grid_for(long long n, int threads, int per_sm = 8) {
+  long long blocks = (n + threads - 1) / threads;
+  long long cap = (long long)kNumSMs * per_sm;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+#define DP_REQUIRE(cond, ...)            \
+  do {                                   \
+    if (!(cond)) {                       \
+      ::dpb::set_error(__VA_ARGS__);     \
+      return DP_ERR_INVALID_ARGUMENT;    \
+    }                                    \
+  } while (0)
+
+// Round-to-nearest float arithmetic that nvcc may not contract into FMA; used
+// wherever the CPU reference's operation order must be reproduced bit for bit.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+// triangle_density_function of electric_potential/src/density_function.h:12-17:
+//   bin_xl = xl + k*bin_size; min(x+size, bin_xl+bin_size) - max(x, bin_xl)
+__device__ __forceinline__ float triangle_overlap(float x, float size, float xl, int k, float bs) {
+  float bin_xl = fadd(xl, fmul((float)k, bs));
+  return fsub(fminf(fadd(x, size), fadd(bin_xl, bs)), fmaxf(x, bin_xl));
+}
+
+// exact_density_function of electric_potential/src/density_function.h:19-36
+__device__ __forceinline__ float exact_overlap(float x, float size, float bin_center, float bs,
+                                               float l, float h, bool fixed_flag) {
+  float half = bs / 2;
+  float bin_xl = fsub(bin_center, half);
+  float bin_xh = fadd(bin_center, half);
+  if (!fixed_flag) {
+    if (bin_xl <= l) bin_xl = fminf(bin_xl, x);
+    if (bin_xh >= h) bin_xh = fmaxf(bin_xh, fadd(x, size));
+  }
+  return fmaxf(0.0f, fsub(fminf(fadd(x, size), bin_xh), fmaxf(x, bin_xl)));
+}
+
+// Bin range of a stretched cell: C int() truncation toward zero, as the
+// reference does (electric_potential/src/electric_density_map.cpp:254-266).
+__device__ __forceinline__ void triangle_bin_range(float x, float size, float lo, float inv_bs,
+                                                   int nbins, int& b0, int& b1) {
+  int l = (int)fmul(fsub(x, lo), inv_bs);
+  int h = (int)fmul(fsub(fadd(x, size), lo), inv_bs) + 1;
+  b0 = max(l, 0);
+  b1 = min(h, nbins);
+}
+
+// fixed-point conversion of one bin contribution: float * 2^f, truncated to a
+// signed 64-bit integer (the CPU reference's `long sv = v * scale_factor`)
+__device__ __forceinline__ long long to_fixed(float v, float scale) {
+  return (long long)fmul(v, scale);
+}
+
+}  // namespace dpb

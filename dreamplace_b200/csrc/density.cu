@@ -1,0 +1,433 @@
+// Density scatter kernels: triangle (stretched-cell) model in fp32 and in
+// 64-bit fixed point, the exact-overlap maps, and the overflow reduction.
+//
+// Semantics follow the reference CPU ops (paths relative to dreamplace/ops):
+//   electric_potential/src/electric_density_map.cpp:100-152, 216-268
+//   electric_potential/src/electric_density_map.cpp:155-213, 270-309
+//   electric_potential/src/density_function.h:12-36
+//   utility/src/atomic_ops.h:43-54 (fixed-point add and final conversion)
+//   density_map/src/density_map.cpp (exact DensityMap)
+//   electric_potential/electric_overflow.py:260-278 (overflow / max density)
+//
+// Layout: one thread per scattered cell; cells are addressed through
+// sorted_node_map (movable, ascending width, so neighbouring threads have
+// similar loop trip counts) followed by the filler range.  A warp whose lanes
+// hit the same bin combines their contributions with a match/reduce before
+// one atomic, which removes most same-address serialisation when cells are
+// clustered (the GP starts with every movable cell at the die centre).
+#include "common.cuh"
+
+namespace dpb {
+
+struct TriangleArgs {
+  const float* x; const float* y;
+  const float* sx; const float* sy; const float* ox; const float* oy; const float* ratio;
+  float xl, yl, bsx, bsy, inv_bsx, inv_bsy;
+  int num_bins_x, num_bins_y;
+  int num_movable, num_filler, filler_begin;
+  const int* sorted_node_map;
+};
+
+__device__ __forceinline__ int scatter_node_index(const TriangleArgs& a, int idx) {
+  if (idx < a.num_movable) return a.sorted_node_map ? a.sorted_node_map[idx] : idx;
+  return a.filler_begin + (idx - a.num_movable);
+}
+
+// Adds v to map[bin] after combining the lanes of the warp that target the
+// same bin: one atomic per distinct bin instead of one per lane.
+template <typename T, typename U>
+__device__ __forceinline__ void combined_add(U* map, int bin, T v, unsigned active) {
+  unsigned peers = __match_any_sync(active, bin);
+  int leader = __ffs(peers) - 1;
+  unsigned rest = peers & (peers - 1);  // peers without the leader
+  T sum = v;
+  while (rest) {  // identical trip sequence on every lane of the group
+    int src = __ffs(rest) - 1;
+    rest &= rest - 1;
+    sum += __shfl_sync(peers, v, src);
+  }
+  if ((int)(threadIdx.x & 31) == leader) atomicAdd(map + bin, (U)sum);
+}
+
+// Each lane walks its cell's bins in k-major, h-minor order.  All lanes of the
+// warp iterate together up to the warp's largest trip count so that
+// __match_any_sync sees every lane that is still issuing an update.
+template <bool kFixed>
+__global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, int total,
+                                                               float fx_scale, float* map_f32,
+                                                               unsigned long long* map_fx) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    int idx = base + threadIdx.x;
+    bool valid = idx < total;
+    int kx0 = 0, kx1 = 0, hy0 = 0, hy1 = 0;
+    float nx = 0.f, ny = 0.f, sx = 0.f, sy = 0.f, r = 0.f;
+    if (valid) {
+      int i = scatter_node_index(a, idx);
+      sx = a.sx[i];
+      sy = a.sy[i];
+      nx = fadd(a.x[i], a.ox[i]);
+      ny = fadd(a.y[i], a.oy[i]);
+      r = a.ratio[i];
+      triangle_bin_range(nx, sx, a.xl, a.inv_bsx, a.num_bins_x, kx0, kx1);
+      triangle_bin_range(ny, sy, a.yl, a.inv_bsy, a.num_bins_y, hy0, hy1);
+    }
+    int nkx = max(kx1 - kx0, 0), nhy = max(hy1 - hy0, 0);
+    int trips = nkx * nhy;
+    // warp-uniform loop bound
+    int max_trips = trips;
+    for (int o = 16; o > 0; o >>= 1) max_trips = max(max_trips, __shfl_xor_sync(0xffffffffu, max_trips, o));
+    float px_r = 0.f;
+    int cur_k = -1;
+    for (int t = 0; t < max_trips; ++t) {
+      bool live = t < trips;
+      unsigned active = __ballot_sync(0xffffffffu, live);
+      if (live) {
+        int k = kx0 + t / nhy;
+        int h = hy0 + t % nhy;
+        if (k != cur_k) {
+          float px = triangle_overlap(nx, sx, a.xl, k, a.bsx);
+          px_r = fmul(px, r);
+          cur_k = k;
+        }
+        float py = triangle_overlap(ny, sy, a.yl, h, a.bsy);
+        float area = fmul(px_r, py);
+        int bin = k * a.num_bins_y + h;
+        if (kFixed) {
+          combined_add<long long, unsigned long long>(map_fx, bin, to_fixed(area, fx_scale), active);
+        } else {
+          combined_add<float, float>(map_f32, bin, area, active);
+        }
+      }
+    }
+  }
+}
+
+// out = (float)((double)init + (double)fixed * 2^-f)  (utility/src/atomic_ops.h:48-54)
+__global__ void fixed_to_float_kernel(const long long* fixed, const float* init, double inv_scale,
+                                      float* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double base = init ? (double)init[i] : 0.0;
+    out[i] = (float)(base + (double)fixed[i] * inv_scale);
+  }
+}
+
+__global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+static int copy_map(const float* src, float* dst, int n, cudaStream_t s) {
+  if (src == dst) return DP_OK;
+  if ((n & 3) == 0 && ((uintptr_t)src & 15) == 0 && ((uintptr_t)dst & 15) == 0) {
+    copy_kernel<<<grid_for(n / 4, 256), 256, 0, s>>>((const float4*)src, (float4*)dst, n / 4);
+    return check_launch("copy_map");
+  }
+  cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) {
+    set_error("copy_map: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}
+
+static int validate_triangle(const float* pos, int num_nodes, const float* sx, const float* sy,
+                             const float* ox, const float* oy, const float* ratio, int nm, int nf,
+                             int nbx, int nby, float bsx, float bsy, const float* out) {
+  DP_REQUIRE(pos && sx && sy && ox && oy && ratio && out, "density_map: null pointer argument");
+  DP_REQUIRE(num_nodes >= 0 && nm >= 0 && nf >= 0 && nm + nf <= num_nodes,
+             "density_map: inconsistent node counts (nodes %d movable %d filler %d)", num_nodes, nm, nf);
+  DP_REQUIRE(nbx > 0 && nby > 0 && (long long)nbx * nby < (1ll << 31), "density_map: bad bin grid %dx%d", nbx, nby);
+  DP_REQUIRE(bsx > 0 && bsy > 0, "density_map: bin sizes must be positive");
+  return DP_OK;
+}
+
+static TriangleArgs make_args(const float* pos, int num_nodes, const float* sx, const float* sy,
+                              const float* ox, const float* oy, const float* ratio, float xl,
+                              float yl, float bsx, float bsy, float ibx, float iby, int nm, int nf,
+                              int nbx, int nby, const int* sorted) {
+  TriangleArgs a;
+  a.x = pos; a.y = pos + num_nodes;
+  a.sx = sx; a.sy = sy; a.ox = ox; a.oy = oy; a.ratio = ratio;
+  a.xl = xl; a.yl = yl; a.bsx = bsx; a.bsy = bsy; a.inv_bsx = ibx; a.inv_bsy = iby;
+  a.num_bins_x = nbx; a.num_bins_y = nby;
+  a.num_movable = nm; a.num_filler = nf; a.filler_begin = num_nodes - nf;
+  a.sorted_node_map = sorted;
+  return a;
+}
+
+// Exact-overlap scatter of one node range (fixed_node_flag selects the
+// boundary-extension rule of exact_density_function).
+template <bool kFixed>
+__global__ void exact_scatter_kernel(const float* x, const float* y, const float* sx, const float* sy,
+                                     const float* bcx, const float* bcy, int begin, int end,
+                                     float xl, float yl, float xh, float yh, float bsx, float bsy,
+                                     int nbx, int nby, bool fixed_node_flag, bool use_centers,
+                                     float fx_scale, float* map_f32, unsigned long long* map_fx) {
+  for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    float bxl = x[i], byl = y[i];
+    float bxh = fadd(bxl, sx[i]), byh = fadd(byl, sy[i]);
+    int k0 = max((int)__fdiv_rn(fsub(bxl, xl), bsx), 0);
+    int k1 = min((int)ceilf(__fdiv_rn(fsub(bxh, xl), bsx)) + 1, nbx);
+    int h0 = max((int)__fdiv_rn(fsub(byl, yl), bsy), 0);
+    int h1 = min((int)ceilf(__fdiv_rn(fsub(byh, yl), bsy)) + 1, nby);
+    float wx = fsub(bxh, bxl), wy = fsub(byh, byl);
+    for (int k = k0; k < k1; ++k) {
+      float cx = use_centers ? bcx[k] : fadd(fadd(xl, fmul((float)k, bsx)), bsx / 2);
+      float px = exact_overlap(bxl, wx, cx, bsx, xl, xh, fixed_node_flag);
+      for (int h = h0; h < h1; ++h) {
+        float cy = use_centers ? bcy[h] : fadd(fadd(yl, fmul((float)h, bsy)), bsy / 2);
+        float py = exact_overlap(byl, wy, cy, bsy, yl, yh, fixed_node_flag);
+        float area = fmul(px, py);
+        int bin = k * nby + h;
+        if (kFixed)
+          atomicAdd(map_fx + bin, (unsigned long long)to_fixed(area, fx_scale));
+        else
+          atomicAdd(map_f32 + bin, area);
+      }
+    }
+  }
+}
+
+// DensityMap exact-overlap scatter (density_map/src/density_map.cpp:
+// distributeBox2Bin): bin size (xh-xl)/num_bins in float, y range widened by
+// two bins each side, the last bin in each direction extended to the cell edge.
+template <bool kFixed>
+__global__ void box_scatter_kernel(const float* x, const float* y, const float* sx, const float* sy, int begin,
+                                   int end, float xl, float yl, float xh, float yh, int nbx, int nby,
+                                   float fx_scale, float* map_f32, unsigned long long* map_fx) {
+  const float bsx = __fdiv_rn(fsub(xh, xl), (float)nbx);
+  const float bsy = __fdiv_rn(fsub(yh, yl), (float)nby);
+  for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    float bxl = x[i], byl = y[i];
+    float bxh = fadd(bxl, sx[i]), byh = fadd(byl, sy[i]);
+    int k0 = max((int)__fdiv_rn(fsub(bxl, xl), bsx), 0);
+    int k1 = min((int)ceilf(__fdiv_rn(fsub(bxh, xl), bsx)) + 1, nbx);
+    float two_bsy = fmul(2.0f, bsy);
+    int h0 = max((int)__fdiv_rn(fsub(fsub(byl, yl), two_bsy), bsy), 0);
+    int h1 = min((int)ceilf(__fdiv_rn(fadd(fsub(byh, yl), two_bsy), bsy)) + 1, nby);
+    for (int k = k0; k < k1; ++k) {
+      float bin_xl = fadd(xl, fmul(bsx, (float)k));
+      float bin_xh = fminf(fadd(bin_xl, bsx), xh);
+      if (k + 1 == nbx) bin_xh = bxh;
+      float px = fmaxf(0.0f, fsub(fminf(bxh, bin_xh), fmaxf(bxl, bin_xl)));
+      for (int h = h0; h < h1; ++h) {
+        float bin_yl = fadd(yl, fmul(bsy, (float)h));
+        float bin_yh = fminf(fadd(bin_yl, bsy), yh);
+        if (h + 1 == nby) bin_yh = byh;
+        float py = fmaxf(0.0f, fsub(fminf(byh, bin_yh), fmaxf(byl, bin_yl)));
+        float area = fmul(px, py);
+        int bin = k * nby + h;
+        if (kFixed)
+          atomicAdd(map_fx + bin, (unsigned long long)to_fixed(area, fx_scale));
+        else
+          atomicAdd(map_f32 + bin, area);
+      }
+    }
+  }
+}
+
+__global__ void clamp_max_kernel(float* map, int n, float vmax) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    map[i] = fminf(map[i], vmax);
+}
+
+// order-preserving float <-> uint32 key: key(a) < key(b) iff a < b; key 0 is
+// below every float, so a zero-filled slot is a valid start for atomicMax
+__device__ __forceinline__ unsigned float_key(float f) {
+  unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void overflow_kernel(const float* __restrict__ map, int n, double target_area,
+                                double* acc, unsigned* maxkey) {
+  double s = 0.0;
+  float m = -INFINITY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float d = map[i];
+    double over = (double)d - target_area;
+    s += over > 0.0 ? over : 0.0;
+    m = fmaxf(m, d);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  __shared__ double ss[32];
+  __shared__ float sm[32];
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { ss[w] = s; sm[w] = m; }
+  __syncthreads();
+  if (w == 0) {
+    int nw = blockDim.x >> 5;
+    s = l < nw ? ss[l] : 0.0;
+    m = l < nw ? sm[l] : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if (l == 0) {
+      atomicAdd(acc, s);
+      atomicMax(maxkey, float_key(m));
+    }
+  }
+}
+
+__global__ void overflow_finish_kernel(double* out2, const unsigned* maxkey, double bin_area,
+                                       float* out2_f32) {
+  double mx = (double)key_float(*maxkey) / bin_area;
+  out2[1] = mx;
+  if (out2_f32) {
+    out2_f32[0] = (float)out2[0];
+    out2_f32[1] = (float)mx;
+  }
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+
+extern "C" int dp_density_map_f32(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                  const float* ox, const float* oy, const float* ratio,
+                                  const float* init, float xl, float yl, float xh, float yh,
+                                  float bsx, float bsy, float ibx, float iby, int nm, int nf,
+                                  int nbx, int nby, const int* sorted, float* out,
+                                  dp_stream_t stream) {
+  int rc = validate_triangle(pos, num_nodes, sx, sy, ox, oy, ratio, nm, nf, nbx, nby, bsx, bsy, out);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  int nbins = nbx * nby;
+  if (init) {
+    rc = copy_map(init, out, nbins, s);
+    if (rc) return rc;
+  } else {
+    cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
+  }
+  int total = nm + nf;
+  if (total == 0) return DP_OK;
+  TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, nm, nf, nbx, nby, sorted);
+  triangle_scatter_kernel<false><<<grid_for(total, 256, 16), 256, 0, s>>>(a, total, 0.f, out, nullptr);
+  return check_launch("dp_density_map_f32");
+}
+
+extern "C" int dp_density_map_fx64(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                   const float* ox, const float* oy, const float* ratio,
+                                   const float* init, float xl, float yl, float xh, float yh,
+                                   float bsx, float bsy, float ibx, float iby, int nm, int nf,
+                                   int nbx, int nby, const int* sorted, int fraction_bits,
+                                   int64_t* scratch, float* out, dp_stream_t stream) {
+  int rc = validate_triangle(pos, num_nodes, sx, sy, ox, oy, ratio, nm, nf, nbx, nby, bsx, bsy, out);
+  if (rc) return rc;
+  DP_REQUIRE(scratch, "dp_density_map_fx64: scratch_fixed is required");
+  DP_REQUIRE(fraction_bits >= 0 && fraction_bits <= 62, "dp_density_map_fx64: bad fraction_bits %d", fraction_bits);
+  cudaStream_t s = as_stream(stream);
+  int nbins = nbx * nby;
+  cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
+  int total = nm + nf;
+  float scale = ldexpf(1.0f, fraction_bits);
+  if (total > 0) {
+    TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, nm, nf, nbx, nby, sorted);
+    triangle_scatter_kernel<true><<<grid_for(total, 256, 16), 256, 0, s>>>(
+        a, total, scale, nullptr, reinterpret_cast<unsigned long long*>(scratch));
+    rc = check_launch("dp_density_map_fx64 scatter");
+    if (rc) return rc;
+  }
+  fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
+                                                            ldexp(1.0, -fraction_bits), out, nbins);
+  return check_launch("dp_density_map_fx64 convert");
+}
+
+extern "C" int dp_fixed_density_map(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                    const float* bcx, const float* bcy, float xl, float yl, float xh,
+                                    float yh, float bsx, float bsy, int nm, int nt, int nbx, int nby,
+                                    int deterministic, int fraction_bits, int64_t* scratch,
+                                    float* out, dp_stream_t stream) {
+  DP_REQUIRE(pos && sx && sy && bcx && bcy && out, "dp_fixed_density_map: null pointer argument");
+  DP_REQUIRE(nm >= 0 && nt >= 0 && nm + nt <= num_nodes, "dp_fixed_density_map: bad node counts");
+  DP_REQUIRE(nbx > 0 && nby > 0, "dp_fixed_density_map: bad bin grid");
+  DP_REQUIRE(!deterministic || scratch, "dp_fixed_density_map: deterministic mode needs scratch_fixed");
+  cudaStream_t s = as_stream(stream);
+  int nbins = nbx * nby;
+  cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
+  if (nt == 0) return DP_OK;
+  const float* x = pos;
+  const float* y = pos + num_nodes;
+  int blocks = grid_for(nt, 128, 8);
+  if (deterministic) {
+    cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
+    exact_scatter_kernel<true><<<blocks, 128, 0, s>>>(x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
+                                                      bsx, bsy, nbx, nby, true, true,
+                                                      ldexpf(1.0f, fraction_bits), nullptr,
+                                                      reinterpret_cast<unsigned long long*>(scratch));
+    int rc = check_launch("dp_fixed_density_map scatter");
+    if (rc) return rc;
+    fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, nullptr,
+                                                              ldexp(1.0, -fraction_bits), out, nbins);
+    rc = check_launch("dp_fixed_density_map convert");
+    if (rc) return rc;
+  } else {
+    exact_scatter_kernel<false><<<blocks, 128, 0, s>>>(x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
+                                                       bsx, bsy, nbx, nby, true, true, 0.f, out, nullptr);
+    int rc = check_launch("dp_fixed_density_map scatter");
+    if (rc) return rc;
+  }
+  float vmax = (float)((double)bsx * (double)bsy);
+  clamp_max_kernel<<<grid_for(nbins, 256), 256, 0, s>>>(out, nbins, vmax);
+  return check_launch("dp_fixed_density_map clamp");
+}
+
+extern "C" int dp_density_map_exact(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                    const int* rb, const int* re, int nranges, float xl, float yl,
+                                    float xh, float yh, int nbx, int nby, int deterministic,
+                                    int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
+  DP_REQUIRE(pos && sx && sy && out, "dp_density_map_exact: null pointer argument");
+  DP_REQUIRE(nranges >= 0 && (nranges == 0 || (rb && re)), "dp_density_map_exact: bad ranges");
+  DP_REQUIRE(nbx > 0 && nby > 0, "dp_density_map_exact: bad bin grid");
+  DP_REQUIRE(!deterministic || scratch, "dp_density_map_exact: deterministic mode needs scratch_fixed");
+  cudaStream_t s = as_stream(stream);
+  int nbins = nbx * nby;
+  const float* x = pos;
+  const float* y = pos + num_nodes;
+  for (int r = 0; r < nranges; ++r) {
+    DP_REQUIRE(rb[r] >= 0 && re[r] <= num_nodes, "dp_density_map_exact: range %d out of bounds", r);
+    int n = re[r] - rb[r];
+    if (n <= 0) continue;
+    if (deterministic) {
+      // each range is converted onto the running map on its own, as the reference does
+      cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
+      box_scatter_kernel<true><<<grid_for(n, 128, 8), 128, 0, s>>>(
+          x, y, sx, sy, rb[r], re[r], xl, yl, xh, yh, nbx, nby, ldexpf(1.0f, fraction_bits), nullptr,
+          reinterpret_cast<unsigned long long*>(scratch));
+      int rc = check_launch("dp_density_map_exact scatter");
+      if (rc) return rc;
+      fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, out,
+                                                                ldexp(1.0, -fraction_bits), out, nbins);
+      rc = check_launch("dp_density_map_exact convert");
+      if (rc) return rc;
+    } else {
+      box_scatter_kernel<false><<<grid_for(n, 128, 8), 128, 0, s>>>(x, y, sx, sy, rb[r], re[r], xl, yl, xh, yh,
+                                                                    nbx, nby, 0.f, out, nullptr);
+      int rc = check_launch("dp_density_map_exact scatter");
+      if (rc) return rc;
+    }
+  }
+  return DP_OK;
+}
+
+extern "C" int dp_density_overflow(const float* map, int nbins, double target_area, double bin_area,
+                                   double* out2, float* out2_f32, dp_stream_t stream) {
+  DP_REQUIRE(map && out2 && nbins > 0, "dp_density_overflow: bad arguments");
+  cudaStream_t s = as_stream(stream);
+  // out2[0] accumulates the overflow; out2[1] holds the max key until the
+  // finishing kernel replaces it with max / bin_area.
+  cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
+  unsigned* maxslot = reinterpret_cast<unsigned*>(out2 + 1);
+  overflow_kernel<<<grid_for(nbins, 256, 4), 256, 0, s>>>(map, nbins, target_area, out2, maxslot);
+  int rc = check_launch("dp_density_overflow");
+  if (rc) return rc;
+  overflow_finish_kernel<<<1, 1, 0, s>>>(out2, maxslot, bin_area, out2_f32);
+  return check_launch("dp_density_overflow finish");
+}

@@ -1,0 +1,157 @@
+// Epilogues of the Poisson-solve GEMMs, shared by the SIMT (fp32) and the
+// tcgen05 (tf32 / bf16 / split-bf16) kernels.  Each epilogue consumes one
+// output element value v = alpha * C[m,n] at (m, n).
+#pragma once
+#include "common.cuh"
+
+namespace dpb {
+
+// operand storage formats of a GEMM input / intermediate
+enum OperandFmt { kFmtF32 = 0, kFmtBF16 = 1, kFmtSplit = 2 };
+
+inline int operand_fmt(int precision) {
+  switch (precision) {
+    case DP_PREC_BF16: return kFmtBF16;
+    case DP_PREC_SPLIT_BF16: return kFmtSplit;
+    default: return kFmtF32;
+  }
+}
+
+struct EpiParams {
+  int kind;  // DP_EPI_*
+  float alpha;
+  int ldc;
+  int fmt;  // OperandFmt of operand-typed outputs (STORE_T, SPECTRAL)
+  int M, N;
+  float* out_f32;
+  __nv_bfloat16* out_hi;
+  __nv_bfloat16* out_lo;
+  float* sp_f32[3];
+  __nv_bfloat16* sp_hi[3];
+  __nv_bfloat16* sp_lo[3];
+  float wv_scale;
+  float two_pi_over_m, two_pi_over_n;
+  const float* rho;
+  double* energy;
+};
+
+__device__ __forceinline__ void store_operand(int fmt, float v, size_t idx, float* f32,
+                                              __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  if (fmt == kFmtF32) {
+    f32[idx] = v;
+  } else {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[idx] = h;
+    if (fmt == kFmtSplit) lo[idx] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+}
+
+// Spectral weights as the reference builds them in fp32
+// (electric_potential/electric_potential.py:504-519):
+//   wu = u*(2pi/M); wv = v*(2pi/N)*(bsx/bsy); d = wu^2 + wv^2 (1 at [0,0]);
+//   inv = 1/d (0 at [0,0]); wx = wu*inv*0.5; wy = wv*inv*0.5
+__device__ __forceinline__ void spectral_weights(const EpiParams& p, int u, int v, float& wx,
+                                                 float& wy, float& winv) {
+  float wu = __fmul_rn((float)u, p.two_pi_over_m);
+  float wv = __fmul_rn(__fmul_rn((float)v, p.two_pi_over_n), p.wv_scale);
+  float d = __fadd_rn(__fmul_rn(wu, wu), __fmul_rn(wv, wv));
+  if (u == 0 && v == 0) d = 1.0f;
+  float inv = __fdiv_rn(1.0f, d);
+  if (u == 0 && v == 0) inv = 0.0f;
+  winv = inv;
+  wx = __fmul_rn(__fmul_rn(wu, inv), 0.5f);
+  wy = __fmul_rn(__fmul_rn(wv, inv), 0.5f);
+}
+
+// Applies the epilogue to one element.  Returns the contribution to the
+// energy dot product (ENERGY) or 0.
+__device__ __forceinline__ double epi_apply(const EpiParams& p, int m, int n, float acc) {
+  float v = __fmul_rn(acc, p.alpha);
+  switch (p.kind) {
+    case DP_EPI_STORE:
+      p.out_f32[(size_t)m * p.ldc + n] = v;
+      return 0.0;
+    case DP_EPI_STORE_T:
+      store_operand(p.fmt, v, (size_t)n * p.ldc + m, p.out_f32, p.out_hi, p.out_lo);
+      return 0.0;
+    case DP_EPI_SPECTRAL: {
+      float wx, wy, winv;
+      spectral_weights(p, m, n, wx, wy, winv);
+      size_t idx = (size_t)m * p.ldc + n;
+      store_operand(p.fmt, __fmul_rn(v, wx), idx, p.sp_f32[0], p.sp_hi[0], p.sp_lo[0]);
+      store_operand(p.fmt, __fmul_rn(v, wy), idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
+      if (p.sp_f32[2] || p.sp_hi[2])
+        store_operand(p.fmt, __fmul_rn(v, winv), idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
+      return 0.0;
+    }
+    case DP_EPI_ENERGY: {
+      size_t idx = (size_t)m * p.ldc + n;
+      if (p.out_f32) p.out_f32[idx] = v;
+      return (double)__fmul_rn(v, p.rho[idx]);
+    }
+  }
+  return 0.0;
+}
+
+// Host: builds the device-side epilogue parameters from a public problem.
+inline EpiParams make_epi(const dp_gemm_problem& q, int precision, int M, int N) {
+  EpiParams e;
+  memset(&e, 0, sizeof(e));
+  e.kind = q.epilogue;
+  e.alpha = q.alpha;
+  e.ldc = q.ldc;
+  e.fmt = operand_fmt(precision);
+  e.M = M;
+  e.N = N;
+  e.out_f32 = q.out_f32;
+  e.out_hi = (__nv_bfloat16*)q.out_hi;
+  e.out_lo = (__nv_bfloat16*)q.out_lo;
+  for (int i = 0; i < 3; ++i) {
+    e.sp_f32[i] = q.spec_out_f32[i];
+    e.sp_hi[i] = (__nv_bfloat16*)q.spec_out_hi[i];
+    e.sp_lo[i] = (__nv_bfloat16*)q.spec_out_lo[i];
+  }
+  e.wv_scale = q.wv_scale;
+  e.two_pi_over_m = (float)(2.0 * M_PI / M);
+  e.two_pi_over_n = (float)(2.0 * M_PI / N);
+  e.rho = q.rho;
+  e.energy = q.energy_f64;
+  return e;
+}
+
+inline int validate_problem(const dp_gemm_problem& q, int precision, int M, int N, int K) {
+  DP_REQUIRE(q.a_hi && q.b_hi, "dp_transform_gemm: null operand");
+  DP_REQUIRE(precision != DP_PREC_SPLIT_BF16 || (q.a_lo && q.b_lo),
+             "dp_transform_gemm: split-bf16 needs lo operands");
+  DP_REQUIRE(q.lda >= K && q.ldb >= K, "dp_transform_gemm: leading dimension smaller than K");
+  int fmt = operand_fmt(precision);
+  switch (q.epilogue) {
+    case DP_EPI_STORE:
+      DP_REQUIRE(q.out_f32 && q.ldc >= N, "dp_transform_gemm: STORE needs out_f32 and ldc >= N");
+      break;
+    case DP_EPI_STORE_T:
+      DP_REQUIRE(q.ldc >= M, "dp_transform_gemm: STORE_T needs ldc >= M");
+      DP_REQUIRE(fmt == kFmtF32 ? q.out_f32 != nullptr : q.out_hi != nullptr,
+                 "dp_transform_gemm: STORE_T output missing");
+      DP_REQUIRE(fmt != kFmtSplit || q.out_lo, "dp_transform_gemm: STORE_T split output needs out_lo");
+      break;
+    case DP_EPI_SPECTRAL:
+      DP_REQUIRE(q.ldc >= N, "dp_transform_gemm: SPECTRAL needs ldc >= N");
+      for (int i = 0; i < 2; ++i) {
+        DP_REQUIRE(fmt == kFmtF32 ? q.spec_out_f32[i] != nullptr : q.spec_out_hi[i] != nullptr,
+                   "dp_transform_gemm: SPECTRAL output %d missing", i);
+        DP_REQUIRE(fmt != kFmtSplit || q.spec_out_lo[i], "dp_transform_gemm: SPECTRAL lo output %d missing", i);
+      }
+      DP_REQUIRE(fmt != kFmtSplit || !q.spec_out_hi[2] || q.spec_out_lo[2],
+                 "dp_transform_gemm: SPECTRAL lo output 2 missing");
+      break;
+    case DP_EPI_ENERGY:
+      DP_REQUIRE(q.rho && q.energy_f64 && q.ldc >= N, "dp_transform_gemm: ENERGY needs rho and energy_f64");
+      break;
+    default:
+      DP_REQUIRE(false, "dp_transform_gemm: unknown epilogue %d", q.epilogue);
+  }
+  return DP_OK;
+}
+
+}  // namespace dpb

@@ -1,0 +1,88 @@
+// Field gather: the electric force on every movable and filler cell, the
+// hand-written adjoint of the density scatter (electric_potential.py:219-275).
+//
+// Per cell the sum runs in the CPU reference's order
+// (electric_potential/src/electric_force.cpp:114-166): k-major over the
+// stretched cell's x bins, h-minor over y bins, area = px*py, gx += area*Ex,
+// then gx *= ratio, then * grad_pos, all with round-to-nearest and no FMA
+// contraction, so the result equals the CPU op bit for bit given the same
+// field maps.  One thread per cell; the two 4 MB field maps stay resident in
+// L2 across the gather.
+#include "common.cuh"
+
+namespace dpb {
+
+__global__ void __launch_bounds__(256) electric_force_kernel(
+    const float* __restrict__ grad_pos, int nbx, int nby, const float* __restrict__ ex,
+    const float* __restrict__ ey, const float* __restrict__ x, const float* __restrict__ y,
+    const float* __restrict__ sx_c, const float* __restrict__ sy_c, const float* __restrict__ ox,
+    const float* __restrict__ oy, const float* __restrict__ ratio, float xl, float yl, float bsx,
+    float bsy, float ibx, float iby, int num_movable, int filler_begin, int total,
+    const int* __restrict__ sorted, float scale, float* __restrict__ gx_out,
+    float* __restrict__ gy_out) {
+  const float g = grad_pos[0];
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    int i = idx < num_movable ? (sorted ? sorted[idx] : idx) : filler_begin + (idx - num_movable);
+    float sx = sx_c[i], sy = sy_c[i];
+    float nx = fadd(x[i], ox[i]);
+    float ny = fadd(y[i], oy[i]);
+    int k0, k1, h0, h1;
+    triangle_bin_range(nx, sx, xl, ibx, nbx, k0, k1);
+    triangle_bin_range(ny, sy, yl, iby, nby, h0, h1);
+    float gx = 0.f, gy = 0.f;
+    for (int k = k0; k < k1; ++k) {
+      float px = triangle_overlap(nx, sx, xl, k, bsx);
+      const float* exr = ex + (size_t)k * nby;
+      const float* eyr = ey + (size_t)k * nby;
+      for (int h = h0; h < h1; ++h) {
+        float py = triangle_overlap(ny, sy, yl, h, bsy);
+        float area = fmul(px, py);
+        gx = fadd(gx, fmul(area, __ldg(exr + h)));
+        gy = fadd(gy, fmul(area, __ldg(eyr + h)));
+      }
+    }
+    float r = ratio[i];
+    gx = fmul(fmul(fmul(gx, r), g), scale);
+    gy = fmul(fmul(fmul(gy, r), g), scale);
+    gx_out[i] = gx;
+    gy_out[i] = gy;
+  }
+}
+
+__global__ void zero_range_kernel(float* a, int begin, int end, float* b) {
+  for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    a[i] = 0.f;
+    b[i] = 0.f;
+  }
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+
+extern "C" int dp_electric_force(const float* grad_pos, int nbx, int nby, const float* ex,
+                                 const float* ey, const float* pos, int num_nodes, const float* sx,
+                                 const float* sy, const float* ox, const float* oy,
+                                 const float* ratio, float xl, float yl, float xh, float yh,
+                                 float bsx, float bsy, float ibx, float iby, int nm, int nf,
+                                 const int* sorted, float scale, float* out, dp_stream_t stream) {
+  DP_REQUIRE(grad_pos && ex && ey && pos && sx && sy && ox && oy && ratio && out,
+             "dp_electric_force: null pointer argument");
+  DP_REQUIRE(nm >= 0 && nf >= 0 && nm + nf <= num_nodes, "dp_electric_force: bad node counts");
+  DP_REQUIRE(nbx > 0 && nby > 0, "dp_electric_force: bad bin grid");
+  cudaStream_t s = as_stream(stream);
+  float* gx = out;
+  float* gy = out + num_nodes;
+  int fixed_begin = nm, fixed_end = num_nodes - nf;
+  if (fixed_end > fixed_begin) {
+    zero_range_kernel<<<grid_for(fixed_end - fixed_begin, 256), 256, 0, s>>>(gx, fixed_begin, fixed_end, gy);
+    int rc = check_launch("dp_electric_force zero");
+    if (rc) return rc;
+  }
+  int total = nm + nf;
+  if (total == 0) return DP_OK;
+  electric_force_kernel<<<grid_for(total, 256, 16), 256, 0, s>>>(
+      grad_pos, nbx, nby, ex, ey, pos, pos + num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx,
+      iby, nm, num_nodes - nf, total, sorted, scale, gx, gy);
+  return check_launch("dp_electric_force");
+}

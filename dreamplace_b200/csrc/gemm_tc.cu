@@ -1,0 +1,352 @@
+// tcgen05 tensor-core GEMMs for the Poisson solve (TF32, BF16, split-BF16).
+//
+// C[m,n] = sum_k A[m,k] * B[n,k], A and B K-contiguous in global memory.
+// One CTA computes a 128 x BN tile: TMA (128-byte swizzle, no multicast)
+// stages A and B k-blocks into a STAGES-deep shared-memory ring, one thread
+// issues tcgen05.mma (M=128, N=BN) into a TMEM accumulator, and all four
+// warps read the accumulator back with tcgen05.ld for the fused epilogue
+// (transposed operand store with bf16 hi/lo split, spectral scaling, fp32
+// field store, or the energy dot product; epilogue.cuh).
+//
+// Split-BF16 runs three passes over K into the same accumulator:
+// A_hi*B_hi + A_hi*B_lo + A_lo*B_hi (the lo*lo term is below fp32 rounding).
+//
+// Every wait on an mbarrier is bounded by a clock budget; on expiry the
+// kernel records an error code in g_tc_status, drains what it issued and
+// returns, so a broken launch reports instead of hanging the GPU.
+#include <cuda.h>
+#include "epilogue.cuh"
+
+namespace dpb {
+
+__device__ int g_tc_status = 0;
+
+constexpr int TC_BM = 128;
+constexpr int TC_THREADS = 128;
+constexpr long long kWaitBudgetCycles = 4000000000ll;  // ~2 s at 2 GHz
+
+struct TcBatch {
+  CUtensorMap a_hi[3];
+  CUtensorMap a_lo[3];
+  CUtensorMap b_hi[3];
+  CUtensorMap b_lo[3];
+  EpiParams epi[3];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; returns false (and records `code`) when the budget runs out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  long long start = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - start > kWaitBudgetCycles) {
+      atomicCAS(&g_tc_status, 0, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_addr(dst)), "l"(map), "r"(smem_addr(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template <bool kTF32>
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  if (kTF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+  }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor: K-major operand tile in the 128-byte
+// swizzle layout TMA writes (rows of 128 B, 8-row atoms of 1024 B).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address, bits [0,14)
+  d |= (uint64_t)1 << 16;                     // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;           // stride byte offset: 8-row group pitch
+  d |= (uint64_t)1 << 46;                     // descriptor version (tcgen05)
+  d |= (uint64_t)2 << 61;                     // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: D fp32, A/B bf16 (1) or tf32 (2), both K-major, M=128, N=BN.
+template <bool kTF32, int BN>
+__host__ __device__ constexpr uint32_t make_idesc() {
+  return (1u << 4)                                   // D format fp32
+         | ((kTF32 ? 2u : 1u) << 7)                  // A format
+         | ((kTF32 ? 2u : 1u) << 10)                 // B format
+         | ((uint32_t)(BN >> 3) << 17)               // N >> 3
+         | ((uint32_t)(TC_BM >> 4) << 24);           // M >> 4
+}
+
+template <int PREC, int BN, int STAGES>
+struct TcConfig {
+  static constexpr bool kTF32 = PREC == DP_PREC_TF32;
+  static constexpr bool kSplit = PREC == DP_PREC_SPLIT_BF16;
+  static constexpr int kElem = kTF32 ? 4 : 2;
+  static constexpr int kBK = 128 / kElem;                 // elements per 128-byte row
+  static constexpr int kMmaK = 32 / kElem;                // K per tcgen05.mma
+  static constexpr int kMmaPerBlock = kBK / kMmaK;        // = 4
+  static constexpr int kABytes = TC_BM * 128;
+  static constexpr int kBBytes = BN * 128;
+  static constexpr int kStageBytes = kABytes + kBBytes;
+  static constexpr int kSmemBytes = STAGES * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+  static constexpr int kPasses = kSplit ? 3 : 1;
+};
+
+template <int PREC, int BN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcBatch batch, int M,
+                                                                 int N, int K) {
+  using Cfg = TcConfig<PREC, BN, STAGES>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* tiles = smem;
+  uint64_t* full_bar = (uint64_t*)(smem + STAGES * Cfg::kStageBytes);
+  uint64_t* empty_bar = full_bar + STAGES;
+  uint64_t* acc_bar = empty_bar + STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(acc_bar + 1);
+
+  const int z = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
+  const int kb_per_pass = (K + Cfg::kBK - 1) / Cfg::kBK;
+  const int total_kb = kb_per_pass * Cfg::kPasses;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(acc_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&batch.a_hi[z]) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&batch.b_hi[z]) : "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    for (int kb = 0; kb < total_kb; ++kb) {
+      int s = kb % STAGES, round = kb / STAGES;
+      if (round > 0 && !mbar_wait(&empty_bar[s], (round - 1) & 1, 1)) break;
+      int pass = kb / kb_per_pass, kx = (kb % kb_per_pass) * Cfg::kBK;
+      const CUtensorMap* amap = (Cfg::kSplit && pass == 2) ? &batch.a_lo[z] : &batch.a_hi[z];
+      const CUtensorMap* bmap = (Cfg::kSplit && pass == 1) ? &batch.b_lo[z] : &batch.b_hi[z];
+      uint8_t* sa = tiles + s * Cfg::kStageBytes;
+      uint8_t* sb = sa + Cfg::kABytes;
+      mbar_expect_tx(&full_bar[s], Cfg::kStageBytes);
+      tma_load_2d(sa, amap, &full_bar[s], kx, m0);
+      tma_load_2d(sb, bmap, &full_bar[s], kx, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    constexpr uint32_t idesc = make_idesc<Cfg::kTF32, BN>();
+    for (int kb = 0; kb < total_kb; ++kb) {
+      int s = kb % STAGES, round = kb / STAGES;
+      if (!mbar_wait(&full_bar[s], round & 1, 2)) break;
+      tc_fence_after();
+      uint32_t sa = smem_addr(tiles + s * Cfg::kStageBytes);
+      uint32_t sb = sa + Cfg::kABytes;
+      uint64_t adesc = sw128_desc(sa), bdesc = sw128_desc(sb);
+#pragma unroll
+      for (int kk = 0; kk < Cfg::kMmaPerBlock; ++kk) {
+        // advance the start address by 32 bytes per K step inside the swizzle row
+        tc_mma<Cfg::kTF32>(tmem_base, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
+                           (kb > 0 || kk > 0) ? 1u : 0u);
+      }
+      tc_commit(&empty_bar[s]);  // frees the stage once these MMAs retire
+    }
+    tc_commit(acc_bar);  // accumulator complete (also on the error path: drains issued MMAs)
+  }
+  __syncwarp();
+
+  // ---- epilogue: warp w owns accumulator rows 32w..32w+31 ----
+  const EpiParams& P = batch.epi[z];
+  double e = 0.0;
+  if (mbar_wait(acc_bar, 0, 3)) {
+    tc_fence_after();
+    const int m = m0 + warp * 32 + lane;
+    const uint32_t row_addr = tmem_base + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 16) {
+      float v[16];
+      tmem_ld16(row_addr + (uint32_t)c, v);
+      if (m < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          int n = n0 + c + j;
+          if (n < N) e += epi_apply(P, m, n, v[j]);
+        }
+      }
+    }
+  }
+  if (P.kind == DP_EPI_ENERGY) {
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (lane == 0 && e != 0.0) atomicAdd(P.energy, e);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(BN) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------- host side
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled get_encode_fn() {
+  static PFN_encodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encodeTiled)p;
+  }
+  return fn;
+}
+
+// rows x K matrix, K contiguous, leading dimension ld (elements), box = box_rows x (128 bytes)
+static int encode_operand(CUtensorMap* map, const void* ptr, int rows, int K, int ld, int elem_bytes,
+                          int box_rows) {
+  PFN_encodeTiled enc = get_encode_fn();
+  DP_REQUIRE(enc, "dp_transform_gemm: cuTensorMapEncodeTiled unavailable");
+  DP_REQUIRE(((uintptr_t)ptr & 15) == 0, "dp_transform_gemm: operand base must be 16-byte aligned");
+  DP_REQUIRE(((long long)ld * elem_bytes) % 16 == 0, "dp_transform_gemm: operand row pitch must be a multiple of 16 bytes");
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * elem_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)(128 / elem_bytes), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                   const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  DP_REQUIRE(r == CUDA_SUCCESS, "dp_transform_gemm: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return DP_OK;
+}
+
+template <int PREC, int BN, int STAGES>
+static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, cudaStream_t s) {
+  using Cfg = TcConfig<PREC, BN, STAGES>;
+  static TcBatch batch;  // host staging; copied into the launch's parameter buffer
+  memset(&batch, 0, sizeof(batch));
+  for (int i = 0; i < count; ++i) {
+    const dp_gemm_problem& q = probs[i];
+    int rc = encode_operand(&batch.a_hi[i], q.a_hi, M, K, q.lda, Cfg::kElem, TC_BM);
+    if (!rc) rc = encode_operand(&batch.b_hi[i], q.b_hi, N, K, q.ldb, Cfg::kElem, BN);
+    if (!rc && Cfg::kSplit) rc = encode_operand(&batch.a_lo[i], q.a_lo, M, K, q.lda, Cfg::kElem, TC_BM);
+    if (!rc && Cfg::kSplit) rc = encode_operand(&batch.b_lo[i], q.b_lo, N, K, q.ldb, Cfg::kElem, BN);
+    if (rc) return rc;
+    batch.epi[i] = make_epi(q, PREC, M, N);
+  }
+  auto kern = tc_gemm_kernel<PREC, BN, STAGES>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::kSmemBytes);
+    if (e != cudaSuccess) {
+      set_error("dp_transform_gemm: cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+      return DP_ERR_CUDA;
+    }
+    configured = true;
+  }
+  dim3 grid(ceil_div(N, BN), ceil_div(M, TC_BM), count);
+  kern<<<grid, TC_THREADS, Cfg::kSmemBytes, s>>>(batch, M, N, K);
+  return check_launch("dp_transform_gemm(tcgen05)");
+}
+
+int launch_tc_gemm(int precision, int M, int N, int K, const dp_gemm_problem* probs, int count, cudaStream_t s) {
+  switch (precision) {
+    case DP_PREC_TF32: return run_tc<DP_PREC_TF32, 64, 4>(M, N, K, probs, count, s);
+    case DP_PREC_BF16: return run_tc<DP_PREC_BF16, 64, 4>(M, N, K, probs, count, s);
+    case DP_PREC_SPLIT_BF16: return run_tc<DP_PREC_SPLIT_BF16, 64, 4>(M, N, K, probs, count, s);
+  }
+  set_error("dp_transform_gemm: unsupported precision %d", precision);
+  return DP_ERR_UNSUPPORTED;
+}
+
+}  // namespace dpb
+
+// Reads and clears the device-side status word of the tensor-core kernels
+// (0 = no bounded wait expired).  Synchronises the device.
+extern "C" int dp_tc_status(int* status_out) {
+  DP_REQUIRE(status_out, "dp_tc_status: null output");
+  int zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(status_out, dpb::g_tc_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(dpb::g_tc_status, &zero, sizeof(int));
+  if (e != cudaSuccess) {
+    dpb::set_error("dp_tc_status: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}

@@ -1,0 +1,320 @@
+"""Electrostatic density operator: scatter, Poisson solve, field gather.
+
+Drop-in for the reference's ``dreamplace/ops/electric_potential/
+electric_potential.py`` and ``electric_overflow.py``: same classes
+(``ElectricDensityMapFunction``, ``ElectricOverflow``,
+``ElectricPotentialFunction``, ``ElectricPotential``), constructor and
+``forward`` signatures, with one added keyword, ``precision``, selecting the
+Poisson-solve arithmetic (``fp32`` plain form, ``tf32``, ``bf16``,
+``split_bf16``).
+
+Forward (reference electric_potential.py:52-217):
+  density = initial + scatter(movable, filler)           dp_density_map_f32 / _fx64
+  rho = density / bin_area                                (in place, as the reference)
+  a = DCT2(rho);  Ex = IDXST_IDCT(a wu/(wu^2+wv^2)/2);  Ey = IDCT_IDXST(a wv/(...)/2)
+  energy = sum(IDCT2(a/(wu^2+wv^2)) * rho)                unless fast_mode
+as four GEMM launches: rho C_N^T (transposed bf16/fp32 operand out), C_M T with
+the spectral weights in the epilogue, the three right products batched in one
+launch, and the three left products batched with Ex/Ey stores and the energy
+dot product fused (the potential map is never written).
+Backward: the hand-written adjoint ``-electric_force`` (reference :219-275).
+"""
+import logging
+import math
+
+import numpy as np
+import torch
+from torch import nn
+from torch.autograd import Function
+
+from ._native import C, precision_code, require_cuda
+from .dct2_fft2 import (DCT2, EPI_ENERGY, EPI_SPECTRAL, EPI_STORE, EPI_STORE_T, IDCT2, IDCT_IDXST, IDXST_IDCT,
+                        Operand, get_exact_expk, transform_matrices)
+
+logger = logging.getLogger(__name__)
+
+
+def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
+    """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
+
+    Returns (field_map_x, field_map_y, energy_f64[1]); energy is zero when
+    ``fast_mode``.  Four GEMM launches, see the module docstring."""
+    prec = precision_code(precision)
+    M, N = rho.shape
+    dev = rho.device
+    cM, chM, shM = transform_matrices(M, prec, dev)
+    cN, chN, shN = transform_matrices(N, prec, dev)
+    # G1: T1^T = (rho C_N^T)^T, [N, M]
+    t1 = Operand((N, M), prec, dev)
+    g1 = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=1.0, ldc=M)
+    if prec == 0:
+        g1["a_hi"] = rho
+    else:
+        Operand.from_tensor(rho, prec).as_a(g1)
+    cN.as_b(g1)
+    t1.as_out_t(g1)
+    C.transform_gemm(prec, M, N, N, [g1])
+    # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy, a*winv  [M, N]
+    spec = [Operand((M, N), prec, dev) for _ in range(2 if fast_mode else 3)]
+    g2 = dict(lda=M, ldb=M, epilogue=EPI_SPECTRAL, alpha=4.0 / (M * N), ldc=N,
+              wv_scale=float(bin_size_x / bin_size_y))
+    cM.as_a(g2)
+    t1.as_b(g2)
+    for i, s in enumerate(spec):
+        if s.f32 is not None:
+            g2["sp%d_f32" % i] = s.f32
+        else:
+            g2["sp%d_hi" % i] = s.hi
+            g2["sp%d_lo" % i] = s.lo
+    C.transform_gemm(prec, M, N, M, [g2])
+    # G3: U^T = (A R^T)^T for the x field (R = Ch_N), y field (Sh_N) and potential (Ch_N)
+    rights = [chN, shN, chN][:len(spec)]
+    us = [Operand((N, M), prec, dev) for _ in spec]
+    g3 = []
+    for s, r, u in zip(spec, rights, us):
+        d = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=1.0, ldc=M)
+        s.as_a(d)
+        r.as_b(d)
+        u.as_out_t(d)
+        g3.append(d)
+    C.transform_gemm(prec, M, N, N, g3)
+    # G4: Ex = 4 Sh_M Ux, Ey = 4 Ch_M Uy, energy = sum(4 Ch_M Uphi * rho)
+    ex = torch.empty(M, N, dtype=torch.float32, device=dev)
+    ey = torch.empty(M, N, dtype=torch.float32, device=dev)
+    energy = torch.zeros(1, dtype=torch.float64, device=dev)
+    g4 = [shM.as_a(us[0].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ex))),
+          chM.as_a(us[1].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ey)))]
+    if not fast_mode:
+        g4.append(chM.as_a(us[2].as_b(dict(lda=M, ldb=M, epilogue=EPI_ENERGY, alpha=4.0, ldc=N, rho=rho,
+                                           energy=energy))))
+    C.transform_gemm(prec, M, N, M, g4)
+    return ex, ey, energy
+
+
+class ElectricDensityMapFunction(Function):
+    """Density map of movable + filler cells on top of the fixed-cell map.
+
+    Called directly (``ElectricDensityMapFunction.forward(...)``, no ctx) as in
+    the reference electric_overflow.py:57-114."""
+
+    @staticmethod
+    def forward(pos, node_size_x_clamped, node_size_y_clamped, offset_x, offset_y, ratio, bin_center_x,
+                bin_center_y, initial_density_map, target_density, xl, yl, xh, yh, bin_size_x, bin_size_y,
+                num_movable_nodes, num_filler_nodes, padding, padding_mask, num_bins_x, num_bins_y,
+                num_movable_impacted_bins_x, num_movable_impacted_bins_y, num_filler_impacted_bins_x,
+                num_filler_impacted_bins_y, deterministic_flag, sorted_node_map):
+        require_cuda(pos, "pos")
+        output = C.density_map(pos.view(pos.numel()), node_size_x_clamped, node_size_y_clamped, offset_x,
+                               offset_y, ratio, bin_center_x, bin_center_y, initial_density_map,
+                               float(target_density), float(xl), float(yl), float(xh), float(yh),
+                               float(bin_size_x), float(bin_size_y), int(num_movable_nodes),
+                               int(num_filler_nodes), int(padding), int(num_bins_x), int(num_bins_y),
+                               int(num_movable_impacted_bins_x), int(num_movable_impacted_bins_y),
+                               int(num_filler_impacted_bins_x), int(num_filler_impacted_bins_y),
+                               int(bool(deterministic_flag)), sorted_node_map)
+        density_map = output.view([num_bins_x, num_bins_y])
+        if padding > 0:
+            density_map.masked_fill_(padding_mask, target_density * bin_size_x * bin_size_y)
+        return density_map
+
+
+class ElectricOverflow(nn.Module):
+    """Overflow / max-density evaluation (reference electric_overflow.py:117-278)."""
+
+    def __init__(self, node_size_x, node_size_y, bin_center_x, bin_center_y, target_density, xl, yl, xh, yh,
+                 bin_size_x, bin_size_y, num_movable_nodes, num_terminals, num_filler_nodes, padding,
+                 deterministic_flag, sorted_node_map, movable_macro_mask=None):
+        super().__init__()
+        self.node_size_x = node_size_x
+        self.node_size_y = node_size_y
+        self.bin_center_x = bin_center_x
+        self.bin_center_y = bin_center_y
+        self.target_density = target_density
+        self.xl, self.yl, self.xh, self.yh = xl, yl, xh, yh
+        self.bin_size_x = bin_size_x
+        self.bin_size_y = bin_size_y
+        self.num_movable_nodes = num_movable_nodes
+        self.num_terminals = num_terminals
+        self.num_filler_nodes = num_filler_nodes
+        self.padding = padding
+        self.sorted_node_map = sorted_node_map
+        self.movable_macro_mask = movable_macro_mask
+        self.deterministic_flag = deterministic_flag
+        self.reset()
+
+    def reset(self):
+        """Stretched sizes, offsets and area ratios (reference electric_overflow.py:162-227)."""
+        sqrt2 = math.sqrt(2)
+        self.node_size_x_clamped = self.node_size_x.clamp(min=self.bin_size_x * sqrt2)
+        self.offset_x = (self.node_size_x - self.node_size_x_clamped).mul(0.5)
+        self.node_size_y_clamped = self.node_size_y.clamp(min=self.bin_size_y * sqrt2)
+        self.offset_y = (self.node_size_y - self.node_size_y_clamped).mul(0.5)
+        node_areas = self.node_size_x * self.node_size_y
+        self.ratio = node_areas / (self.node_size_x_clamped * self.node_size_y_clamped)
+        self.num_movable_macros = 0
+        if self.target_density < 1 and self.movable_macro_mask is not None:
+            self.num_movable_macros = int(self.movable_macro_mask.sum().item())
+            self.ratio[:self.num_movable_nodes][self.movable_macro_mask] = self.target_density
+        self.num_bins_x = int(round((self.xh - self.xl) / self.bin_size_x))
+        self.num_bins_y = int(round((self.yh - self.yl) / self.bin_size_y))
+        nm, nf = self.num_movable_nodes, self.num_filler_nodes
+        if nm:
+            self.num_movable_impacted_bins_x = int(math.ceil(min(
+                (float(self.node_size_x[:nm].max()) + 2 * sqrt2 * self.bin_size_x) / self.bin_size_x, self.num_bins_x)))
+            self.num_movable_impacted_bins_y = int(math.ceil(min(
+                (float(self.node_size_y[:nm].max()) + 2 * sqrt2 * self.bin_size_y) / self.bin_size_y, self.num_bins_y)))
+        else:
+            self.num_movable_impacted_bins_x = self.num_movable_impacted_bins_y = 0
+        if nf:
+            self.num_filler_impacted_bins_x = int(math.ceil(min(
+                (float(self.node_size_x[-nf:].max()) + 2 * sqrt2 * self.bin_size_x) / self.bin_size_x, self.num_bins_x)))
+            self.num_filler_impacted_bins_y = int(math.ceil(min(
+                (float(self.node_size_y[-nf:].max()) + 2 * sqrt2 * self.bin_size_y) / self.bin_size_y, self.num_bins_y)))
+        else:
+            self.num_filler_impacted_bins_x = self.num_filler_impacted_bins_y = 0
+        dev = self.node_size_x.device
+        self.padding_mask = torch.zeros(self.num_bins_x, self.num_bins_y, dtype=torch.bool, device=dev)
+        if self.padding > 0:
+            self.padding_mask.fill_(True)
+            self.padding_mask[self.padding:self.num_bins_x - self.padding,
+                              self.padding:self.num_bins_y - self.padding] = False
+        self.initial_density_map = None
+
+    def compute_initial_density_map(self, pos):
+        """Fixed-cell map ×target_density (reference electric_overflow.py:229-258)."""
+        nm, nt = self.num_movable_nodes, self.num_terminals
+        if nt == 0:
+            nfx = nfy = 0
+        else:
+            nfx = int(math.ceil(min((float(self.node_size_x[nm:nm + nt].max()) + self.bin_size_x) / self.bin_size_x,
+                                    self.num_bins_x)))
+            nfy = int(math.ceil(min((float(self.node_size_y[nm:nm + nt].max()) + self.bin_size_y) / self.bin_size_y,
+                                    self.num_bins_y)))
+        self.initial_density_map = C.fixed_density_map(
+            pos, self.node_size_x, self.node_size_y, self.bin_center_x, self.bin_center_y, float(self.xl),
+            float(self.yl), float(self.xh), float(self.yh), float(self.bin_size_x), float(self.bin_size_y), nm, nt,
+            self.num_bins_x, self.num_bins_y, nfx, nfy, int(bool(self.deterministic_flag)))
+        self.initial_density_map.mul_(self.target_density)
+
+    def _density_map(self, pos, num_filler_nodes):
+        return ElectricDensityMapFunction.forward(
+            pos, self.node_size_x_clamped, self.node_size_y_clamped, self.offset_x, self.offset_y, self.ratio,
+            self.bin_center_x, self.bin_center_y, self.initial_density_map, self.target_density, self.xl,
+            self.yl, self.xh, self.yh, self.bin_size_x, self.bin_size_y, self.num_movable_nodes,
+            num_filler_nodes, self.padding, self.padding_mask, self.num_bins_x, self.num_bins_y,
+            self.num_movable_impacted_bins_x, self.num_movable_impacted_bins_y,
+            self.num_filler_impacted_bins_x, self.num_filler_impacted_bins_y, self.deterministic_flag,
+            self.sorted_node_map)
+
+    def overflow_f64(self, pos):
+        """(overflow, max_density) accumulated in fp64, as a [2] float64 tensor."""
+        if self.initial_density_map is None:
+            self.compute_initial_density_map(pos)
+        density_map = self._density_map(pos, self.num_filler_nodes)
+        bin_area = self.bin_size_x * self.bin_size_y
+        return C.density_overflow(density_map, float(self.target_density * bin_area), float(bin_area))
+
+    def forward(self, pos):
+        out = self.overflow_f64(pos)
+        return out[0:1].float(), out[1:2].float()
+
+
+class ElectricPotentialFunction(Function):
+    """Energy forward / electric-force backward (reference electric_potential.py:47-275)."""
+
+    @staticmethod
+    def forward(ctx, pos, node_size_x_clamped, node_size_y_clamped, offset_x, offset_y, ratio, bin_center_x,
+                bin_center_y, initial_density_map, target_density, xl, yl, xh, yh, bin_size_x, bin_size_y,
+                num_movable_nodes, num_filler_nodes, padding, padding_mask, num_bins_x, num_bins_y,
+                num_movable_impacted_bins_x, num_movable_impacted_bins_y, num_filler_impacted_bins_x,
+                num_filler_impacted_bins_y, deterministic_flag, sorted_node_map, exact_expkM=None,
+                exact_expkN=None, inv_wu2_plus_wv2=None, wu_by_wu2_plus_wv2_half=None,
+                wv_by_wu2_plus_wv2_half=None, dct2=None, idct2=None, idct_idxst=None, idxst_idct=None,
+                fast_mode=True, precision="fp32"):
+        density_map = ElectricDensityMapFunction.forward(
+            pos, node_size_x_clamped, node_size_y_clamped, offset_x, offset_y, ratio, bin_center_x,
+            bin_center_y, initial_density_map, target_density, xl, yl, xh, yh, bin_size_x, bin_size_y,
+            num_movable_nodes, num_filler_nodes, padding, padding_mask, num_bins_x, num_bins_y,
+            num_movable_impacted_bins_x, num_movable_impacted_bins_y, num_filler_impacted_bins_x,
+            num_filler_impacted_bins_y, deterministic_flag, sorted_node_map)
+        ctx.args = (num_bins_x, num_bins_y, num_movable_impacted_bins_x, num_movable_impacted_bins_y,
+                    num_filler_impacted_bins_x, num_filler_impacted_bins_y)
+        ctx.node = (node_size_x_clamped, node_size_y_clamped, offset_x, offset_y, ratio, bin_center_x,
+                    bin_center_y)
+        ctx.geom = (xl, yl, xh, yh, bin_size_x, bin_size_y, num_movable_nodes, num_filler_nodes)
+        ctx.deterministic_flag = deterministic_flag
+        ctx.sorted_node_map = sorted_node_map
+        ctx.pos = pos
+        density_map.mul_(1.0 / (bin_size_x * bin_size_y))
+        ex, ey, energy = poisson_solve(density_map, bin_size_x, bin_size_y, precision, fast_mode)
+        ctx.field_map_x = ex
+        ctx.field_map_y = ey
+        ctx.density_map = density_map
+        if fast_mode:
+            return torch.zeros(1, dtype=pos.dtype, device=pos.device)
+        return energy.to(pos.dtype).view([])
+
+    @staticmethod
+    def backward(ctx, grad_pos):
+        nbx, nby, a, b, c, d = ctx.args
+        sxc, syc, ox, oy, ratio, bcx, bcy = ctx.node
+        xl, yl, xh, yh, bsx, bsy, nm, nf = ctx.geom
+        g = grad_pos.reshape(1).to(torch.float32)
+        output = C.electric_force(g, nbx, nby, a, b, c, d, ctx.field_map_x.view([-1]), ctx.field_map_y.view([-1]),
+                                  ctx.pos, sxc, syc, ox, oy, ratio, bcx, bcy, float(xl), float(yl), float(xh),
+                                  float(yh), float(bsx), float(bsy), int(nm), int(nf),
+                                  int(bool(ctx.deterministic_flag)), ctx.sorted_node_map, -1.0)
+        return (output,) + (None,) * 38
+
+
+class ElectricPotential(ElectricOverflow):
+    """Electrostatic density penalty (reference electric_potential.py:278-553)."""
+
+    def __init__(self, node_size_x, node_size_y, bin_center_x, bin_center_y, target_density, xl, yl, xh, yh,
+                 bin_size_x, bin_size_y, num_movable_nodes, num_terminals, num_filler_nodes, padding,
+                 deterministic_flag, sorted_node_map, movable_macro_mask=None, fast_mode=False, region_id=None,
+                 fence_regions=None, node2fence_region_map=None, placedb=None, precision="fp32"):
+        if region_id is not None or fence_regions is not None:
+            raise NotImplementedError("fence-region electric fields are not supported by dreamplace_b200")
+        super().__init__(node_size_x=node_size_x, node_size_y=node_size_y, bin_center_x=bin_center_x,
+                         bin_center_y=bin_center_y, target_density=target_density, xl=xl, yl=yl, xh=xh, yh=yh,
+                         bin_size_x=bin_size_x, bin_size_y=bin_size_y, num_movable_nodes=num_movable_nodes,
+                         num_terminals=num_terminals, num_filler_nodes=num_filler_nodes, padding=padding,
+                         deterministic_flag=deterministic_flag, sorted_node_map=sorted_node_map,
+                         movable_macro_mask=movable_macro_mask)
+        self.fast_mode = fast_mode
+        self.precision = precision_code(precision)
+        self.region_id = None
+        self.fence_regions = None
+
+    def reset(self):
+        super().reset()
+        self.exact_expkM = self.exact_expkN = None
+        self.dct2 = self.idct2 = self.idct_idxst = self.idxst_idct = None
+
+    def forward(self, pos, mode="density"):
+        assert mode in {"density", "overflow"}, "Only support density mode or overflow mode"
+        if self.initial_density_map is None:
+            self.compute_initial_density_map(pos)
+            M, N = self.num_bins_x, self.num_bins_y
+            self.exact_expkM = get_exact_expk(M, dtype=pos.dtype, device=pos.device)
+            self.exact_expkN = get_exact_expk(N, dtype=pos.dtype, device=pos.device)
+            self.dct2 = DCT2(self.exact_expkM, self.exact_expkN, self.precision)
+            if not self.fast_mode:
+                self.idct2 = IDCT2(self.exact_expkM, self.exact_expkN, self.precision)
+            self.idct_idxst = IDCT_IDXST(self.exact_expkM, self.exact_expkN, self.precision)
+            self.idxst_idct = IDXST_IDCT(self.exact_expkM, self.exact_expkN, self.precision)
+        if mode == "density":
+            return ElectricPotentialFunction.apply(
+                pos, self.node_size_x_clamped, self.node_size_y_clamped, self.offset_x, self.offset_y,
+                self.ratio, self.bin_center_x, self.bin_center_y, self.initial_density_map, self.target_density,
+                self.xl, self.yl, self.xh, self.yh, self.bin_size_x, self.bin_size_y, self.num_movable_nodes,
+                self.num_filler_nodes, self.padding, self.padding_mask, self.num_bins_x, self.num_bins_y,
+                self.num_movable_impacted_bins_x, self.num_movable_impacted_bins_y,
+                self.num_filler_impacted_bins_x, self.num_filler_impacted_bins_y, self.deterministic_flag,
+                self.sorted_node_map, self.exact_expkM, self.exact_expkN, None, None, None, self.dct2,
+                self.idct2, self.idct_idxst, self.idxst_idct, self.fast_mode, self.precision)
+        density_map = self._density_map(pos, 0)
+        bin_area = self.bin_size_x * self.bin_size_y
+        out = C.density_overflow(density_map, float(self.target_density * bin_area), float(bin_area))
+        return out[0].float(), out[1].float()

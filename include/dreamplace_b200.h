@@ -1,0 +1,228 @@
+/*
+ * dreamplace_b200 C ABI: the global-placement hot path of DREAMPlace as plain
+ * C entry points over device pointers (sm_100a).
+ *
+ * Conventions
+ *  - Every pointer is a device pointer unless its name ends in `_host`.
+ *  - `pos` arrays are [x(n), y(n)] float32, node order movable | fixed | filler.
+ *  - Bin maps are x-major: index = k * num_bins_y + h.
+ *  - Every call is asynchronous on `stream` (NULL = legacy default stream),
+ *    performs no host synchronisation and allocates no memory; scratch
+ *    buffers are passed by the caller.
+ *  - Return value: DP_OK (0) or a negative DP_ERR_* code; dp_last_error()
+ *    returns a message for the calling thread's most recent failure.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the reference project's dreamplace/ops/).
+ */
+#ifndef DREAMPLACE_B200_H
+#define DREAMPLACE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dp_stream_t; /* same type as cudaStream_t */
+
+enum {
+  DP_OK = 0,
+  DP_ERR_INVALID_ARGUMENT = -1,
+  DP_ERR_CUDA = -2,
+  DP_ERR_UNSUPPORTED = -3,
+  DP_ERR_TIMEOUT = -4
+};
+
+/* DCT / Poisson-solve arithmetic */
+enum {
+  DP_PREC_FP32 = 0,       /* SIMT FFMA, fp32 operands (the plain form)            */
+  DP_PREC_TF32 = 1,       /* tcgen05 kind::tf32, fp32 accumulate                   */
+  DP_PREC_BF16 = 2,       /* tcgen05 kind::f16 bf16 x bf16, fp32 accumulate        */
+  DP_PREC_SPLIT_BF16 = 3  /* hi*hi + hi*lo + lo*hi bf16 products, fp32 accumulate  */
+};
+
+const char* dp_last_error(void);
+int dp_version(void);
+/* Number of kernels this library has launched in the calling process. */
+uint64_t dp_launch_count(void);
+
+/* ---- density scatter (electric_potential/src/electric_density_map_cuda.cpp:71-136,
+ *      CPU electric_potential/src/electric_density_map.cpp:100-152) ----------
+ * density_map = initial_density_map + triangle-model scatter of the movable
+ * cells (visited through sorted_node_map when it is non-NULL) and the last
+ * num_filler_nodes nodes.  inv_bin_size_x/y are the float reciprocals the
+ * reference uses for the bin range.  density_map may alias initial_density_map. */
+int dp_density_map_f32(const float* pos, int num_nodes,
+                       const float* node_size_x_clamped, const float* node_size_y_clamped,
+                       const float* offset_x, const float* offset_y, const float* ratio,
+                       const float* initial_density_map,
+                       float xl, float yl, float xh, float yh,
+                       float bin_size_x, float bin_size_y,
+                       float inv_bin_size_x, float inv_bin_size_y,
+                       int num_movable_nodes, int num_filler_nodes,
+                       int num_bins_x, int num_bins_y,
+                       const int* sorted_node_map,
+                       float* density_map, dp_stream_t stream);
+
+/* Deterministic mode: every bin update is trunc(area * 2^fraction_bits) added to a
+ * 64-bit integer map (int64 two's complement, as the reference CPU op's `long`),
+ * then density_map = (float)((double)initial + (double)fixed * 2^-fraction_bits),
+ * the CPU op's conversion (utility/src/atomic_ops.h:48-54).
+ * scratch_fixed: caller-owned int64 [num_bins_x*num_bins_y]; on return it holds
+ * the integer map (bit-exact with the reference CPU op's `buf`). */
+int dp_density_map_fx64(const float* pos, int num_nodes,
+                        const float* node_size_x_clamped, const float* node_size_y_clamped,
+                        const float* offset_x, const float* offset_y, const float* ratio,
+                        const float* initial_density_map,
+                        float xl, float yl, float xh, float yh,
+                        float bin_size_x, float bin_size_y,
+                        float inv_bin_size_x, float inv_bin_size_y,
+                        int num_movable_nodes, int num_filler_nodes,
+                        int num_bins_x, int num_bins_y,
+                        const int* sorted_node_map, int fraction_bits,
+                        int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
+
+/* Exact-overlap fixed-cell map (electric_potential/src/electric_density_map_cuda.cpp:139-183,
+ * CPU electric_potential/src/electric_density_map.cpp:155-213): nodes
+ * [num_movable_nodes, num_movable_nodes+num_terminals), fixed_node_flag=true,
+ * then clamp_max(bin area).  deterministic != 0 uses the int64 fixed-point path
+ * and needs scratch_fixed [num_bins]; otherwise scratch_fixed may be NULL. */
+int dp_fixed_density_map(const float* pos, int num_nodes,
+                         const float* node_size_x, const float* node_size_y,
+                         const float* bin_center_x, const float* bin_center_y,
+                         float xl, float yl, float xh, float yh,
+                         float bin_size_x, float bin_size_y,
+                         int num_movable_nodes, int num_terminals,
+                         int num_bins_x, int num_bins_y,
+                         int deterministic, int fraction_bits,
+                         int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
+
+/* Exact-overlap DensityMap (density_map/src/density_map.cpp:distributeBox2Bin,
+ * CUDA density_map/src/density_map_cuda_kernel.cu:69-170): nodes of each half-open
+ * range [range_begin_host[i], range_end_host[i]) are added onto density_map, which
+ * holds the caller's initial map.  Bin size is (xh-xl)/num_bins_x in float; the y
+ * range is widened by two bins each side; the last bin extends to the cell edge.
+ * Deterministic mode converts each range's int64 map onto density_map in turn. */
+int dp_density_map_exact(const float* pos, int num_nodes,
+                         const float* node_size_x, const float* node_size_y,
+                         const int* range_begin_host, const int* range_end_host, int num_ranges,
+                         float xl, float yl, float xh, float yh,
+                         int num_bins_x, int num_bins_y,
+                         int deterministic, int fraction_bits, int64_t* scratch_fixed,
+                         float* density_map, dp_stream_t stream);
+
+/* Overflow evaluation (electric_potential/electric_overflow.py:260-278):
+ * overflow_out = sum(max(D - target_area, 0)) and max_density_out = max(D)/bin_area,
+ * both accumulated in fp64; out_f32 (optional, 2 floats) receives them rounded. */
+int dp_density_overflow(const float* density_map, int num_bins, double target_area,
+                        double bin_area, double* out2_f64, float* out2_f32,
+                        dp_stream_t stream);
+
+/* ---- field gather (electric_potential/src/electric_force_cuda.cpp:56-124,
+ *      CPU electric_potential/src/electric_force.cpp:76-172) ---------------
+ * grad_out[i] = scale * grad_pos[0] * ratio_i * sum_{k,h} px*py*E[k,h] for movable
+ * (through sorted_node_map when non-NULL) and filler nodes; fixed nodes get 0.
+ * The per-cell sum follows the CPU op's loop order without contraction, so
+ * with scale = -1 the result is bit-identical to -electric_force_cpp(...). */
+int dp_electric_force(const float* grad_pos, int num_bins_x, int num_bins_y,
+                      const float* field_map_x, const float* field_map_y,
+                      const float* pos, int num_nodes,
+                      const float* node_size_x_clamped, const float* node_size_y_clamped,
+                      const float* offset_x, const float* offset_y, const float* ratio,
+                      float xl, float yl, float xh, float yh,
+                      float bin_size_x, float bin_size_y,
+                      float inv_bin_size_x, float inv_bin_size_y,
+                      int num_movable_nodes, int num_filler_nodes,
+                      const int* sorted_node_map, float scale,
+                      float* grad_out, dp_stream_t stream);
+
+/* ---- Poisson solve as GEMMs (replaces dct/src/dct2_fft2_cuda.cpp:14-140) ------
+ * C[m,n] = sum_k A[m,k] * B[n,k]; A [M x K], B [N x K], both K-contiguous.
+ * Operands are fp32 for DP_PREC_FP32/TF32 (a_lo/b_lo ignored), bf16 hi for
+ * DP_PREC_BF16, bf16 hi+lo for DP_PREC_SPLIT_BF16.  `count` independent
+ * problems (1..3) run in one launch; each dp_gemm_problem names its operands
+ * and its epilogue. */
+enum {
+  DP_EPI_STORE = 0,      /* out_f32[m*ldc+n] = alpha*C                                  */
+  DP_EPI_STORE_T = 1,    /* C^T as the next GEMM's operand: out_hi/out_lo (or out_f32) at [n*ldc+m], times alpha */
+  DP_EPI_SPECTRAL = 2,   /* a=alpha*C -> three row-major operands: a*wu/(wu^2+wv^2)/2, a*wv/(...)/2, a/(...) */
+  DP_EPI_ENERGY = 3      /* energy_f64 += sum alpha*C[m,n]*rho[m*ldc+n]; optional out_f32 store */
+};
+
+typedef struct dp_gemm_problem {
+  const void* a_hi; const void* a_lo; const void* b_hi; const void* b_lo;
+  int lda, ldb;         /* leading dimensions in elements */
+  int epilogue;         /* DP_EPI_* */
+  float alpha;
+  int ldc;
+  float* out_f32;       /* STORE / STORE_T(fp32 operand) / ENERGY(optional) */
+  void* out_hi; void* out_lo;  /* STORE_T bf16 operand halves */
+  void* spec_out_hi[3]; void* spec_out_lo[3]; float* spec_out_f32[3]; /* SPECTRAL */
+  float wv_scale;       /* SPECTRAL: bin_size_x / bin_size_y */
+  const float* rho;     /* ENERGY */
+  double* energy_f64;   /* ENERGY accumulator (caller zeroes it) */
+} dp_gemm_problem;
+
+int dp_transform_gemm(int precision, int M, int N, int K,
+                      const dp_gemm_problem* problems_host, int count, dp_stream_t stream);
+
+/* Reads and clears the tensor-core kernels' device status word (0 = every
+ * bounded wait completed; non-zero = a wait expired and the launch returned
+ * early).  Synchronises the device. */
+int dp_tc_status(int* status_out);
+
+/* Operand preparation: out = scale * x, written in the operand format of
+ * `precision` (fp32, bf16 hi, or bf16 hi+lo). */
+int dp_prepare_operand(int precision, const float* x, size_t n, float scale,
+                       float* out_f32, void* out_hi, void* out_lo, dp_stream_t stream);
+
+/* ---- WA wirelength, merged algorithm
+ *      (weighted_average_wirelength/src/weighted_average_wirelength_cuda_merged.cpp:63-160,
+ *       CPU weighted_average_wirelength/src/weighted_average_wirelength_merged.cpp:31-231) ----
+ * forward: per masked net, x and y: max/min, exp sums, partial WL and the per-pin
+ * gradient grad_intermediate [2*num_pins] (unmasked nets' pins are left 0 --
+ * the caller zero-fills).  wl_out[0] = sum_e w_e * partial_e (fp64 accumulate).
+ * partial_wl: caller scratch [num_nets] or NULL. */
+int dp_wa_merged_forward(const float* pin_pos, int num_pins,
+                         const int* flat_netpin, const int* netpin_start, int num_nets,
+                         const float* net_weights, const unsigned char* net_mask,
+                         const float* inv_gamma, float* partial_wl, double* wl_out_f64,
+                         float* wl_out, float* grad_intermediate, dp_stream_t stream);
+/* backward: grad_intermediate *= grad_pos[0] * w_{net(p)} (net masked in), then
+ * pins with pin_mask != 0 are zeroed (weighted_average_wirelength.py:197-213). */
+int dp_wa_merged_backward(const float* grad_pos, const int* pin2net_map,
+                          const float* net_weights, const unsigned char* net_mask,
+                          const unsigned char* pin_mask, int num_pins,
+                          float* grad_intermediate, dp_stream_t stream);
+
+/* ---- adjacent ops on every iteration ---------------------------------------- */
+/* pin_pos/src/pin_pos_cuda_kernel.cu:11-27: pin[p] = pos[node(p)] + offset[p] */
+int dp_pin_pos_forward(const float* pos, int num_nodes, const float* pin_offset_x,
+                       const float* pin_offset_y, const int* pin2node_map, int num_pins,
+                       float* pin_pos, dp_stream_t stream);
+/* pin_pos/src/pin_pos_cuda_kernel.cu:50-74: node grad = sum of its pins' grads */
+int dp_pin_pos_backward(const float* grad_pin_pos, int num_pins,
+                        const int* flat_node2pin_map, const int* flat_node2pin_start_map,
+                        int num_physical_nodes, int num_nodes, float* grad_pos,
+                        dp_stream_t stream);
+/* hpwl/src/hpwl_cuda_kernel.cu:10-39 (net-by-net), fp64 total; out_f32 optional */
+int dp_hpwl(const float* pin_pos, int num_pins, const int* flat_netpin,
+            const int* netpin_start, int num_nets, const float* net_weights,
+            const unsigned char* net_mask, double* out_f64, float* out_f32,
+            dp_stream_t stream);
+/* move_boundary/src/move_boundary_cuda_kernel.cu:10-35, in place */
+int dp_move_boundary(float* pos, int num_nodes, const float* node_size_x,
+                     const float* node_size_y, float xl, float yl, float xh, float yh,
+                     int num_movable_nodes, int num_filler_nodes, dp_stream_t stream);
+/* pin_weight_sum/src/pws_cuda_kernel.cu: node weight = sum of its pins' net weights */
+int dp_pin_weight_sum(const float* net_weights, const int* flat_nodepin,
+                      const int* nodepin_start, const int* pin2net_map,
+                      int num_physical_nodes, int num_nodes, float* node_weights,
+                      dp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,285 @@
+"""GPU parity of every hot-path kernel against the CPU oracle and the reference's
+own CPU ops (golden fixtures).  Bars: bit-exact for fixed-point maps, the
+deterministic force and all pin/net indexing; <= 1e-5 relative for fp32
+gradients; the stated tolerance per Poisson-solve precision."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from dreamplace_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+# Poisson-solve error bars against the fp64 oracle, relative to the max |value|
+FIELD_TOL = {"fp32": 2e-5, "tf32": 5e-3, "bf16": 3e-2, "split_bf16": 2e-4}
+
+
+@pytest.fixture(scope="module")
+def C():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dreamplace_b200._native import C
+    return C
+
+
+def dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return t if dtype is None else t.to(dtype)
+
+
+def small_design():
+    return synthetic.scaled(3000, num_bins=64, seed=7, name="golden_small")
+
+
+def stretched_t(d):
+    sx, sy = dev(d.node_size_x), dev(d.node_size_y)
+    sxc = sx.clamp(min=d.bin_size_x * math.sqrt(2))
+    syc = sy.clamp(min=d.bin_size_y * math.sqrt(2))
+    return sx, sy, sxc, syc, (sx - sxc).mul(0.5), (sy - syc).mul(0.5), sx * sy / (sxc * syc)
+
+
+def sorted_map(d):
+    return dev(np.argsort(d.node_size_x[:d.num_movable_nodes], kind="stable").astype(np.int32))
+
+
+def test_fixed_density_map(C, golden):
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"])
+    sx, sy = dev(d.node_size_x), dev(d.node_size_y)
+    bcx = dev(d.bin_centers(d.xl, d.xh, d.bin_size_x))
+    bcy = dev(d.bin_centers(d.yl, d.yh, d.bin_size_y))
+    for det in (0, 1):
+        out = C.fixed_density_map(pos, sx, sy, bcx, bcy, d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y,
+                                  d.num_movable_nodes, d.num_terminals, d.num_bins_x, d.num_bins_y, 0, 0, det)
+        ref = g["fixed_map_det%d" % det].reshape(-1)
+        got = out.cpu().numpy().reshape(-1)
+        if det:
+            assert np.array_equal(got, ref)
+        else:
+            np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.parametrize("sorted_nodes", [False, True])
+def test_density_map_deterministic_bit_exact(C, golden, sorted_nodes):
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"])
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    init = dev(g["fixed_map_det1"]).mul(d.target_density).view(-1)
+    snm = sorted_map(d) if sorted_nodes else None
+    out = C.density_map(pos, sxc, syc, ox, oy, ratio, init, init, init, d.target_density, d.xl, d.yl, d.xh, d.yh,
+                        d.bin_size_x, d.bin_size_y, d.num_movable_nodes, d.num_filler_nodes, 0, d.num_bins_x,
+                        d.num_bins_y, 0, 0, 0, 0, 1, snm)
+    assert np.array_equal(out.cpu().numpy().reshape(-1), g["density_map_det1"].reshape(-1))
+    # the integer map itself against the C oracle's
+    fx = C.density_map_fixed_point(pos, sxc, syc, ox, oy, ratio, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                                   d.bin_size_y, d.num_movable_nodes, d.num_filler_nodes, d.num_bins_x,
+                                   d.num_bins_y, snm)
+    s = oracle.stretched(d.node_size_x, d.node_size_y, d.bin_size_x, d.bin_size_y)
+    _, ofx = oracle.triangle_density_map(g["pos"], *s, d.num_nodes, d.num_movable_nodes, d.num_filler_nodes,
+                                         d.num_bins_x, d.num_bins_y, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                                         d.bin_size_y, deterministic=True)
+    assert np.array_equal(fx.cpu().numpy(), ofx)
+
+
+def test_density_map_fp32(C, golden):
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"])
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    init = dev(g["fixed_map_det0"]).mul(d.target_density).view(-1)
+    out = C.density_map(pos, sxc, syc, ox, oy, ratio, init, init, init, d.target_density, d.xl, d.yl, d.xh, d.yh,
+                        d.bin_size_x, d.bin_size_y, d.num_movable_nodes, d.num_filler_nodes, 0, d.num_bins_x,
+                        d.num_bins_y, 0, 0, 0, 0, 0, sorted_map(d))
+    ref = g["density_map_det0"].reshape(-1)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-5 * float(np.max(np.abs(ref))))
+
+
+def test_density_map_clustered_start(C):
+    """All movable cells at the die centre (GP iteration 0): the warp-combined
+    atomics must still produce the oracle's integer map exactly."""
+    d = synthetic.config1()
+    pos = d.initial_positions()
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    fx = C.density_map_fixed_point(dev(pos), sxc, syc, ox, oy, ratio, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                                   d.bin_size_y, d.num_movable_nodes, d.num_filler_nodes, d.num_bins_x,
+                                   d.num_bins_y, sorted_map(d))
+    s = oracle.stretched(d.node_size_x, d.node_size_y, d.bin_size_x, d.bin_size_y)
+    _, ofx = oracle.triangle_density_map(pos, *s, d.num_nodes, d.num_movable_nodes, d.num_filler_nodes,
+                                         d.num_bins_x, d.num_bins_y, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                                         d.bin_size_y, deterministic=True)
+    assert np.array_equal(fx.cpu().numpy(), ofx)
+
+
+def test_electric_force_bit_exact(C, golden):
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"])
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    grad = torch.ones(1, device="cuda")
+    for snm in (None, sorted_map(d)):
+        out = C.electric_force(grad, d.num_bins_x, d.num_bins_y, 0, 0, 0, 0, dev(g["field_x"]).view(-1),
+                               dev(g["field_y"]).view(-1), pos, sxc, syc, ox, oy, ratio, pos, pos, d.xl, d.yl, d.xh,
+                               d.yh, d.bin_size_x, d.bin_size_y, d.num_movable_nodes, d.num_filler_nodes, 1, snm,
+                               -1.0)
+        assert np.array_equal(out.cpu().numpy(), g["force"])
+
+
+def test_pin_pos_and_hpwl(C, golden):
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"])
+    pin = C.pin_pos_forward(pos, dev(d.pin_offset_x), dev(d.pin_offset_y), dev(d.pin2node_map))
+    assert np.array_equal(pin.cpu().numpy(), g["pin_pos"])
+    back = C.pin_pos_backward(dev(g["pin_grad_in"]), pos, dev(d.flat_node2pin_map), dev(d.flat_node2pin_start_map),
+                              d.num_physical_nodes)
+    assert np.array_equal(back.cpu().numpy(), g["pin_pos_backward"])
+    deg = np.diff(d.flat_net2pin_start_map)
+    h = C.hpwl_forward(pin, dev(d.flat_net2pin_map), dev(d.flat_net2pin_start_map), dev(d.net_weights),
+                       dev((deg >= 2).astype(np.uint8)))
+    ho = oracle.hpwl(g["pin_pos"], d.flat_net2pin_map, d.flat_net2pin_start_map, (deg >= 2).astype(np.uint8),
+                     d.net_weights)
+    assert math.isclose(float(h.item()), ho, rel_tol=1e-12)
+    assert math.isclose(float(h.item()), float(g["hpwl"]), rel_tol=1e-5)
+
+
+def test_wa_merged_forward_backward(C, golden):
+    g = golden("design_small.npz")
+    d = small_design()
+    pin = dev(g["pin_pos"])
+    mask = dev(g["net_mask"])
+    inv_gamma = torch.tensor([float(g["inv_gamma"])], device="cuda")
+    wl, gi = C.wa_merged_forward(pin, dev(d.flat_net2pin_map), dev(d.flat_net2pin_start_map), dev(d.pin2net_map),
+                                 dev(d.net_weights), mask, inv_gamma)
+    assert math.isclose(float(wl.item()), float(g["wa_wl"]), rel_tol=1e-5)
+    np.testing.assert_allclose(gi.cpu().numpy(), g["wa_grad_intermediate"], rtol=1e-5, atol=1e-6)
+    pin_mask = dev((d.pin2node_map >= d.num_movable_nodes).astype(np.uint8))
+    grad = torch.full((1,), 0.5, device="cuda")
+    out = C.wa_merged_backward(grad, pin, gi.clone(), dev(d.flat_net2pin_map), dev(d.flat_net2pin_start_map),
+                               dev(d.pin2net_map), dev(d.net_weights), mask, inv_gamma, pin_mask)
+    exp = g["wa_grad_intermediate"] * np.float32(0.5)
+    pm = np.concatenate([d.pin2node_map >= d.num_movable_nodes] * 2)
+    exp[pm] = 0
+    np.testing.assert_allclose(out.cpu().numpy(), exp, rtol=1e-5, atol=1e-6)
+
+
+def test_wa_unit_golden(C, golden):
+    g = golden("wa_unit.npz")
+    inv_gamma = torch.tensor([1.0 / float(g["gamma"])], device="cuda")
+    wl, gi = C.wa_merged_forward(dev(g["pos"]), dev(g["flat_netpin"]), dev(g["netpin_start"]), dev(g["pin2net"]),
+                                 dev(g["net_weights"]), dev(g["net_mask"]), inv_gamma)
+    assert math.isclose(float(wl.item()), float(g["wl"]), rel_tol=1e-6)
+    out = C.wa_merged_backward(torch.ones(1, device="cuda"), dev(g["pos"]), gi, dev(g["flat_netpin"]),
+                               dev(g["netpin_start"]), dev(g["pin2net"]), dev(g["net_weights"]), dev(g["net_mask"]),
+                               inv_gamma, None)
+    np.testing.assert_allclose(out.cpu().numpy(), g["grad"], rtol=1e-6, atol=1e-7)
+
+
+def test_move_boundary_and_pws(C):
+    d = synthetic.config1()
+    pos = d.initial_positions()
+    pos[:100] = -50.0
+    pos[d.num_nodes:d.num_nodes + 100] = 1e5
+    t = dev(pos)
+    C.move_boundary_forward(t, dev(d.node_size_x), dev(d.node_size_y), d.xl, d.yl, d.xh, d.yh, d.num_movable_nodes,
+                            d.num_filler_nodes)
+    exp = pos.copy()
+    n = d.num_nodes
+    idx = np.r_[0:d.num_movable_nodes, n - d.num_filler_nodes:n]
+    sx, sy = d.node_size_x, d.node_size_y
+    exp[idx] = np.minimum(np.maximum(pos[idx], np.float32(d.xl)), (np.float32(d.xh) - sx[idx]).astype(np.float32))
+    exp[n + idx] = np.minimum(np.maximum(pos[n + idx], np.float32(d.yl)), (np.float32(d.yh) - sy[idx]).astype(np.float32))
+    assert np.array_equal(t.cpu().numpy(), exp)
+    w = np.random.RandomState(3).uniform(0.5, 2, size=d.num_nets).astype(np.float32)
+    out = C.pws_forward(dev(w), dev(d.flat_node2pin_map), dev(d.flat_node2pin_start_map), dev(d.pin2net_map),
+                        d.num_nodes).cpu().numpy()
+    exp = np.zeros(d.num_nodes, np.float32)
+    for i in range(d.num_physical_nodes):
+        s = np.float32(0)
+        for j in range(d.flat_node2pin_start_map[i], d.flat_node2pin_start_map[i + 1]):
+            s = np.float32(s + w[d.pin2net_map[d.flat_node2pin_map[j]]])
+        exp[i] = s
+    assert np.array_equal(out, exp)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32", "bf16", "split_bf16"])
+@pytest.mark.parametrize("shape", [(64, 64), (128, 256), (1024, 1024)])
+def test_transforms_against_fp64(C, precision, shape):
+    from dreamplace_b200 import dct2_fft2 as dct
+    M, N = shape
+    x = np.random.RandomState(M + N).uniform(-1, 1, size=(M, N)).astype(np.float32)
+    xt = dev(x)
+    for cls, f in ((dct.DCT2, oracle.dct2), (dct.IDCT2, oracle.idct2), (dct.IDCT_IDXST, oracle.idct_idxst),
+                   (dct.IDXST_IDCT, oracle.idxst_idct)):
+        got = cls(precision=precision)(xt).cpu().numpy().astype(np.float64)
+        ref = f(x)
+        err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+        assert err <= FIELD_TOL[precision], (cls.__name__, precision, shape, err)
+    assert C.tc_status() == 0
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32", "bf16", "split_bf16"])
+def test_poisson_solve_against_fp64(C, golden, precision):
+    from dreamplace_b200.electric_potential import poisson_solve
+    g = golden("design_small.npz")
+    d = small_design()
+    dm = g["density_map_det1"].reshape(d.num_bins_x, d.num_bins_y)
+    rho = dev(dm).mul_(1.0 / (d.bin_size_x * d.bin_size_y))
+    ex, ey, energy = poisson_solve(rho, d.bin_size_x, d.bin_size_y, precision)
+    rex, rey, renergy = oracle.poisson(dm, d.bin_size_x, d.bin_size_y)
+    for got, ref in ((ex, rex), (ey, rey)):
+        err = np.max(np.abs(got.cpu().numpy() - ref)) / np.max(np.abs(ref))
+        assert err <= FIELD_TOL[precision], (precision, err)
+    assert abs(float(energy.item()) - renergy) <= FIELD_TOL[precision] * abs(renergy) * 10
+    assert C.tc_status() == 0
+
+
+def test_electric_potential_module_fwd_bwd(C, golden):
+    """Module-level drop-in: energy and gradient against the reference's FFT
+    pipeline outputs (golden) in deterministic mode."""
+    from dreamplace_b200.electric_potential import ElectricPotential
+    g = golden("design_small.npz")
+    d = small_design()
+    pos = dev(g["pos"]).requires_grad_(True)
+    op = ElectricPotential(dev(d.node_size_x), dev(d.node_size_y), dev(d.bin_centers(d.xl, d.xh, d.bin_size_x)),
+                           dev(d.bin_centers(d.yl, d.yh, d.bin_size_y)), d.target_density, d.xl, d.yl, d.xh, d.yh,
+                           d.bin_size_x, d.bin_size_y, d.num_movable_nodes, d.num_terminals, d.num_filler_nodes, 0,
+                           True, sorted_map(d), precision="fp32")
+    energy = op(pos)
+    assert math.isclose(float(energy.item()), float(g["energy"]), rel_tol=1e-4)
+    energy.backward()
+    ref = g["force"]
+    err = np.max(np.abs(pos.grad.cpu().numpy() - ref)) / np.max(np.abs(ref))
+    assert err <= 1e-4
+    ovf, mx = op(pos.detach(), mode="overflow")
+    assert float(ovf) >= 0 and float(mx) > 0
+
+
+def test_density_map_exact_against_reference(C):
+    ref = oracle.load_ref("density_map_cpp")
+    if ref is None:
+        pytest.skip("reference density_map_cpp not built")
+    from dreamplace_b200.placement_ops import DensityMap
+    d = synthetic.config1()
+    pos = d.initial_positions()
+    rng = np.random.RandomState(5)
+    m = d.num_movable_nodes
+    pos[:m] = rng.uniform(d.xl, d.xh, size=m)
+    pos[d.num_nodes:d.num_nodes + m] = rng.uniform(d.yl, d.yh, size=m)
+    ranges = [(0, m), (d.num_nodes - d.num_filler_nodes, d.num_nodes)]
+    for det in (0, 1):
+        exp = torch.zeros(d.num_bins_x, d.num_bins_y)
+        for b, e in ranges:
+            exp = ref.forward(torch.from_numpy(pos), torch.from_numpy(d.node_size_x), torch.from_numpy(d.node_size_y),
+                              exp, d.xl, d.yl, d.xh, d.yh, d.num_bins_x, d.num_bins_y, b, e, det)
+        op = DensityMap(dev(d.node_size_x), dev(d.node_size_y), d.xl, d.yl, d.xh, d.yh, d.num_bins_x, d.num_bins_y,
+                        ranges, det)
+        got = op.forward(dev(pos)).cpu().numpy()
+        if det:
+            assert np.array_equal(got, exp.numpy())
+        else:
+            np.testing.assert_allclose(got, exp.numpy(), rtol=1e-5, atol=1e-3)
