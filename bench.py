@@ -1,0 +1,521 @@
+#!/usr/bin/env python
+"""Benchmark: global-placement iterations per second on the 2.1M-cell design.
+
+Workload: the 2.1M-movable-cell synthetic design (1,000 macros, 2.2M nets,
+~7.1M pins, ~0.99M fillers, 1024x1024 bins, 70% utilisation), seeded.  A
+"step" is one GP iteration of the Nesterov loop (HPWL + overflow evaluation
+and one optimizer step with >= 1 objective/gradient evaluation).  W untimed
+warm-up iterations run first; then K iterations are timed with CUDA events
+(barrier + synchronize on both sides, max over ranks).  The per-iteration
+working set (pin arrays ~200 MB) exceeds the 126 MB L2, so no explicit flush
+is done.
+
+Arms:
+  default            this implementation (split-BF16 Poisson solve unless
+                     --precision), plus the plain fp32 form timed on the same
+                     GPU for the headline comparison
+  --impl reference   the reference's own CPU ops (built from the reference
+                     sources into oracle/_ref) composed into the same GP
+                     iteration, on all host cores
+
+Multi-GPU (--gpus N under torchrun): one design per rank, replicas only (the
+single-design path does not shard); value = iterations of all ranks / max time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "GP iters/s at 2.1M cells, plain FP32 vs split-BF16 DCT, at equal HPWL ±0.1%"
+UNIT = "GP iter/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="split_bf16")
+    ap.add_argument("--design", default="config2", choices=["config1", "config2"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison run")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def make_design(name):
+    from dreamplace_b200 import synthetic
+    return synthetic.config2() if name == "config2" else synthetic.config1()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler(object):
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, local, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ our arm
+class TimedRun(object):
+    """Runs the GP loop and times iterations [warmup, warmup + steps) with CUDA events."""
+
+    def __init__(self, design, precision, world, e2e=False):
+        from dreamplace_b200.nonlinear_place import NonLinearPlace
+        from dreamplace_b200.params import Params
+        self.params = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision=precision,
+                             deterministic_flag=0)
+        self.design = design
+        self.world = world
+        self.placer = NonLinearPlace(self.params, design, "cuda")
+        self.e2e = e2e
+
+    def run(self, warmup, steps, clocks=None):
+        from dreamplace_b200._native import C
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        state = {"launch0": 0, "launch1": 0}
+        pos = self.placer.pos[0]
+        host_pos = torch.empty(pos.numel(), dtype=pos.dtype, pin_memory=True)
+        self.h2d = self.d2h = 0
+
+        def cb(it, metric):
+            if it == warmup - 1:
+                torch.cuda.synchronize()
+                barrier(self.world)
+                torch.cuda.synchronize()
+                if clocks is not None:
+                    clocks.start()
+                state["launch0"] = C.launch_count()
+                start.record()
+            elif warmup <= it < warmup + steps:
+                if self.e2e:
+                    # host round trip of the step's state: positions out and back in, metrics out
+                    host_pos.copy_(pos.data, non_blocking=True)
+                    pos.data.copy_(host_pos, non_blocking=True)
+                    self.h2d = host_pos.numel() * 4
+                    self.d2h = host_pos.numel() * 4 + 3 * 8
+                if it == warmup + steps - 1:
+                    end.record()
+                    torch.cuda.synchronize()
+                    state["launch1"] = C.launch_count()
+
+        t0 = time.time()
+        self.placer(self.params, self.design, max_iterations=warmup + steps, callback=cb)
+        wall = time.time() - t0
+        ms = start.elapsed_time(end)
+        self.launches = state["launch1"] - state["launch0"]
+        self.wall = wall
+        return ms
+
+
+def kernel_roofline(placer, design, peaks, reps=10):
+    """Times the hot kernels of one evaluation on the current positions with CUDA
+    events and returns per-kernel (ms, algorithmic bytes or flops)."""
+    from dreamplace_b200._native import C
+    from dreamplace_b200.electric_potential import ElectricDensityMapFunction, poisson_solve
+    from dreamplace_b200.dct2_fft2 import gemm_flops, precision_code
+    model = placer.model
+    ops = placer.op_collections
+    dc = placer.data_collections
+    pos = dc.pos[0].data
+    ep = ops.density_op
+    n_s = design.num_movable_nodes + design.num_filler_nodes
+    M, N = ep.num_bins_x, ep.num_bins_y
+    P, E = design.num_pins, design.num_nets
+    res = {}
+
+    def timeit(fn):
+        fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    dm_args = lambda: ElectricDensityMapFunction.forward(  # noqa: E731
+        pos, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio, ep.bin_center_x,
+        ep.bin_center_y, ep.initial_density_map, ep.target_density, ep.xl, ep.yl, ep.xh, ep.yh, ep.bin_size_x,
+        ep.bin_size_y, ep.num_movable_nodes, ep.num_filler_nodes, 0, ep.padding_mask, M, N, 0, 0, 0, 0, 0,
+        ep.sorted_node_map)
+    ms = timeit(dm_args)
+    res["density_scatter"] = (ms, 28.0 * n_s + 4.0 * design.num_movable_nodes + 8.0 * M * N, "hbm")
+    dmap = dm_args()
+    rho = dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
+    prec = precision_code(ep.precision)
+    ms = timeit(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, prec, False))
+    res["poisson_gemms"] = (ms, gemm_flops(M, N, prec, 4), "tensor" if prec else "fp32")
+    ex, ey, _ = poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, prec, False)
+    g = torch.ones(1, device="cuda")
+    ms = timeit(lambda: C.electric_force(g, M, N, 0, 0, 0, 0, ex.view(-1), ey.view(-1), pos, ep.node_size_x_clamped,
+                                         ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio, pos, pos,
+                                         ep.xl, ep.yl, ep.xh, ep.yh, ep.bin_size_x, ep.bin_size_y,
+                                         ep.num_movable_nodes, ep.num_filler_nodes, 0, ep.sorted_node_map, -1.0))
+    res["field_gather"] = (ms, 36.0 * n_s + 8.0 * M * N, "hbm")
+    pin = ops.pin_pos_op(pos)
+    ms = timeit(lambda: ops.pin_pos_op(pos))
+    res["pin_pos_forward"] = (ms, 28.0 * P, "hbm")
+    inv_gamma = (1.0 / model.gamma).reshape(1)
+    ms = timeit(lambda: C.wa_merged_forward(pin, dc.flat_net2pin_map, dc.flat_net2pin_start_map, dc.pin2net_map,
+                                            dc.net_weights, dc.net_mask_ignore_large_degrees, inv_gamma))
+    res["wa_forward"] = (ms, 20.0 * P + 17.0 * E, "hbm")
+    return res
+
+
+def roofline_entry(res, peaks):
+    name, (ms, work, bound) = max(res.items(), key=lambda kv: kv[1][0])
+    if bound == "hbm":
+        achieved = work / (ms * 1e-3) / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        unit = "GB/s"
+    else:
+        achieved = work / (ms * 1e-3) / 1e12
+        peak = peaks.get("bf16_tflops", 1590.0) if bound == "tensor" else 74.0
+        unit = "TFLOP/s"
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(name)
+        except (OSError, ValueError):
+            traffic = None
+    return {"kernel": name, "bound": "hbm" if bound == "hbm" else "tensor", "achieved": round(achieved, 2),
+            "peak": peak, "unit": unit, "frac": round(achieved / peak, 4), "traffic": traffic,
+            "ms_per_launch": round(ms, 4), "peak_source": "measured" if peaks else "fallback"}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return {}
+
+
+# ------------------------------------------------------------------ reference CPU arm
+class ReferenceCPUIteration(object):
+    """One GP iteration composed from the reference's own CPU ops (oracle/_ref):
+    HPWL + overflow evaluation, pin_pos, WA merged forward/backward, density map,
+    the four dct2_fft2 transforms, electric force, preconditioning and the
+    Nesterov vector update."""
+
+    def __init__(self, design, threads):
+        import oracle
+        self.mods = {n: oracle.load_ref(n) for n in ("electric_potential_cpp", "dct2_fft2_cpp",
+                                                     "weighted_average_wirelength_cpp_merged", "pin_pos_cpp",
+                                                     "hpwl_cpp", "move_boundary_cpp", "pws_cpp")}
+        missing = [k for k, v in self.mods.items() if v is None]
+        if missing:
+            raise RuntimeError("reference CPU ops not built: %s" % missing)
+        torch.set_num_threads(threads)
+        d = self.d = design
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+        self.pos = t(d.initial_positions())
+        rng = np.random.RandomState(0)
+        n, m = d.num_nodes, d.num_movable_nodes
+        self.pos[:m] = torch.from_numpy(rng.uniform(d.xl, d.xh - 40, size=m).astype(np.float32))
+        self.pos[n:n + m] = torch.from_numpy(rng.uniform(d.yl, d.yh - 12, size=m).astype(np.float32))
+        self.sx, self.sy = t(d.node_size_x), t(d.node_size_y)
+        bsx, bsy = d.bin_size_x, d.bin_size_y
+        self.sxc = self.sx.clamp(min=bsx * math.sqrt(2))
+        self.syc = self.sy.clamp(min=bsy * math.sqrt(2))
+        self.ox = (self.sx - self.sxc).mul(0.5)
+        self.oy = (self.sy - self.syc).mul(0.5)
+        self.ratio = self.sx * self.sy / (self.sxc * self.syc)
+        self.bcx = t(d.bin_centers(d.xl, d.xh, bsx))
+        self.bcy = t(d.bin_centers(d.yl, d.yh, bsy))
+        self.offx, self.offy = t(d.pin_offset_x), t(d.pin_offset_y)
+        self.p2n = t(d.pin2node_map.astype(np.int64))
+        self.fn2p, self.fn2ps = t(d.flat_node2pin_map), t(d.flat_node2pin_start_map)
+        self.fnp, self.fnps = t(d.flat_net2pin_map), t(d.flat_net2pin_start_map)
+        self.p2net = t(d.pin2net_map)
+        self.w = t(d.net_weights)
+        deg = np.diff(d.flat_net2pin_start_map)
+        self.mask_all = t((deg >= 2).astype(np.uint8))
+        self.mask = t(((deg >= 2) & (deg < 100)).astype(np.uint8))
+        self.pin_mask = t(d.pin2node_map >= m)
+        ep = self.mods["electric_potential_cpp"]
+        self.init_map = ep.fixed_density_map(self.pos, self.sx, self.sy, self.bcx, self.bcy, d.xl, d.yl, d.xh, d.yh,
+                                             bsx, bsy, m, d.num_terminals, d.num_bins_x, d.num_bins_y, 0, 0, 0)
+        self.init_map.mul_(d.target_density)
+        M, N = d.num_bins_x, d.num_bins_y
+        u = torch.arange(M, dtype=torch.float32).mul_(np.pi / (2 * M))
+        self.expkM = torch.stack([u.cos(), -u.sin()], -1).contiguous()
+        v = torch.arange(N, dtype=torch.float32).mul_(np.pi / (2 * N))
+        self.expkN = torch.stack([v.cos(), -v.sin()], -1).contiguous()
+        wu = torch.arange(M, dtype=torch.float32).mul(2 * np.pi / M).view(M, 1)
+        wv = torch.arange(N, dtype=torch.float32).mul(2 * np.pi / N).view(1, N).mul_(bsx / bsy)
+        w2 = wu.pow(2) + wv.pow(2)
+        w2[0, 0] = 1.0
+        self.inv = 1.0 / w2
+        self.inv[0, 0] = 0.0
+        self.wx = wu.mul(self.inv).mul_(0.5)
+        self.wy = wv.mul(self.inv).mul_(0.5)
+        self.pws = self.mods["pws_cpp"].forward(self.w, self.fn2p, self.fn2ps, self.p2net, n)
+        self.areas = self.sx * self.sy
+        self.u_k = self.pos.clone()
+        self.g_k = torch.zeros_like(self.pos)
+        self.alpha = 1.0
+        self.inv_gamma = torch.tensor([1.0 / (40 * (bsx + bsy))], dtype=torch.float32)
+
+    def step(self):
+        d, mo = self.d, self.mods
+        ep, dct, wa, pp = mo["electric_potential_cpp"], mo["dct2_fft2_cpp"], mo[
+            "weighted_average_wirelength_cpp_merged"], mo["pin_pos_cpp"]
+        n, m, M, N = d.num_nodes, d.num_movable_nodes, d.num_bins_x, d.num_bins_y
+        bsx, bsy = d.bin_size_x, d.bin_size_y
+        threads = torch.get_num_threads()
+        pos = self.pos
+        mo["move_boundary_cpp"].forward(pos, self.sx, self.sy, d.xl, d.yl, d.xh, d.yh, m, d.num_filler_nodes)
+        # evaluation
+        pin = pp.forward(pos, self.offx, self.offy, self.p2n, self.fn2p, self.fn2ps)
+        hp = mo["hpwl_cpp"].forward(pin, self.fnp, self.fnps, self.w, self.mask_all)
+        dmo = ep.density_map(pos, self.sxc, self.syc, self.ox, self.oy, self.ratio, self.bcx, self.bcy,
+                             self.init_map, d.target_density, d.xl, d.yl, d.xh, d.yh, bsx, bsy, m, 0, 0, M, N,
+                             0, 0, 0, 0, 0)
+        ovf = (dmo - d.target_density * bsx * bsy).clamp_(min=0).sum()
+        # objective and gradient
+        pin = pp.forward(pos, self.offx, self.offy, self.p2n, self.fn2p, self.fn2ps)
+        wl, gi = wa.forward(pin, self.fnp, self.fnps, self.p2net, self.w, self.mask, self.inv_gamma)
+        dm = ep.density_map(pos, self.sxc, self.syc, self.ox, self.oy, self.ratio, self.bcx, self.bcy,
+                            self.init_map, d.target_density, d.xl, d.yl, d.xh, d.yh, bsx, bsy, m,
+                            d.num_filler_nodes, 0, M, N, 0, 0, 0, 0, 0)
+        rho = dm.view(M, N).mul_(1.0 / (bsx * bsy))
+        buf = torch.empty(M, N // 2 + 1, 2)
+        auv, ex, ey, phi = (torch.empty(M, N) for _ in range(4))
+        dct.dct2_fft2(rho, self.expkM, self.expkN, auv, buf, threads)
+        dct.idxst_idct(auv.mul(self.wx), self.expkM, self.expkN, ex, buf, threads)
+        dct.idct_idxst(auv.mul(self.wy), self.expkM, self.expkN, ey, buf, threads)
+        dct.idct2_fft2(auv.mul(self.inv), self.expkM, self.expkN, phi, buf, threads)
+        energy = phi.mul(rho).sum()
+        one = torch.ones(1)
+        gd = -ep.electric_force(one, M, N, 0, 0, 0, 0, ex.view(-1), ey.view(-1), pos, self.sxc, self.syc, self.ox,
+                                self.oy, self.ratio, self.bcx, self.bcy, d.xl, d.yl, d.xh, d.yh, bsx, bsy, m,
+                                d.num_filler_nodes)
+        gw = wa.backward(one, pin, gi, self.fnp, self.fnps, self.p2net, self.w, self.mask, self.inv_gamma)
+        gw[:d.num_pins].masked_fill_(self.pin_mask, 0.0)
+        gw[d.num_pins:].masked_fill_(self.pin_mask, 0.0)
+        gpos = pp.backward(gw, pos, self.offx, self.offy, self.p2n, self.fn2p, self.fn2ps, d.num_physical_nodes)
+        grad = gpos + 1e-3 * gd
+        precond = (self.pws + 1e-3 * self.areas).clamp_(min=1.0)
+        grad.view(2, n).div_(precond)
+        # Nesterov vector update and step-size estimate
+        u = pos - self.alpha * grad
+        v = u + 0.5 * (u - self.u_k)
+        a = torch.sqrt(torch.sum((v - pos) ** 2) / torch.sum((grad - self.g_k) ** 2).clamp_(min=1e-30))
+        self.u_k.copy_(u)
+        self.g_k.copy_(grad)
+        pos.copy_(pos + 1e-6 * (v - pos))
+        return float(hp) + float(ovf) + float(wl) + float(energy) + float(a)
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def time_reference_cpu(design, steps, threads):
+    it = ReferenceCPUIteration(design, threads)
+    it.step()  # warm-up
+    t0 = time.time()
+    for _ in range(steps):
+        it.step()
+    return steps / (time.time() - t0)
+
+
+def run_reference(args):
+    rank, local, world = int(os.environ.get("RANK", "0")), 0, int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    design = make_design(args.design)
+    threads = cpu_threads()
+    it = ReferenceCPUIteration(design, threads)
+    for _ in range(max(args.warmup, 1)):
+        it.step()
+    steps = args.steps
+    t0 = time.time()
+    for _ in range(steps):
+        it.step()
+    dt = time.time() - t0
+    value = steps / dt
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": round(1000 * dt / steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": design.name + ": %d movable cells, %d nets, %d pins, %dx%d bins"
+                       % (design.num_movable_nodes, design.num_nets, design.num_pins, design.num_bins_x,
+                          design.num_bins_y), "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": "%d GP iterations composed from the reference CPU ops (%s)"
+                                       % (steps, cpu_model())},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ main
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, local, world = dist_setup(args.gpus)
+    design = make_design(args.design)
+    peaks = load_peaks()
+    W, K = max(args.warmup, 3), args.steps
+    clocks = ClockSampler(local) if rank == 0 else None
+    run = TimedRun(design, args.precision, world)
+    ms = run.run(W, K, clocks=clocks)
+    clk = clocks.stop() if clocks else None
+    ms = max_over_ranks(ms, world)
+    value = world * K / (ms / 1000.0)
+    launches = run.launches
+    # end-to-end through the public API with a host round trip per step
+    run_e2e = TimedRun(design, args.precision, world, e2e=True)
+    ms_e2e = max_over_ranks(run_e2e.run(W, K), world)
+    e2e_value = world * K / (ms_e2e / 1000.0)
+    roof = roofline_entry(kernel_roofline(run.placer, design, peaks), peaks)
+    plain = None
+    if not args.no_plain and args.precision != "fp32":
+        prun = TimedRun(design, "fp32", world)
+        pms = max_over_ranks(prun.run(W, K), world)
+        pval = world * K / (pms / 1000.0)
+        h_ours = run.placer.metrics[-1][-1][-1]._host[0]
+        h_plain = prun.placer.metrics[-1][-1][-1]._host[0]
+        plain = {"value": round(pval, 3), "ms_per_step": round(pms / K, 3), "speedup": round(value / pval, 3),
+                 "hpwl_rel_diff_at_step": round(abs(h_ours - h_plain) / h_plain, 6), "compared_at_iteration": W + K}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        try:
+            v = time_reference_cpu(design, args.cpu_sample_steps, threads)
+            cpu = {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": "%d GP iterations composed from the reference CPU ops at the same design (%s)"
+                             % (args.cpu_sample_steps, cpu_model())}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": "failed: %s" % e}
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+" + args.precision, "data": "synthetic",
+                "config": {"workload": "%s: %d movable cells, %d macros, %d fillers, %d nets, %d pins, %dx%d bins"
+                           % (design.name, design.num_movable_nodes, design.num_terminals, design.num_filler_nodes,
+                              design.num_nets, design.num_pins, design.num_bins_x, design.num_bins_y),
+                           "dct_precision": args.precision, "parallelism": "replicas%d" % world,
+                           "l2": "per-iteration working set > 126 MB L2, no flush"},
+                "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": run_e2e.h2d,
+                        "d2h_bytes_per_step": run_e2e.d2h},
+                "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "plain_fp32": plain}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

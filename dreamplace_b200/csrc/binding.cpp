@@ -321,6 +321,101 @@ at::Tensor pws_forward(at::Tensor net_weights, at::Tensor flat_nodepin, at::Tens
   return out;
 }
 
+// ---------------------------------------------------------------- engine kernels
+static void* vp(const at::Tensor& t) { return t.data_ptr(); }
+static void* ovp(const c10::optional<at::Tensor>& t) {
+  return (t.has_value() && t->defined() && t->numel() > 0) ? t->data_ptr() : nullptr;
+}
+
+void wa_slot_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
+                     at::Tensor netpin_start, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
+                     at::Tensor inv_gamma, at::Tensor wl_f64, at::Tensor grad_slot) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(slot_node); CHECK_F32(grad_slot);
+  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble, "wl_f64 must be float64");
+  DP_CALL(dp_wa_slot_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
+                             ptr<float>(slot_offy), ptr<int>(netpin_start), netpin_start.numel() - 1,
+                             (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<float>(inv_gamma),
+                             ptr<double>(wl_f64), ptr<float>(grad_slot), slot_node.numel(), cur_stream()));
+}
+
+void wa_node_backward(at::Tensor grad_slot, at::Tensor node_slots, at::Tensor node_start, at::Tensor slot_net,
+                      c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor grad_pos,
+                      int num_movable, int accumulate, at::Tensor grad_out) {
+  CHECK_F32(grad_slot); CHECK_F32(grad_out); CHECK_F32(grad_pos);
+  DP_CALL(dp_wa_node_backward(ptr<float>(grad_slot), grad_slot.numel() / 2, ptr<int>(node_slots),
+                              ptr<int>(node_start), ptr<int>(slot_net), (const float*)ovp(net_weights),
+                              net_mask.data_ptr<uint8_t>(), ptr<float>(grad_pos), num_movable, grad_out.numel() / 2,
+                              accumulate, ptr<float>(grad_out), cur_stream()));
+}
+
+void hpwl_slot(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
+               at::Tensor netpin_start, c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor out) {
+  TORCH_CHECK(out.scalar_type() == at::kDouble, "out must be float64");
+  DP_CALL(dp_hpwl_slot(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
+                       ptr<float>(slot_offy), ptr<int>(netpin_start), netpin_start.numel() - 1,
+                       (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<double>(out), cur_stream()));
+}
+
+void nesterov_init(at::Tensor state, double alpha) { DP_CALL(dp_nesterov_init(ptr<double>(state), alpha, cur_stream())); }
+
+void nesterov_trial(at::Tensor v, at::Tensor g, at::Tensor u, at::Tensor u_new, at::Tensor v_new, at::Tensor state,
+                    at::Tensor sx, at::Tensor sy, double xl, double yl, double xh, double yh, int num_movable,
+                    int num_filler) {
+  DP_CALL(dp_nesterov_trial(ptr<float>(v), ptr<float>(g), ptr<float>(u), ptr<float>(u_new), ptr<float>(v_new),
+                            ptr<double>(state), ptr<float>(sx), ptr<float>(sy), xl, yl, xh, yh, v.numel() / 2,
+                            num_movable, num_filler, cur_stream()));
+}
+
+void precondition_step_size(at::Tensor g_new, at::Tensor g, at::Tensor v_new, at::Tensor v, at::Tensor pws,
+                            at::Tensor area, at::Tensor lam, at::Tensor state) {
+  DP_CALL(dp_precondition_step_size(ptr<float>(g_new), ptr<float>(g), ptr<float>(v_new), ptr<float>(v),
+                                    ptr<float>(pws), ptr<float>(area), ptr<float>(lam), g_new.numel() / 2,
+                                    ptr<double>(state), cur_stream()));
+}
+
+void nesterov_advance(at::Tensor state) { DP_CALL(dp_nesterov_advance(ptr<double>(state), cur_stream())); }
+
+void objective_finish(at::Tensor wl, at::Tensor energy, at::Tensor density_weight, double density_factor,
+                      double quad_c, at::Tensor obj, at::Tensor grad_scale) {
+  DP_CALL(dp_objective_finish(ptr<double>(wl), ptr<double>(energy), ptr<float>(density_weight), (float)density_factor,
+                              (float)quad_c, ptr<double>(obj), ptr<float>(grad_scale), cur_stream()));
+}
+
+// density scatter into a caller-owned map (no allocation; graph friendly)
+void density_map_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio,
+                      at::Tensor init, double xl, double yl, double xh, double yh, double bsx, double bsy,
+                      int num_movable, int num_filler, int nbx, int nby, c10::optional<at::Tensor> sorted_node_map,
+                      int deterministic, c10::optional<at::Tensor> scratch, at::Tensor out) {
+  const int* snm = (const int*)ovp(sorted_node_map);
+  int n = pos.numel() / 2;
+  if (deterministic) {
+    TORCH_CHECK(scratch.has_value(), "deterministic mode needs the int64 scratch map");
+    DP_CALL(dp_density_map_fx64(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                                ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
+                                num_movable, num_filler, nbx, nby, snm, fraction_bits(xl, yl, xh, yh),
+                                ptr<int64_t>(*scratch), ptr<float>(out), cur_stream()));
+  } else {
+    DP_CALL(dp_density_map_f32(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                               ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
+                               num_movable, num_filler, nbx, nby, snm, ptr<float>(out), cur_stream()));
+  }
+}
+
+void density_overflow_into(at::Tensor density_map, double target_area, double bin_area, at::Tensor out2) {
+  DP_CALL(dp_density_overflow(ptr<float>(density_map), density_map.numel(), target_area, bin_area, ptr<double>(out2),
+                              nullptr, cur_stream()));
+}
+
+void electric_force_into(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor pos, at::Tensor sx,
+                         at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio, double xl, double yl,
+                         double xh, double yh, double bsx, double bsy, int nbx, int nby, int num_movable,
+                         int num_filler, c10::optional<at::Tensor> sorted_node_map, double scale, at::Tensor out) {
+  DP_CALL(dp_electric_force(ptr<float>(grad_scale), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(pos),
+                            pos.numel() / 2, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
+                            ptr<float>(ratio), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy), num_movable,
+                            num_filler, (const int*)ovp(sorted_node_map), (float)scale, ptr<float>(out), cur_stream()));
+}
+
 uint64_t launch_count() { return dp_launch_count(); }
 
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
@@ -342,5 +437,16 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("move_boundary_forward", &move_boundary_forward);
   m.def("pws_forward", &pws_forward);
   m.def("launch_count", &launch_count);
+  m.def("wa_slot_forward", &wa_slot_forward);
+  m.def("wa_node_backward", &wa_node_backward);
+  m.def("hpwl_slot", &hpwl_slot);
+  m.def("nesterov_init", &nesterov_init);
+  m.def("nesterov_trial", &nesterov_trial);
+  m.def("precondition_step_size", &precondition_step_size);
+  m.def("nesterov_advance", &nesterov_advance);
+  m.def("objective_finish", &objective_finish);
+  m.def("density_map_into", &density_map_into);
+  m.def("density_overflow_into", &density_overflow_into);
+  m.def("electric_force_into", &electric_force_into);
   m.def("version", &dp_version);
 }

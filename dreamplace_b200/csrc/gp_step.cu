@@ -1,0 +1,427 @@
+// Fused kernels of one global-placement iteration (the engine path).
+//
+// The reference composes an iteration from separate ops: pin_pos -> WA ->
+// (autograd) WA backward -> pin_pos backward, HPWL through pin_pos, and the
+// Nesterov update as a dozen tensor expressions
+// (dreamplace/NesterovAcceleratedGradientOptimizer.py:65-166,
+// dreamplace/PlaceObj.py:37-132).  Here:
+//
+//  * pins are visited in "slot" order (the flat_netpin order): per slot the
+//    owning node and the pin offsets are stored contiguously, so the WA and
+//    HPWL kernels gather node positions (resident in L2) instead of reading a
+//    materialised pin-position array;
+//  * WA backward and the pin -> node sum are one gather over a node -> slot
+//    CSR, in the reference's per-node pin order, so the node gradient equals
+//    pin_pos backward of the reference's per-pin gradient bit for bit;
+//  * the Nesterov trial point, the move-boundary clamp, the preconditioner
+//    and both step-size norms (fp64) are two streaming passes over the
+//    position / gradient vectors, and a one-thread kernel finishes the step
+//    size, the backtracking test and the momentum scalars on the device.
+#include "common.cuh"
+
+namespace dpb {
+
+// Fixed-order reductions: every block writes its partial sum(s) to
+// partials[blockIdx.x] (and partials[gridDim.x + blockIdx.x]); a one-block
+// finisher adds the partials in a fixed tree order, so totals are
+// bit-reproducible run to run (the deterministic mode's requirement).
+constexpr int kMaxReduceBlocks = 1184;  // 148 SMs x 8
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block sum of (a, b) written to partials; blockDim.x must be 256
+__device__ __forceinline__ void block_partial2(double a, double b, double* partials) {
+  __shared__ double sa[8], sb[8];
+  a = warp_sum(a);
+  b = warp_sum(b);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int i = 0; i < 8; ++i) { ta += sa[i]; tb += sb[i]; }
+    partials[blockIdx.x] = ta;
+    partials[gridDim.x + blockIdx.x] = tb;
+  }
+}
+
+__device__ __forceinline__ void block_partial1(double a, double* partials) {
+  __shared__ double sa[8];
+  a = warp_sum(a);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sa[w] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0;
+    for (int i = 0; i < 8; ++i) ta += sa[i];
+    partials[blockIdx.x] = ta;
+  }
+}
+
+// one block of 256 threads: out[k] = sum of partials[k*count .. k*count+count)
+__device__ __forceinline__ double finish_sum(const double* partials, int count) {
+  __shared__ double sh[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < count; i += 256) v += partials[i];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void finish_sum_kernel(const double* partials, int count, double* out) {
+  double r = finish_sum(partials, count);
+  if (threadIdx.x == 0) out[0] = r;
+}
+
+// ---------------------------------------------------------------- WA fused
+__global__ void __launch_bounds__(256) wa_slot_forward_kernel(
+    const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ slot_node,
+    const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ netpin_start,
+    int num_nets, const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
+    const float* __restrict__ inv_gamma_p, double* __restrict__ partials, float* __restrict__ gx,
+    float* __restrict__ gy) {
+  const float inv_gamma = *inv_gamma_p;
+  double contrib = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
+    {
+      int b = netpin_start[i], e = netpin_start[i + 1];
+      if (net_mask[i]) {
+        float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
+        for (int j = b; j < e; ++j) {
+          int n = slot_node[j];
+          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+          x_max = fmaxf(xx, x_max);
+          x_min = fminf(xx, x_min);
+          y_max = fmaxf(yy, y_max);
+          y_min = fminf(yy, y_min);
+        }
+        float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
+        for (int j = b; j < e; ++j) {
+          int n = slot_node[j];
+          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+          float ex = expf(fmul(fsub(xx, x_max), inv_gamma));
+          float enx = expf(fmul(fsub(x_min, xx), inv_gamma));
+          xe_p = fadd(xe_p, fmul(xx, ex));
+          xe_n = fadd(xe_n, fmul(xx, enx));
+          e_p = fadd(e_p, ex);
+          e_n = fadd(e_n, enx);
+          float ey = expf(fmul(fsub(yy, y_max), inv_gamma));
+          float eny = expf(fmul(fsub(y_min, yy), inv_gamma));
+          ye_p = fadd(ye_p, fmul(yy, ey));
+          ye_n = fadd(ye_n, fmul(yy, eny));
+          f_p = fadd(f_p, ey);
+          f_n = fadd(f_n, eny);
+        }
+        float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                        __fdiv_rn(ye_n, f_n));
+        contrib += (double)(net_weights ? fmul(wl, net_weights[i]) : wl);
+        float b_x = __fdiv_rn(inv_gamma, e_p);
+        float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
+        float b_nx = __fdiv_rn(-inv_gamma, e_n);
+        float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
+        float b_y = __fdiv_rn(inv_gamma, f_p);
+        float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
+        float b_ny = __fdiv_rn(-inv_gamma, f_n);
+        float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
+        for (int j = b; j < e; ++j) {
+          int n = slot_node[j];
+          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+          float ex = expf(fmul(fsub(xx, x_max), inv_gamma));
+          float enx = expf(fmul(fsub(x_min, xx), inv_gamma));
+          gx[j] = fsub(fmul(fadd(a_x, fmul(b_x, xx)), ex), fmul(fadd(a_nx, fmul(b_nx, xx)), enx));
+          float ey = expf(fmul(fsub(yy, y_max), inv_gamma));
+          float eny = expf(fmul(fsub(y_min, yy), inv_gamma));
+          gy[j] = fsub(fmul(fadd(a_y, fmul(b_y, yy)), ey), fmul(fadd(a_ny, fmul(b_ny, yy)), eny));
+        }
+      } else {
+        for (int j = b; j < e; ++j) {
+          gx[j] = 0.f;
+          gy[j] = 0.f;
+        }
+      }
+    }
+  }
+  block_partial1(contrib, partials);
+}
+
+// node grad (+)= sum over the node's pins, in flat_node2pin order, of
+// (gi * g) * w_net  -- zero for nodes >= num_movable (all their pins are masked)
+__global__ void wa_node_backward_kernel(const float* __restrict__ gx, const float* __restrict__ gy,
+                                        const int* __restrict__ node_slots, const int* __restrict__ node_start,
+                                        const int* __restrict__ slot_net, const float* __restrict__ net_weights,
+                                        const unsigned char* __restrict__ net_mask, const float* __restrict__ grad_p,
+                                        int num_movable, int num_nodes, int accumulate, float* __restrict__ out_x,
+                                        float* __restrict__ out_y) {
+  const float g = *grad_p;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
+    float sx = 0.f, sy = 0.f;
+    if (i < num_movable) {
+      for (int k = node_start[i]; k < node_start[i + 1]; ++k) {
+        int s = node_slots[k];
+        float vx = fmul(gx[s], g), vy = fmul(gy[s], g);
+        if (net_weights) {
+          int net = slot_net[s];
+          if (net_mask[net]) {
+            float w = net_weights[net];
+            vx = fmul(vx, w);
+            vy = fmul(vy, w);
+          }
+        }
+        sx = fadd(sx, vx);
+        sy = fadd(sy, vy);
+      }
+    }
+    if (accumulate) {
+      out_x[i] = fadd(sx, out_x[i]);
+      out_y[i] = fadd(sy, out_y[i]);
+    } else {
+      out_x[i] = sx;
+      out_y[i] = sy;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) hpwl_slot_kernel(const float* __restrict__ x, const float* __restrict__ y,
+                                                        const int* __restrict__ slot_node,
+                                                        const float* __restrict__ slot_offx,
+                                                        const float* __restrict__ slot_offy,
+                                                        const int* __restrict__ netpin_start, int num_nets,
+                                                        const float* __restrict__ net_weights,
+                                                        const unsigned char* __restrict__ net_mask,
+                                                        double* __restrict__ partials) {
+  double c = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
+    if (net_mask[i]) {
+      float max_x = -FLT_MAX, min_x = FLT_MAX, max_y = -FLT_MAX, min_y = FLT_MAX;
+      for (int j = netpin_start[i]; j < netpin_start[i + 1]; ++j) {
+        int n = slot_node[j];
+        float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+        min_x = fminf(min_x, xx);
+        max_x = fmaxf(max_x, xx);
+        min_y = fminf(min_y, yy);
+        max_y = fmaxf(max_y, yy);
+      }
+      float h = fsub(fadd(fsub(max_x, min_x), max_y), min_y);
+      if (net_weights) h = fmul(h, net_weights[i]);
+      c += (double)h;
+    }
+  }
+  block_partial1(c, partials);
+}
+
+// ---------------------------------------------------------------- Nesterov
+// Device scalars of the optimizer (one array of doubles):
+enum {
+  NS_ALPHA = 0,      // alpha_k (step size, updated by every trial)
+  NS_A = 1,          // a_k
+  NS_A_NEXT = 2,     // a_{k+1}
+  NS_COEF = 3,       // (a_k - 1) / a_{k+1}
+  NS_ACC_DV = 4,     // sum (v_{k+1} - v_k)^2 accumulator
+  NS_ACC_DG = 5,     // sum (g_{k+1} - g_k)^2 accumulator
+  NS_ALPHA_NEW = 6,  // alpha_{k+1}
+  NS_ACCEPT = 7,     // 1.0 when alpha_{k+1} > 0.95 alpha_k
+  NS_COUNT = 8
+};
+
+// u' = v - alpha g; v' = u' + coef (u' - u); v' clamped into the die for
+// movable and filler nodes (move_boundary semantics).
+__global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* __restrict__ g,
+                                      const float* __restrict__ u, float* __restrict__ u_new,
+                                      float* __restrict__ v_new, const double* __restrict__ st,
+                                      const float* __restrict__ sx, const float* __restrict__ sy, float xl, float yl,
+                                      float xh, float yh, int num_nodes, int num_movable, int num_filler) {
+  const float alpha = (float)st[NS_ALPHA];
+  const float coef = (float)st[NS_COEF];
+  const int n2 = 2 * num_nodes;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    float un = fsub(v[i], fmul(alpha, g[i]));
+    float vn = fadd(un, fmul(coef, fsub(un, u[i])));
+    int node = i < num_nodes ? i : i - num_nodes;
+    if (node < num_movable || node >= num_nodes - num_filler) {
+      if (i < num_nodes) {
+        vn = fmaxf(vn, xl);
+        vn = fminf(vn, fsub(xh, sx[node]));
+      } else {
+        vn = fmaxf(vn, yl);
+        vn = fminf(vn, fsub(yh, sy[node]));
+      }
+    }
+    u_new[i] = un;
+    v_new[i] = vn;
+  }
+}
+
+// g' /= max(1, pws + lambda*area) in place, and per-block fp64 sums of
+// (v' - v)^2 and (g' - g)^2 (finished by nesterov_finish_kernel).
+__global__ void __launch_bounds__(256) precondition_norms_kernel(
+    float* __restrict__ g_new, const float* __restrict__ g, const float* __restrict__ v_new,
+    const float* __restrict__ v, const float* __restrict__ pws, const float* __restrict__ area,
+    const float* __restrict__ lam_p, int num_nodes, double* __restrict__ partials) {
+  const float lam = *lam_p;
+  const int n2 = 2 * num_nodes;
+  double dv = 0.0, dg = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    {
+      int node = i < num_nodes ? i : i - num_nodes;
+      float p = fmaxf(fadd(pws[node], fmul(lam, area[node])), 1.0f);
+      float gn = __fdiv_rn(g_new[i], p);
+      g_new[i] = gn;
+      double a = (double)v_new[i] - (double)v[i];
+      double b = (double)gn - (double)g[i];
+      dv += a * a;
+      dg += b * b;
+    }
+  }
+  block_partial2(dv, dg, partials);
+}
+
+__global__ void nesterov_finish_kernel(double* st, const double* partials, int count) {
+  double dv = finish_sum(partials, count);
+  double dg = finish_sum(partials + count, count);
+  if (threadIdx.x != 0) return;
+  st[NS_ACC_DV] = dv;
+  st[NS_ACC_DG] = dg;
+  double an = sqrt(dv / dg);
+  double accept = an > 0.95 * st[NS_ALPHA] ? 1.0 : 0.0;
+  st[NS_ALPHA_NEW] = an;
+  st[NS_ACCEPT] = accept;
+  st[NS_ALPHA] = an;  // the reference copies alpha_{k+1} into alpha_k after every trial
+}
+
+// called once per accepted step: a_k <- a_{k+1}; a_{k+2}, coef for the next step
+__global__ void nesterov_advance_kernel(double* st) {
+  double a = st[NS_A_NEXT];
+  st[NS_A] = a;
+  double an = (1.0 + sqrt(4.0 * a * a + 1.0)) / 2.0;
+  st[NS_A_NEXT] = an;
+  st[NS_COEF] = (a - 1.0) / an;
+}
+
+__global__ void nesterov_init_kernel(double* st, double alpha) {
+  st[NS_ALPHA] = alpha;
+  st[NS_A] = 1.0;
+  double an = (1.0 + sqrt(5.0)) / 2.0;
+  st[NS_A_NEXT] = an;
+  st[NS_COEF] = 0.0;
+  for (int i = NS_ACC_DV; i < NS_COUNT; ++i) st[i] = 0.0;
+}
+
+// objective = wl + lambda_eff * D' with D' = D (1 + c D) under the quadratic
+// penalty (c > 0) and lambda_eff = density_factor * density_weight; the density
+// gradient's scale (d objective / d D) goes to grad_scale for the force kernel
+// (dreamplace/PlaceObj.py:293-320).
+__global__ void objective_finish_kernel(const double* wl, const double* energy, const float* density_weight,
+                                        float density_factor, float quad_c, double* obj, float* grad_scale) {
+  double lam = (double)density_factor * (double)density_weight[0];
+  double d = energy[0];
+  double dp = quad_c > 0.f ? d * (1.0 + (double)quad_c * d) : d;
+  obj[0] = wl[0] + lam * dp;
+  double dd = quad_c > 0.f ? 1.0 + 2.0 * (double)quad_c * d : 1.0;
+  grad_scale[0] = (float)(lam * dd);
+}
+
+}  // namespace dpb
+
+using namespace dpb;
+
+extern "C" int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
+                                   float density_factor, float quad_c, double* obj, float* grad_scale,
+                                   dp_stream_t stream) {
+  DP_REQUIRE(wl && energy && density_weight && obj && grad_scale, "dp_objective_finish: null pointer");
+  objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, density_factor, quad_c, obj,
+                                                         grad_scale);
+  return check_launch("dp_objective_finish");
+}
+
+extern "C" int dp_wa_slot_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                                  const float* slot_offy, const int* netpin_start, int num_nets,
+                                  const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
+                                  double* wl_f64, float* grad_slot, int num_slots, dp_stream_t stream) {
+  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && netpin_start && net_mask && inv_gamma && wl_f64 &&
+                 grad_slot,
+             "dp_wa_slot_forward: null pointer argument");
+  cudaStream_t s = as_stream(stream);
+  int blocks = grid_for(num_nets, 256, 8);
+  double* partials = wl_f64 + 1;
+  wa_slot_forward_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
+                                               num_nets, net_weights, net_mask, inv_gamma, partials, grad_slot,
+                                               grad_slot + num_slots);
+  int rc = check_launch("dp_wa_slot_forward");
+  if (rc) return rc;
+  finish_sum_kernel<<<1, 256, 0, s>>>(partials, blocks, wl_f64);
+  return check_launch("dp_wa_slot_forward finish");
+}
+
+extern "C" int dp_wa_node_backward(const float* grad_slot, int num_slots, const int* node_slots,
+                                   const int* node_start, const int* slot_net, const float* net_weights,
+                                   const unsigned char* net_mask, const float* grad_pos, int num_movable,
+                                   int num_nodes, int accumulate, float* grad_out, dp_stream_t stream) {
+  DP_REQUIRE(grad_slot && node_slots && node_start && grad_pos && grad_out, "dp_wa_node_backward: null pointer");
+  DP_REQUIRE(!net_weights || (slot_net && net_mask), "dp_wa_node_backward: net weights need slot_net and net_mask");
+  if (num_nodes == 0) return DP_OK;
+  wa_node_backward_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+      grad_slot, grad_slot + num_slots, node_slots, node_start, slot_net, net_weights, net_mask, grad_pos,
+      num_movable, num_nodes, accumulate, grad_out, grad_out + num_nodes);
+  return check_launch("dp_wa_node_backward");
+}
+
+extern "C" int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                            const float* slot_offy, const int* netpin_start, int num_nets, const float* net_weights,
+                            const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
+  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && netpin_start && net_mask && out_f64,
+             "dp_hpwl_slot: null pointer argument");
+  cudaStream_t s = as_stream(stream);
+  int blocks = grid_for(num_nets, 256, 8);
+  double* partials = out_f64 + 1;
+  hpwl_slot_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
+                                         num_nets, net_weights, net_mask, partials);
+  int rc = check_launch("dp_hpwl_slot");
+  if (rc) return rc;
+  finish_sum_kernel<<<1, 256, 0, s>>>(partials, blocks, out_f64);
+  return check_launch("dp_hpwl_slot finish");
+}
+
+extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream) {
+  DP_REQUIRE(state, "dp_nesterov_init: null state");
+  nesterov_init_kernel<<<1, 1, 0, as_stream(stream)>>>(state, alpha);
+  return check_launch("dp_nesterov_init");
+}
+
+extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
+                                 const double* state, const float* sx, const float* sy, float xl, float yl, float xh,
+                                 float yh, int num_nodes, int num_movable, int num_filler, dp_stream_t stream) {
+  DP_REQUIRE(v && g && u && u_new && v_new && state && sx && sy, "dp_nesterov_trial: null pointer");
+  if (num_nodes == 0) return DP_OK;
+  nesterov_trial_kernel<<<grid_for(2ll * num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+      v, g, u, u_new, v_new, state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable, num_filler);
+  return check_launch("dp_nesterov_trial");
+}
+
+extern "C" int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, const float* v,
+                                         const float* pws, const float* area, const float* lambda_, int num_nodes,
+                                         double* state, dp_stream_t stream) {
+  DP_REQUIRE(g_new && g && v_new && v && pws && area && lambda_ && state, "dp_precondition_step_size: null pointer");
+  cudaStream_t s = as_stream(stream);
+  int blocks = grid_for(2ll * num_nodes, 256, 4);
+  double* partials = state + DP_NESTEROV_STATE_DOUBLES;
+  precondition_norms_kernel<<<blocks, 256, 0, s>>>(g_new, g, v_new, v, pws, area, lambda_, num_nodes, partials);
+  int rc = check_launch("dp_precondition_step_size");
+  if (rc) return rc;
+  nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
+  return check_launch("dp_precondition_step_size finish");
+}
+
+extern "C" int dp_nesterov_advance(double* state, dp_stream_t stream) {
+  DP_REQUIRE(state, "dp_nesterov_advance: null state");
+  nesterov_advance_kernel<<<1, 1, 0, as_stream(stream)>>>(state);
+  return check_launch("dp_nesterov_advance");
+}

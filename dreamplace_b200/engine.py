@@ -1,0 +1,275 @@
+"""Graph-captured global-placement iteration.
+
+The same iteration as ``NonLinearPlace`` + ``NesterovAcceleratedGradientOptimizer``
+(dreamplace/NonLinearPlace.py:377-526, dreamplace/NesterovAcceleratedGradientOptimizer.py:65-166),
+re-organised for the GPU:
+
+* the objective and its gradient are computed by the hand-written adjoints
+  directly (no autograd): WA forward with the pin gather fused in, the density
+  scatter, the four Poisson GEMM launches, the field gather writing the
+  density gradient (scaled by lambda on the device) and the WA backward fused
+  with the pin -> node sum accumulating the wirelength gradient on top;
+* the Nesterov trial point, move-boundary clamp, preconditioner and the fp64
+  step-size estimate run as fused kernels on ping-pong buffers (v, u, g for
+  step k and k+1), so an accepted step swaps a parity bit instead of copying;
+* one iteration (HPWL + overflow evaluation at v_k and the first Nesterov
+  trial) is one CUDA graph replay, a retried trial another; the host reads a
+  handful of fp64 scalars once per trial and makes the loop decisions.
+"""
+import math
+
+import numpy as np
+import torch
+
+from ._native import C, precision_code
+from .electric_potential import poisson_solve
+
+# device scalar slots of the optimizer state (gp_step.cu)
+NS_ALPHA, NS_A, NS_A_NEXT, NS_COEF, NS_ACC_DV, NS_ACC_DG, NS_ALPHA_NEW, NS_ACCEPT = range(8)
+NESTEROV_STATE = 8
+REDUCE_DOUBLES = 1280
+# metric slots
+M_HPWL, M_OVF, M_MAXD, M_ACCEPT, M_ALPHA, M_OBJ, M_WL, M_ENERGY = range(8)
+
+
+class GPEngine(object):
+    def __init__(self, params, design, data, ops, model, use_graphs=True):
+        self.params = params
+        self.design = d = design
+        self.data = data
+        self.ops = ops
+        self.model = model
+        self.use_graphs = use_graphs
+        dev = data.pos[0].device
+        self.dev = dev
+        n = d.num_nodes
+        P = d.num_pins
+        fnp = data.flat_net2pin_map.long()
+        self.slot_node = data.pin2node_map[fnp].to(torch.int32).contiguous()
+        self.slot_offx = data.pin_offset_x[fnp].contiguous()
+        self.slot_offy = data.pin_offset_y[fnp].contiguous()
+        self.slot_net = data.pin2net_map[fnp].to(torch.int32).contiguous()
+        slot_of_pin = torch.empty(P, dtype=torch.int64, device=dev)
+        slot_of_pin[fnp] = torch.arange(P, device=dev)
+        self.node_slots = slot_of_pin[data.flat_node2pin_map.long()].to(torch.int32).contiguous()
+        self.node_start = data.flat_node2pin_start_map
+        self.netpin_start = data.flat_net2pin_start_map
+        ep = ops.density_op
+        self.ep = ep
+        self.ovf_op = ops.density_overflow_op
+        # ping-pong state
+        pos = data.pos[0]
+        self.V = [pos.data.clone(), torch.empty_like(pos.data)]
+        self.U = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
+        self.G = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
+        self.tmp = torch.empty_like(pos.data)
+        self.gi = torch.empty(2 * P, dtype=torch.float32, device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        # optimizer scalars + fixed-order reduction scratch (include/dreamplace_b200.h)
+        self.state = torch.zeros(NESTEROV_STATE + 2 * REDUCE_DOUBLES, **f64)
+        self.wl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
+        self.wl64 = self.wl64_buf[0:1]
+        self.obj64 = torch.zeros(1, **f64)
+        self.hpwl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
+        self.hpwl64 = self.hpwl64_buf[0:1]
+        self.ovf2 = torch.zeros(2, **f64)
+        self.metrics = torch.zeros(8, **f64)
+        self.metrics_host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
+        self.grad_scale = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.one = torch.ones(1, dtype=torch.float32, device=dev)
+        self.inv_gamma = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.dmap = torch.empty(ep.num_bins_x, ep.num_bins_y, dtype=torch.float32, device=dev)
+        self.omap = torch.empty_like(self.dmap)
+        self.det = bool(params.deterministic_flag)
+        self.scratch = torch.empty(ep.num_bins_x * ep.num_bins_y, dtype=torch.int64, device=dev) if self.det else None
+        self.prec = precision_code(ep.precision)
+        self.parity = 0
+        self.graphs = {}
+        self.pool = None
+        self.graph_key = None
+        self.trials = 0
+        self.last_energy = None
+        self._quad_c = 0.0
+
+    # ---------------------------------------------------------------- pieces
+    def _density(self, v, num_filler, out):
+        ep = self.ep
+        C.density_map_into(v, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio,
+                           ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl), float(ep.xh), float(ep.yh),
+                           float(ep.bin_size_x), float(ep.bin_size_y), ep.num_movable_nodes, num_filler,
+                           ep.num_bins_x, ep.num_bins_y, ep.sorted_node_map, int(self.det), self.scratch, out)
+
+    def wirelength(self, v):
+        """WA forward at node positions v: fp64 total in self.wl64, per-slot gradient in self.gi."""
+        dc = self.data
+        self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
+        C.wa_slot_forward(v, self.slot_node, self.slot_offx, self.slot_offy, self.netpin_start, dc.net_weights,
+                          dc.net_mask_ignore_large_degrees, self.inv_gamma, self.wl64_buf, self.gi)
+
+    def wl_grad_into(self, g, accumulate):
+        dc = self.data
+        C.wa_node_backward(self.gi, self.node_slots, self.node_start, self.slot_net, dc.net_weights,
+                           dc.net_mask_ignore_large_degrees, self.one, self.design.num_movable_nodes, int(accumulate), g)
+
+    def density_energy(self, v):
+        """Density map, Poisson solve; returns (ex, ey, energy_f64[1])."""
+        ep = self.ep
+        self._density(v, ep.num_filler_nodes, self.dmap)
+        self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
+        return poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
+
+    def density_grad_into(self, v, ex, ey, scale_t, g):
+        ep = self.ep
+        C.electric_force_into(scale_t, ex.view(-1), ey.view(-1), v, ep.node_size_x_clamped, ep.node_size_y_clamped,
+                              ep.offset_x, ep.offset_y, ep.ratio, float(ep.xl), float(ep.yl), float(ep.xh),
+                              float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y,
+                              ep.num_movable_nodes, ep.num_filler_nodes, ep.sorted_node_map, -1.0, g)
+
+    def obj_and_raw_grad(self, v, g):
+        """obj (fp64, self.obj64) and the un-preconditioned gradient into g."""
+        m = self.model
+        self.wirelength(v)
+        ex, ey, energy = self.density_energy(v)
+        C.objective_finish(self.wl64, energy, m.density_weight, float(m.density_factor), self._quad_c,
+                           self.obj64, self.grad_scale)
+        self.density_grad_into(v, ex, ey, self.grad_scale, g)
+        self.wl_grad_into(g, True)
+        self.last_energy = energy
+        return energy
+
+    def precondition(self, g, v_ref, g_ref, v_new):
+        m = self.model
+        if m.ops.precondition_op._pws is None:
+            m.ops.precondition_op._pws = m.ops.pws_op(self.data.net_weights)
+        C.precondition_step_size(g, g_ref, v_new, v_ref, m.ops.precondition_op._pws, self.data.node_areas,
+                                 m.density_weight, self.state)
+
+    def evaluate(self, v):
+        d, dc = self.design, self.data
+        C.hpwl_slot(v, self.slot_node, self.slot_offx, self.slot_offy, self.netpin_start, dc.net_weights,
+                    dc.net_mask_all, self.hpwl64_buf)
+        self._density(v, 0, self.omap)
+        ba = self.ovf_op.bin_size_x * self.ovf_op.bin_size_y
+        C.density_overflow_into(self.omap, float(self.ovf_op.target_density * ba), float(ba), self.ovf2)
+
+    def move_boundary(self, v):
+        d = self.design
+        C.move_boundary_forward(v, self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl),
+                                float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+
+    # ---------------------------------------------------------------- setup
+    def initial_learning_rate(self, lr):
+        """|x0 - x1| / |g0 - g1| after x1 = x0 - lr g0 (PlaceObj.estimate_initial_learning_rate)."""
+        v0, g0, g1, x1 = self.V[0], self.G[0], self.G[1], self.V[1]
+        self._quad_c = 0.0
+        self.obj_and_raw_grad(v0, g0)
+        self.precondition(g0, v0, g0, v0)
+        torch.sub(v0, g0, alpha=lr, out=x1)
+        self.obj_and_raw_grad(x1, g1)
+        self.precondition(g1, v0, g0, x1)
+        return float((torch.dist(v0.double(), x1.double()) / torch.dist(g0.double(), g1.double())).item())
+
+    def initialize_density_weight(self):
+        """lambda0 = density_weight * |grad WL|_1 / |grad D|_1 (PlaceObj.initialize_density_weight)."""
+        v = self.V[self.parity]
+        self.wirelength(v)
+        self.wl_grad_into(self.tmp, False)
+        wl_norm = self.tmp.double().abs().sum()
+        ex, ey, energy = self.density_energy(v)
+        self.density_grad_into(v, ex, ey, self.one, self.tmp)
+        d_norm = self.tmp.double().abs().sum()
+        self.model.init_density = energy.float().clone()
+        m = self.model
+        m.density_weight = (self.params.density_weight * wl_norm / d_norm).to(torch.float32).reshape(1)
+        m.density_weight_grad_precond = torch.where(m.init_density > 0, 1 / m.init_density, m.init_density)
+        m.quad_penalty_coeff = m.density_quad_coeff / 2 * m.density_weight_grad_precond
+
+    def start_optimizer(self, lr):
+        """First optimizer step's set-up: g_k at v_k, g_k_1 at v_k - lr g_k, alpha_k."""
+        p = self.parity
+        v, g, u = self.V[p], self.G[p], self.U[p]
+        self._quad_c = 0.0
+        self.obj_and_raw_grad(v, g)
+        self.precondition(g, v, g, v)
+        u.copy_(v)
+        x1, g1 = self.V[1 - p], self.G[1 - p]
+        torch.sub(v, g, alpha=lr, out=x1)
+        self.obj_and_raw_grad(x1, g1)
+        self.precondition(g1, v, g, x1)
+        alpha = float((torch.dist(v.double(), x1.double()) / torch.dist(g.double(), g1.double())).item())
+        C.nesterov_init(self.state, alpha)
+        return alpha
+
+    # ---------------------------------------------------------------- iteration
+    def _trial(self, p):
+        d = self.design
+        v, g, u = self.V[p], self.G[p], self.U[p]
+        vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
+        C.nesterov_trial(v, g, u, un, vn, self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
+                         float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+        energy = self.obj_and_raw_grad(vn, gn)
+        self.precondition(gn, v, g, vn)
+        torch.cat([self.hpwl64, self.ovf2, self.state[NS_ACCEPT:NS_ACCEPT + 1], self.state[NS_ALPHA:NS_ALPHA + 1],
+                   self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
+
+    def _body(self, p, with_eval):
+        if with_eval:
+            self.move_boundary(self.V[p])
+            self.evaluate(self.V[p])
+        self._trial(p)
+
+    def _graph(self, p, with_eval):
+        key = (p, with_eval)
+        g = self.graphs.get(key)
+        if g is None:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                # warm-up on the side stream (state is restored below)
+                saved = self.state.clone()
+                self._body(p, with_eval)
+                self.state.copy_(saved)
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, pool=self.pool):
+                self._body(p, with_eval)
+            if self.pool is None:
+                self.pool = g.pool()
+            self.graphs[key] = g
+        return g
+
+    def _run(self, p, with_eval):
+        if self.use_graphs:
+            self._graph(p, with_eval).replay()
+        else:
+            self._body(p, with_eval)
+        self.metrics_host.copy_(self.metrics, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.metrics_host.numpy().copy()
+
+    def _check_graph_key(self):
+        m = self.model
+        key = (float(m.density_factor), bool(m.quad_penalty))
+        if key != self.graph_key:
+            self.graphs = {}
+            self._quad_c = float(m.quad_penalty_coeff.item()) if m.quad_penalty else 0.0
+            self.graph_key = key
+
+    def step(self):
+        """One GP iteration: evaluation at v_k, then Nesterov trials until accepted
+        (<= 10).  Returns (hpwl, overflow / total movable area, max_density, objective, trials)."""
+        self._check_graph_key()
+        p = self.parity
+        mh = self._run(p, True)
+        hpwl, ovf, maxd = mh[M_HPWL], mh[M_OVF], mh[M_MAXD]
+        trials = 1
+        while mh[M_ACCEPT] == 0.0 and trials < 10:
+            mh = self._run(p, False)
+            trials += 1
+        C.nesterov_advance(self.state)
+        self.parity = 1 - p
+        self.trials += trials
+        return (float(hpwl), float(ovf) / self.design.total_movable_node_area, float(maxd), float(mh[M_OBJ]), trials)
+
+    def current_position(self):
+        return self.V[self.parity]

@@ -5,16 +5,27 @@ Mirrors the reference's ``NonLinearPlace.__call__`` for the default flow
 loops Lgamma / Llambda / Lsub with their stop criteria, per-iteration HPWL and
 overflow evaluation (dreamplace/EvalMetrics.py:100-141), density-weight and
 gamma updates, best-position tracking, divergence rollback and the plateau
-rule that turns on the quadratic density penalty.  The per-iteration metrics
-(HPWL and overflow, accumulated in fp64) are read back once per iteration.
+rule that turns on the quadratic density penalty.
+
+Two executions of the same iteration:
+
+* ``params.gp_engine = "graph"`` (default): ``engine.GPEngine`` -- fused
+  kernels, no autograd, one CUDA-graph replay per Nesterov trial;
+* ``params.gp_engine = "autograd"``: the reference-shaped path through the
+  drop-in ops, ``torch.autograd`` and ``nesterov.NesterovAcceleratedGradientOptimizer``.
+
+The per-iteration metrics (HPWL and overflow in fp64) are read back once per
+iteration in both.
 """
 import logging
+import math
 import time
 
 import numpy as np
 import torch
 from torch import nn
 
+from .engine import GPEngine
 from .nesterov import NesterovAcceleratedGradientOptimizer
 from .params import Params
 from .place_obj import PlaceDataCollection, PlaceObj, build_ops
@@ -23,36 +34,94 @@ logger = logging.getLogger(__name__)
 
 
 class EvalMetrics(object):
-    """Per-iteration metrics (reference dreamplace/EvalMetrics.py)."""
+    """Per-iteration metrics (reference dreamplace/EvalMetrics.py); host floats."""
 
-    def __init__(self, iteration=None, detailed_step=None):
+    def __init__(self, iteration, hpwl, overflow, max_density, objective=None):
         self.iteration = iteration
-        self.detailed_step = detailed_step
-        self.objective = None
-        self.hpwl = None
-        self.overflow = None
-        self.max_density = None
+        self.hpwl = hpwl
+        self.overflow = overflow
+        self.max_density = max_density
+        self.objective = objective
         self.gamma = None
         self.density_weight = None
 
-    def evaluate(self, design, ops, pos):
-        with torch.no_grad():
-            self.hpwl = ops.hpwl_f64_op(pos)[0]
-            ovf = ops.density_overflow_op.overflow_f64(pos)
-            self.overflow = (ovf[0] / design.total_movable_node_area).reshape(1)
-            self.max_density = ovf[1].reshape(1)
-
-    def host(self):
-        """(hpwl, overflow, max_density) as python floats (one device read)."""
-        v = torch.stack([self.hpwl.reshape(()), self.overflow.reshape(()), self.max_density.reshape(())]).cpu()
-        self._host = (float(v[0]), float(v[1]), float(v[2]))
-        return self._host
+    @property
+    def _host(self):
+        return (self.hpwl, self.overflow, self.max_density)
 
     def __str__(self):
-        h = getattr(self, "_host", None)
-        if h is None:
-            return "iteration %s" % self.iteration
-        return "iteration %4d, HPWL %.6E, Overflow %.6E, MaxDensity %.3E" % (self.iteration, h[0], h[1], h[2])
+        return "iteration %4d, HPWL %.6E, Overflow %.6E, MaxDensity %.3E" % (self.iteration, self.hpwl,
+                                                                            self.overflow, self.max_density)
+
+
+class _AutogradStepper(object):
+    """The reference-shaped iteration: drop-in ops + autograd + Nesterov optimizer."""
+
+    def __init__(self, placer, model, params, design, lr0):
+        self.placer, self.model, self.params, self.design = placer, model, params, design
+        self.pos = placer.data_collections.pos[0]
+        self.opt = NesterovAcceleratedGradientOptimizer(placer.parameters(), lr=0.0,
+                                                        obj_and_grad_fn=model.obj_and_grad_fn,
+                                                        constraint_fn=placer.op_collections.move_boundary_op)
+        if params.gp_noise_ratio > 0.0:
+            model.ops.noise_op(self.pos, params.gp_noise_ratio)
+        lr = model.estimate_initial_learning_rate(self.pos, lr0)
+        for g in self.opt.param_groups:
+            g["lr"] = lr.data
+
+    def step(self, first):
+        m, ops, d = self.model, self.placer.op_collections, self.design
+        pos = self.pos
+        ops.move_boundary_op(pos)
+        if float(m.density_weight.mean()) == 0.0:
+            m.initialize_density_weight(self.params, d)
+        self.opt.zero_grad(set_to_none=False)
+        with torch.no_grad():
+            hp = ops.hpwl_f64_op(pos)[0]
+            ovf = ops.density_overflow_op.overflow_f64(pos)
+        self.opt.step()
+        obj = self.opt.param_groups[0]["obj_k_1"][0]
+        v = torch.stack([hp.reshape(()), ovf[0], ovf[1], obj.reshape(()).double()]).cpu().numpy()
+        return float(v[0]), float(v[1]) / d.total_movable_node_area, float(v[2]), float(v[3])
+
+    def position(self):
+        return self.pos.data
+
+    def set_position(self, t):
+        self.pos.data.copy_(t)
+
+
+class _EngineStepper(object):
+    """The graph-captured iteration of engine.GPEngine."""
+
+    def __init__(self, placer, model, params, design, lr0, use_graphs):
+        self.model, self.params, self.design = model, params, design
+        pos = placer.data_collections.pos[0]
+        ep = model.ops.density_op
+        if ep.initial_density_map is None:
+            ep.compute_initial_density_map(pos.data)
+        ov = model.ops.density_overflow_op
+        if ov.initial_density_map is None:
+            ov.compute_initial_density_map(pos.data)
+        self.eng = GPEngine(params, design, placer.data_collections, placer.op_collections, model, use_graphs)
+        if params.gp_noise_ratio > 0.0:
+            model.ops.noise_op(self.eng.V[0], params.gp_noise_ratio)
+        self.lr = self.eng.initial_learning_rate(lr0)
+
+    def step(self, first):
+        e = self.eng
+        if first:
+            e.move_boundary(e.V[e.parity])
+            e.initialize_density_weight()
+            e.start_optimizer(self.lr)
+        h, o, md, obj, trials = e.step()
+        return h, o, md, obj
+
+    def position(self):
+        return self.eng.current_position()
+
+    def set_position(self, t):
+        self.eng.current_position().copy_(t)
 
 
 class NonLinearPlace(nn.Module):
@@ -78,16 +147,15 @@ class NonLinearPlace(nn.Module):
             gp["iteration"] = max_iterations
         model = PlaceObj(0.0, params, design, self.data_collections, self.op_collections, gp).to(self.device)
         self.model = model
-        pos = self.data_collections.pos[0]
-        optimizer = NesterovAcceleratedGradientOptimizer(self.parameters(), lr=0.0,
-                                                         obj_and_grad_fn=model.obj_and_grad_fn,
-                                                         constraint_fn=self.op_collections.move_boundary_op)
-        self.optimizer = optimizer
-        if params.gp_noise_ratio > 0.0:
-            model.ops.noise_op(pos, params.gp_noise_ratio)
-        lr = model.estimate_initial_learning_rate(pos, gp["learning_rate"])
-        for g in optimizer.param_groups:
-            g["lr"] = lr.data
+        mode = getattr(params, "gp_engine", "graph")
+        if mode == "autograd":
+            stepper = _AutogradStepper(self, model, params, design, gp["learning_rate"])
+        else:
+            stepper = _EngineStepper(self, model, params, design, gp["learning_rate"], mode == "graph")
+        self.stepper = stepper
+        base_gamma = model.base_gamma(params, design)
+        ref_hpwl = params.RePlAce_ref_hpwl
+        lower, upper = params.RePlAce_LOWER_PCOF, params.RePlAce_UPPER_PCOF
         all_metrics = []
         best = {"metric": None, "pos": None}
         overflow_list = [1.0]
@@ -95,6 +163,7 @@ class NonLinearPlace(nn.Module):
         last_perturb_iter = -50
         stop_placement = False
         iteration = 0
+        flat_llambda = 0
         self.iteration_times = []
 
         def check_divergence(window=50, threshold=0.05):
@@ -105,7 +174,7 @@ class NonLinearPlace(nn.Module):
             overflow_diff = np.sum(np.maximum(0, np.sign(x[1:, 1] - x[:-1, 1]))) / (x.shape[0] - 1)
             overflow_range = np.max(x[:, 1]) - np.min(x[:, 1])
             wl_mean = np.mean(x[:, 0])
-            bh, bo = best["metric"]._host[0], best["metric"]._host[1]
+            bh, bo = best["metric"].hpwl, best["metric"].overflow
             wl_ratio = (wl_mean - bh) / bh
             overflow_ratio = (overflow_mean - max(params.stop_overflow, bo)) / bo
             if wl_ratio > threshold * 1.2:
@@ -132,28 +201,19 @@ class NonLinearPlace(nn.Module):
                 for Lsub_step in range(model.Lsub_iteration):
                     if (params.stop_overflow * 1.1 < overflow_list[-1] < params.stop_overflow * 4
                             and check_divergence(50, overflow_list[-1])):
-                        self.pos[0].data.copy_(best["pos"])
+                        stepper.set_position(best["pos"])
                         stop_placement = True
                         logger.error("possible DIVERGENCE detected, roll back to the best position recorded")
                     t0 = time.time()
-                    cur = EvalMetrics(iteration, (Lgamma_step, Llambda_step, Lsub_step))
+                    h, o, md, obj = stepper.step(iteration == 0)
+                    cur = EvalMetrics(iteration, h, o, md, obj)
                     lsub.append(cur)
-                    self.op_collections.move_boundary_op(pos)
-                    if float(model.density_weight.mean()) == 0.0:
-                        model.initialize_density_weight(params, design)
-                    optimizer.zero_grad(set_to_none=False)
-                    cur.evaluate(design, self.op_collections, pos)
-                    optimizer.step()
-                    cur.gamma = model.gamma.data.clone()
-                    cur.density_weight = model.density_weight.data.clone()
-                    cur.objective = optimizer.param_groups[0]["obj_k_1"][0].data.clone()
-                    h, o, md = cur.host()
-                    if best["metric"] is None or best["metric"]._host[1] > o:
+                    if best["metric"] is None or best["metric"].overflow > o:
                         best["metric"] = cur
                         if best["pos"] is None:
-                            best["pos"] = self.pos[0].data.clone()
+                            best["pos"] = stepper.position().clone()
                         else:
-                            best["pos"].copy_(self.pos[0].data)
+                            best["pos"].copy_(stepper.position())
                     overflow_list.append(o)
                     divergence_list.append([h, o])
                     if iteration - last_perturb_iter > 50 and check_plateau(overflow_list, 15, 0.001):
@@ -167,14 +227,27 @@ class NonLinearPlace(nn.Module):
                     iteration += 1
                     if self._lsub_stop(model, lsub):
                         break
-                if Lgamma_step * model.Llambda_density_weight_iteration + Llambda_step + 1 > 1:
+                flat_llambda += 1
+                if flat_llambda > 1:
+                    # RePlAce hpwl-mode density weight update (dreamplace/PlaceObj.py:840-851)
                     prev = llam[-2][-1] if len(llam) > 1 else all_metrics[-2][-1][-1]
-                    model.ops.update_density_weight_op(llam[-1][-1], prev, Lgamma_step + 1)
+                    delta = llam[-1][-1].hpwl - prev.hpwl
+                    if delta < 0:
+                        mu = upper * max(math.pow(0.9999, float(flat_llambda)), 0.98)
+                    else:
+                        mu = upper * min(max(math.pow(upper, -delta / ref_hpwl), lower), upper)
+                    with torch.no_grad():
+                        model.density_weight.mul_(mu)
                 if self._llambda_stop(params, llam):
                     break
-            model.ops.update_gamma_op(Lgamma_step, llam[-1][-1].overflow)
+            # gamma = base * 10^((overflow - 0.1) * 20/9 - 1) (dreamplace/PlaceObj.py:901-915)
+            coef = math.pow(10, (llam[-1][-1].overflow - 0.1) * 20 / 9 - 1)
+            with torch.no_grad():
+                model.gamma.fill_(base_gamma * coef)
             if self._lgamma_stop(params, design, Lgamma_step, all_metrics, best) or stop_placement:
                 break
+        with torch.no_grad():
+            self.pos[0].data.copy_(stepper.position())
         self.metrics = all_metrics
         self.best = best
         return all_metrics
@@ -183,28 +256,28 @@ class NonLinearPlace(nn.Module):
     def _lsub_stop(model, lsub):
         w = max(min(model.Lsub_iteration // 2, 3), 1)
         if len(lsub) >= 2 * w:
-            cur = sum(float(lsub[-1 - i].objective) for i in range(w)) / w
-            prev = sum(float(lsub[-1 - w - i].objective) for i in range(w)) / w
+            cur = sum(lsub[-1 - i].objective for i in range(w)) / w
+            prev = sum(lsub[-1 - w - i].objective for i in range(w)) / w
             return cur >= prev * 0.999
         return False
 
     @staticmethod
     def _llambda_stop(params, llam):
         if len(llam) > 1:
-            cur, prev = llam[-1][-1]._host, llam[-2][-1]._host
-            return (cur[1] < params.stop_overflow and cur[0] > prev[0]) or cur[2] < 1.0
+            cur, prev = llam[-1][-1], llam[-2][-1]
+            return (cur.overflow < params.stop_overflow and cur.hpwl > prev.hpwl) or cur.max_density < 1.0
         return False
 
     @staticmethod
     def _lgamma_stop(params, design, step, metrics, best):
         if len(metrics) > 1:
-            cur, prev = metrics[-1][-1][-1]._host, metrics[-2][-1][-1]._host
-            if step > 100 and ((cur[1] < params.stop_overflow and cur[0] > prev[0])
-                               or cur[2] < design.target_density):
+            cur, prev = metrics[-1][-1][-1], metrics[-2][-1][-1]
+            if step > 100 and ((cur.overflow < params.stop_overflow and cur.hpwl > prev.hpwl)
+                               or cur.max_density < design.target_density):
                 return True
         if len(metrics) > 50:
-            cur, prev = metrics[-1][-1][-1]._host, metrics[-50][-1][-1]._host
-            if cur[1] > prev[1] and cur[0] > best["metric"]._host[0] * 2:
+            cur, prev = metrics[-1][-1][-1], metrics[-50][-1][-1]
+            if cur.overflow > prev.overflow and cur.hpwl > best["metric"].hpwl * 2:
                 return True
         return False
 
@@ -215,5 +288,5 @@ def place(design, params=None, device=None, max_iterations=None, callback=None):
     placer = NonLinearPlace(params, design, device)
     metrics = placer(params, design, max_iterations=max_iterations, callback=callback)
     last = metrics[-1][-1][-1]
-    return placer, {"iterations": last.iteration + 1, "hpwl": last._host[0], "overflow": last._host[1],
-                    "max_density": last._host[2]}
+    return placer, {"iterations": last.iteration + 1, "hpwl": last.hpwl, "overflow": last.overflow,
+                    "max_density": last.max_density}

@@ -28,6 +28,11 @@ extern "C" {
 typedef struct CUstream_st* dp_stream_t; /* same type as cudaStream_t */
 
 enum {
+  DP_REDUCE_DOUBLES = 1280,         /* 1 result + per-block partials of a fixed-order fp64 sum */
+  DP_NESTEROV_STATE_DOUBLES = 8
+};
+
+enum {
   DP_OK = 0,
   DP_ERR_INVALID_ARGUMENT = -1,
   DP_ERR_CUDA = -2,
@@ -221,6 +226,55 @@ int dp_pin_weight_sum(const float* net_weights, const int* flat_nodepin,
                       const int* nodepin_start, const int* pin2net_map,
                       int num_physical_nodes, int num_nodes, float* node_weights,
                       dp_stream_t stream);
+
+/* ---- fused global-placement iteration (engine path) -------------------------
+ * "Slots" are pin positions in flat_netpin order: slot_node[j] =
+ * pin2node[flat_netpin[j]], slot_offx/y[j] = pin offsets of that pin.
+ * dp_wa_slot_forward = pin_pos + WA merged forward of the reference
+ * (pin_pos/src/pin_pos_cuda_kernel.cu:11-27 + weighted_average_wirelength/src/
+ * weighted_average_wirelength_cuda_merged_kernel.cu:15-85): per-slot gradient
+ * grad_slot [2*num_slots] and the fp64 total.  wl_f64 holds DP_REDUCE_DOUBLES
+ * doubles: [0] receives the total, the rest is scratch for the fixed-order
+ * (run-to-run reproducible) reduction. */
+int dp_wa_slot_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                       const float* slot_offy, const int* netpin_start, int num_nets,
+                       const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
+                       double* wl_f64, float* grad_slot, int num_slots, dp_stream_t stream);
+/* WA backward + pin_pos backward (weighted_average_wirelength.py:197-213 +
+ * pin_pos/src/pin_pos_cuda_kernel.cu:50-74): grad_out[node] (+)= sum over the
+ * node's pins, in flat_node2pin order (node_slots = slot of each pin), of
+ * grad_slot * grad_pos[0] * w_net; nodes >= num_movable get 0 (pin mask). */
+int dp_wa_node_backward(const float* grad_slot, int num_slots, const int* node_slots,
+                        const int* node_start, const int* slot_net, const float* net_weights,
+                        const unsigned char* net_mask, const float* grad_pos, int num_movable,
+                        int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
+/* HPWL through the slot gather (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64 holds
+ * DP_REDUCE_DOUBLES doubles, [0] receives the fp64 total. */
+int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                 const float* slot_offy, const int* netpin_start, int num_nets, const float* net_weights,
+                 const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
+/* Nesterov step of NesterovAcceleratedGradientOptimizer.step_nobb
+ * (dreamplace/NesterovAcceleratedGradientOptimizer.py:65-166) on device
+ * scalars state[DP_NESTEROV_STATE_DOUBLES + 2 * DP_REDUCE_DOUBLES] (fp64):
+ * alpha_k, a_k, a_{k+1}, coef, two norms, alpha_{k+1}, accept flag, then
+ * reduction scratch. */
+int dp_nesterov_init(double* state, double alpha, dp_stream_t stream);
+/* u' = v - alpha g; v' = clamp_die(u' + coef (u' - u)) (move_boundary semantics) */
+int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
+                      const double* state, const float* node_size_x, const float* node_size_y,
+                      float xl, float yl, float xh, float yh, int num_nodes, int num_movable,
+                      int num_filler, dp_stream_t stream);
+/* g' /= max(1, pws + lambda*area) (dreamplace/PlaceObj.py:69-103), then
+ * alpha' = |v'-v| / |g'-g| in fp64, accept = alpha' > 0.95 alpha, alpha <- alpha' */
+int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, const float* v,
+                              const float* pws, const float* area, const float* lambda_, int num_nodes,
+                              double* state, dp_stream_t stream);
+/* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
+int dp_nesterov_advance(double* state, dp_stream_t stream);
+/* obj = wl + lambda_eff * D (1 + c D); grad_scale = d obj / d D */
+int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
+                        float density_factor, float quad_c, double* obj, float* grad_scale,
+                        dp_stream_t stream);
 
 #ifdef __cplusplus
 }
