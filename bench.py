@@ -167,6 +167,11 @@ class TimedRun(object):
         state = {"launch0": 0, "launch1": 0}
         pos = self.placer.pos[0]
         host_pos = torch.empty(pos.numel(), dtype=pos.dtype, pin_memory=True)
+
+        def launches():
+            st = getattr(self.placer, "stepper", None)
+            eng = getattr(st, "eng", None)
+            return eng.kernels_launched if eng is not None else C.launch_count()
         self.h2d = self.d2h = 0
 
         def cb(it, metric):
@@ -176,19 +181,20 @@ class TimedRun(object):
                 torch.cuda.synchronize()
                 if clocks is not None:
                     clocks.start()
-                state["launch0"] = C.launch_count()
+                state["launch0"] = launches()
                 start.record()
             elif warmup <= it < warmup + steps:
                 if self.e2e:
                     # host round trip of the step's state: positions out and back in, metrics out
-                    host_pos.copy_(pos.data, non_blocking=True)
-                    pos.data.copy_(host_pos, non_blocking=True)
+                    cur = self.placer.stepper.position()
+                    host_pos.copy_(cur, non_blocking=True)
+                    cur.copy_(host_pos, non_blocking=True)
                     self.h2d = host_pos.numel() * 4
                     self.d2h = host_pos.numel() * 4 + 3 * 8
                 if it == warmup + steps - 1:
                     end.record()
                     torch.cuda.synchronize()
-                    state["launch1"] = C.launch_count()
+                    state["launch1"] = launches()
 
         t0 = time.time()
         self.placer(self.params, self.design, max_iterations=warmup + steps, callback=cb)
@@ -199,59 +205,53 @@ class TimedRun(object):
         return ms
 
 
-def kernel_roofline(placer, design, peaks, reps=10):
-    """Times the hot kernels of one evaluation on the current positions with CUDA
-    events and returns per-kernel (ms, algorithmic bytes or flops)."""
-    from dreamplace_b200._native import C
-    from dreamplace_b200.electric_potential import ElectricDensityMapFunction, poisson_solve
-    from dreamplace_b200.dct2_fft2 import gemm_flops, precision_code
-    model = placer.model
-    ops = placer.op_collections
-    dc = placer.data_collections
-    pos = dc.pos[0].data
-    ep = ops.density_op
-    n_s = design.num_movable_nodes + design.num_filler_nodes
-    M, N = ep.num_bins_x, ep.num_bins_y
-    P, E = design.num_pins, design.num_nets
-    res = {}
-
-    def timeit(fn):
+def _graph_time(fn, reps=20):
+    """Device time of fn per call: fn captured once in a CUDA graph, replayed reps times."""
+    fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
         fn()
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        for _ in range(reps):
-            fn()
-        e.record()
-        torch.cuda.synchronize()
-        return s.elapsed_time(e) / reps
+    g.replay()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        g.replay()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
 
-    dm_args = lambda: ElectricDensityMapFunction.forward(  # noqa: E731
-        pos, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio, ep.bin_center_x,
-        ep.bin_center_y, ep.initial_density_map, ep.target_density, ep.xl, ep.yl, ep.xh, ep.yh, ep.bin_size_x,
-        ep.bin_size_y, ep.num_movable_nodes, ep.num_filler_nodes, 0, ep.padding_mask, M, N, 0, 0, 0, 0, 0,
-        ep.sorted_node_map)
-    ms = timeit(dm_args)
-    res["density_scatter"] = (ms, 28.0 * n_s + 4.0 * design.num_movable_nodes + 8.0 * M * N, "hbm")
-    dmap = dm_args()
-    rho = dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
-    prec = precision_code(ep.precision)
-    ms = timeit(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, prec, False))
-    res["poisson_gemms"] = (ms, gemm_flops(M, N, prec, 4), "tensor" if prec else "fp32")
-    ex, ey, _ = poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, prec, False)
-    g = torch.ones(1, device="cuda")
-    ms = timeit(lambda: C.electric_force(g, M, N, 0, 0, 0, 0, ex.view(-1), ey.view(-1), pos, ep.node_size_x_clamped,
-                                         ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio, pos, pos,
-                                         ep.xl, ep.yl, ep.xh, ep.yh, ep.bin_size_x, ep.bin_size_y,
-                                         ep.num_movable_nodes, ep.num_filler_nodes, 0, ep.sorted_node_map, -1.0))
-    res["field_gather"] = (ms, 36.0 * n_s + 8.0 * M * N, "hbm")
-    pin = ops.pin_pos_op(pos)
-    ms = timeit(lambda: ops.pin_pos_op(pos))
-    res["pin_pos_forward"] = (ms, 28.0 * P, "hbm")
-    inv_gamma = (1.0 / model.gamma).reshape(1)
-    ms = timeit(lambda: C.wa_merged_forward(pin, dc.flat_net2pin_map, dc.flat_net2pin_start_map, dc.pin2net_map,
-                                            dc.net_weights, dc.net_mask_ignore_large_degrees, inv_gamma))
-    res["wa_forward"] = (ms, 20.0 * P + 17.0 * E, "hbm")
+
+def kernel_roofline(placer, design, peaks, reps=20):
+    """Device time of each piece of one GP iteration of the engine (each piece
+    graph-captured and replayed) with its algorithmic bytes or flops."""
+    from dreamplace_b200.dct2_fft2 import gemm_flops
+    from dreamplace_b200.electric_potential import poisson_solve
+    eng = placer.stepper.eng
+    d = design
+    ep = eng.ep
+    n_s = d.num_movable_nodes + d.num_filler_nodes
+    M, N = ep.num_bins_x, ep.num_bins_y
+    P, E, n = d.num_pins, d.num_nets, d.num_nodes
+    p = eng.parity
+    v, g, u = eng.V[p], eng.G[p], eng.U[p]
+    res = {}
+    res["density_scatter"] = (_graph_time(lambda: eng._density(v, ep.num_filler_nodes, eng.dmap), reps),
+                              28.0 * n_s + 4.0 * n_s + 8.0 * M * N, "hbm")
+    rho = eng.dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
+    res["poisson_gemms"] = (_graph_time(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec), reps),
+                            gemm_flops(M, N, eng.prec, 4), "tensor" if eng.prec else "fp32")
+    ex, ey, _ = poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec)
+    res["field_gather"] = (_graph_time(lambda: eng.density_grad_into(v, ex, ey, eng.one, eng.tmp), reps),
+                           36.0 * n_s + 8.0 * M * N, "hbm")
+    res["wa_forward"] = (_graph_time(lambda: eng.wirelength(v), reps), 20.0 * P + 9.0 * E + 8.0 * n, "hbm")
+    res["wa_backward_pin_sum"] = (_graph_time(lambda: eng.wl_grad_into(eng.tmp, True), reps),
+                                  16.0 * P + 16.0 * n, "hbm")
+    res["hpwl"] = (_graph_time(lambda: eng.evaluate(v), reps), 12.0 * P + 5.0 * E + 8.0 * n, "hbm")
+    saved = eng.state.clone()
+    res["nesterov_trial"] = (_graph_time(lambda: eng.nesterov_trial_only(p), reps), 20.0 * 2 * n, "hbm")
+    eng.state.copy_(saved)
     return res
 
 

@@ -139,10 +139,10 @@ at::Tensor density_map_exact(at::Tensor pos, at::Tensor sx, at::Tensor sy, std::
 at::Tensor density_overflow(at::Tensor density_map, double target_area, double bin_area) {
   CHECK_CUDA_T(density_map); CHECK_CONTIG(density_map); CHECK_F32(density_map);
   c10::cuda::CUDAGuard guard(density_map.device());
-  auto out = at::empty({2}, density_map.options().dtype(at::kDouble));
+  auto out = at::empty({DP_REDUCE_DOUBLES}, density_map.options().dtype(at::kDouble));
   DP_CALL(dp_density_overflow(ptr<float>(density_map), density_map.numel(), target_area, bin_area, ptr<double>(out),
                               nullptr, cur_stream()));
-  return out;
+  return out.narrow(0, 0, 2);
 }
 
 at::Tensor electric_force(at::Tensor grad_pos, int nbx, int nby, int, int, int, int, at::Tensor ex, at::Tensor ey,
@@ -238,7 +238,7 @@ std::vector<at::Tensor> wa_merged_forward(at::Tensor pos, at::Tensor flat_netpin
   int num_pins = pos.numel() / 2;
   auto grad_intermediate = at::empty_like(pos);
   auto wl = at::empty({}, pos.options());
-  auto wl64 = at::empty({1}, pos.options().dtype(at::kDouble));
+  auto wl64 = at::empty({DP_REDUCE_DOUBLES}, pos.options().dtype(at::kDouble));
   auto ig = inv_gamma.contiguous();
   DP_CALL(dp_wa_merged_forward(ptr<float>(pos), num_pins, ptr<int>(flat_netpin), ptr<int>(netpin_start), num_nets,
                                net_weights.numel() ? ptr<float>(net_weights) : nullptr, net_mask.data_ptr<uint8_t>(),
@@ -295,11 +295,11 @@ at::Tensor hpwl_forward(at::Tensor pin_pos, at::Tensor flat_netpin, at::Tensor n
                         at::Tensor net_mask) {
   CHECK_FLAT(pin_pos); CHECK_EVEN(pin_pos); CHECK_F32(pin_pos);
   c10::cuda::CUDAGuard guard(pin_pos.device());
-  auto out = at::empty({1}, pin_pos.options().dtype(at::kDouble));
+  auto out = at::empty({DP_REDUCE_DOUBLES}, pin_pos.options().dtype(at::kDouble));
   DP_CALL(dp_hpwl(ptr<float>(pin_pos), pin_pos.numel() / 2, ptr<int>(flat_netpin), ptr<int>(netpin_start),
                   netpin_start.numel() - 1, net_weights.numel() ? ptr<float>(net_weights) : nullptr,
                   net_mask.data_ptr<uint8_t>(), ptr<double>(out), nullptr, cur_stream()));
-  return out;
+  return out.narrow(0, 0, 1);
 }
 
 at::Tensor move_boundary_forward(at::Tensor pos, at::Tensor sx, at::Tensor sy, double xl, double yl, double xh,
@@ -401,6 +401,20 @@ void density_map_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor o
   }
 }
 
+void density_map_ordered_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy,
+                              at::Tensor ratio, c10::optional<at::Tensor> init, double xl, double yl, double xh,
+                              double yh, double bsx, double bsy, int nbx, int nby, at::Tensor order, int count,
+                              int deterministic, c10::optional<at::Tensor> scratch, at::Tensor out) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(order);
+  TORCH_CHECK(count <= order.numel(), "count exceeds the order array");
+  TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
+  DP_CALL(dp_density_map_ordered(ptr<float>(pos), pos.numel() / 2, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox),
+                                 ptr<float>(oy), ptr<float>(ratio), (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
+                                 inv_f(bsx), inv_f(bsy), nbx, nby, ptr<int>(order), count, deterministic,
+                                 fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch), ptr<float>(out),
+                                 cur_stream()));
+}
+
 void density_overflow_into(at::Tensor density_map, double target_area, double bin_area, at::Tensor out2) {
   DP_CALL(dp_density_overflow(ptr<float>(density_map), density_map.numel(), target_area, bin_area, ptr<double>(out2),
                               nullptr, cur_stream()));
@@ -447,6 +461,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("objective_finish", &objective_finish);
   m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);
+  m.def("density_map_ordered_into", &density_map_ordered_into);
   m.def("electric_force_into", &electric_force_into);
   m.def("version", &dp_version);
 }

@@ -1,6 +1,6 @@
 // C ABI runtime pieces: per-thread error messages, launch accounting, version.
 #include <stdarg.h>
-#include "common.cuh"
+#include "reduce.cuh"
 
 namespace dpb {
 
@@ -15,6 +15,19 @@ void set_error(const char* fmt, ...) {
 }
 
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+__global__ void finish_sum_kernel(double* buf, int count, float* out_f32) {
+  double r = finish_sum(buf + 1, count);
+  if (threadIdx.x == 0) {
+    buf[0] = r;
+    if (out_f32) *out_f32 = (float)r;
+  }
+}
+
+int launch_finish_sum(double* buf, int count, float* out_f32, cudaStream_t s) {
+  finish_sum_kernel<<<1, kReduceThreads, 0, s>>>(buf, count, out_f32);
+  return check_launch("finish_sum");
+}
 
 }  // namespace dpb
 

@@ -15,7 +15,9 @@
 // hit the same bin combines their contributions with a match/reduce before
 // one atomic, which removes most same-address serialisation when cells are
 // clustered (the GP starts with every movable cell at the die centre).
-#include "common.cuh"
+#include <climits>
+#include <type_traits>
+#include "reduce.cuh"
 
 namespace dpb {
 
@@ -98,6 +100,116 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
         } else {
           combined_add<float, float>(map_f32, bin, area, active);
         }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- tiled scatter
+// Cells are visited in the caller's order (a spatial order refreshed every few
+// iterations).  Each CTA takes kTileCells consecutive cells, reduces their bin
+// bounding box, and when it fits in shared memory accumulates there (shared
+// atomics) and flushes each touched bin with one global atomic; otherwise it
+// adds straight to global memory.  The fixed-point map is order independent,
+// so the deterministic result is unchanged by the tiling.
+constexpr int kTileThreads = 256;
+constexpr int kTileCellsPerThread = 4;
+constexpr int kTileCells = kTileThreads * kTileCellsPerThread;
+constexpr int kTileSmemBytes = 96 * 1024;
+
+template <bool kFixed>
+__global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(TriangleArgs a, const int* __restrict__ order,
+                                                                         int count, float fx_scale, float* map_f32,
+                                                                         unsigned long long* map_fx) {
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
+  Acc* tile = reinterpret_cast<Acc*>(tile_raw);
+  constexpr int kCap = kTileSmemBytes / sizeof(Acc);
+  __shared__ int red[4][kTileThreads / 32];
+  const int base = blockIdx.x * kTileCells;
+  int kx0[kTileCellsPerThread], kx1[kTileCellsPerThread], hy0[kTileCellsPerThread], hy1[kTileCellsPerThread];
+  float nx[kTileCellsPerThread], ny[kTileCellsPerThread], sxs[kTileCellsPerThread], sys[kTileCellsPerThread],
+      rr[kTileCellsPerThread];
+  int bk0 = INT_MAX, bk1 = INT_MIN, bh0 = INT_MAX, bh1 = INT_MIN;
+#pragma unroll
+  for (int c = 0; c < kTileCellsPerThread; ++c) {
+    int idx = base + c * kTileThreads + threadIdx.x;
+    kx0[c] = kx1[c] = hy0[c] = hy1[c] = 0;
+    if (idx < count) {
+      int i = order[idx];
+      sxs[c] = a.sx[i];
+      sys[c] = a.sy[i];
+      nx[c] = fadd(a.x[i], a.ox[i]);
+      ny[c] = fadd(a.y[i], a.oy[i]);
+      rr[c] = a.ratio[i];
+      triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, kx0[c], kx1[c]);
+      triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, hy0[c], hy1[c]);
+      if (kx1[c] > kx0[c] && hy1[c] > hy0[c]) {
+        bk0 = min(bk0, kx0[c]);
+        bk1 = max(bk1, kx1[c]);
+        bh0 = min(bh0, hy0[c]);
+        bh1 = max(bh1, hy1[c]);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    bk0 = min(bk0, __shfl_xor_sync(0xffffffffu, bk0, o));
+    bk1 = max(bk1, __shfl_xor_sync(0xffffffffu, bk1, o));
+    bh0 = min(bh0, __shfl_xor_sync(0xffffffffu, bh0, o));
+    bh1 = max(bh1, __shfl_xor_sync(0xffffffffu, bh1, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    red[0][w] = bk0;
+    red[1][w] = bk1;
+    red[2][w] = bh0;
+    red[3][w] = bh1;
+  }
+  __syncthreads();
+  bk0 = INT_MAX; bk1 = INT_MIN; bh0 = INT_MAX; bh1 = INT_MIN;
+#pragma unroll
+  for (int i = 0; i < kTileThreads / 32; ++i) {
+    bk0 = min(bk0, red[0][i]);
+    bk1 = max(bk1, red[1][i]);
+    bh0 = min(bh0, red[2][i]);
+    bh1 = max(bh1, red[3][i]);
+  }
+  if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
+  const int W = bk1 - bk0, H = bh1 - bh0;
+  const bool use_tile = (long long)W * H <= kCap;
+  if (use_tile) {
+    for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = 0;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < kTileCellsPerThread; ++c) {
+    for (int k = kx0[c]; k < kx1[c]; ++k) {
+      float px = triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx);
+      float pxr = fmul(px, rr[c]);
+      for (int h = hy0[c]; h < hy1[c]; ++h) {
+        float py = triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy);
+        float area = fmul(pxr, py);
+        if (use_tile) {
+          Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
+          atomicAdd(&tile[(k - bk0) * H + (h - bh0)], v);
+        } else if (kFixed) {
+          atomicAdd(map_fx + k * a.num_bins_y + h, (unsigned long long)to_fixed(area, fx_scale));
+        } else {
+          atomicAdd(map_f32 + k * a.num_bins_y + h, area);
+        }
+      }
+    }
+  }
+  if (use_tile) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < W * H; t += kTileThreads) {
+      Acc v = tile[t];
+      if (v != (Acc)0) {
+        int bin = (bk0 + t / H) * a.num_bins_y + bh0 + t % H;
+        if (kFixed)
+          atomicAdd(map_fx + bin, (unsigned long long)v);
+        else
+          atomicAdd(map_f32 + bin, (float)v);
       }
     }
   }
@@ -243,7 +355,7 @@ __device__ __forceinline__ float key_float(unsigned k) {
 }
 
 __global__ void overflow_kernel(const float* __restrict__ map, int n, double target_area,
-                                double* acc, unsigned* maxkey) {
+                                double* partials, unsigned* maxkey) {
   double s = 0.0;
   float m = -INFINITY;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -252,32 +364,16 @@ __global__ void overflow_kernel(const float* __restrict__ map, int n, double tar
     s += over > 0.0 ? over : 0.0;
     m = fmaxf(m, d);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    s += __shfl_xor_sync(0xffffffffu, s, o);
-    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  }
-  __shared__ double ss[32];
-  __shared__ float sm[32];
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { ss[w] = s; sm[w] = m; }
-  __syncthreads();
-  if (w == 0) {
-    int nw = blockDim.x >> 5;
-    s = l < nw ? ss[l] : 0.0;
-    m = l < nw ? sm[l] : -INFINITY;
-    for (int o = 16; o > 0; o >>= 1) {
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    }
-    if (l == 0) {
-      atomicAdd(acc, s);
-      atomicMax(maxkey, float_key(m));
-    }
-  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxkey, float_key(m));  // max is order independent
+  block_partial(s, partials);
 }
 
 __global__ void overflow_finish_kernel(double* out2, const unsigned* maxkey, double bin_area,
-                                       float* out2_f32) {
+                                       float* out2_f32, const double* partials, int count) {
+  double total = finish_sum(partials, count);
+  if (threadIdx.x != 0) return;
+  out2[0] = total;
   double mx = (double)key_float(*maxkey) / bin_area;
   out2[1] = mx;
   if (out2_f32) {
@@ -421,13 +517,58 @@ extern "C" int dp_density_overflow(const float* map, int nbins, double target_ar
                                    double* out2, float* out2_f32, dp_stream_t stream) {
   DP_REQUIRE(map && out2 && nbins > 0, "dp_density_overflow: bad arguments");
   cudaStream_t s = as_stream(stream);
-  // out2[0] accumulates the overflow; out2[1] holds the max key until the
-  // finishing kernel replaces it with max / bin_area.
-  cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
-  unsigned* maxslot = reinterpret_cast<unsigned*>(out2 + 1);
-  overflow_kernel<<<grid_for(nbins, 256, 4), 256, 0, s>>>(map, nbins, target_area, out2, maxslot);
+  // out2: [0] overflow, [1] max density, [2] max key, [3..] block partials
+  int blocks = grid_for(nbins, 256, 4);
+  unsigned* maxslot = reinterpret_cast<unsigned*>(out2 + 2);
+  cudaMemsetAsync(maxslot, 0, sizeof(double), s);
+  overflow_kernel<<<blocks, 256, 0, s>>>(map, nbins, target_area, out2 + 3, maxslot);
   int rc = check_launch("dp_density_overflow");
   if (rc) return rc;
-  overflow_finish_kernel<<<1, 1, 0, s>>>(out2, maxslot, bin_area, out2_f32);
+  overflow_finish_kernel<<<1, kReduceThreads, 0, s>>>(out2, maxslot, bin_area, out2_f32, out2 + 3, blocks);
   return check_launch("dp_density_overflow finish");
+}
+
+// Order-driven scatter (see tiled_scatter_kernel): `order` lists the nodes to
+// scatter (movable and/or filler indices, any order).
+extern "C" int dp_density_map_ordered(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                      const float* ox, const float* oy, const float* ratio, const float* init,
+                                      float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
+                                      float iby, int nbx, int nby, const int* order, int count, int deterministic,
+                                      int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
+  int rc = validate_triangle(pos, num_nodes, sx, sy, ox, oy, ratio, 0, 0, nbx, nby, bsx, bsy, out);
+  if (rc) return rc;
+  DP_REQUIRE(count >= 0 && count <= num_nodes && (count == 0 || order), "dp_density_map_ordered: bad order");
+  DP_REQUIRE(!deterministic || scratch, "dp_density_map_ordered: deterministic mode needs scratch_fixed");
+  cudaStream_t s = as_stream(stream);
+  int nbins = nbx * nby;
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(tiled_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes);
+    cudaFuncSetAttribute(tiled_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes);
+    configured = true;
+  }
+  TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, 0, 0, nbx, nby, nullptr);
+  int blocks = ceil_div(count, kTileCells);
+  if (deterministic) {
+    DP_REQUIRE(fraction_bits >= 0 && fraction_bits <= 62, "dp_density_map_ordered: bad fraction_bits");
+    cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
+    if (blocks > 0) {
+      tiled_scatter_kernel<true><<<blocks, kTileThreads, kTileSmemBytes, s>>>(
+          a, order, count, ldexpf(1.0f, fraction_bits), nullptr, reinterpret_cast<unsigned long long*>(scratch));
+      rc = check_launch("dp_density_map_ordered scatter");
+      if (rc) return rc;
+    }
+    fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
+                                                              ldexp(1.0, -fraction_bits), out, nbins);
+    return check_launch("dp_density_map_ordered convert");
+  }
+  if (init) {
+    rc = copy_map(init, out, nbins, s);
+    if (rc) return rc;
+  } else {
+    cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
+  }
+  if (blocks == 0) return DP_OK;
+  tiled_scatter_kernel<false><<<blocks, kTileThreads, kTileSmemBytes, s>>>(a, order, count, 0.f, out, nullptr);
+  return check_launch("dp_density_map_ordered scatter");
 }

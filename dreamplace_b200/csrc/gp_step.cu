@@ -17,24 +17,13 @@
 //    and both step-size norms (fp64) are two streaming passes over the
 //    position / gradient vectors, and a one-thread kernel finishes the step
 //    size, the backtracking test and the momentum scalars on the device.
-#include "common.cuh"
+#include "reduce.cuh"
 
 namespace dpb {
 
-// Fixed-order reductions: every block writes its partial sum(s) to
-// partials[blockIdx.x] (and partials[gridDim.x + blockIdx.x]); a one-block
-// finisher adds the partials in a fixed tree order, so totals are
-// bit-reproducible run to run (the deterministic mode's requirement).
-constexpr int kMaxReduceBlocks = 1184;  // 148 SMs x 8
-
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// block sum of (a, b) written to partials; blockDim.x must be 256
+// two-value block partial: partials[blockIdx.x], partials[gridDim.x + blockIdx.x]
 __device__ __forceinline__ void block_partial2(double a, double b, double* partials) {
-  __shared__ double sa[8], sb[8];
+  __shared__ double sa[kReduceThreads / 32], sb[kReduceThreads / 32];
   a = warp_sum(a);
   b = warp_sum(b);
   int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -42,44 +31,10 @@ __device__ __forceinline__ void block_partial2(double a, double b, double* parti
   __syncthreads();
   if (threadIdx.x == 0) {
     double ta = 0.0, tb = 0.0;
-    for (int i = 0; i < 8; ++i) { ta += sa[i]; tb += sb[i]; }
+    for (int i = 0; i < kReduceThreads / 32; ++i) { ta += sa[i]; tb += sb[i]; }
     partials[blockIdx.x] = ta;
     partials[gridDim.x + blockIdx.x] = tb;
   }
-}
-
-__device__ __forceinline__ void block_partial1(double a, double* partials) {
-  __shared__ double sa[8];
-  a = warp_sum(a);
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sa[w] = a;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double ta = 0.0;
-    for (int i = 0; i < 8; ++i) ta += sa[i];
-    partials[blockIdx.x] = ta;
-  }
-}
-
-// one block of 256 threads: out[k] = sum of partials[k*count .. k*count+count)
-__device__ __forceinline__ double finish_sum(const double* partials, int count) {
-  __shared__ double sh[256];
-  double v = 0.0;
-  for (int i = threadIdx.x; i < count; i += 256) v += partials[i];
-  sh[threadIdx.x] = v;
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-    __syncthreads();
-  }
-  double r = sh[0];
-  __syncthreads();
-  return r;
-}
-
-__global__ void finish_sum_kernel(const double* partials, int count, double* out) {
-  double r = finish_sum(partials, count);
-  if (threadIdx.x == 0) out[0] = r;
 }
 
 // ---------------------------------------------------------------- WA fused
@@ -150,7 +105,7 @@ __global__ void __launch_bounds__(256) wa_slot_forward_kernel(
       }
     }
   }
-  block_partial1(contrib, partials);
+  block_partial(contrib, partials);
 }
 
 // node grad (+)= sum over the node's pins, in flat_node2pin order, of
@@ -215,7 +170,7 @@ __global__ void __launch_bounds__(256) hpwl_slot_kernel(const float* __restrict_
       c += (double)h;
     }
   }
-  block_partial1(c, partials);
+  block_partial(c, partials);
 }
 
 // ---------------------------------------------------------------- Nesterov
@@ -352,13 +307,13 @@ extern "C" int dp_wa_slot_forward(const float* pos, int num_nodes, const int* sl
   cudaStream_t s = as_stream(stream);
   int blocks = grid_for(num_nets, 256, 8);
   double* partials = wl_f64 + 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   wa_slot_forward_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
                                                num_nets, net_weights, net_mask, inv_gamma, partials, grad_slot,
                                                grad_slot + num_slots);
   int rc = check_launch("dp_wa_slot_forward");
   if (rc) return rc;
-  finish_sum_kernel<<<1, 256, 0, s>>>(partials, blocks, wl_f64);
-  return check_launch("dp_wa_slot_forward finish");
+  return launch_finish_sum(wl_f64, blocks, nullptr, s);
 }
 
 extern "C" int dp_wa_node_backward(const float* grad_slot, int num_slots, const int* node_slots,
@@ -382,12 +337,12 @@ extern "C" int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_nod
   cudaStream_t s = as_stream(stream);
   int blocks = grid_for(num_nets, 256, 8);
   double* partials = out_f64 + 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   hpwl_slot_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
                                          num_nets, net_weights, net_mask, partials);
   int rc = check_launch("dp_hpwl_slot");
   if (rc) return rc;
-  finish_sum_kernel<<<1, 256, 0, s>>>(partials, blocks, out_f64);
-  return check_launch("dp_hpwl_slot finish");
+  return launch_finish_sum(out_f64, blocks, nullptr, s);
 }
 
 extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream) {
@@ -412,6 +367,7 @@ extern "C" int dp_precondition_step_size(float* g_new, const float* g, const flo
   DP_REQUIRE(g_new && g && v_new && v && pws && area && lambda_ && state, "dp_precondition_step_size: null pointer");
   cudaStream_t s = as_stream(stream);
   int blocks = grid_for(2ll * num_nodes, 256, 4);
+  if (2 * blocks > 2 * DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
   precondition_norms_kernel<<<blocks, 256, 0, s>>>(g_new, g, v_new, v, pws, area, lambda_, num_nodes, partials);
   int rc = check_launch("dp_precondition_step_size");

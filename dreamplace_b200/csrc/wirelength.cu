@@ -12,28 +12,9 @@
 // a = (1.0 - b*S1)/S0 in double as the C++ expression promotes it, no FMA
 // contraction); only exp() differs (CUDA expf, <= 2 ulp).  Totals are
 // accumulated in fp64.
-#include "common.cuh"
+#include "reduce.cuh"
 
 namespace dpb {
-
-__device__ __forceinline__ void block_add_double(double v, double* out) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __shared__ double sh[32];
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    int nw = blockDim.x >> 5;
-    v = l < nw ? sh[l] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (l == 0 && v != 0.0) atomicAdd(out, v);
-  }
-  __syncthreads();
-}
-
-struct WaStats {
-  float mx, mn, s_p, s_n, xs_p, xs_n;
-};
 
 __device__ __forceinline__ float wa_exp(float a) { return expf(a); }
 
@@ -41,15 +22,12 @@ __global__ void __launch_bounds__(256) wa_merged_forward_kernel(
     const float* __restrict__ px, const float* __restrict__ py, const int* __restrict__ flat_netpin,
     const int* __restrict__ netpin_start, int num_nets, const float* __restrict__ net_weights,
     const unsigned char* __restrict__ net_mask, const float* __restrict__ inv_gamma_p,
-    float* __restrict__ partial_wl, double* __restrict__ wl_total, float* __restrict__ gx,
+    float* __restrict__ partial_wl, double* __restrict__ partials, float* __restrict__ gx,
     float* __restrict__ gy) {
   const float inv_gamma = *inv_gamma_p;
-  int nets_per_iter = gridDim.x * blockDim.x;
-  int iters = (num_nets + nets_per_iter - 1) / nets_per_iter;
-  for (int it = 0; it < iters; ++it) {
-    int i = it * nets_per_iter + blockIdx.x * blockDim.x + threadIdx.x;
-    double contrib = 0.0;
-    if (i < num_nets) {
+  double contrib = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
+    {
       int b = netpin_start[i], e = netpin_start[i + 1];
       if (net_mask[i]) {
         float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
@@ -84,7 +62,7 @@ __global__ void __launch_bounds__(256) wa_merged_forward_kernel(
         float w = net_weights ? net_weights[i] : 1.0f;
         float pw = net_weights ? fmul(wl, w) : wl;
         if (partial_wl) partial_wl[i] = pw;
-        contrib = (double)pw;
+        contrib += (double)pw;
         float b_x = __fdiv_rn(inv_gamma, e_p);
         float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
         float b_nx = __fdiv_rn(-inv_gamma, e_n);
@@ -112,11 +90,10 @@ __global__ void __launch_bounds__(256) wa_merged_forward_kernel(
         }
       }
     }
-    block_add_double(contrib, wl_total);
   }
+  block_partial(contrib, partials);
 }
 
-__global__ void finish_scalar_kernel(const double* v, float* out) { *out = (float)*v; }
 
 __global__ void wa_merged_backward_kernel(const float* __restrict__ grad_pos,
                                           const int* __restrict__ pin2net,
@@ -179,13 +156,10 @@ __global__ void __launch_bounds__(256) hpwl_kernel(const float* __restrict__ px,
                                                    const int* __restrict__ netpin_start, int num_nets,
                                                    const float* __restrict__ net_weights,
                                                    const unsigned char* __restrict__ net_mask,
-                                                   double* __restrict__ total) {
-  int per = gridDim.x * blockDim.x;
-  int iters = (num_nets + per - 1) / per;
-  for (int it = 0; it < iters; ++it) {
-    int i = it * per + blockIdx.x * blockDim.x + threadIdx.x;
-    double c = 0.0;
-    if (i < num_nets && net_mask[i]) {
+                                                   double* __restrict__ partials) {
+  double c = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
+    if (net_mask[i]) {
       float max_x = -FLT_MAX, min_x = FLT_MAX, max_y = -FLT_MAX, min_y = FLT_MAX;
       for (int j = netpin_start[i]; j < netpin_start[i + 1]; ++j) {
         int p = flat_netpin[j];
@@ -197,10 +171,10 @@ __global__ void __launch_bounds__(256) hpwl_kernel(const float* __restrict__ px,
       }
       float h = fsub(fadd(fsub(max_x, min_x), max_y), min_y);
       if (net_weights) h = fmul(h, net_weights[i]);
-      c = (double)h;
+      c += (double)h;
     }
-    block_add_double(c, total);
   }
+  block_partial(c, partials);
 }
 
 __global__ void move_boundary_kernel(float* __restrict__ x, float* __restrict__ y,
@@ -243,19 +217,14 @@ extern "C" int dp_wa_merged_forward(const float* pin_pos, int num_pins, const in
              "dp_wa_merged_forward: null pointer argument");
   DP_REQUIRE(num_pins >= 0 && num_nets >= 0, "dp_wa_merged_forward: negative sizes");
   cudaStream_t s = as_stream(stream);
-  cudaMemsetAsync(wl_f64, 0, sizeof(double), s);
-  if (num_nets > 0) {
-    wa_merged_forward_kernel<<<grid_for(num_nets, 256, 8), 256, 0, s>>>(
-        pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets, net_weights, net_mask,
-        inv_gamma, partial_wl, wl_f64, grad_intermediate, grad_intermediate + num_pins);
-    int rc = check_launch("dp_wa_merged_forward");
-    if (rc) return rc;
-  }
-  if (wl_out) {
-    finish_scalar_kernel<<<1, 1, 0, s>>>(wl_f64, wl_out);
-    return check_launch("dp_wa_merged_forward finish");
-  }
-  return DP_OK;
+  int blocks = num_nets > 0 ? grid_for(num_nets, 256, 8) : 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
+  wa_merged_forward_kernel<<<blocks, 256, 0, s>>>(pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets,
+                                                 net_weights, net_mask, inv_gamma, partial_wl, wl_f64 + 1,
+                                                 grad_intermediate, grad_intermediate + num_pins);
+  int rc = check_launch("dp_wa_merged_forward");
+  if (rc) return rc;
+  return launch_finish_sum(wl_f64, blocks, wl_out, s);
 }
 
 extern "C" int dp_wa_merged_backward(const float* grad_pos, const int* pin2net_map,
@@ -300,19 +269,13 @@ extern "C" int dp_hpwl(const float* pin_pos, int num_pins, const int* flat_netpi
                        dp_stream_t stream) {
   DP_REQUIRE(pin_pos && flat_netpin && netpin_start && net_mask && out_f64, "dp_hpwl: null pointer argument");
   cudaStream_t s = as_stream(stream);
-  cudaMemsetAsync(out_f64, 0, sizeof(double), s);
-  if (num_nets > 0) {
-    hpwl_kernel<<<grid_for(num_nets, 256, 8), 256, 0, s>>>(pin_pos, pin_pos + num_pins, flat_netpin,
-                                                          netpin_start, num_nets, net_weights, net_mask,
-                                                          out_f64);
-    int rc = check_launch("dp_hpwl");
-    if (rc) return rc;
-  }
-  if (out_f32) {
-    finish_scalar_kernel<<<1, 1, 0, s>>>(out_f64, out_f32);
-    return check_launch("dp_hpwl finish");
-  }
-  return DP_OK;
+  int blocks = num_nets > 0 ? grid_for(num_nets, 256, 8) : 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
+  hpwl_kernel<<<blocks, 256, 0, s>>>(pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets, net_weights,
+                                    net_mask, out_f64 + 1);
+  int rc = check_launch("dp_hpwl");
+  if (rc) return rc;
+  return launch_finish_sum(out_f64, blocks, out_f32, s);
 }
 
 extern "C" int dp_move_boundary(float* pos, int num_nodes, const float* sx, const float* sy, float xl,

@@ -72,7 +72,8 @@ class GPEngine(object):
         self.obj64 = torch.zeros(1, **f64)
         self.hpwl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
         self.hpwl64 = self.hpwl64_buf[0:1]
-        self.ovf2 = torch.zeros(2, **f64)
+        self.ovf2_buf = torch.zeros(REDUCE_DOUBLES, **f64)
+        self.ovf2 = self.ovf2_buf[0:2]
         self.metrics = torch.zeros(8, **f64)
         self.metrics_host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
         self.grad_scale = torch.zeros(1, dtype=torch.float32, device=dev)
@@ -83,8 +84,16 @@ class GPEngine(object):
         self.det = bool(params.deterministic_flag)
         self.scratch = torch.empty(ep.num_bins_x * ep.num_bins_y, dtype=torch.int64, device=dev) if self.det else None
         self.prec = precision_code(ep.precision)
+        # spatial visiting order of the scattered cells (movable block, then filler
+        # block), refreshed every `sort_interval` iterations
+        nm, nf = d.num_movable_nodes, d.num_filler_nodes
+        self.order = torch.cat([torch.arange(nm, device=dev), torch.arange(n - nf, n, device=dev)]).to(torch.int32)
+        self.sort_interval = int(getattr(params, "sort_interval", 10))
+        self.iterations = 0
         self.parity = 0
         self.graphs = {}
+        self.graph_kernels = {}
+        self.kernels_launched = 0  # this library's kernels, graph replays included
         self.pool = None
         self.graph_key = None
         self.trials = 0
@@ -94,10 +103,29 @@ class GPEngine(object):
     # ---------------------------------------------------------------- pieces
     def _density(self, v, num_filler, out):
         ep = self.ep
-        C.density_map_into(v, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio,
-                           ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl), float(ep.xh), float(ep.yh),
-                           float(ep.bin_size_x), float(ep.bin_size_y), ep.num_movable_nodes, num_filler,
-                           ep.num_bins_x, ep.num_bins_y, ep.sorted_node_map, int(self.det), self.scratch, out)
+        count = ep.num_movable_nodes + (num_filler if num_filler else 0)
+        C.density_map_ordered_into(v, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y,
+                                   ep.ratio, ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
+                                   float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
+                                   ep.num_bins_x, ep.num_bins_y, self.order, count, int(self.det), self.scratch, out)
+
+    def refresh_order(self, v):
+        """Sort movable and filler cells by 16x16-bin tile, then by bin inside the
+        tile (keeps each scatter block's cells on a compact patch of bins)."""
+        d, ep = self.design, self.ep
+        n, nm, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+        with torch.no_grad():
+            cx = v[:n] + 0.5 * self.data.node_size_x
+            cy = v[n:] + 0.5 * self.data.node_size_y
+            kx = ((cx - ep.xl) * (1.0 / ep.bin_size_x)).clamp_(0, ep.num_bins_x - 1).to(torch.int64)
+            hy = ((cy - ep.yl) * (1.0 / ep.bin_size_y)).clamp_(0, ep.num_bins_y - 1).to(torch.int64)
+            tiles_y = (ep.num_bins_y + 15) >> 4
+            key = (((kx >> 4) * tiles_y + (hy >> 4)) << 8) | ((kx & 15) << 4) | (hy & 15)
+            om = torch.argsort(key[:nm]).to(torch.int32)
+            self.order[:nm].copy_(om)
+            if nf:
+                of = torch.argsort(key[n - nf:]).to(torch.int32).add_(n - nf)
+                self.order[nm:].copy_(of)
 
     def wirelength(self, v):
         """WA forward at node positions v: fp64 total in self.wl64, per-slot gradient in self.gi."""
@@ -150,7 +178,7 @@ class GPEngine(object):
                     dc.net_mask_all, self.hpwl64_buf)
         self._density(v, 0, self.omap)
         ba = self.ovf_op.bin_size_x * self.ovf_op.bin_size_y
-        C.density_overflow_into(self.omap, float(self.ovf_op.target_density * ba), float(ba), self.ovf2)
+        C.density_overflow_into(self.omap, float(self.ovf_op.target_density * ba), float(ba), self.ovf2_buf)
 
     def move_boundary(self, v):
         d = self.design
@@ -212,6 +240,13 @@ class GPEngine(object):
         torch.cat([self.hpwl64, self.ovf2, self.state[NS_ACCEPT:NS_ACCEPT + 1], self.state[NS_ALPHA:NS_ALPHA + 1],
                    self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
 
+    def nesterov_trial_only(self, p):
+        """The trial-point kernel alone (used for per-kernel timing)."""
+        d = self.design
+        C.nesterov_trial(self.V[p], self.G[p], self.U[p], self.U[1 - p], self.V[1 - p], self.state,
+                         self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
+                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+
     def _body(self, p, with_eval):
         if with_eval:
             self.move_boundary(self.V[p])
@@ -231,8 +266,10 @@ class GPEngine(object):
                 self.state.copy_(saved)
             torch.cuda.current_stream().wait_stream(s)
             g = torch.cuda.CUDAGraph()
+            before = C.launch_count()
             with torch.cuda.graph(g, pool=self.pool):
                 self._body(p, with_eval)
+            self.graph_kernels[key] = C.launch_count() - before
             if self.pool is None:
                 self.pool = g.pool()
             self.graphs[key] = g
@@ -241,8 +278,11 @@ class GPEngine(object):
     def _run(self, p, with_eval):
         if self.use_graphs:
             self._graph(p, with_eval).replay()
+            self.kernels_launched += self.graph_kernels[(p, with_eval)]
         else:
+            before = C.launch_count()
             self._body(p, with_eval)
+            self.kernels_launched += C.launch_count() - before
         self.metrics_host.copy_(self.metrics, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.metrics_host.numpy().copy()
@@ -260,6 +300,9 @@ class GPEngine(object):
         (<= 10).  Returns (hpwl, overflow / total movable area, max_density, objective, trials)."""
         self._check_graph_key()
         p = self.parity
+        if self.sort_interval > 0 and self.iterations % self.sort_interval == 0:
+            self.refresh_order(self.V[p])
+        self.iterations += 1
         mh = self._run(p, True)
         hpwl, ovf, maxd = mh[M_HPWL], mh[M_OVF], mh[M_MAXD]
         trials = 1
@@ -267,6 +310,7 @@ class GPEngine(object):
             mh = self._run(p, False)
             trials += 1
         C.nesterov_advance(self.state)
+        self.kernels_launched += 1
         self.parity = 1 - p
         self.trials += trials
         return (float(hpwl), float(ovf) / self.design.total_movable_node_area, float(maxd), float(mh[M_OBJ]), trials)

@@ -89,6 +89,23 @@ int dp_density_map_fx64(const float* pos, int num_nodes,
                         const int* sorted_node_map, int fraction_bits,
                         int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
 
+/* Order-driven triangle scatter: the nodes order[0..count) (movable and/or
+ * filler indices, any order) are added onto initial_density_map (may be NULL =
+ * zeros).  Same arithmetic as dp_density_map_f32 / _fx64; blocks of consecutive
+ * cells accumulate in a shared-memory tile over their bin bounding box, so a
+ * spatial order turns most global atomics into shared ones.  deterministic != 0
+ * selects the int64 fixed-point path (scratch_fixed [num_bins] required). */
+int dp_density_map_ordered(const float* pos, int num_nodes,
+                           const float* node_size_x_clamped, const float* node_size_y_clamped,
+                           const float* offset_x, const float* offset_y, const float* ratio,
+                           const float* initial_density_map,
+                           float xl, float yl, float xh, float yh,
+                           float bin_size_x, float bin_size_y,
+                           float inv_bin_size_x, float inv_bin_size_y,
+                           int num_bins_x, int num_bins_y,
+                           const int* order, int count, int deterministic, int fraction_bits,
+                           int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
+
 /* Exact-overlap fixed-cell map (electric_potential/src/electric_density_map_cuda.cpp:139-183,
  * CPU electric_potential/src/electric_density_map.cpp:155-213): nodes
  * [num_movable_nodes, num_movable_nodes+num_terminals), fixed_node_flag=true,
@@ -119,8 +136,9 @@ int dp_density_map_exact(const float* pos, int num_nodes,
                          float* density_map, dp_stream_t stream);
 
 /* Overflow evaluation (electric_potential/electric_overflow.py:260-278):
- * overflow_out = sum(max(D - target_area, 0)) and max_density_out = max(D)/bin_area,
- * both accumulated in fp64; out_f32 (optional, 2 floats) receives them rounded. */
+ * out2_f64[0] = sum(max(D - target_area, 0)), out2_f64[1] = max(D)/bin_area, in fp64
+ * with a fixed-order (reproducible) sum; out2_f64 holds DP_REDUCE_DOUBLES doubles,
+ * [2..] are scratch.  out_f32 (optional, 2 floats) receives both rounded. */
 int dp_density_overflow(const float* density_map, int num_bins, double target_area,
                         double bin_area, double* out2_f64, float* out2_f32,
                         dp_stream_t stream);
@@ -188,8 +206,9 @@ int dp_prepare_operand(int precision, const float* x, size_t n, float scale,
  *       CPU weighted_average_wirelength/src/weighted_average_wirelength_merged.cpp:31-231) ----
  * forward: per masked net, x and y: max/min, exp sums, partial WL and the per-pin
  * gradient grad_intermediate [2*num_pins] (unmasked nets' pins are left 0 --
- * the caller zero-fills).  wl_out[0] = sum_e w_e * partial_e (fp64 accumulate).
- * partial_wl: caller scratch [num_nets] or NULL. */
+ * the caller zero-fills).  wl_out_f64 holds DP_REDUCE_DOUBLES doubles: [0] =
+ * sum_e w_e * partial_e (fixed-order fp64 sum), [1..] scratch; wl_out (optional)
+ * receives it rounded.  partial_wl: per-net weighted WL [num_nets] or NULL. */
 int dp_wa_merged_forward(const float* pin_pos, int num_pins,
                          const int* flat_netpin, const int* netpin_start, int num_nets,
                          const float* net_weights, const unsigned char* net_mask,
@@ -212,7 +231,8 @@ int dp_pin_pos_backward(const float* grad_pin_pos, int num_pins,
                         const int* flat_node2pin_map, const int* flat_node2pin_start_map,
                         int num_physical_nodes, int num_nodes, float* grad_pos,
                         dp_stream_t stream);
-/* hpwl/src/hpwl_cuda_kernel.cu:10-39 (net-by-net), fp64 total; out_f32 optional */
+/* hpwl/src/hpwl_cuda_kernel.cu:10-39 (net-by-net); out_f64 holds DP_REDUCE_DOUBLES
+ * doubles, [0] = fixed-order fp64 total; out_f32 optional */
 int dp_hpwl(const float* pin_pos, int num_pins, const int* flat_netpin,
             const int* netpin_start, int num_nets, const float* net_weights,
             const unsigned char* net_mask, double* out_f64, float* out_f32,
