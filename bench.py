@@ -138,13 +138,19 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(v, world):
+def max_over_ranks(v, world, device="cuda"):
+    """Max of a per-rank float over all ranks (NCCL on the GPU path, gloo on CPU)."""
     if world == 1:
         return v
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(steps, world, ms_max):
+    """Whole-job iterations/s of `world` independent replicas timed by the slowest rank."""
+    return world * steps / (ms_max / 1000.0)
 
 
 # ------------------------------------------------------------------ our arm
@@ -168,6 +174,11 @@ class TimedRun(object):
         pos = self.placer.pos[0]
         host_pos = torch.empty(pos.numel(), dtype=pos.dtype, pin_memory=True)
 
+        def trials():
+            st = getattr(self.placer, "stepper", None)
+            eng = getattr(st, "eng", None)
+            return eng.trials if eng is not None else 0
+
         def launches():
             st = getattr(self.placer, "stepper", None)
             eng = getattr(st, "eng", None)
@@ -182,6 +193,7 @@ class TimedRun(object):
                 if clocks is not None:
                     clocks.start()
                 state["launch0"] = launches()
+                state["trials0"] = trials()
                 start.record()
             elif warmup <= it < warmup + steps:
                 if self.e2e:
@@ -195,12 +207,14 @@ class TimedRun(object):
                     end.record()
                     torch.cuda.synchronize()
                     state["launch1"] = launches()
+                    state["trials1"] = trials()
 
         t0 = time.time()
         self.placer(self.params, self.design, max_iterations=warmup + steps, callback=cb)
         wall = time.time() - t0
         ms = start.elapsed_time(end)
         self.launches = state["launch1"] - state["launch0"]
+        self.trials = state.get("trials1", 0) - state.get("trials0", 0)
         self.wall = wall
         return ms
 
@@ -471,13 +485,14 @@ def main():
     ms = run.run(W, K, clocks=clocks)
     clk = clocks.stop() if clocks else None
     ms = max_over_ranks(ms, world)
-    value = world * K / (ms / 1000.0)
+    value = replica_value(K, world, ms)
     launches = run.launches
     # end-to-end through the public API with a host round trip per step
     run_e2e = TimedRun(design, args.precision, world, e2e=True)
     ms_e2e = max_over_ranks(run_e2e.run(W, K), world)
     e2e_value = world * K / (ms_e2e / 1000.0)
-    roof = roofline_entry(kernel_roofline(run.placer, design, peaks), peaks)
+    pieces = kernel_roofline(run.placer, design, peaks)
+    roof = roofline_entry(pieces, peaks)
     plain = None
     if not args.no_plain and args.precision != "fp32":
         prun = TimedRun(design, "fp32", world)
@@ -509,6 +524,8 @@ def main():
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": run_e2e.h2d,
                         "d2h_bytes_per_step": run_e2e.d2h},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "kernel_ms": {k: round(v[0], 4) for k, v in pieces.items()},
+                "trials_per_step": round(run.trials / max(K, 1), 3),
                 "plain_fp32": plain}
         print(json.dumps(line))
     if world > 1:

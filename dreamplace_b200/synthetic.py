@@ -193,6 +193,25 @@ def _make_nets(rng, num_nets, num_physical, window=500, local_frac=0.7, p=0.45, 
 
 def _finish(name, seed, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, mac_y, mac_w, mac_h,
             num_nets, num_bins, target_density, rng):
+    nphys = mov_w.shape[0] + mac_w.shape[0]
+    size_x = np.concatenate([mov_w, mac_w]).astype(np.float32)
+    size_y = np.concatenate([mov_h, mac_h]).astype(np.float32)
+    start, net_of_pin, pin2node = _make_nets(rng, num_nets, nphys)
+    P = pin2node.shape[0]
+    off_x = (rng.random_sample(P) * size_x[pin2node]).astype(np.float32)
+    off_y = (rng.random_sample(P) * size_y[pin2node]).astype(np.float32)
+    d = _finish_from_arrays(name, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, mac_y, mac_w, mac_h, pin2node,
+                            net_of_pin, start, off_x, off_y, np.ones(num_nets, dtype=np.float32), num_bins,
+                            target_density)
+    d.seed = seed
+    return d
+
+
+def _finish_from_arrays(name, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, mac_y, mac_w, mac_h, pin2node,
+                        net_of_pin, start, off_x, off_y, net_weights, num_bins, target_density):
+    """Design from netlist arrays (pins in net order): node/pin CSR maps, areas,
+    utilisation, target density, movable macros and fillers as the reference's
+    PlaceDB derives them."""
     m = mov_w.shape[0]
     f_num = mac_w.shape[0]
     nphys = m + f_num
@@ -202,13 +221,9 @@ def _finish(name, seed, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, mac_y, 
     node_y = np.zeros(nphys, dtype=np.float32)
     node_x[m:] = mac_x
     node_y[m:] = mac_y
-
-    start, net_of_pin, pin2node = _make_nets(rng, num_nets, nphys)
     P = pin2node.shape[0]
-    off_x = (rng.random_sample(P) * size_x[pin2node]).astype(np.float32)
-    off_y = (rng.random_sample(P) * size_y[pin2node]).astype(np.float32)
+    num_nets = start.shape[0] - 1
     flat_net2pin = np.arange(P, dtype=np.int32)
-    # node -> pin CSR (stable order of pin ids)
     order = np.argsort(pin2node, kind="stable").astype(np.int32)
     counts = np.bincount(pin2node, minlength=nphys)
     node_start = np.zeros(nphys + 1, dtype=np.int32)
@@ -245,14 +260,15 @@ def _finish(name, seed, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, mac_y, 
         row_height=float(row_height), site_width=1.0,
         num_movable_nodes=m, num_terminals=f_num, num_filler_nodes=n_fill,
         node_size_x=size_x, node_size_y=size_y, node_x=node_x, node_y=node_y,
-        pin_offset_x=off_x, pin_offset_y=off_y, pin2node_map=pin2node, pin2net_map=net_of_pin,
-        flat_net2pin_map=flat_net2pin, flat_net2pin_start_map=start,
+        pin_offset_x=np.asarray(off_x, np.float32), pin_offset_y=np.asarray(off_y, np.float32),
+        pin2node_map=np.asarray(pin2node, np.int32), pin2net_map=np.asarray(net_of_pin, np.int32),
+        flat_net2pin_map=flat_net2pin, flat_net2pin_start_map=np.asarray(start, np.int32),
         flat_node2pin_map=order, flat_node2pin_start_map=node_start,
-        net_weights=np.ones(num_nets, dtype=np.float32),
+        net_weights=np.asarray(net_weights, np.float32),
         num_bins_x=num_bins, num_bins_y=num_bins, target_density=float(target_density),
         total_movable_node_area=total_movable_node_area,
         total_fixed_node_area=total_fixed_node_area, total_space_area=total_space_area,
-        movable_macro_mask=movable_macro_mask, seed=seed,
+        movable_macro_mask=movable_macro_mask, seed=0,
         extra={"filler_size": (filler_w, filler_h), "cell_utilization": cell_utilization})
 
 
