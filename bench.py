@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host round-trip run (profiling)")
+    ap.add_argument("--no-roofline", action="store_true", help="skip the per-kernel timing (profiling)")
     return ap.parse_args()
 
 
@@ -488,11 +490,14 @@ def main():
     value = replica_value(K, world, ms)
     launches = run.launches
     # end-to-end through the public API with a host round trip per step
-    run_e2e = TimedRun(design, args.precision, world, e2e=True)
-    ms_e2e = max_over_ranks(run_e2e.run(W, K), world)
-    e2e_value = world * K / (ms_e2e / 1000.0)
-    pieces = kernel_roofline(run.placer, design, peaks)
-    roof = roofline_entry(pieces, peaks)
+    e2e = None
+    if not args.no_e2e:
+        run_e2e = TimedRun(design, args.precision, world, e2e=True)
+        ms_e2e = max_over_ranks(run_e2e.run(W, K), world)
+        e2e = {"value": round(replica_value(K, world, ms_e2e), 3), "unit": UNIT,
+               "h2d_bytes_per_step": run_e2e.h2d, "d2h_bytes_per_step": run_e2e.d2h}
+    pieces = {} if args.no_roofline else kernel_roofline(run.placer, design, peaks)
+    roof = roofline_entry(pieces, peaks) if pieces else None
     plain = None
     if not args.no_plain and args.precision != "fp32":
         prun = TimedRun(design, "fp32", world)
@@ -521,8 +526,7 @@ def main():
                               design.num_nets, design.num_pins, design.num_bins_x, design.num_bins_y),
                            "dct_precision": args.precision, "parallelism": "replicas%d" % world,
                            "l2": "per-iteration working set > 126 MB L2, no flush"},
-                "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": run_e2e.h2d,
-                        "d2h_bytes_per_step": run_e2e.d2h},
+                "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "kernel_ms": {k: round(v[0], 4) for k, v in pieces.items()},
                 "trials_per_step": round(run.trials / max(K, 1), 3),

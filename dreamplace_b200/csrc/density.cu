@@ -181,8 +181,45 @@ __global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(Triangle
     for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = 0;
     __syncthreads();
   }
+  // Dense boxes (more cell-bin updates than bins, e.g. the clustered start of
+  // GP) first combine the lanes of a warp that hit the same bin, so each bin
+  // takes one shared atomic per warp instead of one per lane.
+  const bool combine = use_tile && (long long)W * H * 4 < (long long)kTileCells;
 #pragma unroll
   for (int c = 0; c < kTileCellsPerThread; ++c) {
+    const int nk = max(kx1[c] - kx0[c], 0), nh = max(hy1[c] - hy0[c], 0);
+    const int trips = nk * nh;
+    if (combine) {
+      int max_trips = trips;
+      for (int o = 16; o > 0; o >>= 1) max_trips = max(max_trips, __shfl_xor_sync(0xffffffffu, max_trips, o));
+      float pxr = 0.f;
+      int cur_k = -1;
+      for (int t = 0; t < max_trips; ++t) {
+        const bool live = t < trips;
+        const unsigned active = __ballot_sync(0xffffffffu, live);
+        if (live) {
+          const int k = kx0[c] + t / nh, h = hy0[c] + t % nh;
+          if (k != cur_k) {
+            pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
+            cur_k = k;
+          }
+          const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
+          const int slot = (k - bk0) * H + (h - bh0);
+          const unsigned peers = __match_any_sync(active, slot);
+          const int leader = __ffs(peers) - 1;
+          const Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
+          Acc sum = v;  // peers' own values are shuffled, never the running sum
+          unsigned rest = peers & (peers - 1);
+          while (rest) {
+            const int src = __ffs(rest) - 1;
+            rest &= rest - 1;
+            sum += __shfl_sync(peers, v, src);
+          }
+          if ((int)(threadIdx.x & 31) == leader) atomicAdd(&tile[slot], sum);
+        }
+      }
+      continue;
+    }
     for (int k = kx0[c]; k < kx1[c]; ++k) {
       float px = triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx);
       float pxr = fmul(px, rr[c]);

@@ -38,6 +38,12 @@ __device__ __forceinline__ void block_partial2(double a, double b, double* parti
 }
 
 // ---------------------------------------------------------------- WA fused
+// Nets of degree <= kWaCache keep their pin coordinates and the four
+// exponentials per pin in registers between the three passes (max/min, sums,
+// gradient), so the gather and expf run once per pin; larger nets re-read.
+// The arithmetic is the same either way.
+constexpr int kWaCache = 6;
+
 __global__ void __launch_bounds__(256) wa_slot_forward_kernel(
     const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ slot_node,
     const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ netpin_start,
@@ -47,62 +53,95 @@ __global__ void __launch_bounds__(256) wa_slot_forward_kernel(
   const float inv_gamma = *inv_gamma_p;
   double contrib = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
-    {
-      int b = netpin_start[i], e = netpin_start[i + 1];
-      if (net_mask[i]) {
-        float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
-        for (int j = b; j < e; ++j) {
-          int n = slot_node[j];
-          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-          x_max = fmaxf(xx, x_max);
-          x_min = fminf(xx, x_min);
-          y_max = fmaxf(yy, y_max);
-          y_min = fminf(yy, y_min);
-        }
-        float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
-        for (int j = b; j < e; ++j) {
-          int n = slot_node[j];
-          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-          float ex = expf(fmul(fsub(xx, x_max), inv_gamma));
-          float enx = expf(fmul(fsub(x_min, xx), inv_gamma));
-          xe_p = fadd(xe_p, fmul(xx, ex));
-          xe_n = fadd(xe_n, fmul(xx, enx));
-          e_p = fadd(e_p, ex);
-          e_n = fadd(e_n, enx);
-          float ey = expf(fmul(fsub(yy, y_max), inv_gamma));
-          float eny = expf(fmul(fsub(y_min, yy), inv_gamma));
-          ye_p = fadd(ye_p, fmul(yy, ey));
-          ye_n = fadd(ye_n, fmul(yy, eny));
-          f_p = fadd(f_p, ey);
-          f_n = fadd(f_n, eny);
-        }
-        float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                        __fdiv_rn(ye_n, f_n));
-        contrib += (double)(net_weights ? fmul(wl, net_weights[i]) : wl);
-        float b_x = __fdiv_rn(inv_gamma, e_p);
-        float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
-        float b_nx = __fdiv_rn(-inv_gamma, e_n);
-        float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
-        float b_y = __fdiv_rn(inv_gamma, f_p);
-        float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
-        float b_ny = __fdiv_rn(-inv_gamma, f_n);
-        float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
-        for (int j = b; j < e; ++j) {
-          int n = slot_node[j];
-          float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-          float ex = expf(fmul(fsub(xx, x_max), inv_gamma));
-          float enx = expf(fmul(fsub(x_min, xx), inv_gamma));
-          gx[j] = fsub(fmul(fadd(a_x, fmul(b_x, xx)), ex), fmul(fadd(a_nx, fmul(b_nx, xx)), enx));
-          float ey = expf(fmul(fsub(yy, y_max), inv_gamma));
-          float eny = expf(fmul(fsub(y_min, yy), inv_gamma));
-          gy[j] = fsub(fmul(fadd(a_y, fmul(b_y, yy)), ey), fmul(fadd(a_ny, fmul(b_ny, yy)), eny));
-        }
-      } else {
-        for (int j = b; j < e; ++j) {
-          gx[j] = 0.f;
-          gy[j] = 0.f;
-        }
+    const int b = netpin_start[i], e = netpin_start[i + 1];
+    const int deg = e - b;
+    if (!net_mask[i]) {
+      for (int j = b; j < e; ++j) {
+        gx[j] = 0.f;
+        gy[j] = 0.f;
       }
+      continue;
+    }
+    float cx[kWaCache], cy[kWaCache];
+    float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
+#pragma unroll
+    for (int q = 0; q < kWaCache; ++q) {
+      if (q < deg) {
+        const int n = slot_node[b + q];
+        cx[q] = fadd(slot_offx[b + q], x[n]);
+        cy[q] = fadd(slot_offy[b + q], y[n]);
+        x_max = fmaxf(cx[q], x_max);
+        x_min = fminf(cx[q], x_min);
+        y_max = fmaxf(cy[q], y_max);
+        y_min = fminf(cy[q], y_min);
+      }
+    }
+    for (int j = b + kWaCache; j < e; ++j) {
+      const int n = slot_node[j];
+      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+      x_max = fmaxf(xx, x_max);
+      x_min = fminf(xx, x_min);
+      y_max = fmaxf(yy, y_max);
+      y_min = fminf(yy, y_min);
+    }
+    float ex[kWaCache], enx[kWaCache], ey[kWaCache], eny[kWaCache];
+    float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
+#pragma unroll
+    for (int q = 0; q < kWaCache; ++q) {
+      if (q < deg) {
+        ex[q] = expf(fmul(fsub(cx[q], x_max), inv_gamma));
+        enx[q] = expf(fmul(fsub(x_min, cx[q]), inv_gamma));
+        xe_p = fadd(xe_p, fmul(cx[q], ex[q]));
+        xe_n = fadd(xe_n, fmul(cx[q], enx[q]));
+        e_p = fadd(e_p, ex[q]);
+        e_n = fadd(e_n, enx[q]);
+        ey[q] = expf(fmul(fsub(cy[q], y_max), inv_gamma));
+        eny[q] = expf(fmul(fsub(y_min, cy[q]), inv_gamma));
+        ye_p = fadd(ye_p, fmul(cy[q], ey[q]));
+        ye_n = fadd(ye_n, fmul(cy[q], eny[q]));
+        f_p = fadd(f_p, ey[q]);
+        f_n = fadd(f_n, eny[q]);
+      }
+    }
+    for (int j = b + kWaCache; j < e; ++j) {
+      const int n = slot_node[j];
+      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+      const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
+      xe_p = fadd(xe_p, fmul(xx, a1));
+      xe_n = fadd(xe_n, fmul(xx, a2));
+      e_p = fadd(e_p, a1);
+      e_n = fadd(e_n, a2);
+      const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
+      ye_p = fadd(ye_p, fmul(yy, a3));
+      ye_n = fadd(ye_n, fmul(yy, a4));
+      f_p = fadd(f_p, a3);
+      f_n = fadd(f_n, a4);
+    }
+    const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                          __fdiv_rn(ye_n, f_n));
+    contrib += (double)(net_weights ? fmul(wl, net_weights[i]) : wl);
+    const float b_x = __fdiv_rn(inv_gamma, e_p);
+    const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
+    const float b_nx = __fdiv_rn(-inv_gamma, e_n);
+    const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
+    const float b_y = __fdiv_rn(inv_gamma, f_p);
+    const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
+    const float b_ny = __fdiv_rn(-inv_gamma, f_n);
+    const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
+#pragma unroll
+    for (int q = 0; q < kWaCache; ++q) {
+      if (q < deg) {
+        gx[b + q] = fsub(fmul(fadd(a_x, fmul(b_x, cx[q])), ex[q]), fmul(fadd(a_nx, fmul(b_nx, cx[q])), enx[q]));
+        gy[b + q] = fsub(fmul(fadd(a_y, fmul(b_y, cy[q])), ey[q]), fmul(fadd(a_ny, fmul(b_ny, cy[q])), eny[q]));
+      }
+    }
+    for (int j = b + kWaCache; j < e; ++j) {
+      const int n = slot_node[j];
+      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
+      const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
+      gx[j] = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
+      const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
+      gy[j] = fsub(fmul(fadd(a_y, fmul(b_y, yy)), a3), fmul(fadd(a_ny, fmul(b_ny, yy)), a4));
     }
   }
   block_partial(contrib, partials);
