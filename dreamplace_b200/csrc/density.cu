@@ -16,6 +16,7 @@
 // one atomic, which removes most same-address serialisation when cells are
 // clustered (the GP starts with every movable cell at the die centre).
 #include <climits>
+#include <mutex>
 #include <type_traits>
 #include "reduce.cuh"
 
@@ -608,4 +609,62 @@ extern "C" int dp_density_map_ordered(const float* pos, int num_nodes, const flo
   if (blocks == 0) return DP_OK;
   tiled_scatter_kernel<false><<<blocks, kTileThreads, kTileSmemBytes, s>>>(a, order, count, 0.f, out, nullptr);
   return check_launch("dp_density_map_ordered scatter");
+}
+
+// ---------------------------------------------------------------- allocation-free variant
+// Some callers of this library cannot allocate device memory at the point
+// where they place: hosts that reserve the whole GPU up front under a fixed
+// memory budget, code running inside another framework's stream capture
+// (where cudaMalloc is not permitted and may synchronise the device), and
+// FFI hosts (Go / Java / JavaScript bindings) that never link the CUDA
+// allocator.  dp_density_map_fx64_noalloc serves them: the deterministic
+// scatter's int64 scratch map lives in the file-scope device array below, of
+// at most DP_NOALLOC_MAX_BINS bins, which every GPU that loads the library
+// holds until the process exits.
+static __device__ __align__(256) unsigned long long g_noalloc_fixed_map[DP_NOALLOC_MAX_BINS];
+
+// Host code may not use g_noalloc_fixed_map as an address: the symbol names a
+// host-side stand-in.  The device address is looked up once per device, with
+// that device current, and cached.
+static int noalloc_scratch_address(int64_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("dp_density_map_fx64_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  constexpr int kMaxDevices = 64;
+  DP_REQUIRE(dev >= 0 && dev < kMaxDevices, "dp_density_map_fx64_noalloc: device ordinal %d out of range", dev);
+  static void* addr[kMaxDevices] = {};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_fixed_map);
+    if (e != cudaSuccess || !p) {
+      set_error("dp_density_map_fx64_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return DP_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = static_cast<int64_t*>(addr[dev]);
+  return DP_OK;
+}
+
+extern "C" int dp_density_map_fx64_noalloc(const float* pos, int num_nodes, const float* sx, const float* sy,
+                                           const float* ox, const float* oy, const float* ratio, const float* init,
+                                           float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
+                                           float iby, int nm, int nf, int nbx, int nby, const int* sorted,
+                                           int fraction_bits, float* out, dp_stream_t stream) {
+  DP_REQUIRE(nbx > 0 && nby > 0, "dp_density_map_fx64_noalloc: bad bin grid %dx%d", nbx, nby);
+  DP_REQUIRE((long long)nbx * nby <= DP_NOALLOC_MAX_BINS,
+             "dp_density_map_fx64_noalloc: %d x %d bins exceed the built-in scratch of %d bins; "
+             "use dp_density_map_fx64 with a caller-owned scratch map",
+             nbx, nby, (int)DP_NOALLOC_MAX_BINS);
+  int64_t* scratch = nullptr;
+  int rc = noalloc_scratch_address(&scratch);
+  if (rc) return rc;
+  // the scratch is zero-filled inside dp_density_map_fx64 before the scatter
+  return dp_density_map_fx64(pos, num_nodes, sx, sy, ox, oy, ratio, init, xl, yl, xh, yh, bsx, bsy, ibx, iby, nm,
+                             nf, nbx, nby, sorted, fraction_bits, scratch, out, stream);
 }

@@ -29,7 +29,8 @@ typedef struct CUstream_st* dp_stream_t; /* same type as cudaStream_t */
 
 enum {
   DP_REDUCE_DOUBLES = 1280,         /* 1 result + per-block partials of a fixed-order fp64 sum */
-  DP_NESTEROV_STATE_DOUBLES = 8
+  DP_NESTEROV_STATE_DOUBLES = 8,
+  DP_NOALLOC_MAX_BINS = 1048576     /* 1024 x 1024: scratch of dp_density_map_fx64_noalloc */
 };
 
 enum {
@@ -88,6 +89,28 @@ int dp_density_map_fx64(const float* pos, int num_nodes,
                         int num_bins_x, int num_bins_y,
                         const int* sorted_node_map, int fraction_bits,
                         int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
+
+/* No counterpart in the reference.  Same result as dp_density_map_fx64, for
+ * callers that cannot allocate device memory (a host that reserved the GPU
+ * under a fixed budget, code inside another framework's stream capture where
+ * cudaMalloc is not allowed, FFI hosts without the CUDA allocator).  The int64
+ * scratch map is a built-in device array of DP_NOALLOC_MAX_BINS bins (8 MiB,
+ * held by every GPU that loads the library until exit); larger grids are
+ * rejected with DP_ERR_INVALID_ARGUMENT.  The first call on a device looks up
+ * the array's device address, so make that first call before any stream
+ * capture.  All calls share the one array (it keeps the last call's integer
+ * map): calls that overlap on the GPU -- different streams or threads -- race. */
+int dp_density_map_fx64_noalloc(const float* pos, int num_nodes,
+                                const float* node_size_x_clamped, const float* node_size_y_clamped,
+                                const float* offset_x, const float* offset_y, const float* ratio,
+                                const float* initial_density_map,
+                                float xl, float yl, float xh, float yh,
+                                float bin_size_x, float bin_size_y,
+                                float inv_bin_size_x, float inv_bin_size_y,
+                                int num_movable_nodes, int num_filler_nodes,
+                                int num_bins_x, int num_bins_y,
+                                const int* sorted_node_map, int fraction_bits,
+                                float* density_map, dp_stream_t stream);
 
 /* Order-driven triangle scatter: the nodes order[0..count) (movable and/or
  * filler indices, any order) are added onto initial_density_map (may be NULL =
