@@ -430,6 +430,47 @@ void electric_force_into(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at
                             num_filler, (const int*)ovp(sorted_node_map), (float)scale, ptr<float>(out), cur_stream()));
 }
 
+at::Tensor plan_net_chunks(at::Tensor netpin_start_cpu, int max_pins) {
+  TORCH_CHECK(!netpin_start_cpu.is_cuda() && netpin_start_cpu.scalar_type() == at::kInt, "netpin_start must be int32 on CPU");
+  auto ns = netpin_start_cpu.contiguous();
+  int num_nets = ns.numel() - 1;
+  auto out = at::empty({num_nets + 1}, ns.options());
+  int count = 0;
+  DP_CALL(dp_plan_net_chunks(ns.data_ptr<int>(), num_nets, max_pins, out.data_ptr<int>(), &count));
+  return out.narrow(0, 0, count + 1).clone();
+}
+
+void wa_chunk_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
+                      at::Tensor slot_net, at::Tensor netpin_start, at::Tensor chunk_net,
+                      c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor inv_gamma,
+                      at::Tensor csr_pos, at::Tensor wl_f64, at::Tensor grad_node_order) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(chunk_net); CHECK_I32(csr_pos); CHECK_F32(grad_node_order);
+  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
+  DP_CALL(dp_wa_chunk_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
+                              ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(netpin_start), ptr<int>(chunk_net),
+                              chunk_net.numel() - 1, (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
+                              ptr<float>(inv_gamma), ptr<int>(csr_pos), ptr<double>(wl_f64),
+                              ptr<float>(grad_node_order), slot_node.numel(), cur_stream()));
+}
+
+void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy, at::Tensor slot_net,
+                at::Tensor netpin_start, at::Tensor chunk_net, c10::optional<at::Tensor> net_weights,
+                at::Tensor net_mask, at::Tensor out_f64) {
+  TORCH_CHECK(out_f64.scalar_type() == at::kDouble && out_f64.numel() >= DP_REDUCE_DOUBLES, "out_f64 too small");
+  DP_CALL(dp_hpwl_chunk(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
+                        ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(netpin_start), ptr<int>(chunk_net),
+                        chunk_net.numel() - 1, (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
+                        ptr<double>(out_f64), cur_stream()));
+}
+
+void node_pin_sum(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor grad_pos, int num_movable,
+                  int accumulate, at::Tensor grad_out) {
+  CHECK_F32(grad_node_order); CHECK_F32(grad_out); CHECK_I32(node_start);
+  DP_CALL(dp_node_pin_sum(ptr<float>(grad_node_order), grad_node_order.numel() / 2, ptr<int>(node_start),
+                          ptr<float>(grad_pos), num_movable, grad_out.numel() / 2, accumulate, ptr<float>(grad_out),
+                          cur_stream()));
+}
+
 uint64_t launch_count() { return dp_launch_count(); }
 
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
@@ -462,6 +503,10 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);
   m.def("density_map_ordered_into", &density_map_ordered_into);
+  m.def("plan_net_chunks", &plan_net_chunks);
+  m.def("wa_chunk_forward", &wa_chunk_forward);
+  m.def("hpwl_chunk", &hpwl_chunk);
+  m.def("node_pin_sum", &node_pin_sum);
   m.def("electric_force_into", &electric_force_into);
   m.def("version", &dp_version);
 }

@@ -17,6 +17,7 @@
 //    and both step-size norms (fp64) are two streaming passes over the
 //    position / gradient vectors, and a one-thread kernel finishes the step
 //    size, the backtracking test and the momentum scalars on the device.
+#include <climits>
 #include "reduce.cuh"
 
 namespace dpb {
@@ -419,4 +420,319 @@ extern "C" int dp_nesterov_advance(double* state, dp_stream_t stream) {
   DP_REQUIRE(state, "dp_nesterov_advance: null state");
   nesterov_advance_kernel<<<1, 1, 0, as_stream(stream)>>>(state);
   return check_launch("dp_nesterov_advance");
+}
+
+// ============================================================== warp-per-chunk WA / HPWL
+// Nets are packed (in order) into chunks of at most 32 pins (host planner
+// dp_plan_net_chunks); a net with more than 32 pins is a chunk of its own.
+// One warp per chunk, one lane per pin: the pin gather is issued by all
+// lanes at once, and every per-net max / min / sum is a segmented shuffle
+// reduction over the lanes of that net (log2(32) steps), so no lane waits on
+// another net's degree.  The WA gradient is written to the pin's position in
+// node-CSR order (csr_pos), which makes the pin -> node sum of the backward a
+// contiguous streaming read.
+namespace dpb {
+
+struct SegInfo {
+  int end;   // last lane of this lane's net within the warp
+  int head;  // first lane of this lane's net within the warp
+};
+
+template <typename Op>
+__device__ __forceinline__ float seg_reduce(float v, const SegInfo& sg, int lane, Op op) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    float u = __shfl_down_sync(0xffffffffu, v, o);
+    if (lane + o <= sg.end) v = op(v, u);
+  }
+  return __shfl_sync(0xffffffffu, v, sg.head);  // the head lane holds its whole net
+}
+
+struct MaxOp { __device__ float operator()(float a, float b) const { return fmaxf(a, b); } };
+struct MinOp { __device__ float operator()(float a, float b) const { return fminf(a, b); } };
+struct AddOp { __device__ float operator()(float a, float b) const { return fadd(a, b); } };
+
+__device__ __forceinline__ float warp_all(float v, int kind) {
+  for (int o = 16; o > 0; o >>= 1) {
+    float u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = kind == 0 ? fmaxf(v, u) : kind == 1 ? fminf(v, u) : fadd(v, u);
+  }
+  return v;
+}
+
+// per-lane segment info from the lane's net id (net ids of a chunk are
+// non-decreasing across lanes); lanes past the chunk get net = INT_MAX
+__device__ __forceinline__ SegInfo segment_of(int net, int lane) {
+  unsigned same = __match_any_sync(0xffffffffu, net);
+  SegInfo sg;
+  sg.head = __ffs(same) - 1;
+  sg.end = 31 - __clz(same);
+  return sg;
+}
+
+template <bool kGrad>
+__global__ void __launch_bounds__(256) wa_chunk_kernel(
+    const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ slot_node,
+    const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ slot_net,
+    const int* __restrict__ netpin_start, const int* __restrict__ chunk_net, int num_chunks,
+    const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
+    const float* __restrict__ inv_gamma_p, const int* __restrict__ csr_pos, double* __restrict__ partials,
+    float* __restrict__ gnx, float* __restrict__ gny) {
+  const float inv_gamma = kGrad ? *inv_gamma_p : 0.f;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double contrib = 0.0;
+  for (int c = warp; c < num_chunks; c += nwarps) {
+    const int n0 = chunk_net[c], n1 = chunk_net[c + 1];
+    const int s0 = netpin_start[n0], s1 = netpin_start[n1];
+    const int np = s1 - s0;
+    if (np <= 32) {
+      const bool valid = lane < np;
+      const int s = s0 + lane;
+      const int net = valid ? slot_net[s] : INT_MAX;
+      const SegInfo sg = segment_of(net, lane);
+      const bool on = valid && net_mask[net];
+      float xx = 0.f, yy = 0.f;
+      if (valid) {
+        const int n = slot_node[s];
+        xx = fadd(slot_offx[s], x[n]);
+        yy = fadd(slot_offy[s], y[n]);
+      }
+      const float x_max = seg_reduce(valid ? xx : -FLT_MAX, sg, lane, MaxOp());
+      const float x_min = seg_reduce(valid ? xx : FLT_MAX, sg, lane, MinOp());
+      const float y_max = seg_reduce(valid ? yy : -FLT_MAX, sg, lane, MaxOp());
+      const float y_min = seg_reduce(valid ? yy : FLT_MAX, sg, lane, MinOp());
+      if (!kGrad) {  // HPWL
+        if (on && lane == sg.head) {
+          float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+          if (net_weights) h = fmul(h, net_weights[net]);
+          contrib += (double)h;
+        }
+        continue;
+      }
+      float ex = 0.f, enx = 0.f, ey = 0.f, eny = 0.f;
+      if (on) {
+        ex = expf(fmul(fsub(xx, x_max), inv_gamma));
+        enx = expf(fmul(fsub(x_min, xx), inv_gamma));
+        ey = expf(fmul(fsub(yy, y_max), inv_gamma));
+        eny = expf(fmul(fsub(y_min, yy), inv_gamma));
+      }
+      const float e_p = seg_reduce(ex, sg, lane, AddOp());
+      const float e_n = seg_reduce(enx, sg, lane, AddOp());
+      const float xe_p = seg_reduce(fmul(xx, ex), sg, lane, AddOp());
+      const float xe_n = seg_reduce(fmul(xx, enx), sg, lane, AddOp());
+      const float f_p = seg_reduce(ey, sg, lane, AddOp());
+      const float f_n = seg_reduce(eny, sg, lane, AddOp());
+      const float ye_p = seg_reduce(fmul(yy, ey), sg, lane, AddOp());
+      const float ye_n = seg_reduce(fmul(yy, eny), sg, lane, AddOp());
+      if (!valid) continue;
+      float gxv = 0.f, gyv = 0.f;
+      if (on) {
+        const float w = net_weights ? net_weights[net] : 1.0f;
+        if (lane == sg.head) {
+          const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                                __fdiv_rn(ye_n, f_n));
+          contrib += (double)(net_weights ? fmul(wl, w) : wl);
+        }
+        const float b_x = __fdiv_rn(inv_gamma, e_p);
+        const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
+        const float b_nx = __fdiv_rn(-inv_gamma, e_n);
+        const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
+        const float b_y = __fdiv_rn(inv_gamma, f_p);
+        const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
+        const float b_ny = __fdiv_rn(-inv_gamma, f_n);
+        const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
+        gxv = fsub(fmul(fadd(a_x, fmul(b_x, xx)), ex), fmul(fadd(a_nx, fmul(b_nx, xx)), enx));
+        gyv = fsub(fmul(fadd(a_y, fmul(b_y, yy)), ey), fmul(fadd(a_ny, fmul(b_ny, yy)), eny));
+        if (net_weights) {  // the backward's net-weight factor, folded in
+          gxv = fmul(gxv, w);
+          gyv = fmul(gyv, w);
+        }
+      }
+      const int q = csr_pos[s];
+      gnx[q] = gxv;
+      gny[q] = gyv;
+    } else {
+      // one net with more than 32 pins: lanes stride over its pins
+      const int net = n0;
+      const bool on = net_mask[net];
+      float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
+      for (int s = s0 + lane; s < s1; s += 32) {
+        const int n = slot_node[s];
+        const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+        x_max = fmaxf(x_max, xx);
+        x_min = fminf(x_min, xx);
+        y_max = fmaxf(y_max, yy);
+        y_min = fminf(y_min, yy);
+      }
+      x_max = warp_all(x_max, 0);
+      x_min = warp_all(x_min, 1);
+      y_max = warp_all(y_max, 0);
+      y_min = warp_all(y_min, 1);
+      if (!kGrad) {
+        if (on && lane == 0) {
+          float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+          if (net_weights) h = fmul(h, net_weights[net]);
+          contrib += (double)h;
+        }
+        continue;
+      }
+      float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
+      for (int s = s0 + lane; s < s1; s += 32) {
+        const int n = slot_node[s];
+        const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+        const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
+        const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
+        xe_p = fadd(xe_p, fmul(xx, a1));
+        xe_n = fadd(xe_n, fmul(xx, a2));
+        e_p = fadd(e_p, a1);
+        e_n = fadd(e_n, a2);
+        ye_p = fadd(ye_p, fmul(yy, a3));
+        ye_n = fadd(ye_n, fmul(yy, a4));
+        f_p = fadd(f_p, a3);
+        f_n = fadd(f_n, a4);
+      }
+      xe_p = warp_all(xe_p, 2); xe_n = warp_all(xe_n, 2); e_p = warp_all(e_p, 2); e_n = warp_all(e_n, 2);
+      ye_p = warp_all(ye_p, 2); ye_n = warp_all(ye_n, 2); f_p = warp_all(f_p, 2); f_n = warp_all(f_n, 2);
+      const float w = net_weights ? net_weights[net] : 1.0f;
+      if (on && lane == 0) {
+        const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                              __fdiv_rn(ye_n, f_n));
+        contrib += (double)(net_weights ? fmul(wl, w) : wl);
+      }
+      const float b_x = __fdiv_rn(inv_gamma, e_p);
+      const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
+      const float b_nx = __fdiv_rn(-inv_gamma, e_n);
+      const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
+      const float b_y = __fdiv_rn(inv_gamma, f_p);
+      const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
+      const float b_ny = __fdiv_rn(-inv_gamma, f_n);
+      const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
+      for (int s = s0 + lane; s < s1; s += 32) {
+        float gxv = 0.f, gyv = 0.f;
+        if (on) {
+          const int n = slot_node[s];
+          const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+          const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
+          const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
+          gxv = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
+          gyv = fsub(fmul(fadd(a_y, fmul(b_y, yy)), a3), fmul(fadd(a_ny, fmul(b_ny, yy)), a4));
+          if (net_weights) {
+            gxv = fmul(gxv, w);
+            gyv = fmul(gyv, w);
+          }
+        }
+        const int q = csr_pos[s];
+        gnx[q] = gxv;
+        gny[q] = gyv;
+      }
+    }
+  }
+  block_partial(contrib, partials);
+}
+
+// node grad (+)= grad_pos[0] * sum of its pins' (weighted) gradients, which
+// sit contiguously in node-CSR order; nodes >= num_movable get 0
+__global__ void node_sum_kernel(const float* __restrict__ gnx, const float* __restrict__ gny,
+                                const int* __restrict__ node_start, const float* __restrict__ grad_p,
+                                int num_movable, int num_nodes, int accumulate, float* __restrict__ out_x,
+                                float* __restrict__ out_y) {
+  const float g = *grad_p;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
+    float sx = 0.f, sy = 0.f;
+    if (i < num_movable) {
+      for (int k = node_start[i]; k < node_start[i + 1]; ++k) {
+        sx = fadd(sx, fmul(gnx[k], g));
+        sy = fadd(sy, fmul(gny[k], g));
+      }
+    }
+    if (accumulate) {
+      out_x[i] = fadd(sx, out_x[i]);
+      out_y[i] = fadd(sy, out_y[i]);
+    } else {
+      out_x[i] = sx;
+      out_y[i] = sy;
+    }
+  }
+}
+
+}  // namespace dpb
+
+extern "C" int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
+                                  int* num_chunks) {
+  DP_REQUIRE(netpin_start_host && chunk_net_host && num_chunks && max_pins > 0, "dp_plan_net_chunks: bad arguments");
+  int c = 0;
+  int e = 0;
+  while (e < num_nets) {
+    chunk_net_host[c++] = e;
+    int pins = netpin_start_host[e + 1] - netpin_start_host[e];
+    ++e;
+    if (pins <= max_pins) {
+      while (e < num_nets && pins + (netpin_start_host[e + 1] - netpin_start_host[e]) <= max_pins) {
+        pins += netpin_start_host[e + 1] - netpin_start_host[e];
+        ++e;
+      }
+    }
+  }
+  chunk_net_host[c] = num_nets;
+  *num_chunks = c;
+  return DP_OK;
+}
+
+static int launch_chunks(bool grad, const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                         const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
+                         int num_chunks, const float* net_weights, const unsigned char* net_mask,
+                         const float* inv_gamma, const int* csr_pos, double* out_f64, float* gnode, int num_slots,
+                         cudaStream_t s) {
+  using namespace dpb;
+  int blocks = num_chunks > 0 ? ceil_div((long long)num_chunks * 32, 256) : 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
+  if (grad)
+    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, slot_net,
+                                                netpin_start, chunk_net, num_chunks, net_weights, net_mask, inv_gamma,
+                                                csr_pos, out_f64 + 1, gnode, gnode + num_slots);
+  else
+    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, slot_net,
+                                                 netpin_start, chunk_net, num_chunks, net_weights, net_mask,
+                                                 nullptr, nullptr, out_f64 + 1, nullptr, nullptr);
+  int rc = check_launch(grad ? "dp_wa_chunk_forward" : "dp_hpwl_chunk");
+  if (rc) return rc;
+  return launch_finish_sum(out_f64, blocks, nullptr, s);
+}
+
+extern "C" int dp_wa_chunk_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                                   const float* slot_offy, const int* slot_net, const int* netpin_start,
+                                   const int* chunk_net, int num_chunks, const float* net_weights,
+                                   const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
+                                   double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream) {
+  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
+                 inv_gamma && csr_pos && wl_f64 && grad_node_order,
+             "dp_wa_chunk_forward: null pointer argument");
+  return launch_chunks(true, pos, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
+                       num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
+                       dpb::as_stream(stream));
+}
+
+extern "C" int dp_hpwl_chunk(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                             const float* slot_offy, const int* slot_net, const int* netpin_start,
+                             const int* chunk_net, int num_chunks, const float* net_weights,
+                             const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
+  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
+                 out_f64,
+             "dp_hpwl_chunk: null pointer argument");
+  return launch_chunks(false, pos, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
+                       num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0,
+                       dpb::as_stream(stream));
+}
+
+extern "C" int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start,
+                               const float* grad_pos, int num_movable, int num_nodes, int accumulate, float* grad_out,
+                               dp_stream_t stream) {
+  DP_REQUIRE(grad_node_order && node_start && grad_pos && grad_out, "dp_node_pin_sum: null pointer argument");
+  if (num_nodes == 0) return DP_OK;
+  dpb::node_sum_kernel<<<dpb::grid_for(num_nodes, 256, 8), 256, 0, dpb::as_stream(stream)>>>(
+      grad_node_order, grad_node_order + num_slots, node_start, grad_pos, num_movable, num_nodes, accumulate, grad_out,
+      grad_out + num_nodes);
+  return dpb::check_launch("dp_node_pin_sum");
 }

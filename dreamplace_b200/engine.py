@@ -54,6 +54,13 @@ class GPEngine(object):
         self.node_slots = slot_of_pin[data.flat_node2pin_map.long()].to(torch.int32).contiguous()
         self.node_start = data.flat_node2pin_start_map
         self.netpin_start = data.flat_net2pin_start_map
+        # warp-per-chunk WA / HPWL: nets packed into <= 32-pin chunks; the WA
+        # gradient lands at each pin's position in node-CSR order
+        self.chunk_net = C.plan_net_chunks(self.netpin_start.cpu(), 32).to(dev)
+        csr_pos = torch.empty(P, dtype=torch.int64, device=dev)
+        csr_pos[self.node_slots.long()] = torch.arange(P, device=dev)
+        self.csr_pos = csr_pos.to(torch.int32)
+        self.gnode = torch.empty(2 * P, dtype=torch.float32, device=dev)
         ep = ops.density_op
         self.ep = ep
         self.ovf_op = ops.density_overflow_op
@@ -63,7 +70,6 @@ class GPEngine(object):
         self.U = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
         self.G = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
         self.tmp = torch.empty_like(pos.data)
-        self.gi = torch.empty(2 * P, dtype=torch.float32, device=dev)
         f64 = dict(dtype=torch.float64, device=dev)
         # optimizer scalars + fixed-order reduction scratch (include/dreamplace_b200.h)
         self.state = torch.zeros(NESTEROV_STATE + 2 * REDUCE_DOUBLES, **f64)
@@ -128,16 +134,17 @@ class GPEngine(object):
                 self.order[nm:].copy_(of)
 
     def wirelength(self, v):
-        """WA forward at node positions v: fp64 total in self.wl64, per-slot gradient in self.gi."""
+        """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
+        net weight) in node-CSR order in self.gnode."""
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
-        C.wa_slot_forward(v, self.slot_node, self.slot_offx, self.slot_offy, self.netpin_start, dc.net_weights,
-                          dc.net_mask_ignore_large_degrees, self.inv_gamma, self.wl64_buf, self.gi)
+        C.wa_chunk_forward(v, self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
+                           self.chunk_net, dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
+                           self.csr_pos, self.wl64_buf, self.gnode)
 
     def wl_grad_into(self, g, accumulate):
         dc = self.data
-        C.wa_node_backward(self.gi, self.node_slots, self.node_start, self.slot_net, dc.net_weights,
-                           dc.net_mask_ignore_large_degrees, self.one, self.design.num_movable_nodes, int(accumulate), g)
+        C.node_pin_sum(self.gnode, self.node_start, self.one, self.design.num_movable_nodes, int(accumulate), g)
 
     def density_energy(self, v):
         """Density map, Poisson solve; returns (ex, ey, energy_f64[1])."""
@@ -174,8 +181,8 @@ class GPEngine(object):
 
     def evaluate(self, v):
         d, dc = self.design, self.data
-        C.hpwl_slot(v, self.slot_node, self.slot_offx, self.slot_offy, self.netpin_start, dc.net_weights,
-                    dc.net_mask_all, self.hpwl64_buf)
+        C.hpwl_chunk(v, self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
+                     self.chunk_net, dc.net_weights, dc.net_mask_all, self.hpwl64_buf)
         self._density(v, 0, self.omap)
         ba = self.ovf_op.bin_size_x * self.ovf_op.bin_size_y
         C.density_overflow_into(self.omap, float(self.ovf_op.target_density * ba), float(ba), self.ovf2_buf)

@@ -314,6 +314,29 @@ int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, 
                               double* state, dp_stream_t stream);
 /* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
 int dp_nesterov_advance(double* state, dp_stream_t stream);
+/* Host planner: packs nets, in order, into chunks of at most max_pins pins (a
+ * larger net is a chunk of its own).  chunk_net_host [num_nets + 1] receives the
+ * first net of each chunk followed by num_nets; *num_chunks their count. */
+int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
+                       int* num_chunks);
+/* WA forward, one warp per net chunk (max_pins = 32), one lane per pin; per-net
+ * reductions are segmented warp shuffles.  The per-pin gradient, times the net
+ * weight, is written at csr_pos[slot] (the pin's position in node-CSR order) of
+ * grad_node_order [2 * num_slots]; masked nets write 0.  wl_f64: DP_REDUCE_DOUBLES. */
+int dp_wa_chunk_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                        const float* slot_offy, const int* slot_net, const int* netpin_start,
+                        const int* chunk_net, int num_chunks, const float* net_weights,
+                        const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
+                        double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream);
+/* HPWL with the same chunking (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
+int dp_hpwl_chunk(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+                  const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
+                  int num_chunks, const float* net_weights, const unsigned char* net_mask, double* out_f64,
+                  dp_stream_t stream);
+/* grad_out[node] (+)= sum over node_start[node]..node_start[node+1] of
+ * grad_node_order * grad_pos[0]; nodes >= num_movable get 0 (pin mask of fixed cells) */
+int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start, const float* grad_pos,
+                    int num_movable, int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
 /* obj = wl + lambda_eff * D (1 + c D); grad_scale = d obj / d D */
 int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
                         float density_factor, float quad_c, double* obj, float* grad_scale,
