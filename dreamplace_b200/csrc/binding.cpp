@@ -203,6 +203,7 @@ void transform_gemm(int precision, int M, int N, int K, py::list problems) {
       q.spec_out_lo[i] = tensor_ptr(d, kl[i]);
     }
     q.wv_scale = dict_get<float>(d, "wv_scale", 1.0f);
+    q.spec_weights = (const float*)tensor_ptr(d, "spec_weights");
     q.rho = (const float*)tensor_ptr(d, "rho");
     q.energy_f64 = (double*)tensor_ptr(d, "energy");
     probs.push_back(q);
@@ -216,6 +217,12 @@ void prepare_operand(int precision, at::Tensor x, double scale, c10::optional<at
   DP_CALL(dp_prepare_operand(precision, ptr<float>(x), x.numel(), (float)scale, optr<float>(out_f32),
                              out_hi.has_value() ? out_hi->data_ptr() : nullptr,
                              out_lo.has_value() ? out_lo->data_ptr() : nullptr, cur_stream()));
+}
+
+at::Tensor spectral_weights(int M, int N, double wv_scale, at::Device device) {
+  auto out = at::empty({3, M, N}, at::TensorOptions().dtype(at::kFloat).device(device));
+  DP_CALL(dp_spectral_weights(M, N, (float)wv_scale, ptr<float>(out), cur_stream()));
+  return out;
 }
 
 int tc_status() {
@@ -358,12 +365,18 @@ void hpwl_slot(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::T
 
 void nesterov_init(at::Tensor state, double alpha) { DP_CALL(dp_nesterov_init(ptr<double>(state), alpha, cur_stream())); }
 
-void nesterov_trial(at::Tensor v, at::Tensor g, at::Tensor u, at::Tensor u_new, at::Tensor v_new, at::Tensor state,
-                    at::Tensor sx, at::Tensor sy, double xl, double yl, double xh, double yh, int num_movable,
-                    int num_filler) {
+void nesterov_trial(at::Tensor v, at::Tensor g, at::Tensor u, at::Tensor u_new, at::Tensor v_new,
+                    c10::optional<at::Tensor> xy_new, at::Tensor state, at::Tensor sx, at::Tensor sy, double xl,
+                    double yl, double xh, double yh, int num_movable, int num_filler) {
   DP_CALL(dp_nesterov_trial(ptr<float>(v), ptr<float>(g), ptr<float>(u), ptr<float>(u_new), ptr<float>(v_new),
-                            ptr<double>(state), ptr<float>(sx), ptr<float>(sy), xl, yl, xh, yh, v.numel() / 2,
-                            num_movable, num_filler, cur_stream()));
+                            (float*)ovp(xy_new), ptr<double>(state), ptr<float>(sx), ptr<float>(sy), xl, yl, xh, yh,
+                            v.numel() / 2, num_movable, num_filler, cur_stream()));
+}
+
+void pack_xy(at::Tensor pos, at::Tensor xy) {
+  CHECK_F32(pos); CHECK_F32(xy);
+  TORCH_CHECK(xy.numel() == pos.numel(), "xy must have as many elements as pos");
+  DP_CALL(dp_pack_xy(ptr<float>(pos), pos.numel() / 2, ptr<float>(xy), cur_stream()));
 }
 
 void precondition_step_size(at::Tensor g_new, at::Tensor g, at::Tensor v_new, at::Tensor v, at::Tensor pws,
@@ -484,6 +497,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("transform_gemm", &transform_gemm);
   m.def("prepare_operand", &prepare_operand);
   m.def("tc_status", &tc_status);
+  m.def("spectral_weights", &spectral_weights);
   m.def("wa_merged_forward", &wa_merged_forward);
   m.def("wa_merged_backward", &wa_merged_backward);
   m.def("pin_pos_forward", &pin_pos_forward);
@@ -499,6 +513,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("nesterov_trial", &nesterov_trial);
   m.def("precondition_step_size", &precondition_step_size);
   m.def("nesterov_advance", &nesterov_advance);
+  m.def("pack_xy", &pack_xy);
   m.def("objective_finish", &objective_finish);
   m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);

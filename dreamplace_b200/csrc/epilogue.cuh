@@ -31,6 +31,7 @@ struct EpiParams {
   __nv_bfloat16* sp_lo[3];
   float wv_scale;
   float two_pi_over_m, two_pi_over_n;
+  const float* spec_w;  // optional precomputed spectral tables [3*M*N]
   const float* rho;
   double* energy;
 };
@@ -76,8 +77,15 @@ __device__ __forceinline__ double epi_apply(const EpiParams& p, int m, int n, fl
       return 0.0;
     case DP_EPI_SPECTRAL: {
       float wx, wy, winv;
-      spectral_weights(p, m, n, wx, wy, winv);
       size_t idx = (size_t)m * p.ldc + n;
+      if (p.spec_w) {
+        size_t t = (size_t)m * p.N + n, mn = (size_t)p.M * p.N;
+        wx = p.spec_w[t];
+        wy = p.spec_w[mn + t];
+        winv = p.spec_w[2 * mn + t];
+      } else {
+        spectral_weights(p, m, n, wx, wy, winv);
+      }
       store_operand(p.fmt, __fmul_rn(v, wx), idx, p.sp_f32[0], p.sp_hi[0], p.sp_lo[0]);
       store_operand(p.fmt, __fmul_rn(v, wy), idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
       if (p.sp_f32[2] || p.sp_hi[2])
@@ -116,6 +124,102 @@ inline EpiParams make_epi(const dp_gemm_problem& q, int precision, int M, int N)
   e.two_pi_over_n = (float)(2.0 * M_PI / N);
   e.rho = q.rho;
   e.energy = q.energy_f64;
+  e.spec_w = q.spec_weights;
+  return e;
+}
+
+// 16 consecutive columns [n0, n0+16) of row m, all in range; vector stores
+// where the row segment is 16-byte aligned (checked by the caller's layout:
+// n0 % 16 == 0 and ldc % 8 == 0).  Returns the ENERGY contribution.
+__device__ __forceinline__ void store_operand16(int fmt, const float* v, size_t idx, float* f32,
+                                                __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  if (fmt == kFmtF32) {
+    float4* d = reinterpret_cast<float4*>(f32 + idx);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    return;
+  }
+  __align__(16) __nv_bfloat16 h[16];
+  __align__(16) __nv_bfloat16 l[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    h[j] = __float2bfloat16_rn(v[j]);
+    l[j] = __float2bfloat16_rn(v[j] - __bfloat162float(h[j]));
+  }
+  uint4* dh = reinterpret_cast<uint4*>(hi + idx);
+  dh[0] = reinterpret_cast<const uint4*>(h)[0];
+  dh[1] = reinterpret_cast<const uint4*>(h)[1];
+  if (fmt == kFmtSplit) {
+    uint4* dl = reinterpret_cast<uint4*>(lo + idx);
+    dl[0] = reinterpret_cast<const uint4*>(l)[0];
+    dl[1] = reinterpret_cast<const uint4*>(l)[1];
+  }
+}
+
+__device__ __forceinline__ double epi_apply_row16(const EpiParams& p, int m, int n0, const float* acc) {
+  float v[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __fmul_rn(acc[j], p.alpha);
+  const size_t idx = (size_t)m * p.ldc + n0;
+  switch (p.kind) {
+    case DP_EPI_STORE: {
+      float4* d = reinterpret_cast<float4*>(p.out_f32 + idx);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      return 0.0;
+    }
+    case DP_EPI_SPECTRAL: {
+      float wx[16], wy[16], wi[16];
+      if (p.spec_w) {
+        const size_t t = (size_t)m * p.N + n0, mn = (size_t)p.M * p.N;
+        const float4* a = reinterpret_cast<const float4*>(p.spec_w + t);
+        const float4* b = reinterpret_cast<const float4*>(p.spec_w + mn + t);
+        const float4* c = reinterpret_cast<const float4*>(p.spec_w + 2 * mn + t);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float4 A = __ldg(a + q), B = __ldg(b + q), Cc = __ldg(c + q);
+          wx[4 * q] = A.x; wx[4 * q + 1] = A.y; wx[4 * q + 2] = A.z; wx[4 * q + 3] = A.w;
+          wy[4 * q] = B.x; wy[4 * q + 1] = B.y; wy[4 * q + 2] = B.z; wy[4 * q + 3] = B.w;
+          wi[4 * q] = Cc.x; wi[4 * q + 1] = Cc.y; wi[4 * q + 2] = Cc.z; wi[4 * q + 3] = Cc.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) spectral_weights(p, m, n0 + j, wx[j], wy[j], wi[j]);
+      }
+      float o[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wx[j]);
+      store_operand16(p.fmt, o, idx, p.sp_f32[0], p.sp_hi[0], p.sp_lo[0]);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wy[j]);
+      store_operand16(p.fmt, o, idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
+      if (p.sp_f32[2] || p.sp_hi[2]) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wi[j]);
+        store_operand16(p.fmt, o, idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
+      }
+      return 0.0;
+    }
+    case DP_EPI_ENERGY: {
+      const float4* r = reinterpret_cast<const float4*>(p.rho + idx);
+      double e = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 R = __ldg(r + q);
+        e += (double)__fmul_rn(v[4 * q], R.x) + (double)__fmul_rn(v[4 * q + 1], R.y) +
+             (double)__fmul_rn(v[4 * q + 2], R.z) + (double)__fmul_rn(v[4 * q + 3], R.w);
+      }
+      if (p.out_f32) {
+        float4* d = reinterpret_cast<float4*>(p.out_f32 + idx);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
+      return e;
+    }
+  }
+  double e = 0.0;  // STORE_T: transposed, element by element
+#pragma unroll
+  for (int j = 0; j < 16; ++j) e += epi_apply(p, m, n0 + j, acc[j]);
   return e;
 }
 

@@ -236,14 +236,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     const int m = m0 + warp * 32 + lane;
     const uint32_t row_addr = tmem_base + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
+    const bool vec_ok = (P.ldc % 8) == 0;
     for (int c = 0; c < BN; c += 16) {
       float v[16];
       tmem_ld16(row_addr + (uint32_t)c, v);
       if (m < M) {
+        if (vec_ok && n0 + c + 16 <= N) {
+          e += epi_apply_row16(P, m, n0 + c, v);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          int n = n0 + c + j;
-          if (n < N) e += epi_apply(P, m, n, v[j]);
+          for (int j = 0; j < 16; ++j) {
+            int n = n0 + c + j;
+            if (n < N) e += epi_apply(P, m, n, v[j]);
+          }
         }
       }
     }
@@ -327,9 +332,17 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
 
 int launch_tc_gemm(int precision, int M, int N, int K, const dp_gemm_problem* probs, int count, cudaStream_t s) {
   switch (precision) {
-    case DP_PREC_TF32: return run_tc<DP_PREC_TF32, 64, 4>(M, N, K, probs, count, s);
-    case DP_PREC_BF16: return run_tc<DP_PREC_BF16, 64, 4>(M, N, K, probs, count, s);
-    case DP_PREC_SPLIT_BF16: return run_tc<DP_PREC_SPLIT_BF16, 64, 4>(M, N, K, probs, count, s);
+    // A single problem runs one CTA per SM with an 8-deep TMA ring; batched
+    // problems (3x the tiles) run two CTAs per SM with 4 stages each.
+    case DP_PREC_TF32:
+      return count == 1 ? run_tc<DP_PREC_TF32, 64, 8>(M, N, K, probs, count, s)
+                        : run_tc<DP_PREC_TF32, 64, 4>(M, N, K, probs, count, s);
+    case DP_PREC_BF16:
+      return count == 1 ? run_tc<DP_PREC_BF16, 64, 8>(M, N, K, probs, count, s)
+                        : run_tc<DP_PREC_BF16, 64, 4>(M, N, K, probs, count, s);
+    case DP_PREC_SPLIT_BF16:
+      return count == 1 ? run_tc<DP_PREC_SPLIT_BF16, 64, 8>(M, N, K, probs, count, s)
+                        : run_tc<DP_PREC_SPLIT_BF16, 64, 4>(M, N, K, probs, count, s);
   }
   set_error("dp_transform_gemm: unsupported precision %d", precision);
   return DP_ERR_UNSUPPORTED;

@@ -228,31 +228,37 @@ enum {
 };
 
 // u' = v - alpha g; v' = u' + coef (u' - u); v' clamped into the die for
-// movable and filler nodes (move_boundary semantics).
+// movable and filler nodes (move_boundary semantics); one thread per node
+// also writes the interleaved copy xy' used by the gather kernels.
 __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* __restrict__ g,
                                       const float* __restrict__ u, float* __restrict__ u_new,
-                                      float* __restrict__ v_new, const double* __restrict__ st,
-                                      const float* __restrict__ sx, const float* __restrict__ sy, float xl, float yl,
-                                      float xh, float yh, int num_nodes, int num_movable, int num_filler) {
+                                      float* __restrict__ v_new, float2* __restrict__ xy_new,
+                                      const double* __restrict__ st, const float* __restrict__ sx,
+                                      const float* __restrict__ sy, float xl, float yl, float xh, float yh,
+                                      int num_nodes, int num_movable, int num_filler) {
   const float alpha = (float)st[NS_ALPHA];
   const float coef = (float)st[NS_COEF];
-  const int n2 = 2 * num_nodes;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
-    float un = fsub(v[i], fmul(alpha, g[i]));
-    float vn = fadd(un, fmul(coef, fsub(un, u[i])));
-    int node = i < num_nodes ? i : i - num_nodes;
-    if (node < num_movable || node >= num_nodes - num_filler) {
-      if (i < num_nodes) {
-        vn = fmaxf(vn, xl);
-        vn = fminf(vn, fsub(xh, sx[node]));
-      } else {
-        vn = fmaxf(vn, yl);
-        vn = fminf(vn, fsub(yh, sy[node]));
-      }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
+    const int j = i + num_nodes;
+    const float ux = fsub(v[i], fmul(alpha, g[i]));
+    const float uy = fsub(v[j], fmul(alpha, g[j]));
+    float vx = fadd(ux, fmul(coef, fsub(ux, u[i])));
+    float vy = fadd(uy, fmul(coef, fsub(uy, u[j])));
+    if (i < num_movable || i >= num_nodes - num_filler) {
+      vx = fminf(fmaxf(vx, xl), fsub(xh, sx[i]));
+      vy = fminf(fmaxf(vy, yl), fsub(yh, sy[i]));
     }
-    u_new[i] = un;
-    v_new[i] = vn;
+    u_new[i] = ux;
+    u_new[j] = uy;
+    v_new[i] = vx;
+    v_new[j] = vy;
+    if (xy_new) xy_new[i] = make_float2(vx, vy);
   }
+}
+
+__global__ void pack_xy_kernel(const float* __restrict__ v, float2* __restrict__ xy, int num_nodes) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x)
+    xy[i] = make_float2(v[i], v[i + num_nodes]);
 }
 
 // g' /= max(1, pws + lambda*area) in place, and per-block fp64 sums of
@@ -392,13 +398,24 @@ extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream)
 }
 
 extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
-                                 const double* state, const float* sx, const float* sy, float xl, float yl, float xh,
-                                 float yh, int num_nodes, int num_movable, int num_filler, dp_stream_t stream) {
+                                 float* xy_new, const double* state, const float* sx, const float* sy, float xl,
+                                 float yl, float xh, float yh, int num_nodes, int num_movable, int num_filler,
+                                 dp_stream_t stream) {
   DP_REQUIRE(v && g && u && u_new && v_new && state && sx && sy, "dp_nesterov_trial: null pointer");
+  DP_REQUIRE(((uintptr_t)xy_new & 7) == 0, "dp_nesterov_trial: xy_new must be 8-byte aligned");
   if (num_nodes == 0) return DP_OK;
-  nesterov_trial_kernel<<<grid_for(2ll * num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
-      v, g, u, u_new, v_new, state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable, num_filler);
+  nesterov_trial_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+      v, g, u, u_new, v_new, reinterpret_cast<float2*>(xy_new), state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable,
+      num_filler);
   return check_launch("dp_nesterov_trial");
+}
+
+extern "C" int dp_pack_xy(const float* pos, int num_nodes, float* xy, dp_stream_t stream) {
+  DP_REQUIRE(pos && xy && ((uintptr_t)xy & 7) == 0, "dp_pack_xy: bad arguments");
+  if (num_nodes == 0) return DP_OK;
+  pack_xy_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(pos, reinterpret_cast<float2*>(xy),
+                                                                            num_nodes);
+  return check_launch("dp_pack_xy");
 }
 
 extern "C" int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, const float* v,
@@ -472,12 +489,12 @@ __device__ __forceinline__ SegInfo segment_of(int net, int lane) {
 
 template <bool kGrad>
 __global__ void __launch_bounds__(256) wa_chunk_kernel(
-    const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ slot_node,
+    const float2* __restrict__ xy, const int* __restrict__ slot_node,
     const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ slot_net,
     const int* __restrict__ netpin_start, const int* __restrict__ chunk_net, int num_chunks,
     const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
     const float* __restrict__ inv_gamma_p, const int* __restrict__ csr_pos, double* __restrict__ partials,
-    float* __restrict__ gnx, float* __restrict__ gny) {
+    float2* __restrict__ gnode) {
   const float inv_gamma = kGrad ? *inv_gamma_p : 0.f;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -490,14 +507,14 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
     if (np <= 32) {
       const bool valid = lane < np;
       const int s = s0 + lane;
-      const int net = valid ? slot_net[s] : INT_MAX;
+      const int net = valid ? __ldcs(slot_net + s) : INT_MAX;
       const SegInfo sg = segment_of(net, lane);
       const bool on = valid && net_mask[net];
       float xx = 0.f, yy = 0.f;
       if (valid) {
-        const int n = slot_node[s];
-        xx = fadd(slot_offx[s], x[n]);
-        yy = fadd(slot_offy[s], y[n]);
+        const float2 p = xy[__ldcs(slot_node + s)];
+        xx = fadd(__ldcs(slot_offx + s), p.x);
+        yy = fadd(__ldcs(slot_offy + s), p.y);
       }
       const float x_max = seg_reduce(valid ? xx : -FLT_MAX, sg, lane, MaxOp());
       const float x_min = seg_reduce(valid ? xx : FLT_MAX, sg, lane, MinOp());
@@ -550,17 +567,15 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
           gyv = fmul(gyv, w);
         }
       }
-      const int q = csr_pos[s];
-      gnx[q] = gxv;
-      gny[q] = gyv;
+      __stcs(gnode + __ldcs(csr_pos + s), make_float2(gxv, gyv));
     } else {
       // one net with more than 32 pins: lanes stride over its pins
       const int net = n0;
       const bool on = net_mask[net];
       float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
       for (int s = s0 + lane; s < s1; s += 32) {
-        const int n = slot_node[s];
-        const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+        const float2 p = xy[slot_node[s]];
+        const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
         x_max = fmaxf(x_max, xx);
         x_min = fminf(x_min, xx);
         y_max = fmaxf(y_max, yy);
@@ -580,8 +595,8 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
       }
       float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
       for (int s = s0 + lane; s < s1; s += 32) {
-        const int n = slot_node[s];
-        const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+        const float2 p = xy[slot_node[s]];
+        const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
         const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
         const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
         xe_p = fadd(xe_p, fmul(xx, a1));
@@ -612,8 +627,8 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
       for (int s = s0 + lane; s < s1; s += 32) {
         float gxv = 0.f, gyv = 0.f;
         if (on) {
-          const int n = slot_node[s];
-          const float xx = fadd(slot_offx[s], x[n]), yy = fadd(slot_offy[s], y[n]);
+          const float2 p = xy[slot_node[s]];
+          const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
           const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
           const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
           gxv = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
@@ -623,9 +638,7 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
             gyv = fmul(gyv, w);
           }
         }
-        const int q = csr_pos[s];
-        gnx[q] = gxv;
-        gny[q] = gyv;
+        gnode[csr_pos[s]] = make_float2(gxv, gyv);
       }
     }
   }
@@ -634,17 +647,18 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
 
 // node grad (+)= grad_pos[0] * sum of its pins' (weighted) gradients, which
 // sit contiguously in node-CSR order; nodes >= num_movable get 0
-__global__ void node_sum_kernel(const float* __restrict__ gnx, const float* __restrict__ gny,
-                                const int* __restrict__ node_start, const float* __restrict__ grad_p,
-                                int num_movable, int num_nodes, int accumulate, float* __restrict__ out_x,
-                                float* __restrict__ out_y) {
+__global__ void node_sum_kernel(const float2* __restrict__ gnode, const int* __restrict__ node_start,
+                                const float* __restrict__ grad_p, int num_movable, int num_nodes, int accumulate,
+                                float* __restrict__ out_x, float* __restrict__ out_y) {
   const float g = *grad_p;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
     float sx = 0.f, sy = 0.f;
     if (i < num_movable) {
-      for (int k = node_start[i]; k < node_start[i + 1]; ++k) {
-        sx = fadd(sx, fmul(gnx[k], g));
-        sy = fadd(sy, fmul(gny[k], g));
+      const int k1 = node_start[i + 1];
+      for (int k = node_start[i]; k < k1; ++k) {
+        const float2 v = __ldcs(gnode + k);
+        sx = fadd(sx, fmul(v.x, g));
+        sy = fadd(sy, fmul(v.y, g));
       }
     }
     if (accumulate) {
@@ -680,7 +694,7 @@ extern "C" int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, in
   return DP_OK;
 }
 
-static int launch_chunks(bool grad, const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                          const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
                          int num_chunks, const float* net_weights, const unsigned char* net_mask,
                          const float* inv_gamma, const int* csr_pos, double* out_f64, float* gnode, int num_slots,
@@ -688,40 +702,44 @@ static int launch_chunks(bool grad, const float* pos, int num_nodes, const int* 
   using namespace dpb;
   int blocks = num_chunks > 0 ? ceil_div((long long)num_chunks * 32, 256) : 1;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
+  const float2* p2 = reinterpret_cast<const float2*>(xy);
   if (grad)
-    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, slot_net,
-                                                netpin_start, chunk_net, num_chunks, net_weights, net_mask, inv_gamma,
-                                                csr_pos, out_f64 + 1, gnode, gnode + num_slots);
+    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
+                                                chunk_net, num_chunks, net_weights, net_mask, inv_gamma, csr_pos,
+                                                out_f64 + 1, reinterpret_cast<float2*>(gnode));
   else
-    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, slot_net,
-                                                 netpin_start, chunk_net, num_chunks, net_weights, net_mask,
-                                                 nullptr, nullptr, out_f64 + 1, nullptr, nullptr);
+    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
+                                                 chunk_net, num_chunks, net_weights, net_mask, nullptr, nullptr,
+                                                 out_f64 + 1, nullptr);
   int rc = check_launch(grad ? "dp_wa_chunk_forward" : "dp_hpwl_chunk");
   if (rc) return rc;
   return launch_finish_sum(out_f64, blocks, nullptr, s);
 }
 
-extern "C" int dp_wa_chunk_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+extern "C" int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                                    const float* slot_offy, const int* slot_net, const int* netpin_start,
                                    const int* chunk_net, int num_chunks, const float* net_weights,
                                    const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
                                    double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream) {
-  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
+  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
                  inv_gamma && csr_pos && wl_f64 && grad_node_order,
              "dp_wa_chunk_forward: null pointer argument");
-  return launch_chunks(true, pos, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
+             "dp_wa_chunk_forward: xy and grad_node_order must be 8-byte aligned");
+  return launch_chunks(true, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
                        num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
                        dpb::as_stream(stream));
 }
 
-extern "C" int dp_hpwl_chunk(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+extern "C" int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                              const float* slot_offy, const int* slot_net, const int* netpin_start,
                              const int* chunk_net, int num_chunks, const float* net_weights,
                              const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
-  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
+  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
                  out_f64,
              "dp_hpwl_chunk: null pointer argument");
-  return launch_chunks(false, pos, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0, "dp_hpwl_chunk: xy must be 8-byte aligned");
+  return launch_chunks(false, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
                        num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0,
                        dpb::as_stream(stream));
 }
@@ -731,8 +749,9 @@ extern "C" int dp_node_pin_sum(const float* grad_node_order, int num_slots, cons
                                dp_stream_t stream) {
   DP_REQUIRE(grad_node_order && node_start && grad_pos && grad_out, "dp_node_pin_sum: null pointer argument");
   if (num_nodes == 0) return DP_OK;
+  DP_REQUIRE(((uintptr_t)grad_node_order & 7) == 0, "dp_node_pin_sum: grad_node_order must be 8-byte aligned");
   dpb::node_sum_kernel<<<dpb::grid_for(num_nodes, 256, 8), 256, 0, dpb::as_stream(stream)>>>(
-      grad_node_order, grad_node_order + num_slots, node_start, grad_pos, num_movable, num_nodes, accumulate, grad_out,
-      grad_out + num_nodes);
+      reinterpret_cast<const float2*>(grad_node_order), node_start, grad_pos, num_movable, num_nodes, accumulate,
+      grad_out, grad_out + num_nodes);
   return dpb::check_launch("dp_node_pin_sum");
 }

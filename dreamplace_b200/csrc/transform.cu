@@ -203,3 +203,27 @@ extern "C" int dp_prepare_operand(int precision, const float* x, size_t n, float
                                                         (__nv_bfloat16*)out_lo);
   return check_launch("dp_prepare_operand");
 }
+
+namespace dpb {
+__global__ void spectral_table_kernel(EpiParams p, float* out) {
+  const size_t mn = (size_t)p.M * p.N;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < mn; t += (size_t)gridDim.x * blockDim.x) {
+    float wx, wy, wi;
+    spectral_weights(p, (int)(t / p.N), (int)(t % p.N), wx, wy, wi);
+    out[t] = wx;
+    out[mn + t] = wy;
+    out[2 * mn + t] = wi;
+  }
+}
+}  // namespace dpb
+
+extern "C" int dp_spectral_weights(int M, int N, float wv_scale, float* out, dp_stream_t stream) {
+  DP_REQUIRE(M > 0 && N > 0 && out, "dp_spectral_weights: bad arguments");
+  dp_gemm_problem q;
+  memset(&q, 0, sizeof(q));
+  q.epilogue = DP_EPI_SPECTRAL;
+  q.wv_scale = wv_scale;
+  EpiParams e = make_epi(q, DP_PREC_FP32, M, N);
+  spectral_table_kernel<<<grid_for((long long)M * N, 256, 8), 256, 0, as_stream(stream)>>>(e, out);
+  return check_launch("dp_spectral_weights");
+}

@@ -34,6 +34,17 @@ from .dct2_fft2 import (DCT2, EPI_ENERGY, EPI_SPECTRAL, EPI_STORE, EPI_STORE_T, 
 logger = logging.getLogger(__name__)
 
 
+_SPECTRAL_CACHE = {}
+
+
+def spectral_tables(M, N, wv_scale, device):
+    """[3, M, N] fp32 tables (wx, wy, winv) of the spectral scaling (cached)."""
+    key = (M, N, float(wv_scale), str(device))
+    if key not in _SPECTRAL_CACHE:
+        _SPECTRAL_CACHE[key] = C.spectral_weights(M, N, float(wv_scale), torch.device(device))
+    return _SPECTRAL_CACHE[key]
+
+
 def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
     """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
 
@@ -57,7 +68,8 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
     # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy, a*winv  [M, N]
     spec = [Operand((M, N), prec, dev) for _ in range(2 if fast_mode else 3)]
     g2 = dict(lda=M, ldb=M, epilogue=EPI_SPECTRAL, alpha=4.0 / (M * N), ldc=N,
-              wv_scale=float(bin_size_x / bin_size_y))
+              wv_scale=float(bin_size_x / bin_size_y),
+              spec_weights=spectral_tables(M, N, float(bin_size_x / bin_size_y), dev))
     cM.as_a(g2)
     t1.as_b(g2)
     for i, s in enumerate(spec):

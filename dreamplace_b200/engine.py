@@ -69,6 +69,9 @@ class GPEngine(object):
         self.V = [pos.data.clone(), torch.empty_like(pos.data)]
         self.U = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
         self.G = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
+        # interleaved (x, y) copies of V[0], V[1] for the gather kernels
+        self.XY = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
+        self._xy_of = {self.V[0].data_ptr(): self.XY[0], self.V[1].data_ptr(): self.XY[1]}
         self.tmp = torch.empty_like(pos.data)
         f64 = dict(dtype=torch.float64, device=dev)
         # optimizer scalars + fixed-order reduction scratch (include/dreamplace_b200.h)
@@ -133,12 +136,19 @@ class GPEngine(object):
                 of = torch.argsort(key[n - nf:]).to(torch.int32).add_(n - nf)
                 self.order[nm:].copy_(of)
 
+    def xy(self, v):
+        return self._xy_of[v.data_ptr()]
+
+    def pack(self, v):
+        """Refresh the interleaved copy of a position buffer written outside the trial kernel."""
+        C.pack_xy(v, self.xy(v))
+
     def wirelength(self, v):
         """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
         net weight) in node-CSR order in self.gnode."""
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
-        C.wa_chunk_forward(v, self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
+        C.wa_chunk_forward(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
                            self.chunk_net, dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
                            self.csr_pos, self.wl64_buf, self.gnode)
 
@@ -181,7 +191,7 @@ class GPEngine(object):
 
     def evaluate(self, v):
         d, dc = self.design, self.data
-        C.hpwl_chunk(v, self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
+        C.hpwl_chunk(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
                      self.chunk_net, dc.net_weights, dc.net_mask_all, self.hpwl64_buf)
         self._density(v, 0, self.omap)
         ba = self.ovf_op.bin_size_x * self.ovf_op.bin_size_y
@@ -191,15 +201,18 @@ class GPEngine(object):
         d = self.design
         C.move_boundary_forward(v, self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl),
                                 float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+        self.pack(v)
 
     # ---------------------------------------------------------------- setup
     def initial_learning_rate(self, lr):
         """|x0 - x1| / |g0 - g1| after x1 = x0 - lr g0 (PlaceObj.estimate_initial_learning_rate)."""
         v0, g0, g1, x1 = self.V[0], self.G[0], self.G[1], self.V[1]
         self._quad_c = 0.0
+        self.pack(v0)
         self.obj_and_raw_grad(v0, g0)
         self.precondition(g0, v0, g0, v0)
         torch.sub(v0, g0, alpha=lr, out=x1)
+        self.pack(x1)
         self.obj_and_raw_grad(x1, g1)
         self.precondition(g1, v0, g0, x1)
         return float((torch.dist(v0.double(), x1.double()) / torch.dist(g0.double(), g1.double())).item())
@@ -229,6 +242,7 @@ class GPEngine(object):
         u.copy_(v)
         x1, g1 = self.V[1 - p], self.G[1 - p]
         torch.sub(v, g, alpha=lr, out=x1)
+        self.pack(x1)
         self.obj_and_raw_grad(x1, g1)
         self.precondition(g1, v, g, x1)
         alpha = float((torch.dist(v.double(), x1.double()) / torch.dist(g.double(), g1.double())).item())
@@ -240,7 +254,7 @@ class GPEngine(object):
         d = self.design
         v, g, u = self.V[p], self.G[p], self.U[p]
         vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
-        C.nesterov_trial(v, g, u, un, vn, self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
+        C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
                          float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
         energy = self.obj_and_raw_grad(vn, gn)
         self.precondition(gn, v, g, vn)
@@ -250,13 +264,15 @@ class GPEngine(object):
     def nesterov_trial_only(self, p):
         """The trial-point kernel alone (used for per-kernel timing)."""
         d = self.design
-        C.nesterov_trial(self.V[p], self.G[p], self.U[p], self.U[1 - p], self.V[1 - p], self.state,
+        C.nesterov_trial(self.V[p], self.G[p], self.U[p], self.U[1 - p], self.V[1 - p], self.XY[1 - p], self.state,
                          self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
                          float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
 
     def _body(self, p, with_eval):
+        # v_k was clamped into the die when it was produced (trial kernel, or
+        # move_boundary + pack at the start / after a rollback), so the
+        # reference's per-iteration move_boundary(pos) is the identity here
         if with_eval:
-            self.move_boundary(self.V[p])
             self.evaluate(self.V[p])
         self._trial(p)
 
@@ -324,3 +340,9 @@ class GPEngine(object):
 
     def current_position(self):
         return self.V[self.parity]
+
+    def set_position(self, t):
+        """Overwrite v_k (divergence rollback), clamped into the die."""
+        v = self.V[self.parity]
+        v.copy_(t)
+        self.move_boundary(v)

@@ -121,7 +121,7 @@ class _EngineStepper(object):
         return self.eng.current_position()
 
     def set_position(self, t):
-        self.eng.current_position().copy_(t)
+        self.eng.set_position(t)
 
 
 class NonLinearPlace(nn.Module):

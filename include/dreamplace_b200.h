@@ -207,12 +207,19 @@ typedef struct dp_gemm_problem {
   void* out_hi; void* out_lo;  /* STORE_T bf16 operand halves */
   void* spec_out_hi[3]; void* spec_out_lo[3]; float* spec_out_f32[3]; /* SPECTRAL */
   float wv_scale;       /* SPECTRAL: bin_size_x / bin_size_y */
+  const float* spec_weights; /* SPECTRAL, optional: [3*M*N] tables wx | wy | winv from
+                                dp_spectral_weights (same values, no per-element divide) */
   const float* rho;     /* ENERGY */
   double* energy_f64;   /* ENERGY accumulator (caller zeroes it) */
 } dp_gemm_problem;
 
 int dp_transform_gemm(int precision, int M, int N, int K,
                       const dp_gemm_problem* problems_host, int count, dp_stream_t stream);
+
+/* Spectral weight tables of the Poisson solve (electric_potential.py:504-519), in
+ * the reference's fp32 arithmetic: out[0:MN] = wu/(wu^2+wv^2)/2, out[MN:2MN] =
+ * wv/(wu^2+wv^2)/2, out[2MN:3MN] = 1/(wu^2+wv^2) (0 at [0,0]). */
+int dp_spectral_weights(int M, int N, float wv_scale, float* out, dp_stream_t stream);
 
 /* Reads and clears the tensor-core kernels' device status word (0 = every
  * bounded wait completed; non-zero = a wait expired and the launch returned
@@ -302,11 +309,14 @@ int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_node, const fl
  * alpha_k, a_k, a_{k+1}, coef, two norms, alpha_{k+1}, accept flag, then
  * reduction scratch. */
 int dp_nesterov_init(double* state, double alpha, dp_stream_t stream);
-/* u' = v - alpha g; v' = clamp_die(u' + coef (u' - u)) (move_boundary semantics) */
+/* u' = v - alpha g; v' = clamp_die(u' + coef (u' - u)) (move_boundary semantics);
+ * xy_new (optional, 8-byte aligned) receives v' interleaved as (x, y) pairs */
 int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
-                      const double* state, const float* node_size_x, const float* node_size_y,
-                      float xl, float yl, float xh, float yh, int num_nodes, int num_movable,
-                      int num_filler, dp_stream_t stream);
+                      float* xy_new, const double* state, const float* node_size_x,
+                      const float* node_size_y, float xl, float yl, float xh, float yh, int num_nodes,
+                      int num_movable, int num_filler, dp_stream_t stream);
+/* xy[2i], xy[2i+1] = pos[i], pos[num_nodes + i] */
+int dp_pack_xy(const float* pos, int num_nodes, float* xy, dp_stream_t stream);
 /* g' /= max(1, pws + lambda*area) (dreamplace/PlaceObj.py:69-103), then
  * alpha' = |v'-v| / |g'-g| in fp64, accept = alpha' > 0.95 alpha, alpha <- alpha' */
 int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, const float* v,
@@ -320,21 +330,24 @@ int dp_nesterov_advance(double* state, dp_stream_t stream);
 int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
                        int* num_chunks);
 /* WA forward, one warp per net chunk (max_pins = 32), one lane per pin; per-net
- * reductions are segmented warp shuffles.  The per-pin gradient, times the net
- * weight, is written at csr_pos[slot] (the pin's position in node-CSR order) of
- * grad_node_order [2 * num_slots]; masked nets write 0.  wl_f64: DP_REDUCE_DOUBLES. */
-int dp_wa_chunk_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+ * reductions are segmented warp shuffles.  Node positions come interleaved
+ * (xy [2 * num_nodes], see dp_pack_xy).  The per-pin gradient, times the net
+ * weight, is written as an (x, y) pair at csr_pos[slot] (the pin's position in
+ * node-CSR order) of grad_node_order [2 * num_slots]; masked nets write 0.
+ * wl_f64: DP_REDUCE_DOUBLES doubles. */
+int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                         const float* slot_offy, const int* slot_net, const int* netpin_start,
                         const int* chunk_net, int num_chunks, const float* net_weights,
                         const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
                         double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream);
 /* HPWL with the same chunking (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
-int dp_hpwl_chunk(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
+int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                   const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
                   int num_chunks, const float* net_weights, const unsigned char* net_mask, double* out_f64,
                   dp_stream_t stream);
-/* grad_out[node] (+)= sum over node_start[node]..node_start[node+1] of
- * grad_node_order * grad_pos[0]; nodes >= num_movable get 0 (pin mask of fixed cells) */
+/* grad_out[node] (+)= sum over k in node_start[node]..node_start[node+1] of the
+ * (x, y) pair grad_node_order[2k..2k+1] * grad_pos[0]; nodes >= num_movable get 0
+ * (pin mask of fixed cells) */
 int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start, const float* grad_pos,
                     int num_movable, int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
 /* obj = wl + lambda_eff * D (1 + c D); grad_scale = d obj / d D */
