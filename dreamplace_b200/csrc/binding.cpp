@@ -414,18 +414,57 @@ void density_map_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor o
   }
 }
 
-void density_map_ordered_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy,
-                              at::Tensor ratio, c10::optional<at::Tensor> init, double xl, double yl, double xh,
-                              double yh, double bsx, double bsy, int nbx, int nby, at::Tensor order, int count,
-                              int deterministic, c10::optional<at::Tensor> scratch, at::Tensor out) {
-  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(order);
-  TORCH_CHECK(count <= order.numel(), "count exceeds the order array");
+void build_cell_records(at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio,
+                        at::Tensor order, int count, at::Tensor rec4, at::Tensor ratio_o,
+                        c10::optional<at::Tensor> inv_order) {
+  CHECK_I32(order); CHECK_F32(rec4); CHECK_F32(ratio_o);
+  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
+              "build_cell_records: buffers smaller than count");
+  DP_CALL(dp_build_cell_records(ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy), ptr<float>(ratio),
+                                ptr<int>(order), count, ptr<float>(rec4), ptr<float>(ratio_o), (int*)ovp(inv_order),
+                                cur_stream()));
+}
+
+void density_map_ordered_into(at::Tensor xy, at::Tensor order, at::Tensor rec4, at::Tensor ratio_o, int count,
+                              c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh, double bsx,
+                              double bsy, int nbx, int nby, int deterministic, c10::optional<at::Tensor> scratch,
+                              at::Tensor out) {
+  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(rec4);
+  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
+              "density_map_ordered_into: buffers smaller than count");
+  TORCH_CHECK(out.numel() == (int64_t)nbx * nby, "density_map_ordered_into: output is not num_bins_x*num_bins_y");
   TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
-  DP_CALL(dp_density_map_ordered(ptr<float>(pos), pos.numel() / 2, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox),
-                                 ptr<float>(oy), ptr<float>(ratio), (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
-                                 inv_f(bsx), inv_f(bsy), nbx, nby, ptr<int>(order), count, deterministic,
-                                 fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch), ptr<float>(out),
-                                 cur_stream()));
+  DP_CALL(dp_density_map_ordered(ptr<float>(xy), ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o), count,
+                                 (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy), nbx, nby,
+                                 deterministic, fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch),
+                                 ptr<float>(out), cur_stream()));
+}
+
+void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy, at::Tensor order,
+                            at::Tensor rec4, at::Tensor ratio_o, int count, double xl, double yl, double bsx,
+                            double bsy, int nbx, int nby, double scale, at::Tensor force_o) {
+  CHECK_FLAT(xy); CHECK_I32(order); CHECK_F32(force_o);
+  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && 2 * count <= force_o.numel(),
+              "electric_force_ordered: buffers smaller than count");
+  TORCH_CHECK(ex.numel() == (int64_t)nbx * nby && ey.numel() == ex.numel(), "electric_force_ordered: field map size");
+  DP_CALL(dp_electric_force_ordered(ptr<float>(grad_scale), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(xy),
+                                    ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o), count, xl, yl, bsx, bsy,
+                                    inv_f(bsx), inv_f(bsy), (float)scale, ptr<float>(force_o), cur_stream()));
+}
+
+void assemble_precondition_step(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor wl_scale,
+                                at::Tensor force_o, at::Tensor inv_order, int num_movable, int num_filler,
+                                at::Tensor pws, at::Tensor area, at::Tensor lambda_, at::Tensor v_new, at::Tensor v,
+                                at::Tensor g, at::Tensor g_new, at::Tensor state) {
+  CHECK_I32(node_start); CHECK_I32(inv_order);
+  int n = v.numel() / 2;
+  TORCH_CHECK(inv_order.numel() >= n && node_start.numel() >= num_movable + 1 && g_new.numel() == 2 * n,
+              "assemble_precondition_step: size mismatch");
+  DP_CALL(dp_assemble_precondition_step(ptr<float>(grad_node_order), ptr<int>(node_start), ptr<float>(wl_scale),
+                                        ptr<float>(force_o), ptr<int>(inv_order), num_movable, num_filler,
+                                        ptr<float>(pws), ptr<float>(area), ptr<float>(lambda_), n, ptr<float>(v_new),
+                                        ptr<float>(v), ptr<float>(g), ptr<float>(g_new), ptr<double>(state),
+                                        cur_stream()));
 }
 
 void density_overflow_into(at::Tensor density_map, double target_area, double bin_area, at::Tensor out2) {
@@ -518,6 +557,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);
   m.def("density_map_ordered_into", &density_map_ordered_into);
+  m.def("build_cell_records", &build_cell_records);
+  m.def("electric_force_ordered", &electric_force_ordered);
+  m.def("assemble_precondition_step", &assemble_precondition_step);
   m.def("plan_net_chunks", &plan_net_chunks);
   m.def("wa_chunk_forward", &wa_chunk_forward);
   m.def("hpwl_chunk", &hpwl_chunk);

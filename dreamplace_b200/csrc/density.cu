@@ -118,14 +118,21 @@ constexpr int kTileCellsPerThread = 4;
 constexpr int kTileCells = kTileThreads * kTileCellsPerThread;
 constexpr int kTileSmemBytes = 96 * 1024;
 
+// Per-cell records in visiting order: rec4 = (stretched width, stretched
+// height, offset x, offset y) and ratio, so a block reads its cells' attributes
+// contiguously and gathers only the node position (one 8-byte load from xy).
 template <bool kFixed>
-__global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(TriangleArgs a, const int* __restrict__ order,
-                                                                         int count, float fx_scale, float* map_f32,
+__global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(TriangleArgs a, const float2* __restrict__ xy,
+                                                                         const int* __restrict__ order,
+                                                                         const float4* __restrict__ rec4,
+                                                                         const float* __restrict__ ratio_o, int count,
+                                                                         float fx_scale, float* map_f32,
                                                                          unsigned long long* map_fx) {
   extern __shared__ __align__(16) unsigned char tile_raw[];
   using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
   Acc* tile = reinterpret_cast<Acc*>(tile_raw);
   constexpr int kCap = kTileSmemBytes / sizeof(Acc);
+  constexpr int kTiny = 16;  // boxes of at most 16 bins accumulate in registers
   __shared__ int red[4][kTileThreads / 32];
   const int base = blockIdx.x * kTileCells;
   int kx0[kTileCellsPerThread], kx1[kTileCellsPerThread], hy0[kTileCellsPerThread], hy1[kTileCellsPerThread];
@@ -137,12 +144,13 @@ __global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(Triangle
     int idx = base + c * kTileThreads + threadIdx.x;
     kx0[c] = kx1[c] = hy0[c] = hy1[c] = 0;
     if (idx < count) {
-      int i = order[idx];
-      sxs[c] = a.sx[i];
-      sys[c] = a.sy[i];
-      nx[c] = fadd(a.x[i], a.ox[i]);
-      ny[c] = fadd(a.y[i], a.oy[i]);
-      rr[c] = a.ratio[i];
+      const float4 r4 = __ldcs(rec4 + idx);
+      const float2 p = xy[order[idx]];
+      sxs[c] = r4.x;
+      sys[c] = r4.y;
+      nx[c] = fadd(p.x, r4.z);
+      ny[c] = fadd(p.y, r4.w);
+      rr[c] = __ldcs(ratio_o + idx);
       triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, kx0[c], kx1[c]);
       triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, hy0[c], hy1[c]);
       if (kx1[c] > kx0[c] && hy1[c] > hy0[c]) {
@@ -177,14 +185,54 @@ __global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(Triangle
   }
   if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
   const int W = bk1 - bk0, H = bh1 - bh0;
+  if (W * H <= kTiny) {
+    // clustered block: per-thread register accumulators, a warp reduction per
+    // bin, one shared atomic per warp and bin, one global atomic per bin
+    Acc acc[kTiny];
+#pragma unroll
+    for (int j = 0; j < kTiny; ++j) acc[j] = (Acc)0;
+#pragma unroll
+    for (int c = 0; c < kTileCellsPerThread; ++c) {
+      for (int k = kx0[c]; k < kx1[c]; ++k) {
+        const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
+        for (int h = hy0[c]; h < hy1[c]; ++h) {
+          const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
+          const Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
+          const int slot = (k - bk0) * H + (h - bh0);
+#pragma unroll
+          for (int j = 0; j < kTiny; ++j)
+            if (j == slot) acc[j] += v;
+        }
+      }
+    }
+    for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = (Acc)0;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kTiny; ++j) {
+      Acc v = acc[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (l == 0 && j < W * H && v != (Acc)0) atomicAdd(&tile[j], v);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < W * H; t += kTileThreads) {
+      Acc v = tile[t];
+      if (v != (Acc)0) {
+        int bin = (bk0 + t / H) * a.num_bins_y + bh0 + t % H;
+        if (kFixed)
+          atomicAdd(map_fx + bin, (unsigned long long)v);
+        else
+          atomicAdd(map_f32 + bin, (float)v);
+      }
+    }
+    return;
+  }
   const bool use_tile = (long long)W * H <= kCap;
   if (use_tile) {
     for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = 0;
     __syncthreads();
   }
-  // Dense boxes (more cell-bin updates than bins, e.g. the clustered start of
-  // GP) first combine the lanes of a warp that hit the same bin, so each bin
-  // takes one shared atomic per warp instead of one per lane.
+  // Dense boxes (more cell-bin updates than bins) first combine the lanes of a
+  // warp that hit the same bin, so each bin takes one shared atomic per warp.
   const bool combine = use_tile && (long long)W * H * 4 < (long long)kTileCells;
 #pragma unroll
   for (int c = 0; c < kTileCellsPerThread; ++c) {
@@ -250,6 +298,19 @@ __global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(Triangle
           atomicAdd(map_f32 + bin, (float)v);
       }
     }
+  }
+}
+
+__global__ void build_records_kernel(const float* __restrict__ sx, const float* __restrict__ sy,
+                                     const float* __restrict__ ox, const float* __restrict__ oy,
+                                     const float* __restrict__ ratio, const int* __restrict__ order, int count,
+                                     float4* __restrict__ rec4, float* __restrict__ ratio_o,
+                                     int* __restrict__ inv_order) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+    const int i = order[idx];
+    rec4[idx] = make_float4(sx[i], sy[i], ox[i], oy[i]);
+    ratio_o[idx] = ratio[i];
+    if (inv_order) inv_order[i] = idx;
   }
 }
 
@@ -568,14 +629,29 @@ extern "C" int dp_density_overflow(const float* map, int nbins, double target_ar
 
 // Order-driven scatter (see tiled_scatter_kernel): `order` lists the nodes to
 // scatter (movable and/or filler indices, any order).
-extern "C" int dp_density_map_ordered(const float* pos, int num_nodes, const float* sx, const float* sy,
-                                      const float* ox, const float* oy, const float* ratio, const float* init,
-                                      float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
-                                      float iby, int nbx, int nby, const int* order, int count, int deterministic,
+// Per-cell records for the order-driven kernels: rec4[idx] = (sx, sy, ox, oy)
+// and ratio_o[idx] of node order[idx]; inv_order[order[idx]] = idx (optional).
+extern "C" int dp_build_cell_records(const float* sx, const float* sy, const float* ox, const float* oy,
+                                     const float* ratio, const int* order, int count, float* rec4, float* ratio_o,
+                                     int* inv_order, dp_stream_t stream) {
+  DP_REQUIRE(sx && sy && ox && oy && ratio && order && rec4 && ratio_o, "dp_build_cell_records: null pointer");
+  DP_REQUIRE(((uintptr_t)rec4 & 15) == 0, "dp_build_cell_records: rec4 must be 16-byte aligned");
+  if (count == 0) return DP_OK;
+  build_records_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+      sx, sy, ox, oy, ratio, order, count, reinterpret_cast<float4*>(rec4), ratio_o, inv_order);
+  return check_launch("dp_build_cell_records");
+}
+
+// Order-driven scatter (see tiled_scatter_kernel): the cells order[0..count)
+// with their records, positions interleaved in xy.
+extern "C" int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
+                                      int count, const float* init, float xl, float yl, float xh, float yh, float bsx,
+                                      float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
                                       int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
-  int rc = validate_triangle(pos, num_nodes, sx, sy, ox, oy, ratio, 0, 0, nbx, nby, bsx, bsy, out);
-  if (rc) return rc;
-  DP_REQUIRE(count >= 0 && count <= num_nodes && (count == 0 || order), "dp_density_map_ordered: bad order");
+  DP_REQUIRE(xy && rec4 && ratio_o && out && (count == 0 || order), "dp_density_map_ordered: null pointer");
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)rec4 & 15) == 0, "dp_density_map_ordered: misaligned xy/rec4");
+  DP_REQUIRE(nbx > 0 && nby > 0 && (long long)nbx * nby < (1ll << 31), "dp_density_map_ordered: bad bin grid");
+  DP_REQUIRE(bsx > 0 && bsy > 0 && count >= 0, "dp_density_map_ordered: bad geometry");
   DP_REQUIRE(!deterministic || scratch, "dp_density_map_ordered: deterministic mode needs scratch_fixed");
   cudaStream_t s = as_stream(stream);
   int nbins = nbx * nby;
@@ -585,14 +661,21 @@ extern "C" int dp_density_map_ordered(const float* pos, int num_nodes, const flo
     cudaFuncSetAttribute(tiled_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes);
     configured = true;
   }
-  TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, 0, 0, nbx, nby, nullptr);
+  TriangleArgs a;
+  memset(&a, 0, sizeof(a));
+  a.xl = xl; a.yl = yl; a.bsx = bsx; a.bsy = bsy; a.inv_bsx = ibx; a.inv_bsy = iby;
+  a.num_bins_x = nbx; a.num_bins_y = nby;
+  const float2* p2 = reinterpret_cast<const float2*>(xy);
+  const float4* r4 = reinterpret_cast<const float4*>(rec4);
   int blocks = ceil_div(count, kTileCells);
+  int rc;
   if (deterministic) {
     DP_REQUIRE(fraction_bits >= 0 && fraction_bits <= 62, "dp_density_map_ordered: bad fraction_bits");
     cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
     if (blocks > 0) {
       tiled_scatter_kernel<true><<<blocks, kTileThreads, kTileSmemBytes, s>>>(
-          a, order, count, ldexpf(1.0f, fraction_bits), nullptr, reinterpret_cast<unsigned long long*>(scratch));
+          a, p2, order, r4, ratio_o, count, ldexpf(1.0f, fraction_bits), nullptr,
+          reinterpret_cast<unsigned long long*>(scratch));
       rc = check_launch("dp_density_map_ordered scatter");
       if (rc) return rc;
     }
@@ -607,7 +690,8 @@ extern "C" int dp_density_map_ordered(const float* pos, int num_nodes, const flo
     cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
   }
   if (blocks == 0) return DP_OK;
-  tiled_scatter_kernel<false><<<blocks, kTileThreads, kTileSmemBytes, s>>>(a, order, count, 0.f, out, nullptr);
+  tiled_scatter_kernel<false><<<blocks, kTileThreads, kTileSmemBytes, s>>>(a, p2, order, r4, ratio_o, count, 0.f,
+                                                                            out, nullptr);
   return check_launch("dp_density_map_ordered scatter");
 }
 

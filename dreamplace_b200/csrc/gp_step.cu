@@ -285,6 +285,48 @@ __global__ void __launch_bounds__(256) precondition_norms_kernel(
   block_partial2(dv, dg, partials);
 }
 
+// g'[i] = (wirelength pin sum of node i, nodes < num_movable) + (force of node i,
+// movable and filler nodes, read from order space through inv_order); then
+// g' /= max(1, pws + lambda*area), and the fp64 step-size norms as above.
+__global__ void __launch_bounds__(256) assemble_precondition_kernel(
+    const float2* __restrict__ gnode, const int* __restrict__ node_start, const float* __restrict__ wl_scale_p,
+    const float2* __restrict__ force_o, const int* __restrict__ inv_order, int num_movable, int num_filler,
+    const float* __restrict__ pws, const float* __restrict__ area, const float* __restrict__ lam_p, int num_nodes,
+    const float* __restrict__ v_new, const float* __restrict__ v, const float* __restrict__ g,
+    float* __restrict__ g_new, double* __restrict__ partials) {
+  const float lam = *lam_p;
+  const float ws = *wl_scale_p;
+  double dv = 0.0, dg = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
+    float sx = 0.f, sy = 0.f;
+    if (i < num_movable) {
+      const int k1 = node_start[i + 1];
+      for (int k = node_start[i]; k < k1; ++k) {
+        const float2 q = __ldcs(gnode + k);
+        sx = fadd(sx, fmul(q.x, ws));
+        sy = fadd(sy, fmul(q.y, ws));
+      }
+    }
+    float fx = 0.f, fy = 0.f;
+    if (i < num_movable || i >= num_nodes - num_filler) {
+      const float2 f = force_o[inv_order[i]];
+      fx = f.x;
+      fy = f.y;
+    }
+    const float p = fmaxf(fadd(pws[i], fmul(lam, area[i])), 1.0f);
+    const float gx = __fdiv_rn(fadd(sx, fx), p);
+    const float gy = __fdiv_rn(fadd(sy, fy), p);
+    const int j = i + num_nodes;
+    g_new[i] = gx;
+    g_new[j] = gy;
+    const double a1 = (double)v_new[i] - (double)v[i], a2 = (double)v_new[j] - (double)v[j];
+    const double b1 = (double)gx - (double)g[i], b2 = (double)gy - (double)g[j];
+    dv += a1 * a1 + a2 * a2;
+    dg += b1 * b1 + b2 * b2;
+  }
+  block_partial2(dv, dg, partials);
+}
+
 __global__ void nesterov_finish_kernel(double* st, const double* partials, int count) {
   double dv = finish_sum(partials, count);
   double dg = finish_sum(partials + count, count);
@@ -754,4 +796,28 @@ extern "C" int dp_node_pin_sum(const float* grad_node_order, int num_slots, cons
       reinterpret_cast<const float2*>(grad_node_order), node_start, grad_pos, num_movable, num_nodes, accumulate,
       grad_out, grad_out + num_nodes);
   return dpb::check_launch("dp_node_pin_sum");
+}
+
+extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const int* node_start,
+                                             const float* wl_scale, const float* force_o, const int* inv_order,
+                                             int num_movable, int num_filler, const float* pws, const float* area,
+                                             const float* lambda_, int num_nodes, const float* v_new, const float* v,
+                                             const float* g, float* g_new, double* state, dp_stream_t stream) {
+  using namespace dpb;
+  DP_REQUIRE(grad_node_order && node_start && wl_scale && force_o && inv_order && pws && area && lambda_ && v_new &&
+                 v && g && g_new && state,
+             "dp_assemble_precondition_step: null pointer argument");
+  DP_REQUIRE(num_nodes > 0 && num_movable >= 0 && num_filler >= 0 && num_movable + num_filler <= num_nodes,
+             "dp_assemble_precondition_step: bad node counts");
+  cudaStream_t s = as_stream(stream);
+  int blocks = grid_for(num_nodes, 256, 4);
+  if (blocks > DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
+  double* partials = state + DP_NESTEROV_STATE_DOUBLES;
+  assemble_precondition_kernel<<<blocks, 256, 0, s>>>(
+      reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
+      inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials);
+  int rc = check_launch("dp_assemble_precondition_step");
+  if (rc) return rc;
+  nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
+  return check_launch("dp_assemble_precondition_step finish");
 }

@@ -97,6 +97,14 @@ class GPEngine(object):
         # block), refreshed every `sort_interval` iterations
         nm, nf = d.num_movable_nodes, d.num_filler_nodes
         self.order = torch.cat([torch.arange(nm, device=dev), torch.arange(n - nf, n, device=dev)]).to(torch.int32)
+        # per-cell records in that order (stretched size, offset, ratio), the
+        # inverse order, and the field force in order space
+        count = nm + nf
+        self.rec4 = torch.empty(4 * count, dtype=torch.float32, device=dev)
+        self.ratio_o = torch.empty(count, dtype=torch.float32, device=dev)
+        self.inv_order = torch.zeros(n, dtype=torch.int32, device=dev)
+        self.force_o = torch.empty(2 * count, dtype=torch.float32, device=dev)
+        self._build_records()
         self.sort_interval = int(getattr(params, "sort_interval", 10))
         self.iterations = 0
         self.parity = 0
@@ -110,13 +118,18 @@ class GPEngine(object):
         self._quad_c = 0.0
 
     # ---------------------------------------------------------------- pieces
+    def _build_records(self):
+        ep = self.ep
+        C.build_cell_records(ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y, ep.ratio,
+                             self.order, self.order.numel(), self.rec4, self.ratio_o, self.inv_order)
+
     def _density(self, v, num_filler, out):
         ep = self.ep
         count = ep.num_movable_nodes + (num_filler if num_filler else 0)
-        C.density_map_ordered_into(v, ep.node_size_x_clamped, ep.node_size_y_clamped, ep.offset_x, ep.offset_y,
-                                   ep.ratio, ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
-                                   float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
-                                   ep.num_bins_x, ep.num_bins_y, self.order, count, int(self.det), self.scratch, out)
+        C.density_map_ordered_into(self.xy(v), self.order, self.rec4, self.ratio_o, count,
+                                   ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl), float(ep.xh),
+                                   float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y), ep.num_bins_x,
+                                   ep.num_bins_y, int(self.det), self.scratch, out)
 
     def refresh_order(self, v):
         """Sort movable and filler cells by 16x16-bin tile, then by bin inside the
@@ -135,6 +148,7 @@ class GPEngine(object):
             if nf:
                 of = torch.argsort(key[n - nf:]).to(torch.int32).add_(n - nf)
                 self.order[nm:].copy_(of)
+            self._build_records()
 
     def xy(self, v):
         return self._xy_of[v.data_ptr()]
@@ -182,12 +196,34 @@ class GPEngine(object):
         self.last_energy = energy
         return energy
 
-    def precondition(self, g, v_ref, g_ref, v_new):
+    def _pws(self):
         m = self.model
         if m.ops.precondition_op._pws is None:
             m.ops.precondition_op._pws = m.ops.pws_op(self.data.net_weights)
-        C.precondition_step_size(g, g_ref, v_new, v_ref, m.ops.precondition_op._pws, self.data.node_areas,
-                                 m.density_weight, self.state)
+        return m.ops.precondition_op._pws
+
+    def precondition(self, g, v_ref, g_ref, v_new):
+        C.precondition_step_size(g, g_ref, v_new, v_ref, self._pws(), self.data.node_areas,
+                                 self.model.density_weight, self.state)
+
+    def objective_and_step(self, v, g, v_new, g_new):
+        """The trial's objective at v_new and its preconditioned gradient into g_new,
+        with the fp64 step-size norms against (v, g): the field force is gathered
+        in visiting order and assembled per node together with the wirelength pin
+        sum, the preconditioner and the norms (one pass over the nodes)."""
+        m, ep, d = self.model, self.ep, self.design
+        self.wirelength(v_new)
+        ex, ey, energy = self.density_energy(v_new)
+        C.objective_finish(self.wl64, energy, m.density_weight, float(m.density_factor), self._quad_c,
+                           self.obj64, self.grad_scale)
+        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xy(v_new), self.order, self.rec4,
+                                 self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
+                                 float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
+        C.assemble_precondition_step(self.gnode, self.node_start, self.one, self.force_o, self.inv_order,
+                                     d.num_movable_nodes, d.num_filler_nodes, self._pws(), self.data.node_areas,
+                                     m.density_weight, v_new, v, g, g_new, self.state)
+        self.last_energy = energy
+        return energy
 
     def evaluate(self, v):
         d, dc = self.design, self.data
@@ -256,8 +292,7 @@ class GPEngine(object):
         vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
         C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
                          float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
-        energy = self.obj_and_raw_grad(vn, gn)
-        self.precondition(gn, v, g, vn)
+        energy = self.objective_and_step(v, g, vn, gn)
         torch.cat([self.hpwl64, self.ovf2, self.state[NS_ACCEPT:NS_ACCEPT + 1], self.state[NS_ALPHA:NS_ALPHA + 1],
                    self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
 
@@ -276,18 +311,22 @@ class GPEngine(object):
             self.evaluate(self.V[p])
         self._trial(p)
 
-    def _graph(self, p, with_eval):
+    def _graph(self, p, with_eval, warm=True):
         key = (p, with_eval)
         g = self.graphs.get(key)
         if g is None:
-            s = torch.cuda.Stream()
-            s.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(s):
-                # warm-up on the side stream (state is restored below)
-                saved = self.state.clone()
-                self._body(p, with_eval)
-                self.state.copy_(saved)
-            torch.cuda.current_stream().wait_stream(s)
+            if warm:
+                # warm-up on a side stream.  Only the body of the current parity
+                # may run here: it writes the step-k+1 buffers, which hold nothing
+                # yet, and the optimizer scalars, which are restored.
+                assert p == self.parity, "graph warm-up must run at the current parity"
+                s = torch.cuda.Stream()
+                s.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(s):
+                    saved = self.state.clone()
+                    self._body(p, with_eval)
+                    self.state.copy_(saved)
+                torch.cuda.current_stream().wait_stream(s)
             g = torch.cuda.CUDAGraph()
             before = C.launch_count()
             with torch.cuda.graph(g, pool=self.pool):
@@ -318,10 +357,25 @@ class GPEngine(object):
             self._quad_c = float(m.quad_penalty_coeff.item()) if m.quad_penalty else 0.0
             self.graph_key = key
 
+    def prepare_graphs(self):
+        """Capture all four graph variants (parity x with/without evaluation) up
+        front, so no capture happens inside a timed or latency-sensitive window."""
+        if not self.use_graphs:
+            return
+        self._check_graph_key()
+        p = self.parity
+        # one warm-up (current parity, with evaluation) initialises every lazy
+        # resource; the other three variants are captured without running
+        self._graph(p, True)
+        for key in ((p, False), (1 - p, True), (1 - p, False)):
+            self._graph(*key, warm=False)
+
     def step(self):
         """One GP iteration: evaluation at v_k, then Nesterov trials until accepted
         (<= 10).  Returns (hpwl, overflow / total movable area, max_density, objective, trials)."""
         self._check_graph_key()
+        if self.use_graphs and len(self.graphs) < 4:
+            self.prepare_graphs()
         p = self.parity
         if self.sort_interval > 0 and self.iterations % self.sort_interval == 0:
             self.refresh_order(self.V[p])

@@ -112,21 +112,27 @@ int dp_density_map_fx64_noalloc(const float* pos, int num_nodes,
                                 const int* sorted_node_map, int fraction_bits,
                                 float* density_map, dp_stream_t stream);
 
-/* Order-driven triangle scatter: the nodes order[0..count) (movable and/or
- * filler indices, any order) are added onto initial_density_map (may be NULL =
- * zeros).  Same arithmetic as dp_density_map_f32 / _fx64; blocks of consecutive
- * cells accumulate in a shared-memory tile over their bin bounding box, so a
- * spatial order turns most global atomics into shared ones.  deterministic != 0
- * selects the int64 fixed-point path (scratch_fixed [num_bins] required). */
-int dp_density_map_ordered(const float* pos, int num_nodes,
-                           const float* node_size_x_clamped, const float* node_size_y_clamped,
-                           const float* offset_x, const float* offset_y, const float* ratio,
-                           const float* initial_density_map,
+/* Per-cell records of the order-driven kernels: for idx < count, rec4[4*idx..] =
+ * (sx, sy, ox, oy) (stretched sizes and offsets) and ratio_o[idx] = ratio of node
+ * order[idx]; inv_order[order[idx]] = idx when inv_order is non-NULL. */
+int dp_build_cell_records(const float* node_size_x_clamped, const float* node_size_y_clamped,
+                          const float* offset_x, const float* offset_y, const float* ratio,
+                          const int* order, int count, float* rec4, float* ratio_o, int* inv_order,
+                          dp_stream_t stream);
+
+/* Order-driven triangle scatter of the cells order[0..count) onto
+ * initial_density_map (NULL = zeros), positions interleaved in xy.  Same
+ * arithmetic as dp_density_map_f32 / _fx64.  Blocks of consecutive cells
+ * accumulate in registers (bin box <= 16 bins) or a shared-memory tile over
+ * their bin box before touching global memory, so a spatial order turns most
+ * global atomics into local ones.  deterministic != 0: int64 fixed point
+ * (scratch_fixed [num_bins] required). */
+int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
+                           int count, const float* initial_density_map,
                            float xl, float yl, float xh, float yh,
                            float bin_size_x, float bin_size_y,
                            float inv_bin_size_x, float inv_bin_size_y,
-                           int num_bins_x, int num_bins_y,
-                           const int* order, int count, int deterministic, int fraction_bits,
+                           int num_bins_x, int num_bins_y, int deterministic, int fraction_bits,
                            int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
 
 /* Exact-overlap fixed-cell map (electric_potential/src/electric_density_map_cuda.cpp:139-183,
@@ -183,6 +189,16 @@ int dp_electric_force(const float* grad_pos, int num_bins_x, int num_bins_y,
                       int num_movable_nodes, int num_filler_nodes,
                       const int* sorted_node_map, float scale,
                       float* grad_out, dp_stream_t stream);
+
+/* Field gather of the cells order[0..count) (records as dp_build_cell_records,
+ * positions interleaved in xy); force_o[2*idx..2*idx+1] = scale * grad_pos[0] *
+ * ratio * sum(px py E), in the CPU op's per-cell order without contraction. */
+int dp_electric_force_ordered(const float* grad_pos, int num_bins_x, int num_bins_y,
+                              const float* field_map_x, const float* field_map_y, const float* xy,
+                              const int* order, const float* rec4, const float* ratio_o, int count,
+                              float xl, float yl, float bin_size_x, float bin_size_y,
+                              float inv_bin_size_x, float inv_bin_size_y, float scale, float* force_o,
+                              dp_stream_t stream);
 
 /* ---- Poisson solve as GEMMs (replaces dct/src/dct2_fft2_cuda.cpp:14-140) ------
  * C[m,n] = sum_k A[m,k] * B[n,k]; A [M x K], B [N x K], both K-contiguous.
@@ -322,6 +338,15 @@ int dp_pack_xy(const float* pos, int num_nodes, float* xy, dp_stream_t stream);
 int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, const float* v,
                               const float* pws, const float* area, const float* lambda_, int num_nodes,
                               double* state, dp_stream_t stream);
+/* Gradient assembly fused with the preconditioner and the step size: for each
+ * node, g' = wl_scale * (pin sum of grad_node_order, nodes < num_movable) +
+ * force_o[inv_order[node]] (movable and filler nodes), then as
+ * dp_precondition_step_size. */
+int dp_assemble_precondition_step(const float* grad_node_order, const int* node_start,
+                                  const float* wl_scale, const float* force_o, const int* inv_order,
+                                  int num_movable, int num_filler, const float* pws, const float* area,
+                                  const float* lambda_, int num_nodes, const float* v_new, const float* v,
+                                  const float* g, float* g_new, double* state, dp_stream_t stream);
 /* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
 int dp_nesterov_advance(double* state, dp_stream_t stream);
 /* Host planner: packs nets, in order, into chunks of at most max_pins pins (a

@@ -39,10 +39,13 @@ def test_engine_matches_autograd_path(design):
 
 
 def test_gp_converges_and_split_bf16_matches_plain(design):
-    _, plain, _ = run(design, "graph", "fp32")
-    _, split, _ = run(design, "graph", "split_bf16")
+    """Deterministic mode (int64 density maps), so the two runs differ only in
+    the Poisson-solve arithmetic."""
+    _, plain, _ = run(design, "graph", "fp32", deterministic=1)
+    _, split, _ = run(design, "graph", "split_bf16", deterministic=1)
     for r in (plain, split):
         assert r["overflow"] <= 0.07 + 1e-9 and r["iterations"] < 1000
+    print("plain", plain, "split", split, "rel", abs(split["hpwl"] - plain["hpwl"]) / plain["hpwl"])
     assert abs(split["hpwl"] - plain["hpwl"]) <= 1e-3 * plain["hpwl"], (split, plain)
 
 

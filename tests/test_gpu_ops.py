@@ -285,10 +285,36 @@ def test_density_map_exact_against_reference(C):
             np.testing.assert_allclose(got, exp.numpy(), rtol=1e-5, atol=1e-3)
 
 
+def spatial_order(d, pos, idx):
+    """Cells sorted by 16x16-bin tile, then bin (the engine's visiting order)."""
+    n = d.num_nodes
+    cx = pos[idx] + 0.5 * d.node_size_x[idx]
+    cy = pos[n + idx] + 0.5 * d.node_size_y[idx]
+    kx = np.clip(((cx - d.xl) / d.bin_size_x).astype(np.int64), 0, d.num_bins_x - 1)
+    hy = np.clip(((cy - d.yl) / d.bin_size_y).astype(np.int64), 0, d.num_bins_y - 1)
+    ty = (d.num_bins_y + 15) >> 4
+    key = (((kx >> 4) * ty + (hy >> 4)) << 8) | ((kx & 15) << 4) | (hy & 15)
+    return idx[np.argsort(key, kind="stable")].astype(np.int32)
+
+
+def pack_xy(pos, n):
+    return dev(np.stack([pos[:n], pos[n:]], axis=1).reshape(-1).astype(np.float32))
+
+
+def records(C, d, order):
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    rec4 = torch.empty(4 * len(order), device="cuda")
+    ratio_o = torch.empty(len(order), device="cuda")
+    inv = torch.zeros(d.num_nodes, dtype=torch.int32, device="cuda")
+    C.build_cell_records(sxc, syc, ox, oy, ratio, dev(order), len(order), rec4, ratio_o, inv)
+    return rec4, ratio_o, inv
+
+
 @pytest.mark.parametrize("layout", ["clustered", "spread"])
 def test_ordered_tiled_scatter(C, layout):
-    """The order-driven, shared-memory-tiled scatter: integer map bit-exact with the
-    oracle for any visiting order; fp32 map within atomic-order tolerance."""
+    """The order-driven scatter over per-cell records (register, shared-tile and
+    global paths): integer map bit-exact with the oracle for any visiting order;
+    fp32 map within atomic-order tolerance."""
     d = synthetic.scaled(20000, num_bins=128, seed=9)
     pos = d.initial_positions()
     n, m = d.num_nodes, d.num_movable_nodes
@@ -296,7 +322,6 @@ def test_ordered_tiled_scatter(C, layout):
         rng = np.random.RandomState(1)
         pos[:m] = rng.uniform(d.xl, d.xh - 40, size=m)
         pos[n:n + m] = rng.uniform(d.yl, d.yh - 12, size=m)
-    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
     s = oracle.stretched(d.node_size_x, d.node_size_y, d.bin_size_x, d.bin_size_y)
     ref_map, ref_fx = oracle.triangle_density_map(pos, *s, n, m, d.num_filler_nodes, d.num_bins_x, d.num_bins_y,
                                                   d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y,
@@ -304,13 +329,64 @@ def test_ordered_tiled_scatter(C, layout):
     f32_map, _ = oracle.triangle_density_map(pos, *s, n, m, d.num_filler_nodes, d.num_bins_x, d.num_bins_y,
                                              d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y)
     idx = np.r_[0:m, n - d.num_filler_nodes:n].astype(np.int32)
-    for order in (idx, np.random.RandomState(2).permutation(idx).astype(np.int32)):
+    xy = pack_xy(pos, n)
+    orders = (idx, np.random.RandomState(2).permutation(idx).astype(np.int32),
+              np.r_[spatial_order(d, pos, idx[:m]), spatial_order(d, pos, idx[m:])].astype(np.int32))
+    for order in orders:
+        rec4, ratio_o, _ = records(C, d, order)
         out = torch.empty(d.num_bins_x * d.num_bins_y, device="cuda")
         scratch = torch.empty(d.num_bins_x * d.num_bins_y, dtype=torch.int64, device="cuda")
-        C.density_map_ordered_into(dev(pos), sxc, syc, ox, oy, ratio, None, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
-                                   d.bin_size_y, d.num_bins_x, d.num_bins_y, dev(order), len(order), 1, scratch, out)
+        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
+                                   d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y, 1, scratch, out)
         assert np.array_equal(scratch.cpu().numpy(), ref_fx)
         assert np.array_equal(out.cpu().numpy(), ref_map)
-        C.density_map_ordered_into(dev(pos), sxc, syc, ox, oy, ratio, None, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
-                                   d.bin_size_y, d.num_bins_x, d.num_bins_y, dev(order), len(order), 0, None, out)
+        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
+                                   d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y, 0, None, out)
         np.testing.assert_allclose(out.cpu().numpy(), f32_map, rtol=1e-4, atol=1e-4 * float(np.max(f32_map)))
+
+
+def test_ordered_force_and_fused_assembly(C, golden):
+    """Field gather over records in visiting order: bit-exact with the golden
+    force per node.  Fused gradient assembly + preconditioner + step-size norms:
+    the gradient bit-exact with pin sum + force + dp_precondition_step_size, the
+    fp64 norms equal up to summation order."""
+    g = golden("design_small.npz")
+    d = small_design()
+    n, m, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+    pos_np = g["pos"].astype(np.float32)
+    idx = np.r_[0:m, n - nf:n].astype(np.int32)
+    order = np.r_[spatial_order(d, pos_np, idx[:m]), spatial_order(d, pos_np, idx[m:])].astype(np.int32)
+    rec4, ratio_o, inv = records(C, d, order)
+    xy = pack_xy(pos_np, n)
+    grad = torch.ones(1, device="cuda")
+    force_o = torch.empty(2 * len(order), device="cuda")
+    fx, fy = dev(g["field_x"]).view(-1), dev(g["field_y"]).view(-1)
+    C.electric_force_ordered(grad, fx, fy, xy, dev(order), rec4, ratio_o, len(order), d.xl, d.yl, d.bin_size_x,
+                             d.bin_size_y, d.num_bins_x, d.num_bins_y, -1.0, force_o)
+    fo = force_o.cpu().numpy().reshape(-1, 2)
+    assert np.array_equal(fo[:, 0], g["force"][order])
+    assert np.array_equal(fo[:, 1], g["force"][n + order])
+
+    # wirelength pin gradient in node-CSR order: any values exercise the sum
+    rng = np.random.RandomState(5)
+    node_start = dev(d.flat_node2pin_start_map.astype(np.int32))
+    gnode = dev(rng.standard_normal(2 * d.num_pins).astype(np.float32))
+    pws = dev(rng.uniform(0, 5, n).astype(np.float32))
+    area = dev((d.node_size_x * d.node_size_y).astype(np.float32))
+    lam = torch.tensor([1e-3], device="cuda")
+    v = dev(pos_np)
+    v_new = v + dev(rng.standard_normal(2 * n).astype(np.float32))
+    g_old = dev(rng.standard_normal(2 * n).astype(np.float32))
+    st_ref = torch.zeros(8 + 2 * 1280, dtype=torch.float64, device="cuda")
+    st_got = st_ref.clone()
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    exp = torch.empty(2 * n, device="cuda")
+    C.electric_force_into(grad, fx, fy, v, sxc, syc, ox, oy, ratio, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                          d.bin_size_y, d.num_bins_x, d.num_bins_y, m, nf, None, -1.0, exp)
+    C.node_pin_sum(gnode, node_start, grad, m, 1, exp)
+    C.precondition_step_size(exp, g_old, v_new, v, pws, area, lam, st_ref)
+    got = torch.empty(2 * n, device="cuda")
+    C.assemble_precondition_step(gnode, node_start, grad, force_o, inv, m, nf, pws, area, lam, v_new, v, g_old, got,
+                                 st_got)
+    assert torch.equal(got, exp)
+    np.testing.assert_allclose(st_got[:8].cpu().numpy(), st_ref[:8].cpu().numpy(), rtol=1e-12)
