@@ -106,58 +106,103 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
   }
 }
 
-// ---------------------------------------------------------------- tiled scatter
+// ---------------------------------------------------------------- window scatter
 // Cells are visited in the caller's order (a spatial order refreshed every few
-// iterations).  Each CTA takes kTileCells consecutive cells, reduces their bin
-// bounding box, and when it fits in shared memory accumulates there (shared
-// atomics) and flushes each touched bin with one global atomic; otherwise it
-// adds straight to global memory.  The fixed-point map is order independent,
-// so the deterministic result is unchanged by the tiling.
-constexpr int kTileThreads = 256;
-constexpr int kTileCellsPerThread = 4;
-constexpr int kTileCells = kTileThreads * kTileCellsPerThread;
-constexpr int kTileSmemBytes = 96 * 1024;
+// iterations, grouping cells whose stretched footprint starts in the same
+// bin), read from per-cell records (stretched width, height, offsets,
+// ratio) with the node position gathered from the interleaved xy array.
+//
+// A stretched cell is at least sqrt(2) bins wide, and a standard cell covers
+// at most kWin x kWin bins.  Each lane computes its cell's kWin px and kWin py
+// overlaps once and forms the kWin x kWin window of bin contributions in
+// registers (fp32, or int64 fixed point converted per contribution as the CPU
+// op does).  A lane keeps one running window while its successive cells start
+// at the same bin.  At the end, a run of lanes whose windows start at the same
+// bin is summed with a segmented shuffle reduction (only as many steps as the
+// longest run needs), and the run's first lane adds the window to the block's
+// shared-memory tile over its bin bounding box (or to global memory when the
+// box does not fit).  The tile is flushed with one global atomic per touched
+// bin.  Cells wider than the window take a plain per-bin loop.  In the
+// clustered start of GP, tens of thousands of cells share a bin, so one warp
+// issues kWin*kWin adds for its 128 cells; when cells are spread each cell
+// flushes its own window and adds only its own bins.  The fixed-point map is
+// independent of the summation order, so the deterministic result does not
+// depend on the visiting order or the tiling.
+constexpr int kWin = 4;
+constexpr int kWsThreads = 256;
+constexpr int kWsCellsPerLane = 4;
+constexpr int kWsWarpCells = 32 * kWsCellsPerLane;
+constexpr int kWsCells = kWsThreads * kWsCellsPerLane;
+constexpr int kWsSmemBytes = 32 * 1024;
 
-// Per-cell records in visiting order: rec4 = (stretched width, stretched
-// height, offset x, offset y) and ratio, so a block reads its cells' attributes
-// contiguously and gathers only the node position (one 8-byte load from xy).
+template <typename Acc>
+__device__ __forceinline__ void add_to(Acc* tile, float* map_f32, unsigned long long* map_fx, bool use_tile, int slot,
+                                       int bin, Acc v) {
+  if (use_tile) {
+    atomicAdd(tile + slot, v);
+  } else if (sizeof(Acc) == 8) {
+    atomicAdd(map_fx + bin, (unsigned long long)v);
+  } else {
+    atomicAdd(map_f32 + bin, (float)v);
+  }
+}
+
+// adds the non-zero entries of a window starting at bin (k0, h0)
+template <typename Acc>
+__device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0, int h0, int bk0, int bh0, int H,
+                                             int nby, bool use_tile, Acc* tile, float* map_f32,
+                                             unsigned long long* map_fx) {
+#pragma unroll
+  for (int kk = 0; kk < kWin; ++kk)
+#pragma unroll
+    for (int hh = 0; hh < kWin; ++hh)
+      if (w[kk][hh] != (Acc)0) {
+        const int k = k0 + kk, h = h0 + hh;
+        add_to<Acc>(tile, map_f32, map_fx, use_tile, (k - bk0) * H + (h - bh0), k * nby + h, w[kk][hh]);
+      }
+}
+
 template <bool kFixed>
-__global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(TriangleArgs a, const float2* __restrict__ xy,
-                                                                         const int* __restrict__ order,
-                                                                         const float4* __restrict__ rec4,
-                                                                         const float* __restrict__ ratio_o, int count,
-                                                                         float fx_scale, float* map_f32,
-                                                                         unsigned long long* map_fx) {
+__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a, const float2* __restrict__ xy,
+                                                                        const int* __restrict__ order,
+                                                                        const float4* __restrict__ rec4,
+                                                                        const float* __restrict__ ratio_o, int count,
+                                                                        float fx_scale, float* map_f32,
+                                                                        unsigned long long* map_fx) {
   extern __shared__ __align__(16) unsigned char tile_raw[];
   using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
   Acc* tile = reinterpret_cast<Acc*>(tile_raw);
-  constexpr int kCap = kTileSmemBytes / sizeof(Acc);
-  constexpr int kTiny = 16;  // boxes of at most 16 bins accumulate in registers
-  __shared__ int red[4][kTileThreads / 32];
-  const int base = blockIdx.x * kTileCells;
-  int kx0[kTileCellsPerThread], kx1[kTileCellsPerThread], hy0[kTileCellsPerThread], hy1[kTileCellsPerThread];
-  float nx[kTileCellsPerThread], ny[kTileCellsPerThread], sxs[kTileCellsPerThread], sys[kTileCellsPerThread],
-      rr[kTileCellsPerThread];
+  constexpr int kCap = kWsSmemBytes / sizeof(Acc);
+  __shared__ int red[4][kWsThreads / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // each warp takes kWsWarpCells consecutive cells, each lane kWsCellsPerLane
+  // consecutive ones, so cells of one window start bin (sorted together) meet
+  // in one lane's running window and then in neighbouring lanes
+  const int wbase = blockIdx.x * kWsCells + warp * kWsWarpCells;
+  float nx[kWsCellsPerLane], ny[kWsCellsPerLane], sxs[kWsCellsPerLane], sys[kWsCellsPerLane], rr[kWsCellsPerLane];
   int bk0 = INT_MAX, bk1 = INT_MIN, bh0 = INT_MAX, bh1 = INT_MIN;
+  unsigned live = 0;
 #pragma unroll
-  for (int c = 0; c < kTileCellsPerThread; ++c) {
-    int idx = base + c * kTileThreads + threadIdx.x;
-    kx0[c] = kx1[c] = hy0[c] = hy1[c] = 0;
+  for (int c = 0; c < kWsCellsPerLane; ++c) {
+    const int idx = wbase + lane * kWsCellsPerLane + c;
+    nx[c] = ny[c] = sxs[c] = sys[c] = rr[c] = 0.f;
     if (idx < count) {
-      const float4 r4 = __ldcs(rec4 + idx);
+      const float4 r4 = __ldg(rec4 + idx);
       const float2 p = xy[order[idx]];
       sxs[c] = r4.x;
       sys[c] = r4.y;
       nx[c] = fadd(p.x, r4.z);
       ny[c] = fadd(p.y, r4.w);
-      rr[c] = __ldcs(ratio_o + idx);
-      triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, kx0[c], kx1[c]);
-      triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, hy0[c], hy1[c]);
-      if (kx1[c] > kx0[c] && hy1[c] > hy0[c]) {
-        bk0 = min(bk0, kx0[c]);
-        bk1 = max(bk1, kx1[c]);
-        bh0 = min(bh0, hy0[c]);
-        bh1 = max(bh1, hy1[c]);
+      rr[c] = __ldg(ratio_o + idx);
+      int k0, k1, h0, h1;
+      triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
+      triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
+      if (k1 > k0 && h1 > h0) {
+        live |= 1u << c;
+        bk0 = min(bk0, k0);
+        bk1 = max(bk1, k1);
+        bh0 = min(bh0, h0);
+        bh1 = max(bh1, h1);
       }
     }
   }
@@ -167,131 +212,123 @@ __global__ void __launch_bounds__(kTileThreads, 2) tiled_scatter_kernel(Triangle
     bh0 = min(bh0, __shfl_xor_sync(0xffffffffu, bh0, o));
     bh1 = max(bh1, __shfl_xor_sync(0xffffffffu, bh1, o));
   }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) {
-    red[0][w] = bk0;
-    red[1][w] = bk1;
-    red[2][w] = bh0;
-    red[3][w] = bh1;
+  if (lane == 0) {
+    red[0][warp] = bk0;
+    red[1][warp] = bk1;
+    red[2][warp] = bh0;
+    red[3][warp] = bh1;
   }
   __syncthreads();
   bk0 = INT_MAX; bk1 = INT_MIN; bh0 = INT_MAX; bh1 = INT_MIN;
 #pragma unroll
-  for (int i = 0; i < kTileThreads / 32; ++i) {
+  for (int i = 0; i < kWsThreads / 32; ++i) {
     bk0 = min(bk0, red[0][i]);
     bk1 = max(bk1, red[1][i]);
     bh0 = min(bh0, red[2][i]);
     bh1 = max(bh1, red[3][i]);
   }
   if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
-  const int W = bk1 - bk0, H = bh1 - bh0;
-  if (W * H <= kTiny) {
-    // clustered block: per-thread register accumulators, a warp reduction per
-    // bin, one shared atomic per warp and bin, one global atomic per bin
-    Acc acc[kTiny];
-#pragma unroll
-    for (int j = 0; j < kTiny; ++j) acc[j] = (Acc)0;
-#pragma unroll
-    for (int c = 0; c < kTileCellsPerThread; ++c) {
-      for (int k = kx0[c]; k < kx1[c]; ++k) {
-        const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
-        for (int h = hy0[c]; h < hy1[c]; ++h) {
-          const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
-          const Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
-          const int slot = (k - bk0) * H + (h - bh0);
-#pragma unroll
-          for (int j = 0; j < kTiny; ++j)
-            if (j == slot) acc[j] += v;
-        }
-      }
-    }
-    for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = (Acc)0;
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kTiny; ++j) {
-      Acc v = acc[j];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (l == 0 && j < W * H && v != (Acc)0) atomicAdd(&tile[j], v);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < W * H; t += kTileThreads) {
-      Acc v = tile[t];
-      if (v != (Acc)0) {
-        int bin = (bk0 + t / H) * a.num_bins_y + bh0 + t % H;
-        if (kFixed)
-          atomicAdd(map_fx + bin, (unsigned long long)v);
-        else
-          atomicAdd(map_f32 + bin, (float)v);
-      }
-    }
-    return;
-  }
-  const bool use_tile = (long long)W * H <= kCap;
+  const int H = bh1 - bh0;
+  const bool use_tile = (long long)(bk1 - bk0) * H <= kCap;
   if (use_tile) {
-    for (int t = threadIdx.x; t < W * H; t += kTileThreads) tile[t] = 0;
+    for (int t = threadIdx.x; t < (bk1 - bk0) * H; t += kWsThreads) tile[t] = (Acc)0;
     __syncthreads();
   }
-  // Dense boxes (more cell-bin updates than bins) first combine the lanes of a
-  // warp that hit the same bin, so each bin takes one shared atomic per warp.
-  const bool combine = use_tile && (long long)W * H * 4 < (long long)kTileCells;
+  const int nby = a.num_bins_y;
+  unsigned wide = 0;
+  // Running window of this lane: consecutive cells of the lane whose windows
+  // start at the same bin accumulate in registers; a new start bin flushes the
+  // previous window with direct adds.
+  Acc acc[kWin][kWin];
 #pragma unroll
-  for (int c = 0; c < kTileCellsPerThread; ++c) {
-    const int nk = max(kx1[c] - kx0[c], 0), nh = max(hy1[c] - hy0[c], 0);
-    const int trips = nk * nh;
-    if (combine) {
-      int max_trips = trips;
-      for (int o = 16; o > 0; o >>= 1) max_trips = max(max_trips, __shfl_xor_sync(0xffffffffu, max_trips, o));
-      float pxr = 0.f;
-      int cur_k = -1;
-      for (int t = 0; t < max_trips; ++t) {
-        const bool live = t < trips;
-        const unsigned active = __ballot_sync(0xffffffffu, live);
-        if (live) {
-          const int k = kx0[c] + t / nh, h = hy0[c] + t % nh;
-          if (k != cur_k) {
-            pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
-            cur_k = k;
-          }
-          const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
-          const int slot = (k - bk0) * H + (h - bh0);
-          const unsigned peers = __match_any_sync(active, slot);
-          const int leader = __ffs(peers) - 1;
-          const Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
-          Acc sum = v;  // peers' own values are shuffled, never the running sum
-          unsigned rest = peers & (peers - 1);
-          while (rest) {
-            const int src = __ffs(rest) - 1;
-            rest &= rest - 1;
-            sum += __shfl_sync(peers, v, src);
-          }
-          if ((int)(threadIdx.x & 31) == leader) atomicAdd(&tile[slot], sum);
-        }
-      }
+  for (int kk = 0; kk < kWin; ++kk)
+#pragma unroll
+    for (int hh = 0; hh < kWin; ++hh) acc[kk][hh] = (Acc)0;
+  int run_key = -1 - lane;  // no window yet: a key no other lane holds
+  int run_k0 = 0, run_h0 = 0;
+#pragma unroll
+  for (int c = 0; c < kWsCellsPerLane; ++c) {
+    if (!(live & (1u << c))) continue;
+    int k0, k1, h0, h1;
+    triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
+    triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
+    const int nk = k1 - k0, nh = h1 - h0;
+    if (nk > kWin || nh > kWin) {
+      wide |= 1u << c;
       continue;
     }
-    for (int k = kx0[c]; k < kx1[c]; ++k) {
-      float px = triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx);
-      float pxr = fmul(px, rr[c]);
-      for (int h = hy0[c]; h < hy1[c]; ++h) {
-        float py = triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy);
-        float area = fmul(pxr, py);
-        if (use_tile) {
-          Acc v = kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
-          atomicAdd(&tile[(k - bk0) * H + (h - bh0)], v);
-        } else if (kFixed) {
-          atomicAdd(map_fx + k * a.num_bins_y + h, (unsigned long long)to_fixed(area, fx_scale));
-        } else {
-          atomicAdd(map_f32 + k * a.num_bins_y + h, area);
+    const int key = k0 * nby + h0;
+    if (key != run_key) {
+      if (run_key >= 0) flush_window<Acc>(acc, run_k0, run_h0, bk0, bh0, H, nby, use_tile, tile, map_f32, map_fx);
+#pragma unroll
+      for (int kk = 0; kk < kWin; ++kk)
+#pragma unroll
+        for (int hh = 0; hh < kWin; ++hh) acc[kk][hh] = (Acc)0;
+      run_key = key;
+      run_k0 = k0;
+      run_h0 = h0;
+    }
+    float py[kWin];
+#pragma unroll
+    for (int hh = 0; hh < kWin; ++hh) py[hh] = hh < nh ? triangle_overlap(ny[c], sys[c], a.yl, h0 + hh, a.bsy) : 0.f;
+#pragma unroll
+    for (int kk = 0; kk < kWin; ++kk) {
+      if (kk < nk) {
+        const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k0 + kk, a.bsx), rr[c]);
+#pragma unroll
+        for (int hh = 0; hh < kWin; ++hh) {
+          if (hh < nh) {
+            const float area = fmul(pxr, py[hh]);
+            acc[kk][hh] += kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
+          }
         }
+      }
+    }
+  }
+  // runs of lanes whose windows start at the same bin are summed into the
+  // run's first lane; lanes without a window hold unique keys
+  {
+    const int prev = __shfl_up_sync(0xffffffffu, run_key, 1);
+    const bool head = lane == 0 || prev != run_key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned later = lane == 31 ? 0u : heads & (0xfffffffeu << lane);
+    const int seg_end = later ? __ffs(later) - 2 : 31;
+    const int run = head ? seg_end - lane + 1 : 0;
+    const int longest = (int)__reduce_max_sync(0xffffffffu, (unsigned)run);
+    for (int o = 1; o < longest; o <<= 1) {
+      const bool take = lane + o <= seg_end;
+#pragma unroll
+      for (int kk = 0; kk < kWin; ++kk)
+#pragma unroll
+        for (int hh = 0; hh < kWin; ++hh) {
+          const Acc t = __shfl_down_sync(0xffffffffu, acc[kk][hh], o);
+          if (take) acc[kk][hh] += t;
+        }
+    }
+    if (head && run_key >= 0) flush_window<Acc>(acc, run_k0, run_h0, bk0, bh0, H, nby, use_tile, tile, map_f32, map_fx);
+  }
+  // cells wider than the window: one add per bin
+#pragma unroll
+  for (int c = 0; c < kWsCellsPerLane; ++c) {
+    if (!(wide & (1u << c))) continue;
+    int k0, k1, h0, h1;
+    triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
+    triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
+    for (int k = k0; k < k1; ++k) {
+      const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
+      for (int h = h0; h < h1; ++h) {
+        const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
+        add_to<Acc>(tile, map_f32, map_fx, use_tile, (k - bk0) * H + (h - bh0), k * nby + h,
+                    kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area);
       }
     }
   }
   if (use_tile) {
     __syncthreads();
-    for (int t = threadIdx.x; t < W * H; t += kTileThreads) {
-      Acc v = tile[t];
+    for (int t = threadIdx.x; t < (bk1 - bk0) * H; t += kWsThreads) {
+      const Acc v = tile[t];
       if (v != (Acc)0) {
-        int bin = (bk0 + t / H) * a.num_bins_y + bh0 + t % H;
+        const int bin = (bk0 + t / H) * nby + bh0 + t % H;
         if (kFixed)
           atomicAdd(map_fx + bin, (unsigned long long)v);
         else
@@ -627,8 +664,6 @@ extern "C" int dp_density_overflow(const float* map, int nbins, double target_ar
   return check_launch("dp_density_overflow finish");
 }
 
-// Order-driven scatter (see tiled_scatter_kernel): `order` lists the nodes to
-// scatter (movable and/or filler indices, any order).
 // Per-cell records for the order-driven kernels: rec4[idx] = (sx, sy, ox, oy)
 // and ratio_o[idx] of node order[idx]; inv_order[order[idx]] = idx (optional).
 extern "C" int dp_build_cell_records(const float* sx, const float* sy, const float* ox, const float* oy,
@@ -642,7 +677,7 @@ extern "C" int dp_build_cell_records(const float* sx, const float* sy, const flo
   return check_launch("dp_build_cell_records");
 }
 
-// Order-driven scatter (see tiled_scatter_kernel): the cells order[0..count)
+// Order-driven scatter (see window_scatter_kernel): the cells order[0..count)
 // with their records, positions interleaved in xy.
 extern "C" int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
                                       int count, const float* init, float xl, float yl, float xh, float yh, float bsx,
@@ -657,8 +692,8 @@ extern "C" int dp_density_map_ordered(const float* xy, const int* order, const f
   int nbins = nbx * nby;
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(tiled_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes);
-    cudaFuncSetAttribute(tiled_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes);
+    cudaFuncSetAttribute(window_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
+    cudaFuncSetAttribute(window_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
     configured = true;
   }
   TriangleArgs a;
@@ -667,13 +702,13 @@ extern "C" int dp_density_map_ordered(const float* xy, const int* order, const f
   a.num_bins_x = nbx; a.num_bins_y = nby;
   const float2* p2 = reinterpret_cast<const float2*>(xy);
   const float4* r4 = reinterpret_cast<const float4*>(rec4);
-  int blocks = ceil_div(count, kTileCells);
+  int blocks = ceil_div(count, kWsCells);
   int rc;
   if (deterministic) {
     DP_REQUIRE(fraction_bits >= 0 && fraction_bits <= 62, "dp_density_map_ordered: bad fraction_bits");
     cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
     if (blocks > 0) {
-      tiled_scatter_kernel<true><<<blocks, kTileThreads, kTileSmemBytes, s>>>(
+      window_scatter_kernel<true><<<blocks, kWsThreads, kWsSmemBytes, s>>>(
           a, p2, order, r4, ratio_o, count, ldexpf(1.0f, fraction_bits), nullptr,
           reinterpret_cast<unsigned long long*>(scratch));
       rc = check_launch("dp_density_map_ordered scatter");
@@ -690,8 +725,8 @@ extern "C" int dp_density_map_ordered(const float* xy, const int* order, const f
     cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
   }
   if (blocks == 0) return DP_OK;
-  tiled_scatter_kernel<false><<<blocks, kTileThreads, kTileSmemBytes, s>>>(a, p2, order, r4, ratio_o, count, 0.f,
-                                                                            out, nullptr);
+  window_scatter_kernel<false><<<blocks, kWsThreads, kWsSmemBytes, s>>>(a, p2, order, r4, ratio_o, count, 0.f, out,
+                                                                         nullptr);
   return check_launch("dp_density_map_ordered scatter");
 }
 

@@ -56,6 +56,8 @@ __global__ void zero_range_kernel(float* a, int begin, int end, float* b) {
   }
 }
 
+constexpr int kForceWin = 4;  // standard cells cover at most 4 x 4 bins
+
 // Field gather over cells in visiting order (engine path): attributes from the
 // per-cell records, position from xy; the force pair is written in order
 // space, force_o[idx] = scale * grad * ratio * sum(px py E), for the gradient
@@ -75,16 +77,40 @@ __global__ void __launch_bounds__(256) electric_force_records_kernel(
     int k0, k1, h0, h1;
     triangle_bin_range(nx, sx, xl, ibx, nbx, k0, k1);
     triangle_bin_range(ny, sy, yl, iby, nby, h0, h1);
+    const int nk = k1 - k0, nh = h1 - h0;
     float gx = 0.f, gy = 0.f;
-    for (int k = k0; k < k1; ++k) {
-      const float px = triangle_overlap(nx, sx, xl, k, bsx);
-      const float* exr = ex + (size_t)k * nby;
-      const float* eyr = ey + (size_t)k * nby;
-      for (int h = h0; h < h1; ++h) {
-        const float py = triangle_overlap(ny, sy, yl, h, bsy);
-        const float area = fmul(px, py);
-        gx = fadd(gx, fmul(area, __ldg(exr + h)));
-        gy = fadd(gy, fmul(area, __ldg(eyr + h)));
+    if (nk <= kForceWin && nh <= kForceWin) {
+      // py computed once per y bin; the sum keeps the k-major, h-minor order
+      float py[kForceWin];
+#pragma unroll
+      for (int hh = 0; hh < kForceWin; ++hh) py[hh] = hh < nh ? triangle_overlap(ny, sy, yl, h0 + hh, bsy) : 0.f;
+#pragma unroll
+      for (int kk = 0; kk < kForceWin; ++kk) {
+        if (kk < nk) {
+          const float px = triangle_overlap(nx, sx, xl, k0 + kk, bsx);
+          const float* exr = ex + (size_t)(k0 + kk) * nby + h0;
+          const float* eyr = ey + (size_t)(k0 + kk) * nby + h0;
+#pragma unroll
+          for (int hh = 0; hh < kForceWin; ++hh) {
+            if (hh < nh) {
+              const float area = fmul(px, py[hh]);
+              gx = fadd(gx, fmul(area, __ldg(exr + hh)));
+              gy = fadd(gy, fmul(area, __ldg(eyr + hh)));
+            }
+          }
+        }
+      }
+    } else {
+      for (int k = k0; k < k1; ++k) {
+        const float px = triangle_overlap(nx, sx, xl, k, bsx);
+        const float* exr = ex + (size_t)k * nby;
+        const float* eyr = ey + (size_t)k * nby;
+        for (int h = h0; h < h1; ++h) {
+          const float py = triangle_overlap(ny, sy, yl, h, bsy);
+          const float area = fmul(px, py);
+          gx = fadd(gx, fmul(area, __ldg(exr + h)));
+          gy = fadd(gy, fmul(area, __ldg(eyr + h)));
+        }
       }
     }
     const float r = __ldcs(ratio_o + idx);

@@ -132,17 +132,19 @@ class GPEngine(object):
                                    ep.num_bins_y, int(self.det), self.scratch, out)
 
     def refresh_order(self, v):
-        """Sort movable and filler cells by 16x16-bin tile, then by bin inside the
-        tile (keeps each scatter block's cells on a compact patch of bins)."""
+        """Sort movable and filler cells by the bin where their stretched footprint
+        starts: 16x16-bin tiles in serpentine order (neighbouring tiles follow each
+        other), then bin inside the tile.  Each scatter block's cells then cover a
+        compact patch of bins, and cells with the same start bin are adjacent."""
         d, ep = self.design, self.ep
         n, nm, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
         with torch.no_grad():
-            cx = v[:n] + 0.5 * self.data.node_size_x
-            cy = v[n:] + 0.5 * self.data.node_size_y
-            kx = ((cx - ep.xl) * (1.0 / ep.bin_size_x)).clamp_(0, ep.num_bins_x - 1).to(torch.int64)
-            hy = ((cy - ep.yl) * (1.0 / ep.bin_size_y)).clamp_(0, ep.num_bins_y - 1).to(torch.int64)
+            kx = ((v[:n] + ep.offset_x - ep.xl) * (1.0 / ep.bin_size_x)).clamp_(0, ep.num_bins_x - 1).to(torch.int64)
+            hy = ((v[n:] + ep.offset_y - ep.yl) * (1.0 / ep.bin_size_y)).clamp_(0, ep.num_bins_y - 1).to(torch.int64)
             tiles_y = (ep.num_bins_y + 15) >> 4
-            key = (((kx >> 4) * tiles_y + (hy >> 4)) << 8) | ((kx & 15) << 4) | (hy & 15)
+            tx, ty = kx >> 4, hy >> 4
+            ty = ty + (tx & 1) * (tiles_y - 1 - 2 * ty)
+            key = ((tx * tiles_y + ty) << 8) | ((kx & 15) << 4) | (hy & 15)
             om = torch.argsort(key[:nm]).to(torch.int32)
             self.order[:nm].copy_(om)
             if nf:

@@ -286,14 +286,17 @@ def test_density_map_exact_against_reference(C):
 
 
 def spatial_order(d, pos, idx):
-    """Cells sorted by 16x16-bin tile, then bin (the engine's visiting order)."""
+    """The engine's visiting order: cells sorted by the bin where their
+    stretched footprint starts, 16x16-bin tiles in serpentine order."""
     n = d.num_nodes
-    cx = pos[idx] + 0.5 * d.node_size_x[idx]
-    cy = pos[n + idx] + 0.5 * d.node_size_y[idx]
-    kx = np.clip(((cx - d.xl) / d.bin_size_x).astype(np.int64), 0, d.num_bins_x - 1)
-    hy = np.clip(((cy - d.yl) / d.bin_size_y).astype(np.int64), 0, d.num_bins_y - 1)
+    s = oracle.stretched(d.node_size_x, d.node_size_y, d.bin_size_x, d.bin_size_y)
+    ox, oy = s[2], s[3]
+    kx = np.clip(((pos[idx] + ox[idx] - d.xl) / d.bin_size_x).astype(np.int64), 0, d.num_bins_x - 1)
+    hy = np.clip(((pos[n + idx] + oy[idx] - d.yl) / d.bin_size_y).astype(np.int64), 0, d.num_bins_y - 1)
     ty = (d.num_bins_y + 15) >> 4
-    key = (((kx >> 4) * ty + (hy >> 4)) << 8) | ((kx & 15) << 4) | (hy & 15)
+    tx, tyy = kx >> 4, hy >> 4
+    tyy = np.where(tx & 1, ty - 1 - tyy, tyy)
+    key = ((tx * ty + tyy) << 8) | ((kx & 15) << 4) | (hy & 15)
     return idx[np.argsort(key, kind="stable")].astype(np.int32)
 
 
