@@ -240,8 +240,23 @@ def _graph_time(fn, reps=20):
 
 
 def kernel_roofline(placer, design, peaks, reps=20):
-    """Device time of each piece of one GP iteration of the engine (each piece
-    graph-captured and replayed) with its algorithmic bytes or flops."""
+    """Device time of each piece of one Nesterov trial of the engine (each piece
+    graph-captured and replayed) with its algorithmic bytes or flops:
+
+    * density_scatter: per scattered cell 16 B record + 4 B ratio + 4 B order
+      index + 8 B position; per bin 4 B initial map read, movable-only map
+      written and read back by the overflow reduction, full map written;
+    * poisson_gemms: the four GEMM launches' flops;
+    * field_gather: per cell the same 32 B as the scatter + 8 B force written;
+      per bin the two field maps read once;
+    * wa_forward (HPWL included): per pin 20 B of pin arrays + 8 B gradient
+      written; per net 4 B start + 2 x 1 B masks + 4 B weight; per node 8 B
+      position;
+    * assemble_precondition: per pin 8 B gradient read; per node 4 B pin
+      start + 4 B inverse order + 8 B force + 4 B pin weight sum + 4 B area +
+      3 x 8 B (v_new, v, g) read + 8 B written;
+    * nesterov_trial: per node 3 x 8 B read (v, g, u), 2 x 8 B written (u, v)
+      + 8 B interleaved copy + 8 B cell size."""
     from dreamplace_b200.dct2_fft2 import gemm_flops
     from dreamplace_b200.electric_potential import poisson_solve
     eng = placer.stepper.eng
@@ -251,22 +266,23 @@ def kernel_roofline(placer, design, peaks, reps=20):
     M, N = ep.num_bins_x, ep.num_bins_y
     P, E, n = d.num_pins, d.num_nets, d.num_nodes
     p = eng.parity
-    v, g, u = eng.V[p], eng.G[p], eng.U[p]
+    q = 1 - p
+    v, g = eng.V[p], eng.G[p]
+    vn, gn = eng.V[q], eng.G[q]
+    saved = eng.state.clone()
     res = {}
-    res["density_scatter"] = (_graph_time(lambda: eng._density(v, ep.num_filler_nodes, eng.dmap), reps),
-                              28.0 * n_s + 4.0 * n_s + 8.0 * M * N, "hbm")
+    res["density_scatter"] = (_graph_time(lambda: eng.scatter_maps(v, eng.O[q]), reps),
+                              32.0 * n_s + 16.0 * M * N, "hbm")
     rho = eng.dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
     res["poisson_gemms"] = (_graph_time(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec), reps),
                             gemm_flops(M, N, eng.prec, 4), "tensor" if eng.prec else "fp32")
     ex, ey, _ = poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec)
-    res["field_gather"] = (_graph_time(lambda: eng.density_grad_into(v, ex, ey, eng.one, eng.tmp), reps),
-                           36.0 * n_s + 8.0 * M * N, "hbm")
-    res["wa_forward"] = (_graph_time(lambda: eng.wirelength(v), reps), 20.0 * P + 9.0 * E + 8.0 * n, "hbm")
-    res["wa_backward_pin_sum"] = (_graph_time(lambda: eng.wl_grad_into(eng.tmp, True), reps),
-                                  16.0 * P + 16.0 * n, "hbm")
-    res["hpwl"] = (_graph_time(lambda: eng.evaluate(v), reps), 12.0 * P + 5.0 * E + 8.0 * n, "hbm")
-    saved = eng.state.clone()
-    res["nesterov_trial"] = (_graph_time(lambda: eng.nesterov_trial_only(p), reps), 20.0 * 2 * n, "hbm")
+    res["field_gather"] = (_graph_time(lambda: eng.field_force(v, ex, ey), reps), 40.0 * n_s + 8.0 * M * N, "hbm")
+    res["wa_forward"] = (_graph_time(lambda: eng.wirelength(v, eng.H[q]), reps), 28.0 * P + 10.0 * E + 8.0 * n,
+                         "hbm")
+    res["assemble_precondition"] = (_graph_time(lambda: eng.assemble(v, g, vn, gn), reps), 8.0 * P + 64.0 * n,
+                                    "hbm")
+    res["nesterov_trial"] = (_graph_time(lambda: eng.nesterov_trial_only(p), reps), 64.0 * n, "hbm")
     eng.state.copy_(saved)
     return res
 

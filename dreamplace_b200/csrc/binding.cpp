@@ -388,10 +388,12 @@ void precondition_step_size(at::Tensor g_new, at::Tensor g, at::Tensor v_new, at
 
 void nesterov_advance(at::Tensor state) { DP_CALL(dp_nesterov_advance(ptr<double>(state), cur_stream())); }
 
-void objective_finish(at::Tensor wl, at::Tensor energy, at::Tensor density_weight, double density_factor,
-                      double quad_c, at::Tensor obj, at::Tensor grad_scale) {
-  DP_CALL(dp_objective_finish(ptr<double>(wl), ptr<double>(energy), ptr<float>(density_weight), (float)density_factor,
-                              (float)quad_c, ptr<double>(obj), ptr<float>(grad_scale), cur_stream()));
+void objective_finish(at::Tensor wl, at::Tensor energy, at::Tensor density_weight, at::Tensor factor_quad,
+                      at::Tensor obj, at::Tensor grad_scale) {
+  CHECK_F32(factor_quad);
+  TORCH_CHECK(factor_quad.numel() >= 2, "factor_quad holds (density_factor, quad_c)");
+  DP_CALL(dp_objective_finish(ptr<double>(wl), ptr<double>(energy), ptr<float>(density_weight),
+                              ptr<float>(factor_quad), ptr<double>(obj), ptr<float>(grad_scale), cur_stream()));
 }
 
 // density scatter into a caller-owned map (no allocation; graph friendly)
@@ -438,6 +440,23 @@ void density_map_ordered_into(at::Tensor xy, at::Tensor order, at::Tensor rec4, 
                                  (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy), nbx, nby,
                                  deterministic, fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch),
                                  ptr<float>(out), cur_stream()));
+}
+
+void density_map_ordered_split(at::Tensor xy, at::Tensor order, at::Tensor rec4, at::Tensor ratio_o, int num_first,
+                               int count, c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh,
+                               double bsx, double bsy, int nbx, int nby, int deterministic,
+                               c10::optional<at::Tensor> scratch, at::Tensor out_first, at::Tensor out_all) {
+  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(rec4);
+  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
+              "density_map_ordered_split: buffers smaller than count");
+  TORCH_CHECK(out_first.numel() == (int64_t)nbx * nby && out_all.numel() == out_first.numel(),
+              "density_map_ordered_split: outputs are not num_bins_x*num_bins_y");
+  TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
+  DP_CALL(dp_density_map_ordered_split(ptr<float>(xy), ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o),
+                                       num_first, count, (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
+                                       inv_f(bsx), inv_f(bsy), nbx, nby, deterministic, fraction_bits(xl, yl, xh, yh),
+                                       (int64_t*)ovp(scratch), ptr<float>(out_first), ptr<float>(out_all),
+                                       cur_stream()));
 }
 
 void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy, at::Tensor order,
@@ -495,14 +514,20 @@ at::Tensor plan_net_chunks(at::Tensor netpin_start_cpu, int max_pins) {
 void wa_chunk_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
                       at::Tensor slot_net, at::Tensor netpin_start, at::Tensor chunk_net,
                       c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor inv_gamma,
-                      at::Tensor csr_pos, at::Tensor wl_f64, at::Tensor grad_node_order) {
+                      at::Tensor csr_pos, at::Tensor wl_f64, at::Tensor grad_node_order,
+                      c10::optional<at::Tensor> hpwl_mask, c10::optional<at::Tensor> hpwl_f64) {
   CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(chunk_net); CHECK_I32(csr_pos); CHECK_F32(grad_node_order);
   TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
+  TORCH_CHECK(!hpwl_f64.has_value() || (hpwl_mask.has_value() && hpwl_f64->scalar_type() == at::kDouble &&
+                                        hpwl_f64->numel() >= DP_REDUCE_DOUBLES),
+              "hpwl_f64 needs hpwl_mask and DP_REDUCE_DOUBLES doubles");
   DP_CALL(dp_wa_chunk_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
                               ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(netpin_start), ptr<int>(chunk_net),
                               chunk_net.numel() - 1, (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
                               ptr<float>(inv_gamma), ptr<int>(csr_pos), ptr<double>(wl_f64),
-                              ptr<float>(grad_node_order), slot_node.numel(), cur_stream()));
+                              ptr<float>(grad_node_order), slot_node.numel(),
+                              hpwl_mask.has_value() ? hpwl_mask->data_ptr<uint8_t>() : nullptr,
+                              (double*)ovp(hpwl_f64), cur_stream()));
 }
 
 void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy, at::Tensor slot_net,
@@ -558,6 +583,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("density_overflow_into", &density_overflow_into);
   m.def("density_map_ordered_into", &density_map_ordered_into);
   m.def("build_cell_records", &build_cell_records);
+  m.def("density_map_ordered_split", &density_map_ordered_split);
   m.def("electric_force_ordered", &electric_force_ordered);
   m.def("assemble_precondition_step", &assemble_precondition_step);
   m.def("plan_net_chunks", &plan_net_chunks);

@@ -679,55 +679,135 @@ extern "C" int dp_build_cell_records(const float* sx, const float* sy, const flo
 
 // Order-driven scatter (see window_scatter_kernel): the cells order[0..count)
 // with their records, positions interleaved in xy.
-extern "C" int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
-                                      int count, const float* init, float xl, float yl, float xh, float yh, float bsx,
-                                      float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
-                                      int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
-  DP_REQUIRE(xy && rec4 && ratio_o && out && (count == 0 || order), "dp_density_map_ordered: null pointer");
-  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)rec4 & 15) == 0, "dp_density_map_ordered: misaligned xy/rec4");
-  DP_REQUIRE(nbx > 0 && nby > 0 && (long long)nbx * nby < (1ll << 31), "dp_density_map_ordered: bad bin grid");
-  DP_REQUIRE(bsx > 0 && bsy > 0 && count >= 0, "dp_density_map_ordered: bad geometry");
-  DP_REQUIRE(!deterministic || scratch, "dp_density_map_ordered: deterministic mode needs scratch_fixed");
-  cudaStream_t s = as_stream(stream);
-  int nbins = nbx * nby;
+namespace {
+
+struct OrderedScatter {
+  TriangleArgs a;
+  const float2* xy;
+  const int* order;
+  const float4* rec4;
+  const float* ratio_o;
+  cudaStream_t s;
+};
+
+// adds cells [begin, end) of the visiting order onto out (fp32) or scratch (fixed)
+int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits, int64_t* scratch,
+                  float* out) {
   static bool configured = false;
   if (!configured) {
     cudaFuncSetAttribute(window_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
     cudaFuncSetAttribute(window_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
     configured = true;
   }
-  TriangleArgs a;
-  memset(&a, 0, sizeof(a));
-  a.xl = xl; a.yl = yl; a.bsx = bsx; a.bsy = bsy; a.inv_bsx = ibx; a.inv_bsy = iby;
-  a.num_bins_x = nbx; a.num_bins_y = nby;
-  const float2* p2 = reinterpret_cast<const float2*>(xy);
-  const float4* r4 = reinterpret_cast<const float4*>(rec4);
-  int blocks = ceil_div(count, kWsCells);
-  int rc;
-  if (deterministic) {
-    DP_REQUIRE(fraction_bits >= 0 && fraction_bits <= 62, "dp_density_map_ordered: bad fraction_bits");
-    cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
-    if (blocks > 0) {
-      window_scatter_kernel<true><<<blocks, kWsThreads, kWsSmemBytes, s>>>(
-          a, p2, order, r4, ratio_o, count, ldexpf(1.0f, fraction_bits), nullptr,
-          reinterpret_cast<unsigned long long*>(scratch));
-      rc = check_launch("dp_density_map_ordered scatter");
-      if (rc) return rc;
-    }
-    fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
-                                                              ldexp(1.0, -fraction_bits), out, nbins);
-    return check_launch("dp_density_map_ordered convert");
-  }
-  if (init) {
-    rc = copy_map(init, out, nbins, s);
-    if (rc) return rc;
-  } else {
-    cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
-  }
-  if (blocks == 0) return DP_OK;
-  window_scatter_kernel<false><<<blocks, kWsThreads, kWsSmemBytes, s>>>(a, p2, order, r4, ratio_o, count, 0.f, out,
-                                                                         nullptr);
+  const int count = end - begin;
+  if (count <= 0) return DP_OK;
+  const int blocks = ceil_div(count, kWsCells);
+  if (deterministic)
+    window_scatter_kernel<true><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
+        o.a, o.xy, o.order + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits), nullptr,
+        reinterpret_cast<unsigned long long*>(scratch));
+  else
+    window_scatter_kernel<false><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
+        o.a, o.xy, o.order + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
   return check_launch("dp_density_map_ordered scatter");
+}
+
+int convert_fixed(const int64_t* scratch, const float* init, int fraction_bits, float* out, int nbins,
+                  cudaStream_t s) {
+  fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
+                                                            ldexp(1.0, -fraction_bits), out, nbins);
+  return check_launch("dp_density_map_ordered convert");
+}
+
+int start_map(const float* init, float* out, int nbins, cudaStream_t s) {
+  if (init) return copy_map(init, out, nbins, s);
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * nbins, s);
+  if (e != cudaSuccess) {
+    set_error("dp_density_map_ordered: cudaMemsetAsync: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}
+
+int ordered_setup(const char* who, const float* xy, const int* order, const float* rec4, const float* ratio_o,
+                  int count, float xl, float yl, float bsx, float bsy, float ibx, float iby, int nbx, int nby,
+                  int deterministic, int fraction_bits, int64_t* scratch, dp_stream_t stream, OrderedScatter& o) {
+  DP_REQUIRE(xy && rec4 && ratio_o && (count == 0 || order), "%s: null pointer", who);
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)rec4 & 15) == 0, "%s: misaligned xy/rec4", who);
+  DP_REQUIRE(nbx > 0 && nby > 0 && (long long)nbx * nby < (1ll << 31), "%s: bad bin grid", who);
+  DP_REQUIRE(bsx > 0 && bsy > 0 && count >= 0, "%s: bad geometry", who);
+  DP_REQUIRE(!deterministic || scratch, "%s: deterministic mode needs scratch_fixed", who);
+  DP_REQUIRE(!deterministic || (fraction_bits >= 0 && fraction_bits <= 62), "%s: bad fraction_bits", who);
+  memset(&o.a, 0, sizeof(o.a));
+  o.a.xl = xl; o.a.yl = yl; o.a.bsx = bsx; o.a.bsy = bsy; o.a.inv_bsx = ibx; o.a.inv_bsy = iby;
+  o.a.num_bins_x = nbx; o.a.num_bins_y = nby;
+  o.xy = reinterpret_cast<const float2*>(xy);
+  o.order = order;
+  o.rec4 = reinterpret_cast<const float4*>(rec4);
+  o.ratio_o = ratio_o;
+  o.s = as_stream(stream);
+  return DP_OK;
+}
+
+}  // namespace
+
+// Order-driven scatter (see window_scatter_kernel): the cells order[0..count)
+// with their records, positions interleaved in xy.
+extern "C" int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
+                                      int count, const float* init, float xl, float yl, float xh, float yh, float bsx,
+                                      float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
+                                      int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
+  OrderedScatter o;
+  int rc = ordered_setup("dp_density_map_ordered", xy, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx,
+                         nby, deterministic, fraction_bits, scratch, stream, o);
+  if (rc) return rc;
+  DP_REQUIRE(out, "dp_density_map_ordered: null output");
+  const int nbins = nbx * nby;
+  if (deterministic) {
+    cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, o.s);
+    rc = scatter_range(o, 0, count, 1, fraction_bits, scratch, nullptr);
+    if (rc) return rc;
+    return convert_fixed(scratch, init, fraction_bits, out, nbins, o.s);
+  }
+  rc = start_map(init, out, nbins, o.s);
+  if (rc) return rc;
+  return scatter_range(o, 0, count, 0, 0, nullptr, out);
+}
+
+// Two maps from one pass over the cells: out_first = init + cells
+// [0, num_first), out_all = init + cells [0, count).  Fixed point: the int64
+// sums are exact, so both maps equal separate scatters bit for bit.  fp32: the
+// second map continues from the first, i.e. the float additions happen in one
+// of the orders the atomic scatter of all cells can take.
+extern "C" int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4,
+                                            const float* ratio_o, int num_first, int count, const float* init,
+                                            float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
+                                            float iby, int nbx, int nby, int deterministic, int fraction_bits,
+                                            int64_t* scratch, float* out_first, float* out_all, dp_stream_t stream) {
+  OrderedScatter o;
+  int rc = ordered_setup("dp_density_map_ordered_split", xy, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby,
+                         nbx, nby, deterministic, fraction_bits, scratch, stream, o);
+  if (rc) return rc;
+  DP_REQUIRE(out_first && out_all && out_first != out_all, "dp_density_map_ordered_split: bad outputs");
+  DP_REQUIRE(num_first >= 0 && num_first <= count, "dp_density_map_ordered_split: bad num_first");
+  const int nbins = nbx * nby;
+  if (deterministic) {
+    cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, o.s);
+    rc = scatter_range(o, 0, num_first, 1, fraction_bits, scratch, nullptr);
+    if (rc) return rc;
+    rc = convert_fixed(scratch, init, fraction_bits, out_first, nbins, o.s);
+    if (rc) return rc;
+    rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr);
+    if (rc) return rc;
+    return convert_fixed(scratch, init, fraction_bits, out_all, nbins, o.s);
+  }
+  rc = start_map(init, out_first, nbins, o.s);
+  if (rc) return rc;
+  rc = scatter_range(o, 0, num_first, 0, 0, nullptr, out_first);
+  if (rc) return rc;
+  rc = copy_map(out_first, out_all, nbins, o.s);
+  if (rc) return rc;
+  return scatter_range(o, num_first, count, 0, 0, nullptr, out_all);
 }
 
 // ---------------------------------------------------------------- allocation-free variant

@@ -363,7 +363,8 @@ __global__ void nesterov_init_kernel(double* st, double alpha) {
 // gradient's scale (d objective / d D) goes to grad_scale for the force kernel
 // (dreamplace/PlaceObj.py:293-320).
 __global__ void objective_finish_kernel(const double* wl, const double* energy, const float* density_weight,
-                                        float density_factor, float quad_c, double* obj, float* grad_scale) {
+                                        const float* factor_quad, double* obj, float* grad_scale) {
+  const float density_factor = factor_quad[0], quad_c = factor_quad[1];
   double lam = (double)density_factor * (double)density_weight[0];
   double d = energy[0];
   double dp = quad_c > 0.f ? d * (1.0 + (double)quad_c * d) : d;
@@ -377,11 +378,9 @@ __global__ void objective_finish_kernel(const double* wl, const double* energy, 
 using namespace dpb;
 
 extern "C" int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
-                                   float density_factor, float quad_c, double* obj, float* grad_scale,
-                                   dp_stream_t stream) {
-  DP_REQUIRE(wl && energy && density_weight && obj && grad_scale, "dp_objective_finish: null pointer");
-  objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, density_factor, quad_c, obj,
-                                                         grad_scale);
+                                   const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream) {
+  DP_REQUIRE(wl && energy && density_weight && factor_quad && obj && grad_scale, "dp_objective_finish: null pointer");
+  objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, factor_quad, obj, grad_scale);
   return check_launch("dp_objective_finish");
 }
 
@@ -536,8 +535,11 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
     const int* __restrict__ netpin_start, const int* __restrict__ chunk_net, int num_chunks,
     const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
     const float* __restrict__ inv_gamma_p, const int* __restrict__ csr_pos, double* __restrict__ partials,
-    float2* __restrict__ gnode) {
+    float2* __restrict__ gnode, const unsigned char* __restrict__ hpwl_mask, double* __restrict__ hpwl_partials) {
   const float inv_gamma = kGrad ? *inv_gamma_p : 0.f;
+  // HPWL riding along the WA forward (hpwl_partials != NULL): the same per-net
+  // value and the same per-thread accumulation order as the kGrad = false pass
+  double hcontrib = 0.0;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -562,6 +564,11 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
       const float x_min = seg_reduce(valid ? xx : FLT_MAX, sg, lane, MinOp());
       const float y_max = seg_reduce(valid ? yy : -FLT_MAX, sg, lane, MaxOp());
       const float y_min = seg_reduce(valid ? yy : FLT_MAX, sg, lane, MinOp());
+      if (kGrad && hpwl_partials && valid && lane == sg.head && hpwl_mask[net]) {
+        float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+        if (net_weights) h = fmul(h, net_weights[net]);
+        hcontrib += (double)h;
+      }
       if (!kGrad) {  // HPWL
         if (on && lane == sg.head) {
           float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
@@ -627,6 +634,11 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
       x_min = warp_all(x_min, 1);
       y_max = warp_all(y_max, 0);
       y_min = warp_all(y_min, 1);
+      if (kGrad && hpwl_partials && lane == 0 && hpwl_mask[net]) {
+        float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+        if (net_weights) h = fmul(h, net_weights[net]);
+        hcontrib += (double)h;
+      }
       if (!kGrad) {
         if (on && lane == 0) {
           float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
@@ -685,6 +697,7 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
     }
   }
   block_partial(contrib, partials);
+  if (kGrad && hpwl_partials) block_partial(hcontrib, hpwl_partials);
 }
 
 // node grad (+)= grad_pos[0] * sum of its pins' (weighted) gradients, which
@@ -740,7 +753,7 @@ static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* s
                          const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
                          int num_chunks, const float* net_weights, const unsigned char* net_mask,
                          const float* inv_gamma, const int* csr_pos, double* out_f64, float* gnode, int num_slots,
-                         cudaStream_t s) {
+                         const unsigned char* hpwl_mask, double* hpwl_f64, cudaStream_t s) {
   using namespace dpb;
   int blocks = num_chunks > 0 ? ceil_div((long long)num_chunks * 32, 256) : 1;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
@@ -748,13 +761,18 @@ static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* s
   if (grad)
     wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
                                                 chunk_net, num_chunks, net_weights, net_mask, inv_gamma, csr_pos,
-                                                out_f64 + 1, reinterpret_cast<float2*>(gnode));
+                                                out_f64 + 1, reinterpret_cast<float2*>(gnode), hpwl_mask,
+                                                hpwl_f64 ? hpwl_f64 + 1 : nullptr);
   else
     wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
                                                  chunk_net, num_chunks, net_weights, net_mask, nullptr, nullptr,
-                                                 out_f64 + 1, nullptr);
+                                                 out_f64 + 1, nullptr, nullptr, nullptr);
   int rc = check_launch(grad ? "dp_wa_chunk_forward" : "dp_hpwl_chunk");
   if (rc) return rc;
+  if (grad && hpwl_f64) {
+    rc = launch_finish_sum(hpwl_f64, blocks, nullptr, s);
+    if (rc) return rc;
+  }
   return launch_finish_sum(out_f64, blocks, nullptr, s);
 }
 
@@ -762,15 +780,17 @@ extern "C" int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* sl
                                    const float* slot_offy, const int* slot_net, const int* netpin_start,
                                    const int* chunk_net, int num_chunks, const float* net_weights,
                                    const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
-                                   double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream) {
+                                   double* wl_f64, float* grad_node_order, int num_slots,
+                                   const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream) {
   DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
                  inv_gamma && csr_pos && wl_f64 && grad_node_order,
              "dp_wa_chunk_forward: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
              "dp_wa_chunk_forward: xy and grad_node_order must be 8-byte aligned");
+  DP_REQUIRE(!hpwl_f64 || hpwl_mask, "dp_wa_chunk_forward: hpwl_f64 needs hpwl_mask");
   return launch_chunks(true, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
                        num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
-                       dpb::as_stream(stream));
+                       hpwl_mask, hpwl_f64, dpb::as_stream(stream));
 }
 
 extern "C" int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
@@ -782,7 +802,7 @@ extern "C" int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_nod
              "dp_hpwl_chunk: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0, "dp_hpwl_chunk: xy must be 8-byte aligned");
   return launch_chunks(false, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
-                       num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0,
+                       num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0, nullptr, nullptr,
                        dpb::as_stream(stream));
 }
 

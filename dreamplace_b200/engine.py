@@ -12,9 +12,11 @@ re-organised for the GPU:
 * the Nesterov trial point, move-boundary clamp, preconditioner and the fp64
   step-size estimate run as fused kernels on ping-pong buffers (v, u, g for
   step k and k+1), so an accepted step swaps a parity bit instead of copying;
-* one iteration (HPWL + overflow evaluation at v_k and the first Nesterov
-  trial) is one CUDA graph replay, a retried trial another; the host reads a
-  handful of fp64 scalars once per trial and makes the loop decisions.
+* one Nesterov trial is one CUDA graph replay; the trial's WA forward also
+  sums the HPWL of the trial point and its scatter also yields the
+  movable-only map, so the evaluation of v_k (HPWL, overflow) reported at
+  iteration k was computed when v_k was produced; the host reads a handful of
+  fp64 scalars once per trial and makes the loop decisions.
 """
 import math
 
@@ -79,17 +81,23 @@ class GPEngine(object):
         self.wl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
         self.wl64 = self.wl64_buf[0:1]
         self.obj64 = torch.zeros(1, **f64)
-        self.hpwl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
-        self.hpwl64 = self.hpwl64_buf[0:1]
-        self.ovf2_buf = torch.zeros(REDUCE_DOUBLES, **f64)
-        self.ovf2 = self.ovf2_buf[0:2]
+        # metrics of v_k and v_{k+1} by parity: the HPWL rides along the trial's
+        # WA forward and the movable-only map (overflow) along its scatter, so
+        # the evaluation of v_k is already on the device when iteration k starts
+        self.H = [torch.zeros(REDUCE_DOUBLES, **f64), torch.zeros(REDUCE_DOUBLES, **f64)]
+        self.O = [torch.zeros(REDUCE_DOUBLES, **f64), torch.zeros(REDUCE_DOUBLES, **f64)]
         self.metrics = torch.zeros(8, **f64)
         self.metrics_host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
         self.grad_scale = torch.zeros(1, dtype=torch.float32, device=dev)
+        # (density factor, quadratic penalty coefficient) read by the objective
+        # kernel on the device, so the captured graphs follow their changes
+        self.factor_quad = torch.tensor([1.0, 0.0], dtype=torch.float32, device=dev)
         self.one = torch.ones(1, dtype=torch.float32, device=dev)
         self.inv_gamma = torch.zeros(1, dtype=torch.float32, device=dev)
         self.dmap = torch.empty(ep.num_bins_x, ep.num_bins_y, dtype=torch.float32, device=dev)
         self.omap = torch.empty_like(self.dmap)
+        self.ovf_area = float(self.ovf_op.bin_size_x * self.ovf_op.bin_size_y)
+        self.ovf_target = float(self.ovf_op.target_density) * self.ovf_area
         self.det = bool(params.deterministic_flag)
         self.scratch = torch.empty(ep.num_bins_x * ep.num_bins_y, dtype=torch.int64, device=dev) if self.det else None
         self.prec = precision_code(ep.precision)
@@ -159,25 +167,57 @@ class GPEngine(object):
         """Refresh the interleaved copy of a position buffer written outside the trial kernel."""
         C.pack_xy(v, self.xy(v))
 
-    def wirelength(self, v):
+    def wirelength(self, v, hpwl_out=None):
         """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
-        net weight) in node-CSR order in self.gnode."""
+        net weight) in node-CSR order in self.gnode; with hpwl_out, the HPWL of v from the
+        same pin reads."""
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
         C.wa_chunk_forward(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
                            self.chunk_net, dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
-                           self.csr_pos, self.wl64_buf, self.gnode)
+                           self.csr_pos, self.wl64_buf, self.gnode,
+                           dc.net_mask_all if hpwl_out is not None else None, hpwl_out)
 
     def wl_grad_into(self, g, accumulate):
         dc = self.data
         C.node_pin_sum(self.gnode, self.node_start, self.one, self.design.num_movable_nodes, int(accumulate), g)
 
-    def density_energy(self, v):
-        """Density map, Poisson solve; returns (ex, ey, energy_f64[1])."""
+    def scatter_maps(self, v, ovf_out):
+        """One scatter of v: the movable-only map (self.omap) and the movable +
+        filler map (self.dmap); (overflow, max density) of v into ovf_out."""
         ep = self.ep
-        self._density(v, ep.num_filler_nodes, self.dmap)
+        C.density_map_ordered_split(self.xy(v), self.order, self.rec4, self.ratio_o, ep.num_movable_nodes,
+                                    self.order.numel(), ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
+                                    float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
+                                    ep.num_bins_x, ep.num_bins_y, int(self.det), self.scratch, self.omap.view(-1),
+                                    self.dmap.view(-1))
+        C.density_overflow_into(self.omap, self.ovf_target, self.ovf_area, ovf_out)
+
+    def density_energy(self, v, ovf_out=None):
+        """Density map, Poisson solve; returns (ex, ey, energy_f64[1]).  With ovf_out,
+        the movable-only map of the same scatter gives (overflow, max density) of v."""
+        ep = self.ep
+        if ovf_out is None:
+            self._density(v, ep.num_filler_nodes, self.dmap)
+        else:
+            self.scatter_maps(v, ovf_out)
         self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
         return poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
+
+    def field_force(self, v, ex, ey):
+        """Field force of every movable and filler cell, in visiting order (self.force_o)."""
+        ep = self.ep
+        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xy(v), self.order, self.rec4,
+                                 self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
+                                 float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
+
+    def assemble(self, v, g, v_new, g_new):
+        """Preconditioned gradient at v_new into g_new (pin sum + force) and the fp64
+        step-size norms against (v, g)."""
+        d = self.design
+        C.assemble_precondition_step(self.gnode, self.node_start, self.one, self.force_o, self.inv_order,
+                                     d.num_movable_nodes, d.num_filler_nodes, self._pws(), self.data.node_areas,
+                                     self.model.density_weight, v_new, v, g, g_new, self.state)
 
     def density_grad_into(self, v, ex, ey, scale_t, g):
         ep = self.ep
@@ -191,8 +231,7 @@ class GPEngine(object):
         m = self.model
         self.wirelength(v)
         ex, ey, energy = self.density_energy(v)
-        C.objective_finish(self.wl64, energy, m.density_weight, float(m.density_factor), self._quad_c,
-                           self.obj64, self.grad_scale)
+        C.objective_finish(self.wl64, energy, m.density_weight, self.factor_quad, self.obj64, self.grad_scale)
         self.density_grad_into(v, ex, ey, self.grad_scale, g)
         self.wl_grad_into(g, True)
         self.last_energy = energy
@@ -208,44 +247,52 @@ class GPEngine(object):
         C.precondition_step_size(g, g_ref, v_new, v_ref, self._pws(), self.data.node_areas,
                                  self.model.density_weight, self.state)
 
-    def objective_and_step(self, v, g, v_new, g_new):
+    def objective_and_step(self, v, g, v_new, g_new, q_new):
         """The trial's objective at v_new and its preconditioned gradient into g_new,
         with the fp64 step-size norms against (v, g): the field force is gathered
         in visiting order and assembled per node together with the wirelength pin
-        sum, the preconditioner and the norms (one pass over the nodes)."""
+        sum, the preconditioner and the norms (one pass over the nodes).  The
+        HPWL and overflow of v_new land in the parity-q_new metric buffers."""
         m, ep, d = self.model, self.ep, self.design
-        self.wirelength(v_new)
-        ex, ey, energy = self.density_energy(v_new)
-        C.objective_finish(self.wl64, energy, m.density_weight, float(m.density_factor), self._quad_c,
-                           self.obj64, self.grad_scale)
-        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xy(v_new), self.order, self.rec4,
-                                 self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
-                                 float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
-        C.assemble_precondition_step(self.gnode, self.node_start, self.one, self.force_o, self.inv_order,
-                                     d.num_movable_nodes, d.num_filler_nodes, self._pws(), self.data.node_areas,
-                                     m.density_weight, v_new, v, g, g_new, self.state)
+        self.wirelength(v_new, self.H[q_new])
+        ex, ey, energy = self.density_energy(v_new, self.O[q_new])
+        C.objective_finish(self.wl64, energy, m.density_weight, self.factor_quad, self.obj64, self.grad_scale)
+        self.field_force(v_new, ex, ey)
+        self.assemble(v, g, v_new, g_new)
         self.last_energy = energy
         return energy
 
-    def evaluate(self, v):
-        d, dc = self.design, self.data
+    def evaluate(self, q):
+        """HPWL and (overflow, max density) of V[q] into the parity-q metric buffers,
+        for a position set from outside the trial kernel."""
+        dc = self.data
+        v = self.V[q]
         C.hpwl_chunk(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
-                     self.chunk_net, dc.net_weights, dc.net_mask_all, self.hpwl64_buf)
+                     self.chunk_net, dc.net_weights, dc.net_mask_all, self.H[q])
         self._density(v, 0, self.omap)
-        ba = self.ovf_op.bin_size_x * self.ovf_op.bin_size_y
-        C.density_overflow_into(self.omap, float(self.ovf_op.target_density * ba), float(ba), self.ovf2_buf)
+        C.density_overflow_into(self.omap, self.ovf_target, self.ovf_area, self.O[q])
 
     def move_boundary(self, v):
         d = self.design
         C.move_boundary_forward(v, self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl),
                                 float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
         self.pack(v)
+        for q in (0, 1):
+            if v.data_ptr() == self.V[q].data_ptr():
+                self.evaluate(q)
 
     # ---------------------------------------------------------------- setup
+    def _plain_objective(self):
+        """Set-up evaluations use the model's density factor without the
+        quadratic penalty; the next step refreshes the loop's values."""
+        self._quad_c = 0.0
+        self.factor_quad.copy_(torch.tensor([float(self.model.density_factor), 0.0], dtype=torch.float32))
+        self.graph_key = None
+
     def initial_learning_rate(self, lr):
         """|x0 - x1| / |g0 - g1| after x1 = x0 - lr g0 (PlaceObj.estimate_initial_learning_rate)."""
         v0, g0, g1, x1 = self.V[0], self.G[0], self.G[1], self.V[1]
-        self._quad_c = 0.0
+        self._plain_objective()
         self.pack(v0)
         self.obj_and_raw_grad(v0, g0)
         self.precondition(g0, v0, g0, v0)
@@ -274,7 +321,7 @@ class GPEngine(object):
         """First optimizer step's set-up: g_k at v_k, g_k_1 at v_k - lr g_k, alpha_k."""
         p = self.parity
         v, g, u = self.V[p], self.G[p], self.U[p]
-        self._quad_c = 0.0
+        self._plain_objective()
         self.obj_and_raw_grad(v, g)
         self.precondition(g, v, g, v)
         u.copy_(v)
@@ -294,9 +341,10 @@ class GPEngine(object):
         vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
         C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
                          float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
-        energy = self.objective_and_step(v, g, vn, gn)
-        torch.cat([self.hpwl64, self.ovf2, self.state[NS_ACCEPT:NS_ACCEPT + 1], self.state[NS_ALPHA:NS_ALPHA + 1],
-                   self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
+        energy = self.objective_and_step(v, g, vn, gn, 1 - p)
+        # HPWL / overflow of v_k (computed when v_k was the trial point), then the trial's scalars
+        torch.cat([self.H[p][0:1], self.O[p][0:2], self.state[NS_ACCEPT:NS_ACCEPT + 1],
+                   self.state[NS_ALPHA:NS_ALPHA + 1], self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
 
     def nesterov_trial_only(self, p):
         """The trial-point kernel alone (used for per-kernel timing)."""
@@ -305,16 +353,15 @@ class GPEngine(object):
                          self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
                          float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
 
-    def _body(self, p, with_eval):
+    def _body(self, p):
         # v_k was clamped into the die when it was produced (trial kernel, or
         # move_boundary + pack at the start / after a rollback), so the
-        # reference's per-iteration move_boundary(pos) is the identity here
-        if with_eval:
-            self.evaluate(self.V[p])
+        # reference's per-iteration move_boundary(pos) is the identity here,
+        # and its evaluation (HPWL, overflow) was computed with it
         self._trial(p)
 
-    def _graph(self, p, with_eval, warm=True):
-        key = (p, with_eval)
+    def _graph(self, p, warm=True):
+        key = p
         g = self.graphs.get(key)
         if g is None:
             if warm:
@@ -326,67 +373,78 @@ class GPEngine(object):
                 s.wait_stream(torch.cuda.current_stream())
                 with torch.cuda.stream(s):
                     saved = self.state.clone()
-                    self._body(p, with_eval)
+                    self._body(p)
                     self.state.copy_(saved)
                 torch.cuda.current_stream().wait_stream(s)
+            # captured on a side stream with capture_begin / capture_end (the
+            # torch.cuda.graph context would also run gc and empty the
+            # allocator cache, which costs a stall inside the GP loop)
             g = torch.cuda.CUDAGraph()
             before = C.launch_count()
-            with torch.cuda.graph(g, pool=self.pool):
-                self._body(p, with_eval)
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                g.capture_begin(pool=self.pool)
+                try:
+                    self._body(p)
+                finally:
+                    g.capture_end()
+            torch.cuda.current_stream().wait_stream(s)
             self.graph_kernels[key] = C.launch_count() - before
             if self.pool is None:
                 self.pool = g.pool()
             self.graphs[key] = g
         return g
 
-    def _run(self, p, with_eval):
+    def _run(self, p):
         if self.use_graphs:
-            self._graph(p, with_eval).replay()
-            self.kernels_launched += self.graph_kernels[(p, with_eval)]
+            self._graph(p).replay()
+            self.kernels_launched += self.graph_kernels[p]
         else:
             before = C.launch_count()
-            self._body(p, with_eval)
+            self._body(p)
             self.kernels_launched += C.launch_count() - before
         self.metrics_host.copy_(self.metrics, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return self.metrics_host.numpy().copy()
 
     def _check_graph_key(self):
+        """Refresh the device copy of (density factor, quadratic penalty
+        coefficient) when the GP loop changed them (no recapture needed)."""
         m = self.model
         key = (float(m.density_factor), bool(m.quad_penalty))
         if key != self.graph_key:
-            self.graphs = {}
             self._quad_c = float(m.quad_penalty_coeff.item()) if m.quad_penalty else 0.0
+            self.factor_quad.copy_(torch.tensor([key[0], self._quad_c], dtype=torch.float32))
             self.graph_key = key
 
     def prepare_graphs(self):
-        """Capture all four graph variants (parity x with/without evaluation) up
-        front, so no capture happens inside a timed or latency-sensitive window."""
+        """Capture the trial graph of both parities up front, so no capture happens
+        inside a timed or latency-sensitive window."""
         if not self.use_graphs:
             return
         self._check_graph_key()
         p = self.parity
-        # one warm-up (current parity, with evaluation) initialises every lazy
-        # resource; the other three variants are captured without running
-        self._graph(p, True)
-        for key in ((p, False), (1 - p, True), (1 - p, False)):
-            self._graph(*key, warm=False)
+        # one warm-up (current parity) initialises every lazy resource; the
+        # other parity is captured without running
+        self._graph(p)
+        self._graph(1 - p, warm=False)
 
     def step(self):
         """One GP iteration: evaluation at v_k, then Nesterov trials until accepted
         (<= 10).  Returns (hpwl, overflow / total movable area, max_density, objective, trials)."""
         self._check_graph_key()
-        if self.use_graphs and len(self.graphs) < 4:
+        if self.use_graphs and len(self.graphs) < 2:
             self.prepare_graphs()
         p = self.parity
         if self.sort_interval > 0 and self.iterations % self.sort_interval == 0:
             self.refresh_order(self.V[p])
         self.iterations += 1
-        mh = self._run(p, True)
+        mh = self._run(p)
         hpwl, ovf, maxd = mh[M_HPWL], mh[M_OVF], mh[M_MAXD]
         trials = 1
         while mh[M_ACCEPT] == 0.0 and trials < 10:
-            mh = self._run(p, False)
+            mh = self._run(p)
             trials += 1
         C.nesterov_advance(self.state)
         self.kernels_launched += 1

@@ -135,6 +135,19 @@ int dp_density_map_ordered(const float* xy, const int* order, const float* rec4,
                            int num_bins_x, int num_bins_y, int deterministic, int fraction_bits,
                            int64_t* scratch_fixed, float* density_map, dp_stream_t stream);
 
+/* Two maps from one pass over the cells: out_first = initial_density_map +
+ * cells [0, num_first) of the order, out_all = initial_density_map + cells
+ * [0, count).  Used for the movable-only map (overflow metric) and the
+ * movable + filler map (Poisson input) of one position, so each cell is
+ * scattered once.  Deterministic: both maps bit-exact with separate scatters. */
+int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4, const float* ratio_o,
+                                 int num_first, int count, const float* initial_density_map,
+                                 float xl, float yl, float xh, float yh,
+                                 float bin_size_x, float bin_size_y,
+                                 float inv_bin_size_x, float inv_bin_size_y,
+                                 int num_bins_x, int num_bins_y, int deterministic, int fraction_bits,
+                                 int64_t* scratch_fixed, float* out_first, float* out_all, dp_stream_t stream);
+
 /* Exact-overlap fixed-cell map (electric_potential/src/electric_density_map_cuda.cpp:139-183,
  * CPU electric_potential/src/electric_density_map.cpp:155-213): nodes
  * [num_movable_nodes, num_movable_nodes+num_terminals), fixed_node_flag=true,
@@ -359,12 +372,15 @@ int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins,
  * (xy [2 * num_nodes], see dp_pack_xy).  The per-pin gradient, times the net
  * weight, is written as an (x, y) pair at csr_pos[slot] (the pin's position in
  * node-CSR order) of grad_node_order [2 * num_slots]; masked nets write 0.
- * wl_f64: DP_REDUCE_DOUBLES doubles. */
+ * wl_f64: DP_REDUCE_DOUBLES doubles.  hpwl_f64 (optional, DP_REDUCE_DOUBLES
+ * doubles): the HPWL of the same pins under hpwl_mask, equal to dp_hpwl_chunk's
+ * result (same per-net values, same summation order), from the same pin reads. */
 int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                         const float* slot_offy, const int* slot_net, const int* netpin_start,
                         const int* chunk_net, int num_chunks, const float* net_weights,
                         const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
-                        double* wl_f64, float* grad_node_order, int num_slots, dp_stream_t stream);
+                        double* wl_f64, float* grad_node_order, int num_slots,
+                        const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream);
 /* HPWL with the same chunking (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
 int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                   const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
@@ -375,10 +391,12 @@ int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const fl
  * (pin mask of fixed cells) */
 int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start, const float* grad_pos,
                     int num_movable, int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
-/* obj = wl + lambda_eff * D (1 + c D); grad_scale = d obj / d D */
+/* obj = wl + lambda_eff * D (1 + c D), lambda_eff = factor_quad[0] *
+ * density_weight, c = factor_quad[1] (0: no quadratic penalty);
+ * grad_scale = d obj / d D.  All operands live on the device, so a captured
+ * graph follows changes of the density factor and penalty. */
 int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
-                        float density_factor, float quad_c, double* obj, float* grad_scale,
-                        dp_stream_t stream);
+                        const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -393,3 +393,37 @@ def test_ordered_force_and_fused_assembly(C, golden):
                                  st_got)
     assert torch.equal(got, exp)
     np.testing.assert_allclose(st_got[:8].cpu().numpy(), st_ref[:8].cpu().numpy(), rtol=1e-12)
+
+
+def test_ordered_split_scatter(C):
+    """Two maps from one pass (movable prefix, all cells): bit-exact with two
+    separate fixed-point scatters; fp32 within atomic-order tolerance."""
+    d = synthetic.scaled(20000, num_bins=128, seed=9)
+    pos = d.initial_positions()
+    n, m, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+    rng = np.random.RandomState(3)
+    pos[:m] = rng.normal((d.xl + d.xh) / 2, 0.05 * (d.xh - d.xl), size=m).clip(d.xl, d.xh - 40)
+    pos[n:n + m] = rng.normal((d.yl + d.yh) / 2, 0.05 * (d.yh - d.yl), size=m).clip(d.yl, d.yh - 12)
+    idx = np.r_[0:m, n - nf:n].astype(np.int32)
+    order = np.r_[spatial_order(d, pos, idx[:m]), spatial_order(d, pos, idx[m:])].astype(np.int32)
+    rec4, ratio_o, _ = records(C, d, order)
+    xy = pack_xy(pos, n)
+    nb = d.num_bins_x * d.num_bins_y
+    init = dev(np.random.RandomState(4).uniform(0, 50, nb).astype(np.float32))
+    scratch = torch.empty(nb, dtype=torch.int64, device="cuda")
+    geo = (d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y)
+    for det in (1, 0):
+        first, full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
+        C.density_map_ordered_split(xy, dev(order), rec4, ratio_o, m, len(order), init, *geo, det,
+                                    scratch if det else None, first, full)
+        exp_first, exp_full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
+        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, m, init, *geo, det, scratch if det else None,
+                                   exp_first)
+        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), init, *geo, det,
+                                   scratch if det else None, exp_full)
+        if det:
+            assert torch.equal(first, exp_first) and torch.equal(full, exp_full)
+        else:
+            tol = 1e-4 * float(exp_full.abs().max())
+            torch.testing.assert_close(first, exp_first, rtol=1e-4, atol=tol)
+            torch.testing.assert_close(full, exp_full, rtol=1e-4, atol=tol)
