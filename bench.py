@@ -44,7 +44,7 @@ UNIT = "GP iter/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split_bf16")
@@ -64,58 +64,80 @@ def make_design(name):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler(object):
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples of SM clock and throttle reasons around the timed region.
+
+    nvidia-smi is started, and its first sample awaited, before the GP warm-up:
+    its start-up (NVML initialisation) can hold the driver for seconds and must
+    not land inside the timed region.  Samples are stamped on arrival; the
+    summary uses those that arrived between begin() and end() plus one
+    sampling period after, or the nearest sample when the region is shorter
+    than a period."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 200
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.t_begin = self.t_end = None
 
-    def start(self):
+    def start(self, ready_timeout=20.0):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < ready_timeout and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def begin(self):
+        self.t_begin = time.time()
+
+    def end(self):
+        self.t_end = time.time()
 
     def stop(self):
         if self.proc is None:
             return None
-        time.sleep(0.25)
+        time.sleep(1.5 * self.PERIOD_MS / 1000.0)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, mx, reasons = [], 0.0, set()
+        parsed = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
             try:
-                sm.append(float(p[1]))
-                mx = max(mx, float(p[2]))
+                sm, mx = float(p[1]), float(p[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+            parsed.append((t, sm, mx, [nm for nm, v in zip(names, p[5:9]) if v.lower().startswith("active")]))
+        if not parsed:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        tb = self.t_begin if self.t_begin is not None else parsed[0][0]
+        te = (self.t_end if self.t_end is not None else parsed[-1][0]) + self.PERIOD_MS / 1000.0
+        inside = [x for x in parsed if tb <= x[0] <= te]
+        if not inside:
+            inside = [min(parsed, key=lambda x: abs(x[0] - tb))]
+        reasons = sorted({r for x in inside for r in x[3]})
+        return {"sm_mhz": statistics.median(x[1] for x in inside), "sm_max_mhz": max(x[2] for x in inside),
+                "reasons": reasons, "samples": len(inside)}
 
 
 # ------------------------------------------------------------------ distributed
@@ -193,7 +215,7 @@ class TimedRun(object):
                 barrier(self.world)
                 torch.cuda.synchronize()
                 if clocks is not None:
-                    clocks.start()
+                    clocks.begin()
                 state["launch0"] = launches()
                 state["trials0"] = trials()
                 start.record()
@@ -208,9 +230,13 @@ class TimedRun(object):
                 if it == warmup + steps - 1:
                     end.record()
                     torch.cuda.synchronize()
+                    if clocks is not None:
+                        clocks.end()
                     state["launch1"] = launches()
                     state["trials1"] = trials()
 
+        if clocks is not None:
+            clocks.start()
         t0 = time.time()
         self.placer(self.params, self.design, max_iterations=warmup + steps, callback=cb)
         wall = time.time() - t0

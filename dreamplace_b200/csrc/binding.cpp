@@ -445,7 +445,11 @@ void density_map_ordered_into(at::Tensor xy, at::Tensor order, at::Tensor rec4, 
 void density_map_ordered_split(at::Tensor xy, at::Tensor order, at::Tensor rec4, at::Tensor ratio_o, int num_first,
                                int count, c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh,
                                double bsx, double bsy, int nbx, int nby, int deterministic,
-                               c10::optional<at::Tensor> scratch, at::Tensor out_first, at::Tensor out_all) {
+                               c10::optional<at::Tensor> scratch, at::Tensor out_first, at::Tensor out_all,
+                               double target_area, double bin_area, c10::optional<at::Tensor> overflow_out) {
+  TORCH_CHECK(!overflow_out.has_value() || (overflow_out->scalar_type() == at::kDouble &&
+                                            overflow_out->numel() >= DP_REDUCE_DOUBLES),
+              "overflow_out needs DP_REDUCE_DOUBLES doubles");
   CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(rec4);
   TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
               "density_map_ordered_split: buffers smaller than count");
@@ -456,7 +460,7 @@ void density_map_ordered_split(at::Tensor xy, at::Tensor order, at::Tensor rec4,
                                        num_first, count, (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
                                        inv_f(bsx), inv_f(bsy), nbx, nby, deterministic, fraction_bits(xl, yl, xh, yh),
                                        (int64_t*)ovp(scratch), ptr<float>(out_first), ptr<float>(out_all),
-                                       cur_stream()));
+                                       target_area, bin_area, (double*)ovp(overflow_out), cur_stream()));
 }
 
 void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy, at::Tensor order,
@@ -512,32 +516,32 @@ at::Tensor plan_net_chunks(at::Tensor netpin_start_cpu, int max_pins) {
 }
 
 void wa_chunk_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
-                      at::Tensor slot_net, at::Tensor netpin_start, at::Tensor chunk_net,
-                      c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor inv_gamma,
-                      at::Tensor csr_pos, at::Tensor wl_f64, at::Tensor grad_node_order,
-                      c10::optional<at::Tensor> hpwl_mask, c10::optional<at::Tensor> hpwl_f64) {
-  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(chunk_net); CHECK_I32(csr_pos); CHECK_F32(grad_node_order);
+                      at::Tensor slot_net, at::Tensor chunk_pin, c10::optional<at::Tensor> net_weights,
+                      at::Tensor net_mask, at::Tensor inv_gamma, at::Tensor csr_pos, at::Tensor wl_f64,
+                      at::Tensor grad_node_order, c10::optional<at::Tensor> hpwl_mask,
+                      c10::optional<at::Tensor> hpwl_f64) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(chunk_pin); CHECK_I32(csr_pos); CHECK_F32(grad_node_order);
   TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
   TORCH_CHECK(!hpwl_f64.has_value() || (hpwl_mask.has_value() && hpwl_f64->scalar_type() == at::kDouble &&
                                         hpwl_f64->numel() >= DP_REDUCE_DOUBLES),
               "hpwl_f64 needs hpwl_mask and DP_REDUCE_DOUBLES doubles");
   DP_CALL(dp_wa_chunk_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                              ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(netpin_start), ptr<int>(chunk_net),
-                              chunk_net.numel() - 1, (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
-                              ptr<float>(inv_gamma), ptr<int>(csr_pos), ptr<double>(wl_f64),
-                              ptr<float>(grad_node_order), slot_node.numel(),
+                              ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(chunk_pin), chunk_pin.numel() - 1,
+                              (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<float>(inv_gamma),
+                              ptr<int>(csr_pos), ptr<double>(wl_f64), ptr<float>(grad_node_order), slot_node.numel(),
                               hpwl_mask.has_value() ? hpwl_mask->data_ptr<uint8_t>() : nullptr,
                               (double*)ovp(hpwl_f64), cur_stream()));
 }
 
 void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy, at::Tensor slot_net,
-                at::Tensor netpin_start, at::Tensor chunk_net, c10::optional<at::Tensor> net_weights,
-                at::Tensor net_mask, at::Tensor out_f64) {
+                at::Tensor chunk_pin, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
+                at::Tensor out_f64) {
+  CHECK_I32(chunk_pin);
   TORCH_CHECK(out_f64.scalar_type() == at::kDouble && out_f64.numel() >= DP_REDUCE_DOUBLES, "out_f64 too small");
   DP_CALL(dp_hpwl_chunk(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                        ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(netpin_start), ptr<int>(chunk_net),
-                        chunk_net.numel() - 1, (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
-                        ptr<double>(out_f64), cur_stream()));
+                        ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(chunk_pin), chunk_pin.numel() - 1,
+                        (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<double>(out_f64),
+                        cur_stream()));
 }
 
 void node_pin_sum(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor grad_pos, int num_movable,

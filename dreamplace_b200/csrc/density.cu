@@ -18,6 +18,7 @@
 #include <climits>
 #include <mutex>
 #include <type_traits>
+#include <cub/block/block_radix_sort.cuh>
 #include "reduce.cuh"
 
 namespace dpb {
@@ -229,9 +230,51 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
   }
   if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
   const int H = bh1 - bh0;
-  const bool use_tile = (long long)(bk1 - bk0) * H <= kCap;
+  const long long box = (long long)(bk1 - bk0) * H;
+  if (box < (1 << 16)) {
+    // Block-local order: the visiting order is refreshed only every few
+    // iterations, while cells keep moving; sorting the block's cells by the
+    // bin where their window starts (relative to the block's bounding box)
+    // restores the runs that the lane windows and the warp reduction rely on.
+    using BlockSort = cub::BlockRadixSort<unsigned, kWsThreads, kWsCellsPerLane, int>;
+    __shared__ typename BlockSort::TempStorage sort_tmp;
+    __shared__ float s_cell[5][kWsCells];
+    unsigned keys[kWsCellsPerLane];
+    int vals[kWsCellsPerLane];
+#pragma unroll
+    for (int c = 0; c < kWsCellsPerLane; ++c) {
+      const int li = warp * kWsWarpCells + lane * kWsCellsPerLane + c;
+      keys[c] = (unsigned)box;  // empty cells sort last
+      if (live & (1u << c)) {
+        int k0, k1, h0, h1;
+        triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
+        triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
+        keys[c] = (unsigned)((k0 - bk0) * H + (h0 - bh0));
+      }
+      vals[c] = li;
+      s_cell[0][li] = nx[c];
+      s_cell[1][li] = ny[c];
+      s_cell[2][li] = sxs[c];
+      s_cell[3][li] = sys[c];
+      s_cell[4][li] = rr[c];
+    }
+    BlockSort(sort_tmp).Sort(keys, vals, 0, 32 - __clz((unsigned)box));
+    __syncthreads();
+    live = 0;
+#pragma unroll
+    for (int c = 0; c < kWsCellsPerLane; ++c) {
+      const int li = vals[c];
+      nx[c] = s_cell[0][li];
+      ny[c] = s_cell[1][li];
+      sxs[c] = s_cell[2][li];
+      sys[c] = s_cell[3][li];
+      rr[c] = s_cell[4][li];
+      if (keys[c] < (unsigned)box) live |= 1u << c;
+    }
+  }
+  const bool use_tile = box <= kCap;
   if (use_tile) {
-    for (int t = threadIdx.x; t < (bk1 - bk0) * H; t += kWsThreads) tile[t] = (Acc)0;
+    for (int t = threadIdx.x; t < (int)box; t += kWsThreads) tile[t] = (Acc)0;
     __syncthreads();
   }
   const int nby = a.num_bins_y;
@@ -505,6 +548,32 @@ __global__ void overflow_kernel(const float* __restrict__ map, int n, double tar
   block_partial(s, partials);
 }
 
+// First map of the split scatter: converts it from fixed point (fixed != NULL)
+// or reads it, optionally copies it to copy_to (start of the second map), and
+// reduces its overflow sum and maximum as overflow_kernel does.
+__global__ void first_map_kernel(const long long* __restrict__ fixed, const float* __restrict__ init,
+                                 double inv_scale, float* first, float* __restrict__ copy_to, int n,
+                                 double target_area, double* partials, unsigned* maxkey) {
+  double s = 0.0;
+  float m = -INFINITY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float d;
+    if (fixed) {
+      d = (float)((init ? (double)init[i] : 0.0) + (double)fixed[i] * inv_scale);
+      first[i] = d;
+    } else {
+      d = first[i];
+    }
+    if (copy_to) copy_to[i] = d;
+    const double over = (double)d - target_area;
+    s += over > 0.0 ? over : 0.0;
+    m = fmaxf(m, d);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxkey, float_key(m));
+  block_partial(s, partials);
+}
+
 __global__ void overflow_finish_kernel(double* out2, const unsigned* maxkey, double bin_area,
                                        float* out2_f32, const double* partials, int count) {
   double total = finish_sum(partials, count);
@@ -775,27 +844,44 @@ extern "C" int dp_density_map_ordered(const float* xy, const int* order, const f
 }
 
 // Two maps from one pass over the cells: out_first = init + cells
-// [0, num_first), out_all = init + cells [0, count).  Fixed point: the int64
-// sums are exact, so both maps equal separate scatters bit for bit.  fp32: the
-// second map continues from the first, i.e. the float additions happen in one
-// of the orders the atomic scatter of all cells can take.
+// [0, num_first), out_all = init + cells [0, count), and optionally the
+// overflow reduction of out_first (as dp_density_overflow) fused into the
+// pass that finishes it.  Fixed point: the int64 sums are exact, so both maps
+// equal separate scatters bit for bit.  fp32: the second map continues from
+// the first, i.e. the float additions happen in one of the orders the atomic
+// scatter of all cells can take.
 extern "C" int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4,
                                             const float* ratio_o, int num_first, int count, const float* init,
                                             float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
                                             float iby, int nbx, int nby, int deterministic, int fraction_bits,
-                                            int64_t* scratch, float* out_first, float* out_all, dp_stream_t stream) {
+                                            int64_t* scratch, float* out_first, float* out_all, double target_area,
+                                            double bin_area, double* overflow_out, dp_stream_t stream) {
   OrderedScatter o;
   int rc = ordered_setup("dp_density_map_ordered_split", xy, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby,
                          nbx, nby, deterministic, fraction_bits, scratch, stream, o);
   if (rc) return rc;
   DP_REQUIRE(out_first && out_all && out_first != out_all, "dp_density_map_ordered_split: bad outputs");
   DP_REQUIRE(num_first >= 0 && num_first <= count, "dp_density_map_ordered_split: bad num_first");
+  DP_REQUIRE(!overflow_out || bin_area > 0, "dp_density_map_ordered_split: bad bin area");
   const int nbins = nbx * nby;
+  const int blocks = grid_for(nbins, 256, 4);
+  unsigned* maxslot = overflow_out ? reinterpret_cast<unsigned*>(overflow_out + 2) : nullptr;
   if (deterministic) {
     cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, o.s);
     rc = scatter_range(o, 0, num_first, 1, fraction_bits, scratch, nullptr);
     if (rc) return rc;
-    rc = convert_fixed(scratch, init, fraction_bits, out_first, nbins, o.s);
+    if (overflow_out) {
+      cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
+      first_map_kernel<<<blocks, 256, 0, o.s>>>((const long long*)scratch, init, ldexp(1.0, -fraction_bits),
+                                                 out_first, nullptr, nbins, target_area, overflow_out + 3, maxslot);
+      rc = check_launch("dp_density_map_ordered_split first map");
+      if (rc) return rc;
+      overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
+                                                            overflow_out + 3, blocks);
+      rc = check_launch("dp_density_map_ordered_split overflow");
+    } else {
+      rc = convert_fixed(scratch, init, fraction_bits, out_first, nbins, o.s);
+    }
     if (rc) return rc;
     rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr);
     if (rc) return rc;
@@ -805,7 +891,18 @@ extern "C" int dp_density_map_ordered_split(const float* xy, const int* order, c
   if (rc) return rc;
   rc = scatter_range(o, 0, num_first, 0, 0, nullptr, out_first);
   if (rc) return rc;
-  rc = copy_map(out_first, out_all, nbins, o.s);
+  if (overflow_out) {
+    cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
+    first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, nbins, target_area,
+                                               overflow_out + 3, maxslot);
+    rc = check_launch("dp_density_map_ordered_split first map");
+    if (rc) return rc;
+    overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
+                                                          overflow_out + 3, blocks);
+    rc = check_launch("dp_density_map_ordered_split overflow");
+  } else {
+    rc = copy_map(out_first, out_all, nbins, o.s);
+  }
   if (rc) return rc;
   return scatter_range(o, num_first, count, 0, 0, nullptr, out_all);
 }

@@ -128,99 +128,123 @@ inline EpiParams make_epi(const dp_gemm_problem& q, int precision, int M, int N)
   return e;
 }
 
-// 16 consecutive columns [n0, n0+16) of row m, all in range; vector stores
-// where the row segment is 16-byte aligned (checked by the caller's layout:
-// n0 % 16 == 0 and ldc % 8 == 0).  Returns the ENERGY contribution.
-__device__ __forceinline__ void store_operand16(int fmt, const float* v, size_t idx, float* f32,
-                                                __nv_bfloat16* hi, __nv_bfloat16* lo) {
+// ---- 8 consecutive elements of one output row (staged epilogue of the
+// tcgen05 kernel).  Same per-element arithmetic as epi_apply; vector memory
+// operations where the addresses are 16-byte aligned, scalar otherwise.
+__device__ __forceinline__ bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+__device__ __forceinline__ void store_operand8(int fmt, const float* v, size_t idx, float* f32,
+                                               __nv_bfloat16* hi, __nv_bfloat16* lo) {
   if (fmt == kFmtF32) {
-    float4* d = reinterpret_cast<float4*>(f32 + idx);
+    float* d = f32 + idx;
+    if (aligned16(d)) {
+      reinterpret_cast<float4*>(d)[0] = make_float4(v[0], v[1], v[2], v[3]);
+      reinterpret_cast<float4*>(d)[1] = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      for (int j = 0; j < 8; ++j) d[j] = v[j];
+    }
     return;
   }
-  __align__(16) __nv_bfloat16 h[16];
-  __align__(16) __nv_bfloat16 l[16];
+  __align__(16) __nv_bfloat16 h[8];
+  __align__(16) __nv_bfloat16 l[8];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
+  for (int j = 0; j < 8; ++j) {
     h[j] = __float2bfloat16_rn(v[j]);
     l[j] = __float2bfloat16_rn(v[j] - __bfloat162float(h[j]));
   }
-  uint4* dh = reinterpret_cast<uint4*>(hi + idx);
-  dh[0] = reinterpret_cast<const uint4*>(h)[0];
-  dh[1] = reinterpret_cast<const uint4*>(h)[1];
+  __nv_bfloat16* dh = hi + idx;
+  if (aligned16(dh)) {
+    *reinterpret_cast<uint4*>(dh) = *reinterpret_cast<const uint4*>(h);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dh[j] = h[j];
+  }
   if (fmt == kFmtSplit) {
-    uint4* dl = reinterpret_cast<uint4*>(lo + idx);
-    dl[0] = reinterpret_cast<const uint4*>(l)[0];
-    dl[1] = reinterpret_cast<const uint4*>(l)[1];
+    __nv_bfloat16* dl = lo + idx;
+    if (aligned16(dl)) {
+      *reinterpret_cast<uint4*>(dl) = *reinterpret_cast<const uint4*>(l);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dl[j] = l[j];
+    }
   }
 }
 
-__device__ __forceinline__ double epi_apply_row16(const EpiParams& p, int m, int n0, const float* acc) {
-  float v[16];
+__device__ __forceinline__ void load8(const float* src, float* v) {
+  if (aligned16(src)) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(src) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
 #pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = __fmul_rn(acc[j], p.alpha);
+    for (int j = 0; j < 8; ++j) v[j] = __ldg(src + j);
+  }
+}
+
+// row-major kinds (STORE, SPECTRAL, ENERGY): elements (m, n0 .. n0+7)
+__device__ __forceinline__ double epi_row8(const EpiParams& p, int m, int n0, const float* acc) {
+  if (n0 + 8 > p.N) {
+    double e = 0.0;
+    for (int j = 0; j < 8 && n0 + j < p.N; ++j) e += epi_apply(p, m, n0 + j, acc[j]);
+    return e;
+  }
+  float v[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = __fmul_rn(acc[j], p.alpha);
   const size_t idx = (size_t)m * p.ldc + n0;
   switch (p.kind) {
-    case DP_EPI_STORE: {
-      float4* d = reinterpret_cast<float4*>(p.out_f32 + idx);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    case DP_EPI_STORE:
+      store_operand8(kFmtF32, v, idx, p.out_f32, nullptr, nullptr);
       return 0.0;
-    }
     case DP_EPI_SPECTRAL: {
-      float wx[16], wy[16], wi[16];
+      float wx[8], wy[8], wi[8];
       if (p.spec_w) {
         const size_t t = (size_t)m * p.N + n0, mn = (size_t)p.M * p.N;
-        const float4* a = reinterpret_cast<const float4*>(p.spec_w + t);
-        const float4* b = reinterpret_cast<const float4*>(p.spec_w + mn + t);
-        const float4* c = reinterpret_cast<const float4*>(p.spec_w + 2 * mn + t);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float4 A = __ldg(a + q), B = __ldg(b + q), Cc = __ldg(c + q);
-          wx[4 * q] = A.x; wx[4 * q + 1] = A.y; wx[4 * q + 2] = A.z; wx[4 * q + 3] = A.w;
-          wy[4 * q] = B.x; wy[4 * q + 1] = B.y; wy[4 * q + 2] = B.z; wy[4 * q + 3] = B.w;
-          wi[4 * q] = Cc.x; wi[4 * q + 1] = Cc.y; wi[4 * q + 2] = Cc.z; wi[4 * q + 3] = Cc.w;
-        }
+        load8(p.spec_w + t, wx);
+        load8(p.spec_w + mn + t, wy);
+        load8(p.spec_w + 2 * mn + t, wi);
       } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) spectral_weights(p, m, n0 + j, wx[j], wy[j], wi[j]);
+        for (int j = 0; j < 8; ++j) spectral_weights(p, m, n0 + j, wx[j], wy[j], wi[j]);
       }
-      float o[16];
+      float o[8];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wx[j]);
-      store_operand16(p.fmt, o, idx, p.sp_f32[0], p.sp_hi[0], p.sp_lo[0]);
+      for (int j = 0; j < 8; ++j) o[j] = __fmul_rn(v[j], wx[j]);
+      store_operand8(p.fmt, o, idx, p.sp_f32[0], p.sp_hi[0], p.sp_lo[0]);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wy[j]);
-      store_operand16(p.fmt, o, idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
+      for (int j = 0; j < 8; ++j) o[j] = __fmul_rn(v[j], wy[j]);
+      store_operand8(p.fmt, o, idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
       if (p.sp_f32[2] || p.sp_hi[2]) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) o[j] = __fmul_rn(v[j], wi[j]);
-        store_operand16(p.fmt, o, idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
+        for (int j = 0; j < 8; ++j) o[j] = __fmul_rn(v[j], wi[j]);
+        store_operand8(p.fmt, o, idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
       }
       return 0.0;
     }
     case DP_EPI_ENERGY: {
-      const float4* r = reinterpret_cast<const float4*>(p.rho + idx);
+      float r[8];
+      load8(p.rho + idx, r);
       double e = 0.0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float4 R = __ldg(r + q);
-        e += (double)__fmul_rn(v[4 * q], R.x) + (double)__fmul_rn(v[4 * q + 1], R.y) +
-             (double)__fmul_rn(v[4 * q + 2], R.z) + (double)__fmul_rn(v[4 * q + 3], R.w);
-      }
-      if (p.out_f32) {
-        float4* d = reinterpret_cast<float4*>(p.out_f32 + idx);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      }
+      for (int j = 0; j < 8; ++j) e += (double)__fmul_rn(v[j], r[j]);
+      if (p.out_f32) store_operand8(kFmtF32, v, idx, p.out_f32, nullptr, nullptr);
       return e;
     }
   }
-  double e = 0.0;  // STORE_T: transposed, element by element
+  return 0.0;
+}
+
+// STORE_T: elements (m0 .. m0+7, n), written to [n*ldc + m]
+__device__ __forceinline__ void epi_store_t8(const EpiParams& p, int n, int m0, const float* acc) {
+  if (m0 + 8 > p.M) {
+    for (int j = 0; j < 8 && m0 + j < p.M; ++j) epi_apply(p, m0 + j, n, acc[j]);
+    return;
+  }
+  float v[8];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) e += epi_apply(p, m, n0 + j, acc[j]);
-  return e;
+  for (int j = 0; j < 8; ++j) v[j] = __fmul_rn(acc[j], p.alpha);
+  store_operand8(p.fmt, v, (size_t)n * p.ldc + m0, p.out_f32, p.out_hi, p.out_lo);
 }
 
 inline int validate_problem(const dp_gemm_problem& q, int precision, int M, int N, int K) {

@@ -8,8 +8,12 @@
 // (transposed operand store with bf16 hi/lo split, spectral scaling, fp32
 // field store, or the energy dot product; epilogue.cuh).
 //
-// Split-BF16 runs three passes over K into the same accumulator:
-// A_hi*B_hi + A_hi*B_lo + A_lo*B_hi (the lo*lo term is below fp32 rounding).
+// Split-BF16 stages A_hi, A_lo, B_hi and B_lo of one k-block together and
+// issues A_hi*B_hi, A_hi*B_lo and A_lo*B_hi on them into the same accumulator
+// (the lo*lo term is below fp32 rounding), so every operand tile crosses L2
+// once per k-block instead of once per product.  The 128 x 128 tile halves
+// the L2 -> SM traffic per output element of a 128 x 64 tile; the transforms
+// are bound by that traffic, not by the tensor pipe.
 //
 // Every wait on an mbarrier is bounded by a clock budget; on expiry the
 // kernel records an error code in g_tc_status, drains what it issued and
@@ -148,9 +152,12 @@ struct TcConfig {
   static constexpr int kMmaPerBlock = kBK / kMmaK;        // = 4
   static constexpr int kABytes = TC_BM * 128;
   static constexpr int kBBytes = BN * 128;
-  static constexpr int kStageBytes = kABytes + kBBytes;
+  // stage layout: A_hi | B_hi (| A_lo | B_lo for split-BF16)
+  static constexpr int kStageBytes = (kSplit ? 2 : 1) * (kABytes + kBBytes);
   static constexpr int kSmemBytes = STAGES * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
-  static constexpr int kPasses = kSplit ? 3 : 1;
+  // the epilogue stages the 128 x BN accumulator (padded rows) in the ring
+  static_assert(STAGES * kStageBytes >= (BN + 4) * TC_BM * 4 && STAGES * kStageBytes >= (TC_BM + 4) * BN * 4,
+                "operand ring too small for the epilogue staging tile");
 };
 
 template <int PREC, int BN, int STAGES>
@@ -168,8 +175,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   const int z = blockIdx.z;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
-  const int kb_per_pass = (K + Cfg::kBK - 1) / Cfg::kBK;
-  const int total_kb = kb_per_pass * Cfg::kPasses;
+  const int total_kb = (K + Cfg::kBK - 1) / Cfg::kBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -197,14 +203,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     for (int kb = 0; kb < total_kb; ++kb) {
       int s = kb % STAGES, round = kb / STAGES;
       if (round > 0 && !mbar_wait(&empty_bar[s], (round - 1) & 1, 1)) break;
-      int pass = kb / kb_per_pass, kx = (kb % kb_per_pass) * Cfg::kBK;
-      const CUtensorMap* amap = (Cfg::kSplit && pass == 2) ? &batch.a_lo[z] : &batch.a_hi[z];
-      const CUtensorMap* bmap = (Cfg::kSplit && pass == 1) ? &batch.b_lo[z] : &batch.b_hi[z];
+      const int kx = kb * Cfg::kBK;
       uint8_t* sa = tiles + s * Cfg::kStageBytes;
       uint8_t* sb = sa + Cfg::kABytes;
       mbar_expect_tx(&full_bar[s], Cfg::kStageBytes);
-      tma_load_2d(sa, amap, &full_bar[s], kx, m0);
-      tma_load_2d(sb, bmap, &full_bar[s], kx, n0);
+      tma_load_2d(sa, &batch.a_hi[z], &full_bar[s], kx, m0);
+      tma_load_2d(sb, &batch.b_hi[z], &full_bar[s], kx, n0);
+      if (Cfg::kSplit) {
+        tma_load_2d(sb + Cfg::kBBytes, &batch.a_lo[z], &full_bar[s], kx, m0);
+        tma_load_2d(sb + Cfg::kBBytes + Cfg::kABytes, &batch.b_lo[z], &full_bar[s], kx, n0);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
@@ -215,12 +223,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       tc_fence_after();
       uint32_t sa = smem_addr(tiles + s * Cfg::kStageBytes);
       uint32_t sb = sa + Cfg::kABytes;
-      uint64_t adesc = sw128_desc(sa), bdesc = sw128_desc(sb);
+      const uint64_t adesc = sw128_desc(sa), bdesc = sw128_desc(sb);
+      const uint64_t alo = sw128_desc(sb + Cfg::kBBytes), blo = sw128_desc(sb + Cfg::kBBytes + Cfg::kABytes);
 #pragma unroll
       for (int kk = 0; kk < Cfg::kMmaPerBlock; ++kk) {
         // advance the start address by 32 bytes per K step inside the swizzle row
-        tc_mma<Cfg::kTF32>(tmem_base, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
-                           (kb > 0 || kk > 0) ? 1u : 0u);
+        const uint64_t dk = (uint64_t)(kk * 2);
+        tc_mma<Cfg::kTF32>(tmem_base, adesc + dk, bdesc + dk, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+        if (Cfg::kSplit) {
+          tc_mma<Cfg::kTF32>(tmem_base, adesc + dk, blo + dk, idesc, 1u);
+          tc_mma<Cfg::kTF32>(tmem_base, alo + dk, bdesc + dk, idesc, 1u);
+        }
       }
       tc_commit(&empty_bar[s]);  // frees the stage once these MMAs retire
     }
@@ -228,28 +241,51 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   }
   __syncwarp();
 
-  // ---- epilogue: warp w owns accumulator rows 32w..32w+31 ----
+  // ---- epilogue ----
+  // The accumulator is staged through shared memory (the operand ring is
+  // drained once the accumulator is complete) in the orientation of the output
+  // rows, then every thread applies the epilogue to 8 consecutive elements of
+  // one output row, so each warp store covers whole row segments instead of
+  // one element of 32 different rows.
   const EpiParams& P = batch.epi[z];
+  const bool acc_ok = mbar_wait(acc_bar, 0, 3);
   double e = 0.0;
-  if (mbar_wait(acc_bar, 0, 3)) {
+  if (__syncthreads_and(acc_ok)) {
     tc_fence_after();
-    const int m = m0 + warp * 32 + lane;
+    const bool trans = P.kind == DP_EPI_STORE_T;
+    float* stage = reinterpret_cast<float*>(tiles);
+    constexpr int kRowPitch = BN + 4;     // stage[m][n] for row-major outputs
+    constexpr int kColPitch = TC_BM + 4;  // stage[n][m] for STORE_T
+    const int r_acc = warp * 32 + lane;   // accumulator row = TMEM lane
     const uint32_t row_addr = tmem_base + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-    const bool vec_ok = (P.ldc % 8) == 0;
     for (int c = 0; c < BN; c += 16) {
       float v[16];
       tmem_ld16(row_addr + (uint32_t)c, v);
-      if (m < M) {
-        if (vec_ok && n0 + c + 16 <= N) {
-          e += epi_apply_row16(P, m, n0 + c, v);
-        } else {
+      if (trans) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            int n = n0 + c + j;
-            if (n < N) e += epi_apply(P, m, n, v[j]);
-          }
-        }
+        for (int j = 0; j < 16; ++j) stage[(c + j) * kColPitch + r_acc] = v[j];
+      } else {
+        float4* d = reinterpret_cast<float4*>(stage + r_acc * kRowPitch + c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
+    }
+    __syncthreads();
+    const int cols = trans ? TC_BM : BN;
+    const int pitch = trans ? kColPitch : kRowPitch;
+    const int segs = cols / 8;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < (trans ? BN : TC_BM) * segs; i += TC_THREADS) {
+      const int r = i / segs, c0 = (i % segs) * 8;
+      float v[8];
+      const float4* src = reinterpret_cast<const float4*>(stage + r * pitch + c0);
+      const float4 a = src[0], b4 = src[1];
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b4.x; v[5] = b4.y; v[6] = b4.z; v[7] = b4.w;
+      if (trans) {
+        if (n0 + r < N) epi_store_t8(P, n0 + r, m0 + c0, v);
+      } else {
+        if (m0 + r < M) e += epi_row8(P, m0 + r, n0 + c0, v);
       }
     }
   }
@@ -332,17 +368,14 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
 
 int launch_tc_gemm(int precision, int M, int N, int K, const dp_gemm_problem* probs, int count, cudaStream_t s) {
   switch (precision) {
-    // A single problem runs one CTA per SM with an 8-deep TMA ring; batched
-    // problems (3x the tiles) run two CTAs per SM with 4 stages each.
+    // 128 x 128 tiles, one CTA per SM: a 6-deep TMA ring of 32 KB stages, or
+    // 3 stages of 64 KB (hi and lo of both operands) for split-BF16.
     case DP_PREC_TF32:
-      return count == 1 ? run_tc<DP_PREC_TF32, 64, 8>(M, N, K, probs, count, s)
-                        : run_tc<DP_PREC_TF32, 64, 4>(M, N, K, probs, count, s);
+      return run_tc<DP_PREC_TF32, 128, 6>(M, N, K, probs, count, s);
     case DP_PREC_BF16:
-      return count == 1 ? run_tc<DP_PREC_BF16, 64, 8>(M, N, K, probs, count, s)
-                        : run_tc<DP_PREC_BF16, 64, 4>(M, N, K, probs, count, s);
+      return run_tc<DP_PREC_BF16, 128, 6>(M, N, K, probs, count, s);
     case DP_PREC_SPLIT_BF16:
-      return count == 1 ? run_tc<DP_PREC_SPLIT_BF16, 64, 8>(M, N, K, probs, count, s)
-                        : run_tc<DP_PREC_SPLIT_BF16, 64, 4>(M, N, K, probs, count, s);
+      return run_tc<DP_PREC_SPLIT_BF16, 128, 3>(M, N, K, probs, count, s);
   }
   set_error("dp_transform_gemm: unsupported precision %d", precision);
   return DP_ERR_UNSUPPORTED;

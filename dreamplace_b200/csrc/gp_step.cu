@@ -532,7 +532,7 @@ template <bool kGrad>
 __global__ void __launch_bounds__(256) wa_chunk_kernel(
     const float2* __restrict__ xy, const int* __restrict__ slot_node,
     const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ slot_net,
-    const int* __restrict__ netpin_start, const int* __restrict__ chunk_net, int num_chunks,
+    const int* __restrict__ chunk_pin, int num_chunks,
     const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
     const float* __restrict__ inv_gamma_p, const int* __restrict__ csr_pos, double* __restrict__ partials,
     float2* __restrict__ gnode, const unsigned char* __restrict__ hpwl_mask, double* __restrict__ hpwl_partials) {
@@ -545,21 +545,22 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double contrib = 0.0;
   for (int c = warp; c < num_chunks; c += nwarps) {
-    const int n0 = chunk_net[c], n1 = chunk_net[c + 1];
-    const int s0 = netpin_start[n0], s1 = netpin_start[n1];
+    const int s0 = chunk_pin[c], s1 = chunk_pin[c + 1];
     const int np = s1 - s0;
     if (np <= 32) {
       const bool valid = lane < np;
       const int s = s0 + lane;
       const int net = valid ? __ldcs(slot_net + s) : INT_MAX;
-      const SegInfo sg = segment_of(net, lane);
-      const bool on = valid && net_mask[net];
+      int cur_csr = 0;
       float xx = 0.f, yy = 0.f;
       if (valid) {
         const float2 p = xy[__ldcs(slot_node + s)];
         xx = fadd(__ldcs(slot_offx + s), p.x);
         yy = fadd(__ldcs(slot_offy + s), p.y);
+        if (kGrad) cur_csr = __ldcs(csr_pos + s);
       }
+      const SegInfo sg = segment_of(net, lane);
+      const bool on = valid && net_mask[net];
       const float x_max = seg_reduce(valid ? xx : -FLT_MAX, sg, lane, MaxOp());
       const float x_min = seg_reduce(valid ? xx : FLT_MAX, sg, lane, MinOp());
       const float y_max = seg_reduce(valid ? yy : -FLT_MAX, sg, lane, MaxOp());
@@ -616,10 +617,10 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
           gyv = fmul(gyv, w);
         }
       }
-      __stcs(gnode + __ldcs(csr_pos + s), make_float2(gxv, gyv));
+      __stcs(gnode + cur_csr, make_float2(gxv, gyv));
     } else {
       // one net with more than 32 pins: lanes stride over its pins
-      const int net = n0;
+      const int net = slot_net[s0];
       const bool on = net_mask[net];
       float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
       for (int s = s0 + lane; s < s1; s += 32) {
@@ -750,7 +751,7 @@ extern "C" int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, in
 }
 
 static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                         const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
+                         const float* slot_offy, const int* slot_net, const int* chunk_pin,
                          int num_chunks, const float* net_weights, const unsigned char* net_mask,
                          const float* inv_gamma, const int* csr_pos, double* out_f64, float* gnode, int num_slots,
                          const unsigned char* hpwl_mask, double* hpwl_f64, cudaStream_t s) {
@@ -759,13 +760,13 @@ static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* s
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   const float2* p2 = reinterpret_cast<const float2*>(xy);
   if (grad)
-    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
-                                                chunk_net, num_chunks, net_weights, net_mask, inv_gamma, csr_pos,
+    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, chunk_pin,
+                                                num_chunks, net_weights, net_mask, inv_gamma, csr_pos,
                                                 out_f64 + 1, reinterpret_cast<float2*>(gnode), hpwl_mask,
                                                 hpwl_f64 ? hpwl_f64 + 1 : nullptr);
   else
-    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, netpin_start,
-                                                 chunk_net, num_chunks, net_weights, net_mask, nullptr, nullptr,
+    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, chunk_pin,
+                                                 num_chunks, net_weights, net_mask, nullptr, nullptr,
                                                  out_f64 + 1, nullptr, nullptr, nullptr);
   int rc = check_launch(grad ? "dp_wa_chunk_forward" : "dp_hpwl_chunk");
   if (rc) return rc;
@@ -777,32 +778,29 @@ static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* s
 }
 
 extern "C" int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                                   const float* slot_offy, const int* slot_net, const int* netpin_start,
-                                   const int* chunk_net, int num_chunks, const float* net_weights,
+                                   const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
+                                   const float* net_weights,
                                    const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
                                    double* wl_f64, float* grad_node_order, int num_slots,
                                    const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream) {
-  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
-                 inv_gamma && csr_pos && wl_f64 && grad_node_order,
+  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && chunk_pin && net_mask && inv_gamma && csr_pos &&
+                 wl_f64 && grad_node_order,
              "dp_wa_chunk_forward: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
              "dp_wa_chunk_forward: xy and grad_node_order must be 8-byte aligned");
   DP_REQUIRE(!hpwl_f64 || hpwl_mask, "dp_wa_chunk_forward: hpwl_f64 needs hpwl_mask");
-  return launch_chunks(true, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
-                       num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
+  return launch_chunks(true, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, chunk_pin, num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
                        hpwl_mask, hpwl_f64, dpb::as_stream(stream));
 }
 
 extern "C" int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                             const float* slot_offy, const int* slot_net, const int* netpin_start,
-                             const int* chunk_net, int num_chunks, const float* net_weights,
+                             const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
+                             const float* net_weights,
                              const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
-  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && netpin_start && chunk_net && net_mask &&
-                 out_f64,
+  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && chunk_pin && net_mask && out_f64,
              "dp_hpwl_chunk: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0, "dp_hpwl_chunk: xy must be 8-byte aligned");
-  return launch_chunks(false, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, netpin_start, chunk_net,
-                       num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0, nullptr, nullptr,
+  return launch_chunks(false, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, chunk_pin, num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0, nullptr, nullptr,
                        dpb::as_stream(stream));
 }
 

@@ -59,6 +59,7 @@ class GPEngine(object):
         # warp-per-chunk WA / HPWL: nets packed into <= 32-pin chunks; the WA
         # gradient lands at each pin's position in node-CSR order
         self.chunk_net = C.plan_net_chunks(self.netpin_start.cpu(), 32).to(dev)
+        self.chunk_pin = self.netpin_start[self.chunk_net.long()].contiguous()
         csr_pos = torch.empty(P, dtype=torch.int64, device=dev)
         csr_pos[self.node_slots.long()] = torch.arange(P, device=dev)
         self.csr_pos = csr_pos.to(torch.int32)
@@ -113,7 +114,7 @@ class GPEngine(object):
         self.inv_order = torch.zeros(n, dtype=torch.int32, device=dev)
         self.force_o = torch.empty(2 * count, dtype=torch.float32, device=dev)
         self._build_records()
-        self.sort_interval = int(getattr(params, "sort_interval", 10))
+        self.sort_interval = int(getattr(params, "sort_interval", 50))
         self.iterations = 0
         self.parity = 0
         self.graphs = {}
@@ -152,11 +153,12 @@ class GPEngine(object):
             tiles_y = (ep.num_bins_y + 15) >> 4
             tx, ty = kx >> 4, hy >> 4
             ty = ty + (tx & 1) * (tiles_y - 1 - 2 * ty)
-            key = ((tx * tiles_y + ty) << 8) | ((kx & 15) << 4) | (hy & 15)
-            om = torch.argsort(key[:nm]).to(torch.int32)
+            # 32-bit keys (tile index * 256 + bin in tile) halve the radix passes
+            key = (((tx * tiles_y + ty) << 8) | ((kx & 15) << 4) | (hy & 15)).to(torch.int32)
+            om = torch.sort(key[:nm]).indices.to(torch.int32)
             self.order[:nm].copy_(om)
             if nf:
-                of = torch.argsort(key[n - nf:]).to(torch.int32).add_(n - nf)
+                of = torch.sort(key[n - nf:]).indices.to(torch.int32).add_(n - nf)
                 self.order[nm:].copy_(of)
             self._build_records()
 
@@ -173,8 +175,8 @@ class GPEngine(object):
         same pin reads."""
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
-        C.wa_chunk_forward(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
-                           self.chunk_net, dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
+        C.wa_chunk_forward(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.chunk_pin,
+                           dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
                            self.csr_pos, self.wl64_buf, self.gnode,
                            dc.net_mask_all if hpwl_out is not None else None, hpwl_out)
 
@@ -190,8 +192,7 @@ class GPEngine(object):
                                     self.order.numel(), ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
                                     float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
                                     ep.num_bins_x, ep.num_bins_y, int(self.det), self.scratch, self.omap.view(-1),
-                                    self.dmap.view(-1))
-        C.density_overflow_into(self.omap, self.ovf_target, self.ovf_area, ovf_out)
+                                    self.dmap.view(-1), self.ovf_target, self.ovf_area, ovf_out)
 
     def density_energy(self, v, ovf_out=None):
         """Density map, Poisson solve; returns (ex, ey, energy_f64[1]).  With ovf_out,
@@ -267,8 +268,8 @@ class GPEngine(object):
         for a position set from outside the trial kernel."""
         dc = self.data
         v = self.V[q]
-        C.hpwl_chunk(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.netpin_start,
-                     self.chunk_net, dc.net_weights, dc.net_mask_all, self.H[q])
+        C.hpwl_chunk(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.chunk_pin,
+                     dc.net_weights, dc.net_mask_all, self.H[q])
         self._density(v, 0, self.omap)
         C.density_overflow_into(self.omap, self.ovf_target, self.ovf_area, self.O[q])
 

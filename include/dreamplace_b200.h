@@ -139,14 +139,17 @@ int dp_density_map_ordered(const float* xy, const int* order, const float* rec4,
  * cells [0, num_first) of the order, out_all = initial_density_map + cells
  * [0, count).  Used for the movable-only map (overflow metric) and the
  * movable + filler map (Poisson input) of one position, so each cell is
- * scattered once.  Deterministic: both maps bit-exact with separate scatters. */
+ * scattered once.  Deterministic: both maps bit-exact with separate scatters.
+ * overflow_out (optional, DP_REDUCE_DOUBLES doubles): dp_density_overflow of
+ * out_first with target_area and bin_area, computed in the same pass. */
 int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4, const float* ratio_o,
                                  int num_first, int count, const float* initial_density_map,
                                  float xl, float yl, float xh, float yh,
                                  float bin_size_x, float bin_size_y,
                                  float inv_bin_size_x, float inv_bin_size_y,
                                  int num_bins_x, int num_bins_y, int deterministic, int fraction_bits,
-                                 int64_t* scratch_fixed, float* out_first, float* out_all, dp_stream_t stream);
+                                 int64_t* scratch_fixed, float* out_first, float* out_all,
+                                 double target_area, double bin_area, double* overflow_out, dp_stream_t stream);
 
 /* Exact-overlap fixed-cell map (electric_potential/src/electric_density_map_cuda.cpp:139-183,
  * CPU electric_potential/src/electric_density_map.cpp:155-213): nodes
@@ -368,7 +371,9 @@ int dp_nesterov_advance(double* state, dp_stream_t stream);
 int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
                        int* num_chunks);
 /* WA forward, one warp per net chunk (max_pins = 32), one lane per pin; per-net
- * reductions are segmented warp shuffles.  Node positions come interleaved
+ * reductions are segmented warp shuffles.  chunk_pin [num_chunks + 1]: first
+ * pin slot of each chunk (netpin_start at the chunk's first net, see
+ * dp_plan_net_chunks), then the pin count.  Node positions come interleaved
  * (xy [2 * num_nodes], see dp_pack_xy).  The per-pin gradient, times the net
  * weight, is written as an (x, y) pair at csr_pos[slot] (the pin's position in
  * node-CSR order) of grad_node_order [2 * num_slots]; masked nets write 0.
@@ -376,16 +381,14 @@ int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins,
  * doubles): the HPWL of the same pins under hpwl_mask, equal to dp_hpwl_chunk's
  * result (same per-net values, same summation order), from the same pin reads. */
 int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                        const float* slot_offy, const int* slot_net, const int* netpin_start,
-                        const int* chunk_net, int num_chunks, const float* net_weights,
-                        const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
-                        double* wl_f64, float* grad_node_order, int num_slots,
+                        const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
+                        const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
+                        const int* csr_pos, double* wl_f64, float* grad_node_order, int num_slots,
                         const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream);
 /* HPWL with the same chunking (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
 int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                  const float* slot_offy, const int* slot_net, const int* netpin_start, const int* chunk_net,
-                  int num_chunks, const float* net_weights, const unsigned char* net_mask, double* out_f64,
-                  dp_stream_t stream);
+                  const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
+                  const float* net_weights, const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
 /* grad_out[node] (+)= sum over k in node_start[node]..node_start[node+1] of the
  * (x, y) pair grad_node_order[2k..2k+1] * grad_pos[0]; nodes >= num_movable get 0
  * (pin mask of fixed cells) */

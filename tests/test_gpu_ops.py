@@ -414,13 +414,18 @@ def test_ordered_split_scatter(C):
     geo = (d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y)
     for det in (1, 0):
         first, full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
+        ovf = torch.zeros(1280, dtype=torch.float64, device="cuda")
+        ba = d.bin_size_x * d.bin_size_y
         C.density_map_ordered_split(xy, dev(order), rec4, ratio_o, m, len(order), init, *geo, det,
-                                    scratch if det else None, first, full)
+                                    scratch if det else None, first, full, 0.9 * ba, ba, ovf)
         exp_first, exp_full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
         C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, m, init, *geo, det, scratch if det else None,
                                    exp_first)
         C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), init, *geo, det,
                                    scratch if det else None, exp_full)
+        exp_ovf = torch.zeros(1280, dtype=torch.float64, device="cuda")
+        C.density_overflow_into(first, 0.9 * ba, ba, exp_ovf)
+        torch.testing.assert_close(ovf[:2], exp_ovf[:2], rtol=1e-12, atol=0)
         if det:
             assert torch.equal(first, exp_first) and torch.equal(full, exp_full)
         else:
