@@ -181,11 +181,13 @@ def replica_value(steps, world, ms_max):
 class TimedRun(object):
     """Runs the GP loop and times iterations [warmup, warmup + steps) with CUDA events."""
 
-    def __init__(self, design, precision, world, e2e=False):
+    def __init__(self, design, precision, world, e2e=False, time_pieces=False):
         from dreamplace_b200.nonlinear_place import NonLinearPlace
         from dreamplace_b200.params import Params
         self.params = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision=precision,
-                             deterministic_flag=0)
+                             deterministic_flag=0, time_pieces=time_pieces)
+        self.dominant = None
+        self.dominant_ms = None
         self.design = design
         self.world = world
         self.placer = NonLinearPlace(self.params, design, "cuda")
@@ -211,6 +213,14 @@ class TimedRun(object):
 
         def cb(it, metric):
             if it == warmup - 1:
+                eng = getattr(getattr(self.placer, "stepper", None), "eng", None)
+                if eng is not None and eng.piece_events is not None:
+                    # the warm-up trials timed every piece; the timed region
+                    # accumulates only the longest one (one event query per trial)
+                    means = eng.piece_means()
+                    if means:
+                        self.dominant = max(means, key=means.get)
+                        eng.reset_piece_times([self.dominant])
                 torch.cuda.synchronize()
                 barrier(self.world)
                 torch.cuda.synchronize()
@@ -232,6 +242,9 @@ class TimedRun(object):
                     torch.cuda.synchronize()
                     if clocks is not None:
                         clocks.end()
+                    eng = getattr(getattr(self.placer, "stepper", None), "eng", None)
+                    if self.dominant is not None and eng is not None:
+                        self.dominant_ms = eng.piece_means().get(self.dominant)
                     state["launch1"] = launches()
                     state["trials1"] = trials()
 
@@ -265,13 +278,12 @@ def _graph_time(fn, reps=20):
     return s.elapsed_time(e) / reps
 
 
-def kernel_roofline(placer, design, peaks, reps=20):
-    """Device time of each piece of one Nesterov trial of the engine (each piece
-    graph-captured and replayed) with its algorithmic bytes or flops:
+def piece_work(design, eng):
+    """Algorithmic bytes (or flops) of each piece of one Nesterov trial:
 
     * density_scatter: per scattered cell 16 B record + 4 B ratio + 4 B order
       index + 8 B position; per bin 4 B initial map read, movable-only map
-      written and read back by the overflow reduction, full map written;
+      written and read back by the fused overflow pass, full map written;
     * poisson_gemms: the four GEMM launches' flops;
     * field_gather: per cell the same 32 B as the scatter + 8 B force written;
       per bin the two field maps read once;
@@ -284,37 +296,45 @@ def kernel_roofline(placer, design, peaks, reps=20):
     * nesterov_trial: per node 3 x 8 B read (v, g, u), 2 x 8 B written (u, v)
       + 8 B interleaved copy + 8 B cell size."""
     from dreamplace_b200.dct2_fft2 import gemm_flops
-    from dreamplace_b200.electric_potential import poisson_solve
-    eng = placer.stepper.eng
-    d = design
-    ep = eng.ep
+    d, ep = design, eng.ep
     n_s = d.num_movable_nodes + d.num_filler_nodes
     M, N = ep.num_bins_x, ep.num_bins_y
     P, E, n = d.num_pins, d.num_nets, d.num_nodes
+    return {"density_scatter": (32.0 * n_s + 16.0 * M * N, "hbm"),
+            "poisson_gemms": (gemm_flops(M, N, eng.prec, 4), "tensor" if eng.prec else "fp32"),
+            "field_gather": (40.0 * n_s + 8.0 * M * N, "hbm"),
+            "wa_forward": (28.0 * P + 10.0 * E + 8.0 * n, "hbm"),
+            "assemble_precondition": (8.0 * P + 64.0 * n, "hbm"),
+            "nesterov_trial": (64.0 * n, "hbm")}
+
+
+def kernel_roofline(placer, design, peaks, reps=20):
+    """Device time of each piece of one Nesterov trial of the engine, each piece
+    graph-captured alone and replayed (warm L2), with its algorithmic work
+    (piece_work)."""
+    from dreamplace_b200.electric_potential import poisson_solve
+    eng = placer.stepper.eng
+    ep = eng.ep
+    work = piece_work(design, eng)
     p = eng.parity
     q = 1 - p
     v, g = eng.V[p], eng.G[p]
     vn, gn = eng.V[q], eng.G[q]
     saved = eng.state.clone()
-    res = {}
-    res["density_scatter"] = (_graph_time(lambda: eng.scatter_maps(v, eng.O[q]), reps),
-                              32.0 * n_s + 16.0 * M * N, "hbm")
+    t = {}
+    t["density_scatter"] = _graph_time(lambda: eng.scatter_maps(v, eng.O[q]), reps)
     rho = eng.dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
-    res["poisson_gemms"] = (_graph_time(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec), reps),
-                            gemm_flops(M, N, eng.prec, 4), "tensor" if eng.prec else "fp32")
+    t["poisson_gemms"] = _graph_time(lambda: poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec), reps)
     ex, ey, _ = poisson_solve(rho, ep.bin_size_x, ep.bin_size_y, eng.prec)
-    res["field_gather"] = (_graph_time(lambda: eng.field_force(v, ex, ey), reps), 40.0 * n_s + 8.0 * M * N, "hbm")
-    res["wa_forward"] = (_graph_time(lambda: eng.wirelength(v, eng.H[q]), reps), 28.0 * P + 10.0 * E + 8.0 * n,
-                         "hbm")
-    res["assemble_precondition"] = (_graph_time(lambda: eng.assemble(v, g, vn, gn), reps), 8.0 * P + 64.0 * n,
-                                    "hbm")
-    res["nesterov_trial"] = (_graph_time(lambda: eng.nesterov_trial_only(p), reps), 64.0 * n, "hbm")
+    t["field_gather"] = _graph_time(lambda: eng.field_force(v, ex, ey), reps)
+    t["wa_forward"] = _graph_time(lambda: eng.wirelength(v, eng.H[q]), reps)
+    t["assemble_precondition"] = _graph_time(lambda: eng.assemble(v, g, vn, gn), reps)
+    t["nesterov_trial"] = _graph_time(lambda: eng.nesterov_trial_only(p), reps)
     eng.state.copy_(saved)
-    return res
+    return {k: (t[k],) + work[k] for k in t}
 
 
-def roofline_entry(res, peaks):
-    name, (ms, work, bound) = max(res.items(), key=lambda kv: kv[1][0])
+def roofline_entry(name, ms, work, bound, peaks, timing):
     if bound == "hbm":
         achieved = work / (ms * 1e-3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
@@ -332,7 +352,8 @@ def roofline_entry(res, peaks):
             traffic = None
     return {"kernel": name, "bound": "hbm" if bound == "hbm" else "tensor", "achieved": round(achieved, 2),
             "peak": peak, "unit": unit, "frac": round(achieved / peak, 4), "traffic": traffic,
-            "ms_per_launch": round(ms, 4), "peak_source": "measured" if peaks else "fallback"}
+            "ms_per_launch": round(ms, 4), "work_per_launch": work, "timing": timing,
+            "peak_source": "measured" if peaks else "fallback"}
 
 
 def load_peaks():
@@ -525,7 +546,7 @@ def main():
     peaks = load_peaks()
     W, K = max(args.warmup, 3), args.steps
     clocks = ClockSampler(local) if rank == 0 else None
-    run = TimedRun(design, args.precision, world)
+    run = TimedRun(design, args.precision, world, time_pieces=not args.no_roofline)
     ms = run.run(W, K, clocks=clocks)
     clk = clocks.stop() if clocks else None
     ms = max_over_ranks(ms, world)
@@ -539,7 +560,12 @@ def main():
         e2e = {"value": round(replica_value(K, world, ms_e2e), 3), "unit": UNIT,
                "h2d_bytes_per_step": run_e2e.h2d, "d2h_bytes_per_step": run_e2e.d2h}
     pieces = {} if args.no_roofline else kernel_roofline(run.placer, design, peaks)
-    roof = roofline_entry(pieces, peaks) if pieces else None
+    roof = None
+    if run.dominant is not None and run.dominant_ms:
+        work, bound = piece_work(design, run.placer.stepper.eng)[run.dominant]
+        roof = roofline_entry(run.dominant, run.dominant_ms, work, bound, peaks,
+                              "CUDA events around the piece inside the captured trial graph, mean over the "
+                              "trials of the timed region")
     plain = None
     if not args.no_plain and args.precision != "fp32":
         prun = TimedRun(design, "fp32", world)
@@ -571,6 +597,7 @@ def main():
                 "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "kernel_ms": {k: round(v[0], 4) for k, v in pieces.items()},
+                "kernel_ms_timing": "each piece captured alone and replayed 20x after the timed region",
                 "trials_per_step": round(run.trials / max(K, 1), 3),
                 "plain_fp32": plain}
         print(json.dumps(line))

@@ -367,10 +367,19 @@ void nesterov_init(at::Tensor state, double alpha) { DP_CALL(dp_nesterov_init(pt
 
 void nesterov_trial(at::Tensor v, at::Tensor g, at::Tensor u, at::Tensor u_new, at::Tensor v_new,
                     c10::optional<at::Tensor> xy_new, at::Tensor state, at::Tensor sx, at::Tensor sy, double xl,
-                    double yl, double xh, double yh, int num_movable, int num_filler) {
+                    double yl, double xh, double yh, int num_movable, int num_filler,
+                    c10::optional<at::Tensor> inv_order, c10::optional<at::Tensor> xy_order) {
+  TORCH_CHECK(!xy_order.has_value() || inv_order.has_value(), "xy_order needs inv_order");
   DP_CALL(dp_nesterov_trial(ptr<float>(v), ptr<float>(g), ptr<float>(u), ptr<float>(u_new), ptr<float>(v_new),
                             (float*)ovp(xy_new), ptr<double>(state), ptr<float>(sx), ptr<float>(sy), xl, yl, xh, yh,
-                            v.numel() / 2, num_movable, num_filler, cur_stream()));
+                            v.numel() / 2, num_movable, num_filler, (const int*)ovp(inv_order),
+                            (float*)ovp(xy_order), cur_stream()));
+}
+
+void gather_order_xy(at::Tensor xy, at::Tensor order, int count, at::Tensor xy_o) {
+  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(xy_o);
+  TORCH_CHECK(count <= order.numel() && 2 * count <= xy_o.numel(), "gather_order_xy: buffers smaller than count");
+  DP_CALL(dp_gather_order_xy(ptr<float>(xy), ptr<int>(order), count, ptr<float>(xy_o), cur_stream()));
 }
 
 void pack_xy(at::Tensor pos, at::Tensor xy) {
@@ -427,22 +436,22 @@ void build_cell_records(at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor 
                                 cur_stream()));
 }
 
-void density_map_ordered_into(at::Tensor xy, at::Tensor order, at::Tensor rec4, at::Tensor ratio_o, int count,
+void density_map_ordered_into(at::Tensor xy_o, at::Tensor rec4, at::Tensor ratio_o, int count,
                               c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh, double bsx,
                               double bsy, int nbx, int nby, int deterministic, c10::optional<at::Tensor> scratch,
                               at::Tensor out) {
-  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(rec4);
-  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
+  CHECK_FLAT(xy_o); CHECK_F32(xy_o); CHECK_F32(rec4);
+  TORCH_CHECK(2 * count <= xy_o.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
               "density_map_ordered_into: buffers smaller than count");
   TORCH_CHECK(out.numel() == (int64_t)nbx * nby, "density_map_ordered_into: output is not num_bins_x*num_bins_y");
   TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
-  DP_CALL(dp_density_map_ordered(ptr<float>(xy), ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o), count,
+  DP_CALL(dp_density_map_ordered(ptr<float>(xy_o), ptr<float>(rec4), ptr<float>(ratio_o), count,
                                  (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy), nbx, nby,
                                  deterministic, fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch),
                                  ptr<float>(out), cur_stream()));
 }
 
-void density_map_ordered_split(at::Tensor xy, at::Tensor order, at::Tensor rec4, at::Tensor ratio_o, int num_first,
+void density_map_ordered_split(at::Tensor xy_o, at::Tensor rec4, at::Tensor ratio_o, int num_first,
                                int count, c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh,
                                double bsx, double bsy, int nbx, int nby, int deterministic,
                                c10::optional<at::Tensor> scratch, at::Tensor out_first, at::Tensor out_all,
@@ -450,28 +459,28 @@ void density_map_ordered_split(at::Tensor xy, at::Tensor order, at::Tensor rec4,
   TORCH_CHECK(!overflow_out.has_value() || (overflow_out->scalar_type() == at::kDouble &&
                                             overflow_out->numel() >= DP_REDUCE_DOUBLES),
               "overflow_out needs DP_REDUCE_DOUBLES doubles");
-  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(order); CHECK_F32(rec4);
-  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
+  CHECK_FLAT(xy_o); CHECK_F32(xy_o); CHECK_F32(rec4);
+  TORCH_CHECK(2 * count <= xy_o.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
               "density_map_ordered_split: buffers smaller than count");
   TORCH_CHECK(out_first.numel() == (int64_t)nbx * nby && out_all.numel() == out_first.numel(),
               "density_map_ordered_split: outputs are not num_bins_x*num_bins_y");
   TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
-  DP_CALL(dp_density_map_ordered_split(ptr<float>(xy), ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o),
+  DP_CALL(dp_density_map_ordered_split(ptr<float>(xy_o), ptr<float>(rec4), ptr<float>(ratio_o),
                                        num_first, count, (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
                                        inv_f(bsx), inv_f(bsy), nbx, nby, deterministic, fraction_bits(xl, yl, xh, yh),
                                        (int64_t*)ovp(scratch), ptr<float>(out_first), ptr<float>(out_all),
                                        target_area, bin_area, (double*)ovp(overflow_out), cur_stream()));
 }
 
-void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy, at::Tensor order,
-                            at::Tensor rec4, at::Tensor ratio_o, int count, double xl, double yl, double bsx,
-                            double bsy, int nbx, int nby, double scale, at::Tensor force_o) {
-  CHECK_FLAT(xy); CHECK_I32(order); CHECK_F32(force_o);
-  TORCH_CHECK(count <= order.numel() && 4 * count <= rec4.numel() && 2 * count <= force_o.numel(),
+void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy_o, at::Tensor rec4,
+                            at::Tensor ratio_o, int count, double xl, double yl, double bsx, double bsy, int nbx,
+                            int nby, double scale, at::Tensor force_o) {
+  CHECK_FLAT(xy_o); CHECK_F32(force_o);
+  TORCH_CHECK(2 * count <= xy_o.numel() && 4 * count <= rec4.numel() && 2 * count <= force_o.numel(),
               "electric_force_ordered: buffers smaller than count");
   TORCH_CHECK(ex.numel() == (int64_t)nbx * nby && ey.numel() == ex.numel(), "electric_force_ordered: field map size");
-  DP_CALL(dp_electric_force_ordered(ptr<float>(grad_scale), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(xy),
-                                    ptr<int>(order), ptr<float>(rec4), ptr<float>(ratio_o), count, xl, yl, bsx, bsy,
+  DP_CALL(dp_electric_force_ordered(ptr<float>(grad_scale), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(xy_o),
+                                    ptr<float>(rec4), ptr<float>(ratio_o), count, xl, yl, bsx, bsy,
                                     inv_f(bsx), inv_f(bsy), (float)scale, ptr<float>(force_o), cur_stream()));
 }
 
@@ -587,6 +596,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("density_overflow_into", &density_overflow_into);
   m.def("density_map_ordered_into", &density_map_ordered_into);
   m.def("build_cell_records", &build_cell_records);
+  m.def("gather_order_xy", &gather_order_xy);
   m.def("density_map_ordered_split", &density_map_ordered_split);
   m.def("electric_force_ordered", &electric_force_ordered);
   m.def("assemble_precondition_step", &assemble_precondition_step);

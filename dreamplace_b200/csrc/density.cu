@@ -111,7 +111,8 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
 // Cells are visited in the caller's order (a spatial order refreshed every few
 // iterations, grouping cells whose stretched footprint starts in the same
 // bin), read from per-cell records (stretched width, height, offsets,
-// ratio) with the node position gathered from the interleaved xy array.
+// ratio) and positions stored in the same order (written there by the
+// Nesterov trial kernel), so every read of the scatter is contiguous.
 //
 // A stretched cell is at least sqrt(2) bins wide, and a standard cell covers
 // at most kWin x kWin bins.  Each lane computes its cell's kWin px and kWin py
@@ -164,8 +165,8 @@ __device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0,
 }
 
 template <bool kFixed>
-__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a, const float2* __restrict__ xy,
-                                                                        const int* __restrict__ order,
+__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a,
+                                                                        const float2* __restrict__ xy_o,
                                                                         const float4* __restrict__ rec4,
                                                                         const float* __restrict__ ratio_o, int count,
                                                                         float fx_scale, float* map_f32,
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
     nx[c] = ny[c] = sxs[c] = sys[c] = rr[c] = 0.f;
     if (idx < count) {
       const float4 r4 = __ldg(rec4 + idx);
-      const float2 p = xy[order[idx]];
+      const float2 p = __ldg(xy_o + idx);
       sxs[c] = r4.x;
       sys[c] = r4.y;
       nx[c] = fadd(p.x, r4.z);
@@ -379,6 +380,12 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
       }
     }
   }
+}
+
+__global__ void gather_order_xy_kernel(const float2* __restrict__ xy, const int* __restrict__ order, int count,
+                                       float2* __restrict__ xy_o) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+    xy_o[idx] = xy[order[idx]];
 }
 
 __global__ void build_records_kernel(const float* __restrict__ sx, const float* __restrict__ sy,
@@ -733,6 +740,16 @@ extern "C" int dp_density_overflow(const float* map, int nbins, double target_ar
   return check_launch("dp_density_overflow finish");
 }
 
+// xy_o[idx] = xy[order[idx]]: positions in visiting order
+extern "C" int dp_gather_order_xy(const float* xy, const int* order, int count, float* xy_o, dp_stream_t stream) {
+  DP_REQUIRE(xy && xy_o && (count == 0 || order), "dp_gather_order_xy: null pointer");
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)xy_o & 7) == 0, "dp_gather_order_xy: misaligned xy / xy_o");
+  if (count == 0) return DP_OK;
+  gather_order_xy_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+      reinterpret_cast<const float2*>(xy), order, count, reinterpret_cast<float2*>(xy_o));
+  return check_launch("dp_gather_order_xy");
+}
+
 // Per-cell records for the order-driven kernels: rec4[idx] = (sx, sy, ox, oy)
 // and ratio_o[idx] of node order[idx]; inv_order[order[idx]] = idx (optional).
 extern "C" int dp_build_cell_records(const float* sx, const float* sy, const float* ox, const float* oy,
@@ -752,8 +769,7 @@ namespace {
 
 struct OrderedScatter {
   TriangleArgs a;
-  const float2* xy;
-  const int* order;
+  const float2* xy_o;
   const float4* rec4;
   const float* ratio_o;
   cudaStream_t s;
@@ -773,11 +789,11 @@ int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic
   const int blocks = ceil_div(count, kWsCells);
   if (deterministic)
     window_scatter_kernel<true><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, o.xy, o.order + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits), nullptr,
+        o.a, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits), nullptr,
         reinterpret_cast<unsigned long long*>(scratch));
   else
     window_scatter_kernel<false><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, o.xy, o.order + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
+        o.a, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
   return check_launch("dp_density_map_ordered scatter");
 }
 
@@ -798,11 +814,11 @@ int start_map(const float* init, float* out, int nbins, cudaStream_t s) {
   return DP_OK;
 }
 
-int ordered_setup(const char* who, const float* xy, const int* order, const float* rec4, const float* ratio_o,
-                  int count, float xl, float yl, float bsx, float bsy, float ibx, float iby, int nbx, int nby,
-                  int deterministic, int fraction_bits, int64_t* scratch, dp_stream_t stream, OrderedScatter& o) {
-  DP_REQUIRE(xy && rec4 && ratio_o && (count == 0 || order), "%s: null pointer", who);
-  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)rec4 & 15) == 0, "%s: misaligned xy/rec4", who);
+int ordered_setup(const char* who, const float* xy_o, const float* rec4, const float* ratio_o, int count, float xl,
+                  float yl, float bsx, float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
+                  int fraction_bits, int64_t* scratch, dp_stream_t stream, OrderedScatter& o) {
+  DP_REQUIRE(xy_o && rec4 && ratio_o, "%s: null pointer", who);
+  DP_REQUIRE(((uintptr_t)xy_o & 7) == 0 && ((uintptr_t)rec4 & 15) == 0, "%s: misaligned xy_o/rec4", who);
   DP_REQUIRE(nbx > 0 && nby > 0 && (long long)nbx * nby < (1ll << 31), "%s: bad bin grid", who);
   DP_REQUIRE(bsx > 0 && bsy > 0 && count >= 0, "%s: bad geometry", who);
   DP_REQUIRE(!deterministic || scratch, "%s: deterministic mode needs scratch_fixed", who);
@@ -810,8 +826,7 @@ int ordered_setup(const char* who, const float* xy, const int* order, const floa
   memset(&o.a, 0, sizeof(o.a));
   o.a.xl = xl; o.a.yl = yl; o.a.bsx = bsx; o.a.bsy = bsy; o.a.inv_bsx = ibx; o.a.inv_bsy = iby;
   o.a.num_bins_x = nbx; o.a.num_bins_y = nby;
-  o.xy = reinterpret_cast<const float2*>(xy);
-  o.order = order;
+  o.xy_o = reinterpret_cast<const float2*>(xy_o);
   o.rec4 = reinterpret_cast<const float4*>(rec4);
   o.ratio_o = ratio_o;
   o.s = as_stream(stream);
@@ -820,15 +835,15 @@ int ordered_setup(const char* who, const float* xy, const int* order, const floa
 
 }  // namespace
 
-// Order-driven scatter (see window_scatter_kernel): the cells order[0..count)
-// with their records, positions interleaved in xy.
-extern "C" int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
-                                      int count, const float* init, float xl, float yl, float xh, float yh, float bsx,
+// Order-driven scatter (see window_scatter_kernel): cells 0..count of the
+// visiting order, positions (xy_o) and attributes (rec4, ratio_o) in that order.
+extern "C" int dp_density_map_ordered(const float* xy_o, const float* rec4, const float* ratio_o, int count,
+                                      const float* init, float xl, float yl, float xh, float yh, float bsx,
                                       float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
                                       int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
   OrderedScatter o;
-  int rc = ordered_setup("dp_density_map_ordered", xy, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx,
-                         nby, deterministic, fraction_bits, scratch, stream, o);
+  int rc = ordered_setup("dp_density_map_ordered", xy_o, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx, nby,
+                         deterministic, fraction_bits, scratch, stream, o);
   if (rc) return rc;
   DP_REQUIRE(out, "dp_density_map_ordered: null output");
   const int nbins = nbx * nby;
@@ -850,15 +865,14 @@ extern "C" int dp_density_map_ordered(const float* xy, const int* order, const f
 // equal separate scatters bit for bit.  fp32: the second map continues from
 // the first, i.e. the float additions happen in one of the orders the atomic
 // scatter of all cells can take.
-extern "C" int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4,
-                                            const float* ratio_o, int num_first, int count, const float* init,
+extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4, const float* ratio_o, int num_first, int count, const float* init,
                                             float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
                                             float iby, int nbx, int nby, int deterministic, int fraction_bits,
                                             int64_t* scratch, float* out_first, float* out_all, double target_area,
                                             double bin_area, double* overflow_out, dp_stream_t stream) {
   OrderedScatter o;
-  int rc = ordered_setup("dp_density_map_ordered_split", xy, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby,
-                         nbx, nby, deterministic, fraction_bits, scratch, stream, o);
+  int rc = ordered_setup("dp_density_map_ordered_split", xy_o, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx,
+                         nby, deterministic, fraction_bits, scratch, stream, o);
   if (rc) return rc;
   DP_REQUIRE(out_first && out_all && out_first != out_all, "dp_density_map_ordered_split: bad outputs");
   DP_REQUIRE(num_first >= 0 && num_first <= count, "dp_density_map_ordered_split: bad num_first");

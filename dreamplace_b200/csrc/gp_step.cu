@@ -235,7 +235,8 @@ __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* 
                                       float* __restrict__ v_new, float2* __restrict__ xy_new,
                                       const double* __restrict__ st, const float* __restrict__ sx,
                                       const float* __restrict__ sy, float xl, float yl, float xh, float yh,
-                                      int num_nodes, int num_movable, int num_filler) {
+                                      int num_nodes, int num_movable, int num_filler,
+                                      const int* __restrict__ inv_order, float2* __restrict__ xy_o) {
   const float alpha = (float)st[NS_ALPHA];
   const float coef = (float)st[NS_COEF];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
@@ -253,6 +254,8 @@ __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* 
     v_new[i] = vx;
     v_new[j] = vy;
     if (xy_new) xy_new[i] = make_float2(vx, vy);
+    // the scattered cells' positions also land in visiting order
+    if (xy_o && (i < num_movable || i >= num_nodes - num_filler)) xy_o[inv_order[i]] = make_float2(vx, vy);
   }
 }
 
@@ -441,13 +444,15 @@ extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream)
 extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
                                  float* xy_new, const double* state, const float* sx, const float* sy, float xl,
                                  float yl, float xh, float yh, int num_nodes, int num_movable, int num_filler,
-                                 dp_stream_t stream) {
+                                 const int* inv_order, float* xy_order, dp_stream_t stream) {
   DP_REQUIRE(v && g && u && u_new && v_new && state && sx && sy, "dp_nesterov_trial: null pointer");
-  DP_REQUIRE(((uintptr_t)xy_new & 7) == 0, "dp_nesterov_trial: xy_new must be 8-byte aligned");
+  DP_REQUIRE(((uintptr_t)xy_new & 7) == 0 && ((uintptr_t)xy_order & 7) == 0,
+             "dp_nesterov_trial: xy_new / xy_order must be 8-byte aligned");
+  DP_REQUIRE(!xy_order || inv_order, "dp_nesterov_trial: xy_order needs inv_order");
   if (num_nodes == 0) return DP_OK;
   nesterov_trial_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
       v, g, u, u_new, v_new, reinterpret_cast<float2*>(xy_new), state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable,
-      num_filler);
+      num_filler, inv_order, reinterpret_cast<float2*>(xy_order));
   return check_launch("dp_nesterov_trial");
 }
 
@@ -492,18 +497,29 @@ extern "C" int dp_nesterov_advance(double* state, dp_stream_t stream) {
 namespace dpb {
 
 struct SegInfo {
-  int end;   // last lane of this lane's net within the warp
-  int head;  // first lane of this lane's net within the warp
+  int end;      // last lane of this lane's net within the warp
+  int head;     // first lane of this lane's net within the warp
+  int longest;  // pins of the largest net in the warp (uniform)
 };
 
-template <typename Op>
-__device__ __forceinline__ float seg_reduce(float v, const SegInfo& sg, int lane, Op op) {
+// Tree reduction over the lanes of each net, towards its head lane; only as
+// many halving steps as the largest net of the warp needs (a chunk of ~3-pin
+// nets takes 2-3 steps instead of 5), then the head's value is broadcast.
+// N values go together: the N shuffles of a step are independent, so their
+// latencies overlap.
+template <int N, typename Op>
+__device__ __forceinline__ void seg_reduce_n(float (&v)[N], const SegInfo& sg, int lane, Op op) {
+  for (int o = 1; o < sg.longest; o <<= 1) {
+    float u[N];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    float u = __shfl_down_sync(0xffffffffu, v, o);
-    if (lane + o <= sg.end) v = op(v, u);
+    for (int i = 0; i < N; ++i) u[i] = __shfl_down_sync(0xffffffffu, v[i], o);
+    if (lane + o <= sg.end) {
+#pragma unroll
+      for (int i = 0; i < N; ++i) v[i] = op(v[i], u[i]);
+    }
   }
-  return __shfl_sync(0xffffffffu, v, sg.head);  // the head lane holds its whole net
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, v[i], sg.head);
 }
 
 struct MaxOp { __device__ float operator()(float a, float b) const { return fmaxf(a, b); } };
@@ -525,6 +541,8 @@ __device__ __forceinline__ SegInfo segment_of(int net, int lane) {
   SegInfo sg;
   sg.head = __ffs(same) - 1;
   sg.end = 31 - __clz(same);
+  // lanes past the chunk (net == INT_MAX) never need their values reduced
+  sg.longest = (int)__reduce_max_sync(0xffffffffu, net == INT_MAX ? 1u : (unsigned)(sg.end - sg.head + 1));
   return sg;
 }
 
@@ -561,10 +579,10 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
       }
       const SegInfo sg = segment_of(net, lane);
       const bool on = valid && net_mask[net];
-      const float x_max = seg_reduce(valid ? xx : -FLT_MAX, sg, lane, MaxOp());
-      const float x_min = seg_reduce(valid ? xx : FLT_MAX, sg, lane, MinOp());
-      const float y_max = seg_reduce(valid ? yy : -FLT_MAX, sg, lane, MaxOp());
-      const float y_min = seg_reduce(valid ? yy : FLT_MAX, sg, lane, MinOp());
+      // max and min in one pass: min(x) = -max(-x) exactly
+      float ext[4] = {valid ? xx : -FLT_MAX, valid ? -xx : -FLT_MAX, valid ? yy : -FLT_MAX, valid ? -yy : -FLT_MAX};
+      seg_reduce_n<4>(ext, sg, lane, MaxOp());
+      const float x_max = ext[0], x_min = -ext[1], y_max = ext[2], y_min = -ext[3];
       if (kGrad && hpwl_partials && valid && lane == sg.head && hpwl_mask[net]) {
         float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
         if (net_weights) h = fmul(h, net_weights[net]);
@@ -585,14 +603,10 @@ __global__ void __launch_bounds__(256) wa_chunk_kernel(
         ey = expf(fmul(fsub(yy, y_max), inv_gamma));
         eny = expf(fmul(fsub(y_min, yy), inv_gamma));
       }
-      const float e_p = seg_reduce(ex, sg, lane, AddOp());
-      const float e_n = seg_reduce(enx, sg, lane, AddOp());
-      const float xe_p = seg_reduce(fmul(xx, ex), sg, lane, AddOp());
-      const float xe_n = seg_reduce(fmul(xx, enx), sg, lane, AddOp());
-      const float f_p = seg_reduce(ey, sg, lane, AddOp());
-      const float f_n = seg_reduce(eny, sg, lane, AddOp());
-      const float ye_p = seg_reduce(fmul(yy, ey), sg, lane, AddOp());
-      const float ye_n = seg_reduce(fmul(yy, eny), sg, lane, AddOp());
+      float sums[8] = {ex, enx, fmul(xx, ex), fmul(xx, enx), ey, eny, fmul(yy, ey), fmul(yy, eny)};
+      seg_reduce_n<8>(sums, sg, lane, AddOp());
+      const float e_p = sums[0], e_n = sums[1], xe_p = sums[2], xe_n = sums[3];
+      const float f_p = sums[4], f_n = sums[5], ye_p = sums[6], ye_n = sums[7];
       if (!valid) continue;
       float gxv = 0.f, gyv = 0.f;
       if (on) {

@@ -32,6 +32,8 @@ NESTEROV_STATE = 8
 REDUCE_DOUBLES = 1280
 # metric slots
 M_HPWL, M_OVF, M_MAXD, M_ACCEPT, M_ALPHA, M_OBJ, M_WL, M_ENERGY = range(8)
+# pieces of one Nesterov trial, in launch order
+PIECES = ("nesterov_trial", "wa_forward", "density_scatter", "poisson_gemms", "field_gather", "assemble_precondition")
 
 
 class GPEngine(object):
@@ -75,6 +77,12 @@ class GPEngine(object):
         # interleaved (x, y) copies of V[0], V[1] for the gather kernels
         self.XY = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
         self._xy_of = {self.V[0].data_ptr(): self.XY[0], self.V[1].data_ptr(): self.XY[1]}
+        # the same positions for the scattered cells, in visiting order (written
+        # by the trial kernel; gathered after a pack or a re-sort)
+        ns = d.num_movable_nodes + d.num_filler_nodes
+        self.XYO = [torch.empty(2 * ns, dtype=torch.float32, device=dev),
+                    torch.empty(2 * ns, dtype=torch.float32, device=dev)]
+        self._xyo_of = {self.V[0].data_ptr(): self.XYO[0], self.V[1].data_ptr(): self.XYO[1]}
         self.tmp = torch.empty_like(pos.data)
         f64 = dict(dtype=torch.float64, device=dev)
         # optimizer scalars + fixed-order reduction scratch (include/dreamplace_b200.h)
@@ -115,6 +123,19 @@ class GPEngine(object):
         self.force_o = torch.empty(2 * count, dtype=torch.float32, device=dev)
         self._build_records()
         self.sort_interval = int(getattr(params, "sort_interval", 50))
+        # how the trial point reaches the visiting-order copy: "gather" (a
+        # gather kernel after the trial) or "trial" (scattered writes in it)
+        self.xyo_mode = getattr(params, "xyo_mode", "gather")
+        # optional per-piece device timing of the trial (CUDA events recorded
+        # inside the captured graph); piece_query selects the pieces whose
+        # durations are accumulated after each trial
+        self.piece_events = None
+        self.piece_query = set(PIECES)
+        self.piece_ms = {k: 0.0 for k in PIECES}
+        self.piece_n = {k: 0 for k in PIECES}
+        if getattr(params, "time_pieces", False):
+            self.piece_events = {k: (torch.cuda.Event(enable_timing=True, external=True),
+                                     torch.cuda.Event(enable_timing=True, external=True)) for k in PIECES}
         self.iterations = 0
         self.parity = 0
         self.graphs = {}
@@ -135,7 +156,7 @@ class GPEngine(object):
     def _density(self, v, num_filler, out):
         ep = self.ep
         count = ep.num_movable_nodes + (num_filler if num_filler else 0)
-        C.density_map_ordered_into(self.xy(v), self.order, self.rec4, self.ratio_o, count,
+        C.density_map_ordered_into(self.xyo(v), self.rec4, self.ratio_o, count,
                                    ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl), float(ep.xh),
                                    float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y), ep.num_bins_x,
                                    ep.num_bins_y, int(self.det), self.scratch, out)
@@ -161,13 +182,19 @@ class GPEngine(object):
                 of = torch.sort(key[n - nf:]).indices.to(torch.int32).add_(n - nf)
                 self.order[nm:].copy_(of)
             self._build_records()
+            C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
 
     def xy(self, v):
         return self._xy_of[v.data_ptr()]
 
+    def xyo(self, v):
+        return self._xyo_of[v.data_ptr()]
+
     def pack(self, v):
-        """Refresh the interleaved copy of a position buffer written outside the trial kernel."""
+        """Refresh the interleaved and the visiting-order copies of a position buffer
+        written outside the trial kernel."""
         C.pack_xy(v, self.xy(v))
+        C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
 
     def wirelength(self, v, hpwl_out=None):
         """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
@@ -188,7 +215,7 @@ class GPEngine(object):
         """One scatter of v: the movable-only map (self.omap) and the movable +
         filler map (self.dmap); (overflow, max density) of v into ovf_out."""
         ep = self.ep
-        C.density_map_ordered_split(self.xy(v), self.order, self.rec4, self.ratio_o, ep.num_movable_nodes,
+        C.density_map_ordered_split(self.xyo(v), self.rec4, self.ratio_o, ep.num_movable_nodes,
                                     self.order.numel(), ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
                                     float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
                                     ep.num_bins_x, ep.num_bins_y, int(self.det), self.scratch, self.omap.view(-1),
@@ -208,7 +235,7 @@ class GPEngine(object):
     def field_force(self, v, ex, ey):
         """Field force of every movable and filler cell, in visiting order (self.force_o)."""
         ep = self.ep
-        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xy(v), self.order, self.rec4,
+        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xyo(v), self.rec4,
                                  self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
                                  float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
 
@@ -255,13 +282,44 @@ class GPEngine(object):
         sum, the preconditioner and the norms (one pass over the nodes).  The
         HPWL and overflow of v_new land in the parity-q_new metric buffers."""
         m, ep, d = self.model, self.ep, self.design
+        self._mark("wa_forward", 0)
         self.wirelength(v_new, self.H[q_new])
-        ex, ey, energy = self.density_energy(v_new, self.O[q_new])
+        self._mark("wa_forward", 1)
+        self._mark("density_scatter", 0)
+        self.scatter_maps(v_new, self.O[q_new])
+        self._mark("density_scatter", 1)
+        self._mark("poisson_gemms", 0)
+        self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
+        ex, ey, energy = poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
+        self._mark("poisson_gemms", 1)
         C.objective_finish(self.wl64, energy, m.density_weight, self.factor_quad, self.obj64, self.grad_scale)
+        self._mark("field_gather", 0)
         self.field_force(v_new, ex, ey)
+        self._mark("field_gather", 1)
+        self._mark("assemble_precondition", 0)
         self.assemble(v, g, v_new, g_new)
+        self._mark("assemble_precondition", 1)
         self.last_energy = energy
         return energy
+
+    def _mark(self, piece, which):
+        if self.piece_events is not None:
+            self.piece_events[piece][which].record()
+
+    def _collect_pieces(self):
+        for k in self.piece_query:
+            a, b = self.piece_events[k]
+            self.piece_ms[k] += a.elapsed_time(b)
+            self.piece_n[k] += 1
+
+    def reset_piece_times(self, query=None):
+        self.piece_query = set(PIECES) if query is None else set(query)
+        self.piece_ms = {k: 0.0 for k in PIECES}
+        self.piece_n = {k: 0 for k in PIECES}
+
+    def piece_means(self):
+        """Mean device ms per trial of each timed piece."""
+        return {k: self.piece_ms[k] / self.piece_n[k] for k in PIECES if self.piece_n[k]}
 
     def evaluate(self, q):
         """HPWL and (overflow, max density) of V[q] into the parity-q metric buffers,
@@ -340,8 +398,14 @@ class GPEngine(object):
         d = self.design
         v, g, u = self.V[p], self.G[p], self.U[p]
         vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
-        C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y, float(d.xl),
-                         float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+        self._mark("nesterov_trial", 0)
+        scatter_write = self.xyo_mode == "trial"
+        C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y,
+                         float(d.xl), float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes,
+                         self.inv_order if scatter_write else None, self.XYO[1 - p] if scatter_write else None)
+        if not scatter_write:
+            C.gather_order_xy(self.XY[1 - p], self.order, self.order.numel(), self.XYO[1 - p])
+        self._mark("nesterov_trial", 1)
         energy = self.objective_and_step(v, g, vn, gn, 1 - p)
         # HPWL / overflow of v_k (computed when v_k was the trial point), then the trial's scalars
         torch.cat([self.H[p][0:1], self.O[p][0:2], self.state[NS_ACCEPT:NS_ACCEPT + 1],
@@ -352,7 +416,7 @@ class GPEngine(object):
         d = self.design
         C.nesterov_trial(self.V[p], self.G[p], self.U[p], self.U[1 - p], self.V[1 - p], self.XY[1 - p], self.state,
                          self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
-                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
+                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes, self.inv_order, self.XYO[1 - p])
 
     def _body(self, p):
         # v_k was clamped into the die when it was produced (trial kernel, or
@@ -407,6 +471,8 @@ class GPEngine(object):
             self.kernels_launched += C.launch_count() - before
         self.metrics_host.copy_(self.metrics, non_blocking=True)
         torch.cuda.current_stream().synchronize()
+        if self.piece_events is not None:
+            self._collect_pieces()
         return self.metrics_host.numpy().copy()
 
     def _check_graph_key(self):

@@ -120,14 +120,19 @@ int dp_build_cell_records(const float* node_size_x_clamped, const float* node_si
                           const int* order, int count, float* rec4, float* ratio_o, int* inv_order,
                           dp_stream_t stream);
 
-/* Order-driven triangle scatter of the cells order[0..count) onto
- * initial_density_map (NULL = zeros), positions interleaved in xy.  Same
+/* Positions in visiting order: xy_o[2*idx..2*idx+1] = xy[2*order[idx]..] for
+ * idx < count (interleaved xy as dp_pack_xy writes it). */
+int dp_gather_order_xy(const float* xy, const int* order, int count, float* xy_o, dp_stream_t stream);
+
+/* Order-driven triangle scatter of the cells 0..count of a visiting order onto
+ * initial_density_map (NULL = zeros); positions (xy_o, interleaved) and
+ * records (rec4, ratio_o) are both stored in that order.  Same
  * arithmetic as dp_density_map_f32 / _fx64.  Blocks of consecutive cells
  * accumulate in registers (bin box <= 16 bins) or a shared-memory tile over
  * their bin box before touching global memory, so a spatial order turns most
  * global atomics into local ones.  deterministic != 0: int64 fixed point
  * (scratch_fixed [num_bins] required). */
-int dp_density_map_ordered(const float* xy, const int* order, const float* rec4, const float* ratio_o,
+int dp_density_map_ordered(const float* xy_o, const float* rec4, const float* ratio_o,
                            int count, const float* initial_density_map,
                            float xl, float yl, float xh, float yh,
                            float bin_size_x, float bin_size_y,
@@ -142,8 +147,7 @@ int dp_density_map_ordered(const float* xy, const int* order, const float* rec4,
  * scattered once.  Deterministic: both maps bit-exact with separate scatters.
  * overflow_out (optional, DP_REDUCE_DOUBLES doubles): dp_density_overflow of
  * out_first with target_area and bin_area, computed in the same pass. */
-int dp_density_map_ordered_split(const float* xy, const int* order, const float* rec4, const float* ratio_o,
-                                 int num_first, int count, const float* initial_density_map,
+int dp_density_map_ordered_split(const float* xy_o, const float* rec4, const float* ratio_o, int num_first, int count, const float* initial_density_map,
                                  float xl, float yl, float xh, float yh,
                                  float bin_size_x, float bin_size_y,
                                  float inv_bin_size_x, float inv_bin_size_y,
@@ -206,12 +210,12 @@ int dp_electric_force(const float* grad_pos, int num_bins_x, int num_bins_y,
                       const int* sorted_node_map, float scale,
                       float* grad_out, dp_stream_t stream);
 
-/* Field gather of the cells order[0..count) (records as dp_build_cell_records,
- * positions interleaved in xy); force_o[2*idx..2*idx+1] = scale * grad_pos[0] *
+/* Field gather of the cells 0..count of a visiting order (records as
+ * dp_build_cell_records, positions in the same order in xy_o); force_o[2*idx..2*idx+1] = scale * grad_pos[0] *
  * ratio * sum(px py E), in the CPU op's per-cell order without contraction. */
 int dp_electric_force_ordered(const float* grad_pos, int num_bins_x, int num_bins_y,
-                              const float* field_map_x, const float* field_map_y, const float* xy,
-                              const int* order, const float* rec4, const float* ratio_o, int count,
+                              const float* field_map_x, const float* field_map_y, const float* xy_o,
+                              const float* rec4, const float* ratio_o, int count,
                               float xl, float yl, float bin_size_x, float bin_size_y,
                               float inv_bin_size_x, float inv_bin_size_y, float scale, float* force_o,
                               dp_stream_t stream);
@@ -346,7 +350,8 @@ int dp_nesterov_init(double* state, double alpha, dp_stream_t stream);
 int dp_nesterov_trial(const float* v, const float* g, const float* u, float* u_new, float* v_new,
                       float* xy_new, const double* state, const float* node_size_x,
                       const float* node_size_y, float xl, float yl, float xh, float yh, int num_nodes,
-                      int num_movable, int num_filler, dp_stream_t stream);
+                      int num_movable, int num_filler, const int* inv_order, float* xy_order,
+                      dp_stream_t stream);
 /* xy[2i], xy[2i+1] = pos[i], pos[num_nodes + i] */
 int dp_pack_xy(const float* pos, int num_nodes, float* xy, dp_stream_t stream);
 /* g' /= max(1, pws + lambda*area) (dreamplace/PlaceObj.py:69-103), then

@@ -304,6 +304,13 @@ def pack_xy(pos, n):
     return dev(np.stack([pos[:n], pos[n:]], axis=1).reshape(-1).astype(np.float32))
 
 
+def order_xy(C, xy, order):
+    """Positions in visiting order (what the trial kernel maintains)."""
+    out = torch.empty(2 * len(order), device="cuda")
+    C.gather_order_xy(xy, dev(order), len(order), out)
+    return out
+
+
 def records(C, d, order):
     sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
     rec4 = torch.empty(4 * len(order), device="cuda")
@@ -339,11 +346,11 @@ def test_ordered_tiled_scatter(C, layout):
         rec4, ratio_o, _ = records(C, d, order)
         out = torch.empty(d.num_bins_x * d.num_bins_y, device="cuda")
         scratch = torch.empty(d.num_bins_x * d.num_bins_y, dtype=torch.int64, device="cuda")
-        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
+        C.density_map_ordered_into(order_xy(C, xy, order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
                                    d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y, 1, scratch, out)
         assert np.array_equal(scratch.cpu().numpy(), ref_fx)
         assert np.array_equal(out.cpu().numpy(), ref_map)
-        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
+        C.density_map_ordered_into(order_xy(C, xy, order), rec4, ratio_o, len(order), None, d.xl, d.yl, d.xh, d.yh,
                                    d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y, 0, None, out)
         np.testing.assert_allclose(out.cpu().numpy(), f32_map, rtol=1e-4, atol=1e-4 * float(np.max(f32_map)))
 
@@ -364,7 +371,7 @@ def test_ordered_force_and_fused_assembly(C, golden):
     grad = torch.ones(1, device="cuda")
     force_o = torch.empty(2 * len(order), device="cuda")
     fx, fy = dev(g["field_x"]).view(-1), dev(g["field_y"]).view(-1)
-    C.electric_force_ordered(grad, fx, fy, xy, dev(order), rec4, ratio_o, len(order), d.xl, d.yl, d.bin_size_x,
+    C.electric_force_ordered(grad, fx, fy, order_xy(C, xy, order), rec4, ratio_o, len(order), d.xl, d.yl, d.bin_size_x,
                              d.bin_size_y, d.num_bins_x, d.num_bins_y, -1.0, force_o)
     fo = force_o.cpu().numpy().reshape(-1, 2)
     assert np.array_equal(fo[:, 0], g["force"][order])
@@ -416,12 +423,12 @@ def test_ordered_split_scatter(C):
         first, full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
         ovf = torch.zeros(1280, dtype=torch.float64, device="cuda")
         ba = d.bin_size_x * d.bin_size_y
-        C.density_map_ordered_split(xy, dev(order), rec4, ratio_o, m, len(order), init, *geo, det,
+        C.density_map_ordered_split(order_xy(C, xy, order), rec4, ratio_o, m, len(order), init, *geo, det,
                                     scratch if det else None, first, full, 0.9 * ba, ba, ovf)
         exp_first, exp_full = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
-        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, m, init, *geo, det, scratch if det else None,
+        C.density_map_ordered_into(order_xy(C, xy, order), rec4, ratio_o, m, init, *geo, det, scratch if det else None,
                                    exp_first)
-        C.density_map_ordered_into(xy, dev(order), rec4, ratio_o, len(order), init, *geo, det,
+        C.density_map_ordered_into(order_xy(C, xy, order), rec4, ratio_o, len(order), init, *geo, det,
                                    scratch if det else None, exp_full)
         exp_ovf = torch.zeros(1280, dtype=torch.float64, device="cuda")
         C.density_overflow_into(first, 0.9 * ba, ba, exp_ovf)
