@@ -64,6 +64,15 @@ __device__ __forceinline__ void spectral_weights(const EpiParams& p, int u, int 
   wy = __fmul_rn(__fmul_rn(wv, inv), 0.5f);
 }
 
+// Energy term of one spectral coefficient a = v at (u, v_idx):
+//   sum_xy rho * IDCT2(a * winv) = M N sum_uv w_u w_v winv_uv a_uv^2,
+// w_0 = 1/2, w_k = 1 otherwise (the DCT-II / DCT-III pair of the transforms),
+// so the potential map is never formed.
+__device__ __forceinline__ double spectral_energy(const EpiParams& p, int u, int vi, float a, float winv) {
+  const double w = (u == 0 ? 0.5 : 1.0) * (vi == 0 ? 0.5 : 1.0);
+  return (double)p.M * (double)p.N * w * (double)winv * (double)a * (double)a;
+}
+
 // Applies the epilogue to one element.  Returns the contribution to the
 // energy dot product (ENERGY) or 0.
 __device__ __forceinline__ double epi_apply(const EpiParams& p, int m, int n, float acc) {
@@ -90,7 +99,7 @@ __device__ __forceinline__ double epi_apply(const EpiParams& p, int m, int n, fl
       store_operand(p.fmt, __fmul_rn(v, wy), idx, p.sp_f32[1], p.sp_hi[1], p.sp_lo[1]);
       if (p.sp_f32[2] || p.sp_hi[2])
         store_operand(p.fmt, __fmul_rn(v, winv), idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
-      return 0.0;
+      return p.energy ? spectral_energy(p, m, n, v, winv) : 0.0;
     }
     case DP_EPI_ENERGY: {
       size_t idx = (size_t)m * p.ldc + n;
@@ -220,7 +229,12 @@ __device__ __forceinline__ double epi_row8(const EpiParams& p, int m, int n0, co
         for (int j = 0; j < 8; ++j) o[j] = __fmul_rn(v[j], wi[j]);
         store_operand8(p.fmt, o, idx, p.sp_f32[2], p.sp_hi[2], p.sp_lo[2]);
       }
-      return 0.0;
+      double e = 0.0;
+      if (p.energy) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) e += spectral_energy(p, m, n0 + j, v[j], wi[j]);
+      }
+      return e;
     }
     case DP_EPI_ENERGY: {
       float r[8];

@@ -1,7 +1,7 @@
 // tcgen05 tensor-core GEMMs for the Poisson solve (TF32, BF16, split-BF16).
 //
 // C[m,n] = sum_k A[m,k] * B[n,k], A and B K-contiguous in global memory.
-// One CTA computes a 128 x BN tile: TMA (128-byte swizzle, no multicast)
+// One CTA computes a 128 x BN tile (BN = 64 or 128): TMA (128-byte swizzle, no multicast)
 // stages A and B k-blocks into a STAGES-deep shared-memory ring, one thread
 // issues tcgen05.mma (M=128, N=BN) into a TMEM accumulator, and all four
 // warps read the accumulator back with tcgen05.ld for the fused epilogue
@@ -11,14 +11,13 @@
 // Split-BF16 stages A_hi, A_lo, B_hi and B_lo of one k-block together and
 // issues A_hi*B_hi, A_hi*B_lo and A_lo*B_hi on them into the same accumulator
 // (the lo*lo term is below fp32 rounding), so every operand tile crosses L2
-// once per k-block instead of once per product.  The 128 x 128 tile halves
-// the L2 -> SM traffic per output element of a 128 x 64 tile; the transforms
-// are bound by that traffic, not by the tensor pipe.
+// once per k-block instead of once per product.
 //
 // Every wait on an mbarrier is bounded by a clock budget; on expiry the
 // kernel records an error code in g_tc_status, drains what it issued and
 // returns, so a broken launch reports instead of hanging the GPU.
 #include <cuda.h>
+#include <cstdlib>
 #include "epilogue.cuh"
 
 namespace dpb {
@@ -289,7 +288,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       }
     }
   }
-  if (P.kind == DP_EPI_ENERGY) {
+  if (P.energy) {  // ENERGY, or SPECTRAL with the spectral-domain energy
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
     if (lane == 0 && e != 0.0) atomicAdd(P.energy, e);
   }
@@ -366,16 +365,34 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
   return check_launch("dp_transform_gemm(tcgen05)");
 }
 
+// Output tile width: a single transform runs 128 x 64 tiles (at 1024 x 1024
+// that is 128 CTAs, where 128 x 128 tiles leave 84 of the 148 SMs idle); a
+// batch of three runs 128 x 128 tiles (192 CTAs in two waves beat 384 in
+// three).  DP_TC_TILE_N=64 or 128 forces one width.
+static int tile_n(int count) {
+  static int forced = [] {
+    const char* e = getenv("DP_TC_TILE_N");
+    return e ? atoi(e) : 0;
+  }();
+  if (forced == 64 || forced == 128) return forced;
+  return count == 1 ? 64 : 128;
+}
+
 int launch_tc_gemm(int precision, int M, int N, int K, const dp_gemm_problem* probs, int count, cudaStream_t s) {
+  const bool wide = tile_n(count) == 128;
   switch (precision) {
-    // 128 x 128 tiles, one CTA per SM: a 6-deep TMA ring of 32 KB stages, or
-    // 3 stages of 64 KB (hi and lo of both operands) for split-BF16.
+    // one CTA per SM; the TMA ring fills ~192 KB of shared memory: 32 KB or
+    // 24 KB stages, or 64 KB / 48 KB stages holding the hi and lo planes of
+    // both operands for split-BF16
     case DP_PREC_TF32:
-      return run_tc<DP_PREC_TF32, 128, 6>(M, N, K, probs, count, s);
+      return wide ? run_tc<DP_PREC_TF32, 128, 6>(M, N, K, probs, count, s)
+                  : run_tc<DP_PREC_TF32, 64, 8>(M, N, K, probs, count, s);
     case DP_PREC_BF16:
-      return run_tc<DP_PREC_BF16, 128, 6>(M, N, K, probs, count, s);
+      return wide ? run_tc<DP_PREC_BF16, 128, 6>(M, N, K, probs, count, s)
+                  : run_tc<DP_PREC_BF16, 64, 8>(M, N, K, probs, count, s);
     case DP_PREC_SPLIT_BF16:
-      return run_tc<DP_PREC_SPLIT_BF16, 128, 3>(M, N, K, probs, count, s);
+      return wide ? run_tc<DP_PREC_SPLIT_BF16, 128, 3>(M, N, K, probs, count, s)
+                  : run_tc<DP_PREC_SPLIT_BF16, 64, 4>(M, N, K, probs, count, s);
   }
   set_error("dp_transform_gemm: unsupported precision %d", precision);
   return DP_ERR_UNSUPPORTED;

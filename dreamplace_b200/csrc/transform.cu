@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) simt_gemm_kernel(SimtBatch batch, int M, 
       if (n < N) e += epi_apply(P.epi, m, n, acc[i][j]);
     }
   }
-  if (P.epi.kind == DP_EPI_ENERGY) {
+  if (P.epi.energy) {  // ENERGY, or SPECTRAL with the spectral-domain energy
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
     __shared__ double red[8];
     if ((tid & 31) == 0) red[tid >> 5] = e;

@@ -14,9 +14,11 @@ Forward (reference electric_potential.py:52-217):
   a = DCT2(rho);  Ex = IDXST_IDCT(a wu/(wu^2+wv^2)/2);  Ey = IDCT_IDXST(a wv/(...)/2)
   energy = sum(IDCT2(a/(wu^2+wv^2)) * rho)                unless fast_mode
 as four GEMM launches: rho C_N^T (transposed bf16/fp32 operand out), C_M T with
-the spectral weights in the epilogue, the three right products batched in one
-launch, and the three left products batched with Ex/Ey stores and the energy
-dot product fused (the potential map is never written).
+the spectral weights in the epilogue, the two right products batched in one
+launch, and the two left products batched with the Ex/Ey stores.  The energy
+is summed in the spectral domain by the second launch's epilogue,
+  sum_xy rho IDCT2(a winv) = M N sum_uv w_u w_v winv_uv a_uv^2 (w_0 = 1/2),
+so the potential map is never formed.
 Backward: the hand-written adjoint ``-electric_force`` (reference :219-275).
 """
 import logging
@@ -65,11 +67,16 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
     cN.as_b(g1)
     t1.as_out_t(g1)
     C.transform_gemm(prec, M, N, N, [g1])
-    # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy, a*winv  [M, N]
-    spec = [Operand((M, N), prec, dev) for _ in range(2 if fast_mode else 3)]
+    # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy  [M, N]; the energy
+    # sum(rho * IDCT2(a*winv)) = MN sum w_u w_v winv a^2 is summed in the same
+    # epilogue, so the potential map is never formed
+    energy = torch.zeros(1, dtype=torch.float64, device=dev)
+    spec = [Operand((M, N), prec, dev) for _ in range(2)]
     g2 = dict(lda=M, ldb=M, epilogue=EPI_SPECTRAL, alpha=4.0 / (M * N), ldc=N,
               wv_scale=float(bin_size_x / bin_size_y),
               spec_weights=spectral_tables(M, N, float(bin_size_x / bin_size_y), dev))
+    if not fast_mode:
+        g2["energy"] = energy
     cM.as_a(g2)
     t1.as_b(g2)
     for i, s in enumerate(spec):
@@ -79,8 +86,8 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
             g2["sp%d_hi" % i] = s.hi
             g2["sp%d_lo" % i] = s.lo
     C.transform_gemm(prec, M, N, M, [g2])
-    # G3: U^T = (A R^T)^T for the x field (R = Ch_N), y field (Sh_N) and potential (Ch_N)
-    rights = [chN, shN, chN][:len(spec)]
+    # G3: U^T = (A R^T)^T for the x field (R = Ch_N) and the y field (Sh_N)
+    rights = [chN, shN]
     us = [Operand((N, M), prec, dev) for _ in spec]
     g3 = []
     for s, r, u in zip(spec, rights, us):
@@ -90,15 +97,11 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
         u.as_out_t(d)
         g3.append(d)
     C.transform_gemm(prec, M, N, N, g3)
-    # G4: Ex = 4 Sh_M Ux, Ey = 4 Ch_M Uy, energy = sum(4 Ch_M Uphi * rho)
+    # G4: Ex = 4 Sh_M Ux, Ey = 4 Ch_M Uy
     ex = torch.empty(M, N, dtype=torch.float32, device=dev)
     ey = torch.empty(M, N, dtype=torch.float32, device=dev)
-    energy = torch.zeros(1, dtype=torch.float64, device=dev)
     g4 = [shM.as_a(us[0].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ex))),
           chM.as_a(us[1].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ey)))]
-    if not fast_mode:
-        g4.append(chM.as_a(us[2].as_b(dict(lda=M, ldb=M, epilogue=EPI_ENERGY, alpha=4.0, ldc=N, rho=rho,
-                                           energy=energy))))
     C.transform_gemm(prec, M, N, M, g4)
     return ex, ey, energy
 

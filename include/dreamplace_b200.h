@@ -229,7 +229,9 @@ int dp_electric_force_ordered(const float* grad_pos, int num_bins_x, int num_bin
 enum {
   DP_EPI_STORE = 0,      /* out_f32[m*ldc+n] = alpha*C                                  */
   DP_EPI_STORE_T = 1,    /* C^T as the next GEMM's operand: out_hi/out_lo (or out_f32) at [n*ldc+m], times alpha */
-  DP_EPI_SPECTRAL = 2,   /* a=alpha*C -> three row-major operands: a*wu/(wu^2+wv^2)/2, a*wv/(...)/2, a/(...) */
+  DP_EPI_SPECTRAL = 2,   /* a=alpha*C -> row-major operands a*wu/(wu^2+wv^2)/2, a*wv/(...)/2 and (optional) a/(...);
+                            with energy_f64: += M N sum w_u w_v a^2/(wu^2+wv^2), w_0 = 1/2 (the potential energy,
+                            sum rho * IDCT2(a/(...)), without forming the potential) */
   DP_EPI_ENERGY = 3      /* energy_f64 += sum alpha*C[m,n]*rho[m*ldc+n]; optional out_f32 store */
 };
 
@@ -246,7 +248,7 @@ typedef struct dp_gemm_problem {
   const float* spec_weights; /* SPECTRAL, optional: [3*M*N] tables wx | wy | winv from
                                 dp_spectral_weights (same values, no per-element divide) */
   const float* rho;     /* ENERGY */
-  double* energy_f64;   /* ENERGY accumulator (caller zeroes it) */
+  double* energy_f64;   /* ENERGY / SPECTRAL energy accumulator (caller zeroes it) */
 } dp_gemm_problem;
 
 int dp_transform_gemm(int precision, int M, int N, int K,
