@@ -553,6 +553,54 @@ void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::
                         cur_stream()));
 }
 
+std::vector<at::Tensor> plan_net_lanes(at::Tensor netpin_start_cpu) {
+  TORCH_CHECK(!netpin_start_cpu.is_cuda() && netpin_start_cpu.scalar_type() == at::kInt,
+              "netpin_start must be int32 on CPU");
+  auto ns = netpin_start_cpu.contiguous();
+  const int num_nets = ns.numel() - 1;
+  int groups = 0, slots = 0;
+  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, &groups, &slots, nullptr, nullptr, nullptr, nullptr));
+  auto opt = ns.options();
+  auto deg = at::empty({groups}, opt), base = at::empty({groups}, opt);
+  auto net = at::empty({32 * (int64_t)groups}, opt), slot = at::empty({slots}, opt);
+  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, &groups, &slots, deg.data_ptr<int>(), base.data_ptr<int>(),
+                            net.data_ptr<int>(), slot.data_ptr<int>()));
+  return {deg, base, net, slot};
+}
+
+void wa_lanes_forward(at::Tensor xy, at::Tensor group_deg, at::Tensor group_base, at::Tensor group_net,
+                      at::Tensor ln_node, at::Tensor ln_offx, at::Tensor ln_offy, at::Tensor ln_csr,
+                      c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor inv_gamma,
+                      at::Tensor wl_f64, at::Tensor grad_node_order, c10::optional<at::Tensor> hpwl_mask,
+                      c10::optional<at::Tensor> hpwl_f64) {
+  CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(group_deg); CHECK_I32(group_base); CHECK_I32(group_net);
+  CHECK_I32(ln_node); CHECK_I32(ln_csr); CHECK_F32(grad_node_order);
+  TORCH_CHECK(group_net.numel() == 32 * group_deg.numel() && group_base.numel() == group_deg.numel(),
+              "wa_lanes_forward: inconsistent plan");
+  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
+  TORCH_CHECK(!hpwl_f64.has_value() || (hpwl_mask.has_value() && hpwl_f64->scalar_type() == at::kDouble &&
+                                        hpwl_f64->numel() >= DP_REDUCE_DOUBLES),
+              "hpwl_f64 needs hpwl_mask and DP_REDUCE_DOUBLES doubles");
+  DP_CALL(dp_wa_lanes_forward(ptr<float>(xy), ptr<int>(group_deg), ptr<int>(group_base), ptr<int>(group_net),
+                              group_deg.numel(), ptr<int>(ln_node), ptr<float>(ln_offx), ptr<float>(ln_offy),
+                              ptr<int>(ln_csr), (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
+                              ptr<float>(inv_gamma), ptr<double>(wl_f64), ptr<float>(grad_node_order),
+                              hpwl_mask.has_value() ? hpwl_mask->data_ptr<uint8_t>() : nullptr,
+                              (double*)ovp(hpwl_f64), cur_stream()));
+}
+
+void hpwl_lanes(at::Tensor xy, at::Tensor group_deg, at::Tensor group_base, at::Tensor group_net, at::Tensor ln_node,
+                at::Tensor ln_offx, at::Tensor ln_offy, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
+                at::Tensor out_f64) {
+  CHECK_FLAT(xy); CHECK_I32(group_deg); CHECK_I32(group_base); CHECK_I32(group_net); CHECK_I32(ln_node);
+  TORCH_CHECK(group_net.numel() == 32 * group_deg.numel(), "hpwl_lanes: inconsistent plan");
+  TORCH_CHECK(out_f64.scalar_type() == at::kDouble && out_f64.numel() >= DP_REDUCE_DOUBLES, "out_f64 too small");
+  DP_CALL(dp_hpwl_lanes(ptr<float>(xy), ptr<int>(group_deg), ptr<int>(group_base), ptr<int>(group_net),
+                        group_deg.numel(), ptr<int>(ln_node), ptr<float>(ln_offx), ptr<float>(ln_offy),
+                        (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<double>(out_f64),
+                        cur_stream()));
+}
+
 void node_pin_sum(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor grad_pos, int num_movable,
                   int accumulate, at::Tensor grad_out) {
   CHECK_F32(grad_node_order); CHECK_F32(grad_out); CHECK_I32(node_start);
@@ -602,6 +650,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("assemble_precondition_step", &assemble_precondition_step);
   m.def("plan_net_chunks", &plan_net_chunks);
   m.def("wa_chunk_forward", &wa_chunk_forward);
+  m.def("plan_net_lanes", &plan_net_lanes);
+  m.def("wa_lanes_forward", &wa_lanes_forward);
+  m.def("hpwl_lanes", &hpwl_lanes);
   m.def("hpwl_chunk", &hpwl_chunk);
   m.def("node_pin_sum", &node_pin_sum);
   m.def("electric_force_into", &electric_force_into);

@@ -853,3 +853,350 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
   return check_launch("dp_assemble_precondition_step finish");
 }
+
+// ============================================================== lane-per-net WA / HPWL
+// Nets of degree d <= kLaneDeg are grouped 32 at a time by degree (host
+// planner dp_plan_net_lanes); one warp takes a group, one lane a whole net.
+// The group's pins are stored transposed (pin j of lane l at base + 32 j + l),
+// so every pin load of the warp is one coalesced access.  A lane holds its
+// net's pins in registers and runs the reference's per-net loops in pin order
+// (so the sums are formed in the CPU op's order), and the per-net terms (the
+// fp64 a terms, the divisions) are issued once per 32 nets instead of once
+// per chunk of ~10 nets.  A larger net is a group of its own, handled by the
+// whole warp with strided loops and warp reductions.
+namespace dpb {
+
+constexpr int kLaneDeg = 8;
+
+struct LaneArgs {
+  const float2* xy;
+  const int* group_deg;
+  const int* group_base;
+  const int* group_net;
+  int num_groups;
+  const int* ln_node;
+  const float* ln_offx;
+  const float* ln_offy;
+  const int* ln_csr;
+  const float* net_weights;
+  const unsigned char* net_mask;
+  const unsigned char* hpwl_mask;
+  const float* inv_gamma;  // device scalar (read once per thread)
+  float2* gnode;
+};
+
+// a = (1 - b * xe) / e evaluated as the reference does (the literal 1.0
+// promotes the expression to double), rounded to float
+__device__ __forceinline__ float wa_a_term(float b, float xe, float e) {
+  return (float)((1.0 - (double)fmul(b, xe)) / (double)e);
+}
+
+template <int D, bool kGrad>
+__device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, int lane, int net, bool hpwl,
+                                         double& contrib, double& hcontrib) {
+  float x[D], y[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const int p = base + 32 * j + lane;
+    const float2 q = A.xy[__ldcs(A.ln_node + p)];
+    x[j] = fadd(__ldcs(A.ln_offx + p), q.x);
+    y[j] = fadd(__ldcs(A.ln_offy + p), q.y);
+  }
+  float x_max = x[0], x_min = x[0], y_max = y[0], y_min = y[0];
+#pragma unroll
+  for (int j = 1; j < D; ++j) {
+    x_max = fmaxf(x_max, x[j]);
+    x_min = fminf(x_min, x[j]);
+    y_max = fmaxf(y_max, y[j]);
+    y_min = fminf(y_min, y[j]);
+  }
+  const float w = A.net_weights ? A.net_weights[net] : 1.0f;
+  if (!kGrad) {  // HPWL pass: net_mask is the HPWL mask
+    if (A.net_mask[net]) {
+      float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+      if (A.net_weights) h = fmul(h, w);
+      contrib += (double)h;
+    }
+    return;
+  }
+  if (hpwl && A.hpwl_mask[net]) {
+    float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+    if (A.net_weights) h = fmul(h, w);
+    hcontrib += (double)h;
+  }
+  if (!A.net_mask[net]) {
+#pragma unroll
+    for (int j = 0; j < D; ++j) __stcs(A.gnode + __ldcs(A.ln_csr + base + 32 * j + lane), make_float2(0.f, 0.f));
+    return;
+  }
+  float ex[D], enx[D], ey[D], eny[D];
+  float e_p = 0.f, e_n = 0.f, xe_p = 0.f, xe_n = 0.f, f_p = 0.f, f_n = 0.f, ye_p = 0.f, ye_n = 0.f;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    ex[j] = expf(fmul(fsub(x[j], x_max), ig));
+    enx[j] = expf(fmul(fsub(x_min, x[j]), ig));
+    ey[j] = expf(fmul(fsub(y[j], y_max), ig));
+    eny[j] = expf(fmul(fsub(y_min, y[j]), ig));
+    e_p = fadd(e_p, ex[j]);
+    e_n = fadd(e_n, enx[j]);
+    xe_p = fadd(xe_p, fmul(x[j], ex[j]));
+    xe_n = fadd(xe_n, fmul(x[j], enx[j]));
+    f_p = fadd(f_p, ey[j]);
+    f_n = fadd(f_n, eny[j]);
+    ye_p = fadd(ye_p, fmul(y[j], ey[j]));
+    ye_n = fadd(ye_n, fmul(y[j], eny[j]));
+  }
+  const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                        __fdiv_rn(ye_n, f_n));
+  contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
+  const float b_x = __fdiv_rn(ig, e_p), a_x = wa_a_term(b_x, xe_p, e_p);
+  const float b_nx = __fdiv_rn(-ig, e_n), a_nx = wa_a_term(b_nx, xe_n, e_n);
+  const float b_y = __fdiv_rn(ig, f_p), a_y = wa_a_term(b_y, ye_p, f_p);
+  const float b_ny = __fdiv_rn(-ig, f_n), a_ny = wa_a_term(b_ny, ye_n, f_n);
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    float gx = fsub(fmul(fadd(a_x, fmul(b_x, x[j])), ex[j]), fmul(fadd(a_nx, fmul(b_nx, x[j])), enx[j]));
+    float gy = fsub(fmul(fadd(a_y, fmul(b_y, y[j])), ey[j]), fmul(fadd(a_ny, fmul(b_ny, y[j])), eny[j]));
+    if (A.net_weights) {
+      gx = fmul(gx, w);
+      gy = fmul(gy, w);
+    }
+    __stcs(A.gnode + __ldcs(A.ln_csr + base + 32 * j + lane), make_float2(gx, gy));
+  }
+}
+
+// a net of degree > kLaneDeg: pins base .. base + deg (contiguous), whole warp
+template <bool kGrad>
+__device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lane, int net, bool hpwl,
+                         double& contrib, double& hcontrib) {
+  float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
+  for (int j = lane; j < deg; j += 32) {
+    const float2 q = A.xy[A.ln_node[base + j]];
+    const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+    x_max = fmaxf(x_max, xx);
+    x_min = fminf(x_min, xx);
+    y_max = fmaxf(y_max, yy);
+    y_min = fminf(y_min, yy);
+  }
+  x_max = warp_all(x_max, 0);
+  x_min = warp_all(x_min, 1);
+  y_max = warp_all(y_max, 0);
+  y_min = warp_all(y_min, 1);
+  const float w = A.net_weights ? A.net_weights[net] : 1.0f;
+  if (!kGrad) {
+    if (lane == 0 && A.net_mask[net]) {
+      float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+      if (A.net_weights) h = fmul(h, w);
+      contrib += (double)h;
+    }
+    return;
+  }
+  if (hpwl && lane == 0 && A.hpwl_mask[net]) {
+    float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+    if (A.net_weights) h = fmul(h, w);
+    hcontrib += (double)h;
+  }
+  const bool on = A.net_mask[net];
+  float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
+  if (on) {
+    for (int j = lane; j < deg; j += 32) {
+      const float2 q = A.xy[A.ln_node[base + j]];
+      const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+      const float a1 = expf(fmul(fsub(xx, x_max), ig)), a2 = expf(fmul(fsub(x_min, xx), ig));
+      const float a3 = expf(fmul(fsub(yy, y_max), ig)), a4 = expf(fmul(fsub(y_min, yy), ig));
+      xe_p = fadd(xe_p, fmul(xx, a1));
+      xe_n = fadd(xe_n, fmul(xx, a2));
+      e_p = fadd(e_p, a1);
+      e_n = fadd(e_n, a2);
+      ye_p = fadd(ye_p, fmul(yy, a3));
+      ye_n = fadd(ye_n, fmul(yy, a4));
+      f_p = fadd(f_p, a3);
+      f_n = fadd(f_n, a4);
+    }
+    xe_p = warp_all(xe_p, 2); xe_n = warp_all(xe_n, 2); e_p = warp_all(e_p, 2); e_n = warp_all(e_n, 2);
+    ye_p = warp_all(ye_p, 2); ye_n = warp_all(ye_n, 2); f_p = warp_all(f_p, 2); f_n = warp_all(f_n, 2);
+    if (lane == 0) {
+      const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                            __fdiv_rn(ye_n, f_n));
+      contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
+    }
+  }
+  const float b_x = on ? __fdiv_rn(ig, e_p) : 0.f, a_x = on ? wa_a_term(b_x, xe_p, e_p) : 0.f;
+  const float b_nx = on ? __fdiv_rn(-ig, e_n) : 0.f, a_nx = on ? wa_a_term(b_nx, xe_n, e_n) : 0.f;
+  const float b_y = on ? __fdiv_rn(ig, f_p) : 0.f, a_y = on ? wa_a_term(b_y, ye_p, f_p) : 0.f;
+  const float b_ny = on ? __fdiv_rn(-ig, f_n) : 0.f, a_ny = on ? wa_a_term(b_ny, ye_n, f_n) : 0.f;
+  for (int j = lane; j < deg; j += 32) {
+    float gx = 0.f, gy = 0.f;
+    if (on) {
+      const float2 q = A.xy[A.ln_node[base + j]];
+      const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+      const float a1 = expf(fmul(fsub(xx, x_max), ig)), a2 = expf(fmul(fsub(x_min, xx), ig));
+      const float a3 = expf(fmul(fsub(yy, y_max), ig)), a4 = expf(fmul(fsub(y_min, yy), ig));
+      gx = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
+      gy = fsub(fmul(fadd(a_y, fmul(b_y, yy)), a3), fmul(fadd(a_ny, fmul(b_ny, yy)), a4));
+      if (A.net_weights) {
+        gx = fmul(gx, w);
+        gy = fmul(gy, w);
+      }
+    }
+    A.gnode[A.ln_csr[base + j]] = make_float2(gx, gy);
+  }
+}
+
+template <bool kGrad>
+__global__ void __launch_bounds__(256, 3) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
+                                                      double* __restrict__ hpwl_partials) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool hpwl = kGrad && hpwl_partials != nullptr;
+  const float ig = kGrad ? *A.inv_gamma : 0.f;
+  double contrib = 0.0, hcontrib = 0.0;
+  for (int g = warp; g < A.num_groups; g += nwarps) {
+    const int deg = A.group_deg[g], base = A.group_base[g];
+    if (deg > kLaneDeg) {
+      warp_net<kGrad>(A, ig, base, deg, lane, A.group_net[32 * g], hpwl, contrib, hcontrib);
+      continue;
+    }
+    const int net = A.group_net[32 * g + lane];
+    if (net < 0) continue;  // padding lane of the last group of a degree
+    switch (deg) {
+      case 1: lane_net<1, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 2: lane_net<2, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 3: lane_net<3, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 4: lane_net<4, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 5: lane_net<5, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 6: lane_net<6, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 7: lane_net<7, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 8: lane_net<8, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      default: break;
+    }
+  }
+  block_partial(contrib, partials);
+  if (hpwl) block_partial(hcontrib, hpwl_partials);
+}
+
+}  // namespace dpb
+
+extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int* num_groups, int* num_lane_slots,
+                                 int* group_deg, int* group_base, int* group_net, int* lane_slot) {
+  using namespace dpb;
+  DP_REQUIRE(netpin_start_host && num_groups && num_lane_slots && num_nets >= 0, "dp_plan_net_lanes: bad arguments");
+  const bool fill = group_deg && group_base && group_net && lane_slot;
+  int g = 0;
+  long long base = 0;
+  for (int d = 1; d <= kLaneDeg; ++d) {
+    int in_group = 0;
+    for (int e = 0; e < num_nets; ++e) {
+      const int s0 = netpin_start_host[e];
+      if (netpin_start_host[e + 1] - s0 != d) continue;
+      if (in_group == 0) {
+        if (fill) {
+          group_deg[g] = d;
+          group_base[g] = (int)base;
+          for (int l = 0; l < 32; ++l) group_net[32 * g + l] = -1;
+          for (int i = 0; i < 32 * d; ++i) lane_slot[base + i] = -1;
+        }
+      }
+      if (fill) {
+        group_net[32 * g + in_group] = e;
+        for (int j = 0; j < d; ++j) lane_slot[base + 32 * j + in_group] = s0 + j;
+      }
+      if (++in_group == 32) {
+        in_group = 0;
+        ++g;
+        base += 32 * d;
+      }
+    }
+    if (in_group) {
+      ++g;
+      base += 32 * d;
+    }
+  }
+  for (int e = 0; e < num_nets; ++e) {
+    const int s0 = netpin_start_host[e], d = netpin_start_host[e + 1] - s0;
+    if (d <= kLaneDeg) continue;
+    if (fill) {
+      group_deg[g] = d;
+      group_base[g] = (int)base;
+      group_net[32 * g] = e;
+      for (int l = 1; l < 32; ++l) group_net[32 * g + l] = -1;
+      for (int j = 0; j < d; ++j) lane_slot[base + j] = s0 + j;
+    }
+    ++g;
+    base += d;
+  }
+  DP_REQUIRE(base < (1ll << 31), "dp_plan_net_lanes: too many pins");
+  *num_groups = g;
+  *num_lane_slots = (int)base;
+  return DP_OK;
+}
+
+static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, double* hpwl_f64, cudaStream_t s) {
+  using namespace dpb;
+  int blocks = A.num_groups > 0 ? ceil_div((long long)A.num_groups * 32, 256) : 1;
+  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
+  if (grad)
+    wa_lane_kernel<true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr);
+  else
+    wa_lane_kernel<false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr);
+  int rc = check_launch(grad ? "dp_wa_lanes_forward" : "dp_hpwl_lanes");
+  if (rc) return rc;
+  if (grad && hpwl_f64) {
+    rc = launch_finish_sum(hpwl_f64, blocks, nullptr, s);
+    if (rc) return rc;
+  }
+  return launch_finish_sum(out_f64, blocks, nullptr, s);
+}
+
+static dpb::LaneArgs lane_args(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
+                               int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
+                               const int* ln_csr, const float* net_weights, const unsigned char* net_mask,
+                               const unsigned char* hpwl_mask, const float* inv_gamma, float* grad_node_order) {
+  dpb::LaneArgs A;
+  A.xy = reinterpret_cast<const float2*>(xy);
+  A.group_deg = group_deg;
+  A.group_base = group_base;
+  A.group_net = group_net;
+  A.num_groups = num_groups;
+  A.ln_node = ln_node;
+  A.ln_offx = ln_offx;
+  A.ln_offy = ln_offy;
+  A.ln_csr = ln_csr;
+  A.net_weights = net_weights;
+  A.net_mask = net_mask;
+  A.hpwl_mask = hpwl_mask;
+  A.inv_gamma = inv_gamma;
+  A.gnode = reinterpret_cast<float2*>(grad_node_order);
+  return A;
+}
+
+extern "C" int dp_wa_lanes_forward(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
+                                   int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
+                                   const int* ln_csr, const float* net_weights, const unsigned char* net_mask,
+                                   const float* inv_gamma, double* wl_f64, float* grad_node_order,
+                                   const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream) {
+  DP_REQUIRE(xy && group_deg && group_base && group_net && ln_node && ln_offx && ln_offy && ln_csr && net_mask &&
+                 inv_gamma && wl_f64 && grad_node_order,
+             "dp_wa_lanes_forward: null pointer argument");
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
+             "dp_wa_lanes_forward: xy and grad_node_order must be 8-byte aligned");
+  DP_REQUIRE(!hpwl_f64 || hpwl_mask, "dp_wa_lanes_forward: hpwl_f64 needs hpwl_mask");
+  DP_REQUIRE(num_groups >= 0, "dp_wa_lanes_forward: bad group count");
+  const dpb::LaneArgs A = lane_args(xy, group_deg, group_base, group_net, num_groups, ln_node, ln_offx, ln_offy,
+                                    ln_csr, net_weights, net_mask, hpwl_mask, inv_gamma, grad_node_order);
+  return launch_lanes(true, A, wl_f64, hpwl_f64, dpb::as_stream(stream));
+}
+
+extern "C" int dp_hpwl_lanes(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
+                             int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
+                             const float* net_weights, const unsigned char* net_mask, double* out_f64,
+                             dp_stream_t stream) {
+  DP_REQUIRE(xy && group_deg && group_base && group_net && ln_node && ln_offx && ln_offy && net_mask && out_f64,
+             "dp_hpwl_lanes: null pointer argument");
+  DP_REQUIRE(((uintptr_t)xy & 7) == 0, "dp_hpwl_lanes: xy must be 8-byte aligned");
+  DP_REQUIRE(num_groups >= 0, "dp_hpwl_lanes: bad group count");
+  const dpb::LaneArgs A = lane_args(xy, group_deg, group_base, group_net, num_groups, ln_node, ln_offx, ln_offy,
+                                    nullptr, net_weights, net_mask, nullptr, nullptr, nullptr);
+  return launch_lanes(false, A, out_f64, nullptr, dpb::as_stream(stream));
+}

@@ -66,6 +66,17 @@ class GPEngine(object):
         csr_pos[self.node_slots.long()] = torch.arange(P, device=dev)
         self.csr_pos = csr_pos.to(torch.int32)
         self.gnode = torch.empty(2 * P, dtype=torch.float32, device=dev)
+        # lane-per-net plan: nets of degree <= 8 grouped 32 at a time by degree,
+        # pin arrays gathered into the transposed lane-slot order
+        g_deg, g_base, g_net, l_slot = C.plan_net_lanes(self.netpin_start.cpu())
+        self.group_deg, self.group_base, self.group_net = g_deg.to(dev), g_base.to(dev), g_net.to(dev)
+        ls = l_slot.to(dev).long()
+        real = ls >= 0
+        ls = ls.clamp(min=0)
+        self.ln_node = torch.where(real, self.slot_node[ls], torch.zeros_like(self.slot_node[ls])).contiguous()
+        self.ln_offx = torch.where(real, self.slot_offx[ls], torch.zeros_like(self.slot_offx[ls])).contiguous()
+        self.ln_offy = torch.where(real, self.slot_offy[ls], torch.zeros_like(self.slot_offy[ls])).contiguous()
+        self.ln_csr = torch.where(real, self.csr_pos[ls], torch.zeros_like(self.csr_pos[ls])).contiguous()
         ep = ops.density_op
         self.ep = ep
         self.ovf_op = ops.density_overflow_op
@@ -202,9 +213,9 @@ class GPEngine(object):
         same pin reads."""
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
-        C.wa_chunk_forward(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.chunk_pin,
-                           dc.net_weights, dc.net_mask_ignore_large_degrees, self.inv_gamma,
-                           self.csr_pos, self.wl64_buf, self.gnode,
+        C.wa_lanes_forward(self.xy(v), self.group_deg, self.group_base, self.group_net, self.ln_node, self.ln_offx,
+                           self.ln_offy, self.ln_csr, dc.net_weights, dc.net_mask_ignore_large_degrees,
+                           self.inv_gamma, self.wl64_buf, self.gnode,
                            dc.net_mask_all if hpwl_out is not None else None, hpwl_out)
 
     def wl_grad_into(self, g, accumulate):
@@ -326,8 +337,8 @@ class GPEngine(object):
         for a position set from outside the trial kernel."""
         dc = self.data
         v = self.V[q]
-        C.hpwl_chunk(self.xy(v), self.slot_node, self.slot_offx, self.slot_offy, self.slot_net, self.chunk_pin,
-                     dc.net_weights, dc.net_mask_all, self.H[q])
+        C.hpwl_lanes(self.xy(v), self.group_deg, self.group_base, self.group_net, self.ln_node, self.ln_offx,
+                     self.ln_offy, dc.net_weights, dc.net_mask_all, self.H[q])
         self._density(v, 0, self.omap)
         C.density_overflow_into(self.omap, self.ovf_target, self.ovf_area, self.O[q])
 

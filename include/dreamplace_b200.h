@@ -396,6 +396,31 @@ int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, co
 int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
                   const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
                   const float* net_weights, const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
+/* Lane-per-net plan (host): nets of degree 1..8 grouped 32 at a time by degree,
+ * in net order within a degree; each larger net a group of its own.  Call with
+ * NULL group_deg / group_base / group_net / lane_slot to get *num_groups and
+ * *num_lane_slots, then with buffers of those sizes (group_net: 32 per group).
+ * Group g of degree d <= 8 stores pin j of lane l at lane slot
+ * group_base[g] + 32 j + l; a larger net stores its pins contiguously from
+ * group_base[g].  lane_slot maps lane slots to pin slots (flat_netpin order),
+ * -1 for padding; group_net holds net ids, -1 for padding lanes. */
+int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int* num_groups, int* num_lane_slots,
+                      int* group_deg, int* group_base, int* group_net, int* lane_slot);
+/* WA forward over a lane plan: one warp per group, one lane per net (degree
+ * <= 8, pins in registers, the reference's per-net loops in pin order) or the
+ * whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the
+ * pin arrays gathered to lane-slot order (ln_csr: the pin's position in
+ * node-CSR order).  Outputs as dp_wa_chunk_forward; hpwl_f64 (optional) equals
+ * dp_hpwl_lanes on the same plan. */
+int dp_wa_lanes_forward(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
+                        int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
+                        const int* ln_csr, const float* net_weights, const unsigned char* net_mask,
+                        const float* inv_gamma, double* wl_f64, float* grad_node_order,
+                        const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream);
+/* HPWL over a lane plan (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
+int dp_hpwl_lanes(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
+                  int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
+                  const float* net_weights, const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
 /* grad_out[node] (+)= sum over k in node_start[node]..node_start[node+1] of the
  * (x, y) pair grad_node_order[2k..2k+1] * grad_pos[0]; nodes >= num_movable get 0
  * (pin mask of fixed cells) */

@@ -439,3 +439,66 @@ def test_ordered_split_scatter(C):
             tol = 1e-4 * float(exp_full.abs().max())
             torch.testing.assert_close(first, exp_first, rtol=1e-4, atol=tol)
             torch.testing.assert_close(full, exp_full, rtol=1e-4, atol=tol)
+
+
+def lane_inputs(C, d):
+    """Slot (flat_netpin) arrays, node-CSR positions and the lane plan of a design."""
+    P = d.num_pins
+    fnp = d.flat_net2pin_map.astype(np.int64)
+    slot_of_pin = np.empty(P, np.int64)
+    slot_of_pin[fnp] = np.arange(P)
+    node_slots = slot_of_pin[d.flat_node2pin_map]
+    csr_pos = np.empty(P, np.int64)
+    csr_pos[node_slots] = np.arange(P)
+    g_deg, g_base, g_net, l_slot = C.plan_net_lanes(torch.from_numpy(d.flat_net2pin_start_map.astype(np.int32)))
+    ls = l_slot.numpy().astype(np.int64)
+    real = ls >= 0
+    ls = np.where(real, ls, 0)
+    ln_node = np.where(real, d.pin2node_map[fnp][ls], 0).astype(np.int32)
+    ln_offx = np.where(real, d.pin_offset_x[fnp][ls], 0).astype(np.float32)
+    ln_offy = np.where(real, d.pin_offset_y[fnp][ls], 0).astype(np.float32)
+    ln_csr = np.where(real, csr_pos[ls], 0).astype(np.int32)
+    plan = (dev(g_deg.numpy()), dev(g_base.numpy()), dev(g_net.numpy()), dev(ln_node), dev(ln_offx), dev(ln_offy))
+    return plan, dev(ln_csr), csr_pos, slot_of_pin, g_deg.numpy()
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_wa_lanes_against_reference(C, golden, weighted):
+    """Lane-per-net WA (nets of degree <= 8 one per lane, larger nets one per
+    warp): value and per-pin gradient against the reference's merged op
+    (golden) or the oracle with random net weights; the HPWL of the same plan
+    against the reference's HPWL."""
+    g = golden("design_small.npz")
+    d = small_design()
+    n, P = d.num_nodes, d.num_pins
+    plan, ln_csr, csr_pos, slot_of_pin, deg = lane_inputs(C, d)
+    assert deg.max() > 8 and deg.min() <= 2  # both the lane and the warp paths run
+    pos = g["pos"].astype(np.float32)
+    xy = pack_xy(pos, n)
+    mask = dev(g["net_mask"])
+    weights = (np.random.RandomState(6).uniform(0.5, 2.0, d.num_nets).astype(np.float32) if weighted
+               else d.net_weights.astype(np.float32))
+    inv_gamma = torch.tensor([float(g["inv_gamma"])], device="cuda")
+    wl = torch.zeros(1280, dtype=torch.float64, device="cuda")
+    hp = torch.zeros(1280, dtype=torch.float64, device="cuda")
+    gnode = torch.empty(2 * P, device="cuda")
+    C.wa_lanes_forward(xy, *plan[:3], *plan[3:], ln_csr, dev(weights), mask, inv_gamma, wl, gnode, mask, hp)
+    got = gnode.cpu().numpy().reshape(-1, 2)[csr_pos[slot_of_pin]]  # per pin id
+    if weighted:
+        ref_wl, _, ref_grad = oracle.wa_merged(g["pin_pos"], d.flat_net2pin_map, d.flat_net2pin_start_map,
+                                               g["net_mask"], weights, float(g["inv_gamma"]))
+        w_pin = weights[d.pin2net_map]
+        exp = np.stack([ref_grad[:P] * w_pin, ref_grad[P:] * w_pin], axis=1)
+    else:
+        ref_wl = float(g["wa_wl"])
+        exp = np.stack([g["wa_grad_intermediate"][:P], g["wa_grad_intermediate"][P:]], axis=1)
+    assert math.isclose(float(wl[0].item()), ref_wl, rel_tol=1e-5)
+    # the gradient bar of the merged op, scaled by the largest net weight
+    np.testing.assert_allclose(got, exp, rtol=1e-5, atol=1e-6 * float(weights.max()))
+    ref_hpwl = oracle.hpwl(g["pin_pos"], d.flat_net2pin_map, d.flat_net2pin_start_map, g["net_mask"], weights)
+    assert math.isclose(float(hp[0].item()), ref_hpwl, rel_tol=1e-6)
+    if not weighted:
+        assert math.isclose(float(hp[0].item()), float(g["hpwl"]), rel_tol=1e-6)
+    alone = torch.zeros(1280, dtype=torch.float64, device="cuda")
+    C.hpwl_lanes(xy, *plan, dev(weights), mask, alone)
+    assert alone[0].item() == hp[0].item()  # same plan, same summation order
