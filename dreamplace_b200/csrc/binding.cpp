@@ -487,7 +487,7 @@ void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey,
 void assemble_precondition_step(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor wl_scale,
                                 at::Tensor force_o, at::Tensor inv_order, int num_movable, int num_filler,
                                 at::Tensor pws, at::Tensor area, at::Tensor lambda_, at::Tensor v_new, at::Tensor v,
-                                at::Tensor g, at::Tensor g_new, at::Tensor state) {
+                                at::Tensor g, at::Tensor g_new, at::Tensor state, c10::optional<at::Tensor> grad_index) {
   CHECK_I32(node_start); CHECK_I32(inv_order);
   int n = v.numel() / 2;
   TORCH_CHECK(inv_order.numel() >= n && node_start.numel() >= num_movable + 1 && g_new.numel() == 2 * n,
@@ -496,7 +496,7 @@ void assemble_precondition_step(at::Tensor grad_node_order, at::Tensor node_star
                                         ptr<float>(force_o), ptr<int>(inv_order), num_movable, num_filler,
                                         ptr<float>(pws), ptr<float>(area), ptr<float>(lambda_), n, ptr<float>(v_new),
                                         ptr<float>(v), ptr<float>(g), ptr<float>(g_new), ptr<double>(state),
-                                        cur_stream()));
+                                        (const int*)ovp(grad_index), cur_stream()));
 }
 
 void density_overflow_into(at::Tensor density_map, double target_area, double bin_area, at::Tensor out2) {
@@ -569,12 +569,12 @@ std::vector<at::Tensor> plan_net_lanes(at::Tensor netpin_start_cpu) {
 }
 
 void wa_lanes_forward(at::Tensor xy, at::Tensor group_deg, at::Tensor group_base, at::Tensor group_net,
-                      at::Tensor ln_node, at::Tensor ln_offx, at::Tensor ln_offy, at::Tensor ln_csr,
+                      at::Tensor ln_node, at::Tensor ln_offx, at::Tensor ln_offy, c10::optional<at::Tensor> ln_csr,
                       c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor inv_gamma,
                       at::Tensor wl_f64, at::Tensor grad_node_order, c10::optional<at::Tensor> hpwl_mask,
                       c10::optional<at::Tensor> hpwl_f64) {
   CHECK_FLAT(xy); CHECK_F32(xy); CHECK_I32(group_deg); CHECK_I32(group_base); CHECK_I32(group_net);
-  CHECK_I32(ln_node); CHECK_I32(ln_csr); CHECK_F32(grad_node_order);
+  CHECK_I32(ln_node); CHECK_F32(grad_node_order);
   TORCH_CHECK(group_net.numel() == 32 * group_deg.numel() && group_base.numel() == group_deg.numel(),
               "wa_lanes_forward: inconsistent plan");
   TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
@@ -583,7 +583,7 @@ void wa_lanes_forward(at::Tensor xy, at::Tensor group_deg, at::Tensor group_base
               "hpwl_f64 needs hpwl_mask and DP_REDUCE_DOUBLES doubles");
   DP_CALL(dp_wa_lanes_forward(ptr<float>(xy), ptr<int>(group_deg), ptr<int>(group_base), ptr<int>(group_net),
                               group_deg.numel(), ptr<int>(ln_node), ptr<float>(ln_offx), ptr<float>(ln_offy),
-                              ptr<int>(ln_csr), (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
+                              (const int*)ovp(ln_csr), (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(),
                               ptr<float>(inv_gamma), ptr<double>(wl_f64), ptr<float>(grad_node_order),
                               hpwl_mask.has_value() ? hpwl_mask->data_ptr<uint8_t>() : nullptr,
                               (double*)ovp(hpwl_f64), cur_stream()));

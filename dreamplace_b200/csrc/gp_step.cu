@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) assemble_precondition_kernel(
     const float2* __restrict__ force_o, const int* __restrict__ inv_order, int num_movable, int num_filler,
     const float* __restrict__ pws, const float* __restrict__ area, const float* __restrict__ lam_p, int num_nodes,
     const float* __restrict__ v_new, const float* __restrict__ v, const float* __restrict__ g,
-    float* __restrict__ g_new, double* __restrict__ partials) {
+    float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index) {
   const float lam = *lam_p;
   const float ws = *wl_scale_p;
   double dv = 0.0, dg = 0.0;
@@ -304,10 +304,22 @@ __global__ void __launch_bounds__(256) assemble_precondition_kernel(
     float sx = 0.f, sy = 0.f;
     if (i < num_movable) {
       const int k1 = node_start[i + 1];
-      for (int k = node_start[i]; k < k1; ++k) {
-        const float2 q = __ldcs(gnode + k);
-        sx = fadd(sx, fmul(q.x, ws));
-        sy = fadd(sy, fmul(q.y, ws));
+      // four pins at a time: their loads are issued together, the sum keeps
+      // the pin order
+      for (int k = node_start[i]; k < k1; k += 4) {
+        float2 q[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          q[t] = make_float2(0.f, 0.f);
+          if (k + t < k1) q[t] = grad_index ? gnode[__ldcs(grad_index + k + t)] : __ldcs(gnode + k + t);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          if (k + t < k1) {
+            sx = fadd(sx, fmul(q[t].x, ws));
+            sy = fadd(sy, fmul(q[t].y, ws));
+          }
+        }
       }
     }
     float fx = 0.f, fy = 0.f;
@@ -834,7 +846,8 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
                                              const float* wl_scale, const float* force_o, const int* inv_order,
                                              int num_movable, int num_filler, const float* pws, const float* area,
                                              const float* lambda_, int num_nodes, const float* v_new, const float* v,
-                                             const float* g, float* g_new, double* state, dp_stream_t stream) {
+                                             const float* g, float* g_new, double* state, const int* grad_index,
+                                             dp_stream_t stream) {
   using namespace dpb;
   DP_REQUIRE(grad_node_order && node_start && wl_scale && force_o && inv_order && pws && area && lambda_ && v_new &&
                  v && g && g_new && state,
@@ -847,7 +860,7 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
   assemble_precondition_kernel<<<blocks, 256, 0, s>>>(
       reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
-      inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials);
+      inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index);
   int rc = check_launch("dp_assemble_precondition_step");
   if (rc) return rc;
   nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
@@ -884,6 +897,10 @@ struct LaneArgs {
   const float* inv_gamma;  // device scalar (read once per thread)
   float2* gnode;
 };
+
+// where the gradient of lane slot p goes: its pin's node-CSR position, or p
+// itself (lane-slot order, gathered by the assembly through grad_index)
+__device__ __forceinline__ int grad_slot(const LaneArgs& A, int p) { return A.ln_csr ? __ldcs(A.ln_csr + p) : p; }
 
 // a = (1 - b * xe) / e evaluated as the reference does (the literal 1.0
 // promotes the expression to double), rounded to float
@@ -926,25 +943,36 @@ __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, 
   }
   if (!A.net_mask[net]) {
 #pragma unroll
-    for (int j = 0; j < D; ++j) __stcs(A.gnode + __ldcs(A.ln_csr + base + 32 * j + lane), make_float2(0.f, 0.f));
+    for (int j = 0; j < D; ++j) __stcs(A.gnode + grad_slot(A, base + 32 * j + lane), make_float2(0.f, 0.f));
     return;
   }
-  float ex[D], enx[D], ey[D], eny[D];
+  // up to 4 pins the exponentials stay in registers for the gradient pass;
+  // larger nets recompute them there (keeps the kernel's register count, and
+  // with it the occupancy, at the small-net level)
+  constexpr bool kKeep = D <= 4;
+  constexpr int K = kKeep ? D : 1;
+  float ex[K], enx[K], ey[K], eny[K];
   float e_p = 0.f, e_n = 0.f, xe_p = 0.f, xe_n = 0.f, f_p = 0.f, f_n = 0.f, ye_p = 0.f, ye_n = 0.f;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    ex[j] = expf(fmul(fsub(x[j], x_max), ig));
-    enx[j] = expf(fmul(fsub(x_min, x[j]), ig));
-    ey[j] = expf(fmul(fsub(y[j], y_max), ig));
-    eny[j] = expf(fmul(fsub(y_min, y[j]), ig));
-    e_p = fadd(e_p, ex[j]);
-    e_n = fadd(e_n, enx[j]);
-    xe_p = fadd(xe_p, fmul(x[j], ex[j]));
-    xe_n = fadd(xe_n, fmul(x[j], enx[j]));
-    f_p = fadd(f_p, ey[j]);
-    f_n = fadd(f_n, eny[j]);
-    ye_p = fadd(ye_p, fmul(y[j], ey[j]));
-    ye_n = fadd(ye_n, fmul(y[j], eny[j]));
+    const float a1 = expf(fmul(fsub(x[j], x_max), ig));
+    const float a2 = expf(fmul(fsub(x_min, x[j]), ig));
+    const float a3 = expf(fmul(fsub(y[j], y_max), ig));
+    const float a4 = expf(fmul(fsub(y_min, y[j]), ig));
+    if (kKeep) {
+      ex[kKeep ? j : 0] = a1;
+      enx[kKeep ? j : 0] = a2;
+      ey[kKeep ? j : 0] = a3;
+      eny[kKeep ? j : 0] = a4;
+    }
+    e_p = fadd(e_p, a1);
+    e_n = fadd(e_n, a2);
+    xe_p = fadd(xe_p, fmul(x[j], a1));
+    xe_n = fadd(xe_n, fmul(x[j], a2));
+    f_p = fadd(f_p, a3);
+    f_n = fadd(f_n, a4);
+    ye_p = fadd(ye_p, fmul(y[j], a3));
+    ye_n = fadd(ye_n, fmul(y[j], a4));
   }
   const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
                         __fdiv_rn(ye_n, f_n));
@@ -955,13 +983,17 @@ __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, 
   const float b_ny = __fdiv_rn(-ig, f_n), a_ny = wa_a_term(b_ny, ye_n, f_n);
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    float gx = fsub(fmul(fadd(a_x, fmul(b_x, x[j])), ex[j]), fmul(fadd(a_nx, fmul(b_nx, x[j])), enx[j]));
-    float gy = fsub(fmul(fadd(a_y, fmul(b_y, y[j])), ey[j]), fmul(fadd(a_ny, fmul(b_ny, y[j])), eny[j]));
+    const float a1 = kKeep ? ex[kKeep ? j : 0] : expf(fmul(fsub(x[j], x_max), ig));
+    const float a2 = kKeep ? enx[kKeep ? j : 0] : expf(fmul(fsub(x_min, x[j]), ig));
+    const float a3 = kKeep ? ey[kKeep ? j : 0] : expf(fmul(fsub(y[j], y_max), ig));
+    const float a4 = kKeep ? eny[kKeep ? j : 0] : expf(fmul(fsub(y_min, y[j]), ig));
+    float gx = fsub(fmul(fadd(a_x, fmul(b_x, x[j])), a1), fmul(fadd(a_nx, fmul(b_nx, x[j])), a2));
+    float gy = fsub(fmul(fadd(a_y, fmul(b_y, y[j])), a3), fmul(fadd(a_ny, fmul(b_ny, y[j])), a4));
     if (A.net_weights) {
       gx = fmul(gx, w);
       gy = fmul(gy, w);
     }
-    __stcs(A.gnode + __ldcs(A.ln_csr + base + 32 * j + lane), make_float2(gx, gy));
+    __stcs(A.gnode + grad_slot(A, base + 32 * j + lane), make_float2(gx, gy));
   }
 }
 
@@ -1039,7 +1071,7 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
         gy = fmul(gy, w);
       }
     }
-    A.gnode[A.ln_csr[base + j]] = make_float2(gx, gy);
+    A.gnode[grad_slot(A, base + j)] = make_float2(gx, gy);
   }
 }
 
@@ -1176,8 +1208,8 @@ extern "C" int dp_wa_lanes_forward(const float* xy, const int* group_deg, const 
                                    const int* ln_csr, const float* net_weights, const unsigned char* net_mask,
                                    const float* inv_gamma, double* wl_f64, float* grad_node_order,
                                    const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream) {
-  DP_REQUIRE(xy && group_deg && group_base && group_net && ln_node && ln_offx && ln_offy && ln_csr && net_mask &&
-                 inv_gamma && wl_f64 && grad_node_order,
+  DP_REQUIRE(xy && group_deg && group_base && group_net && ln_node && ln_offx && ln_offy && net_mask && inv_gamma &&
+                 wl_f64 && grad_node_order,
              "dp_wa_lanes_forward: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
              "dp_wa_lanes_forward: xy and grad_node_order must be 8-byte aligned");

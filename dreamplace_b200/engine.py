@@ -77,6 +77,15 @@ class GPEngine(object):
         self.ln_offx = torch.where(real, self.slot_offx[ls], torch.zeros_like(self.slot_offx[ls])).contiguous()
         self.ln_offy = torch.where(real, self.slot_offy[ls], torch.zeros_like(self.slot_offy[ls])).contiguous()
         self.ln_csr = torch.where(real, self.csr_pos[ls], torch.zeros_like(self.csr_pos[ls])).contiguous()
+        # where the WA gradient lands: "csr" (node-CSR order, scattered writes)
+        # or "lane" (lane-slot order, coalesced writes; the assembly gathers it)
+        self.wa_grad_order = getattr(params, "wa_grad_order", "lane")
+        self.lane_of_csr = None
+        if self.wa_grad_order == "lane":
+            p_idx = torch.arange(ls.numel(), device=dev)[real]
+            self.lane_of_csr = torch.empty(P, dtype=torch.int32, device=dev)
+            self.lane_of_csr[self.csr_pos[ls[real]].long()] = p_idx.to(torch.int32)
+            self.gnode = torch.empty(2 * ls.numel(), dtype=torch.float32, device=dev)
         ep = ops.density_op
         self.ep = ep
         self.ovf_op = ops.density_overflow_op
@@ -214,13 +223,16 @@ class GPEngine(object):
         dc = self.data
         self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
         C.wa_lanes_forward(self.xy(v), self.group_deg, self.group_base, self.group_net, self.ln_node, self.ln_offx,
-                           self.ln_offy, self.ln_csr, dc.net_weights, dc.net_mask_ignore_large_degrees,
+                           self.ln_offy, self.ln_csr if self.lane_of_csr is None else None, dc.net_weights,
+                           dc.net_mask_ignore_large_degrees,
                            self.inv_gamma, self.wl64_buf, self.gnode,
                            dc.net_mask_all if hpwl_out is not None else None, hpwl_out)
 
     def wl_grad_into(self, g, accumulate):
-        dc = self.data
-        C.node_pin_sum(self.gnode, self.node_start, self.one, self.design.num_movable_nodes, int(accumulate), g)
+        gn = self.gnode
+        if self.lane_of_csr is not None:  # lane-slot order -> node-CSR order
+            gn = gn.view(-1, 2)[self.lane_of_csr.long()].reshape(-1).contiguous()
+        C.node_pin_sum(gn, self.node_start, self.one, self.design.num_movable_nodes, int(accumulate), g)
 
     def scatter_maps(self, v, ovf_out):
         """One scatter of v: the movable-only map (self.omap) and the movable +
@@ -256,7 +268,7 @@ class GPEngine(object):
         d = self.design
         C.assemble_precondition_step(self.gnode, self.node_start, self.one, self.force_o, self.inv_order,
                                      d.num_movable_nodes, d.num_filler_nodes, self._pws(), self.data.node_areas,
-                                     self.model.density_weight, v_new, v, g, g_new, self.state)
+                                     self.model.density_weight, v_new, v, g, g_new, self.state, self.lane_of_csr)
 
     def density_grad_into(self, v, ex, ey, scale_t, g):
         ep = self.ep

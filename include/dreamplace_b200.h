@@ -362,14 +362,16 @@ int dp_precondition_step_size(float* g_new, const float* g, const float* v_new, 
                               const float* pws, const float* area, const float* lambda_, int num_nodes,
                               double* state, dp_stream_t stream);
 /* Gradient assembly fused with the preconditioner and the step size: for each
- * node, g' = wl_scale * (pin sum of grad_node_order, nodes < num_movable) +
+ * node, g' = wl_scale * (pin sum of grad_node_order, nodes < num_movable; pin k
+ * of the node-CSR order is element grad_index[k] when grad_index is non-NULL) +
  * force_o[inv_order[node]] (movable and filler nodes), then as
  * dp_precondition_step_size. */
 int dp_assemble_precondition_step(const float* grad_node_order, const int* node_start,
                                   const float* wl_scale, const float* force_o, const int* inv_order,
                                   int num_movable, int num_filler, const float* pws, const float* area,
                                   const float* lambda_, int num_nodes, const float* v_new, const float* v,
-                                  const float* g, float* g_new, double* state, dp_stream_t stream);
+                                  const float* g, float* g_new, double* state, const int* grad_index,
+                                  dp_stream_t stream);
 /* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
 int dp_nesterov_advance(double* state, dp_stream_t stream);
 /* Host planner: packs nets, in order, into chunks of at most max_pins pins (a
@@ -410,8 +412,9 @@ int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int* num_group
  * <= 8, pins in registers, the reference's per-net loops in pin order) or the
  * whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the
  * pin arrays gathered to lane-slot order (ln_csr: the pin's position in
- * node-CSR order).  Outputs as dp_wa_chunk_forward; hpwl_f64 (optional) equals
- * dp_hpwl_lanes on the same plan. */
+ * node-CSR order, where its gradient is written; NULL writes the gradient of
+ * lane slot p at p).  Outputs as dp_wa_chunk_forward; hpwl_f64 (optional)
+ * equals dp_hpwl_lanes on the same plan. */
 int dp_wa_lanes_forward(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
                         int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
                         const int* ln_csr, const float* net_weights, const unsigned char* net_mask,

@@ -397,7 +397,16 @@ def test_ordered_force_and_fused_assembly(C, golden):
     C.precondition_step_size(exp, g_old, v_new, v, pws, area, lam, st_ref)
     got = torch.empty(2 * n, device="cuda")
     C.assemble_precondition_step(gnode, node_start, grad, force_o, inv, m, nf, pws, area, lam, v_new, v, g_old, got,
-                                 st_got)
+                                 st_got, None)
+    # the same pin gradients stored in another order, gathered through grad_index
+    perm = np.random.RandomState(8).permutation(d.num_pins)
+    shuffled = torch.empty_like(gnode).view(-1, 2)
+    shuffled[dev(perm).long()] = gnode.view(-1, 2)
+    got2 = torch.empty(2 * n, device="cuda")
+    st2 = torch.zeros_like(st_ref)
+    C.assemble_precondition_step(shuffled.reshape(-1), node_start, grad, force_o, inv, m, nf, pws, area, lam, v_new, v,
+                                 g_old, got2, st2, dev(perm.astype(np.int32)))
+    assert torch.equal(got2, exp)
     assert torch.equal(got, exp)
     np.testing.assert_allclose(st_got[:8].cpu().numpy(), st_ref[:8].cpu().numpy(), rtol=1e-12)
 
