@@ -16,6 +16,7 @@
 // one atomic, which removes most same-address serialisation when cells are
 // clustered (the GP starts with every movable cell at the die centre).
 #include <climits>
+#include <cstdlib>
 #include <mutex>
 #include <type_traits>
 #include <cub/block/block_radix_sort.cuh>
@@ -164,8 +165,8 @@ __device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0,
       }
 }
 
-template <bool kFixed>
-__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a,
+template <bool kFixed, int kRadixBits>
+__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a, int sort_cells,
                                                                         const float2* __restrict__ xy_o,
                                                                         const float4* __restrict__ rec4,
                                                                         const float* __restrict__ ratio_o, int count,
@@ -232,12 +233,12 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
   if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
   const int H = bh1 - bh0;
   const long long box = (long long)(bk1 - bk0) * H;
-  if (box < (1 << 16)) {
+  if (sort_cells && box < (1 << 16)) {
     // Block-local order: the visiting order is refreshed only every few
     // iterations, while cells keep moving; sorting the block's cells by the
     // bin where their window starts (relative to the block's bounding box)
     // restores the runs that the lane windows and the warp reduction rely on.
-    using BlockSort = cub::BlockRadixSort<unsigned, kWsThreads, kWsCellsPerLane, int>;
+    using BlockSort = cub::BlockRadixSort<unsigned, kWsThreads, kWsCellsPerLane, int, kRadixBits>;
     __shared__ typename BlockSort::TempStorage sort_tmp;
     __shared__ float s_cell[5][kWsCells];
     unsigned keys[kWsCellsPerLane];
@@ -776,25 +777,33 @@ struct OrderedScatter {
 };
 
 // adds cells [begin, end) of the visiting order onto out (fp32) or scratch (fixed)
-int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits, int64_t* scratch,
-                  float* out) {
+template <int kRadixBits>
+int scatter_range_r(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits,
+                    int64_t* scratch, float* out, int sort_cells) {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(window_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
-    cudaFuncSetAttribute(window_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmemBytes);
+    cudaFuncSetAttribute(window_scatter_kernel<false, kRadixBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kWsSmemBytes);
+    cudaFuncSetAttribute(window_scatter_kernel<true, kRadixBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kWsSmemBytes);
     configured = true;
   }
   const int count = end - begin;
   if (count <= 0) return DP_OK;
   const int blocks = ceil_div(count, kWsCells);
   if (deterministic)
-    window_scatter_kernel<true><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits), nullptr,
-        reinterpret_cast<unsigned long long*>(scratch));
+    window_scatter_kernel<true, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
+        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits),
+        nullptr, reinterpret_cast<unsigned long long*>(scratch));
   else
-    window_scatter_kernel<false><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
+    window_scatter_kernel<false, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
+        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
   return check_launch("dp_density_map_ordered scatter");
+}
+
+int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits, int64_t* scratch,
+                  float* out, int sort_cells = 1) {
+  return scatter_range_r<4>(o, begin, end, deterministic, fraction_bits, scratch, out, sort_cells);
 }
 
 int convert_fixed(const int64_t* scratch, const float* init, int fraction_bits, float* out, int nbins,
@@ -864,7 +873,9 @@ extern "C" int dp_density_map_ordered(const float* xy_o, const float* rec4, cons
 // pass that finishes it.  Fixed point: the int64 sums are exact, so both maps
 // equal separate scatters bit for bit.  fp32: the second map continues from
 // the first, i.e. the float additions happen in one of the orders the atomic
-// scatter of all cells can take.
+// scatter of all cells can take.  Only the first range gets the block-local
+// sort (the second one is the engine's fillers, spread about one per bin, for
+// which runs of equal start bins stay short anyway).
 extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4, const float* ratio_o, int num_first, int count, const float* init,
                                             float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
                                             float iby, int nbx, int nby, int deterministic, int fraction_bits,
@@ -897,7 +908,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4
       rc = convert_fixed(scratch, init, fraction_bits, out_first, nbins, o.s);
     }
     if (rc) return rc;
-    rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr);
+    rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr, 0);
     if (rc) return rc;
     return convert_fixed(scratch, init, fraction_bits, out_all, nbins, o.s);
   }
@@ -918,7 +929,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4
     rc = copy_map(out_first, out_all, nbins, o.s);
   }
   if (rc) return rc;
-  return scatter_range(o, num_first, count, 0, 0, nullptr, out_all);
+  return scatter_range(o, num_first, count, 0, 0, nullptr, out_all, 0);
 }
 
 // ---------------------------------------------------------------- allocation-free variant
