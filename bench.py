@@ -284,7 +284,8 @@ def piece_work(design, eng):
     * density_scatter: per scattered cell 16 B record + 4 B ratio + 4 B order
       index + 8 B position; per bin 4 B initial map read, movable-only map
       written and read back by the fused overflow pass, full map written;
-    * poisson_gemms: the four GEMM launches' flops;
+    * poisson_gemms: the GEMM flops of one solve (three 2-D transforms, x3
+      for split-BF16; the energy is summed in the spectral domain);
     * field_gather: per cell the same 32 B as the scatter + 8 B force written;
       per bin the two field maps read once;
     * wa_forward (HPWL included): per pin 20 B of pin arrays + 8 B gradient
@@ -295,13 +296,13 @@ def piece_work(design, eng):
       3 x 8 B (v_new, v, g) read + 8 B written;
     * nesterov_trial: per node 3 x 8 B read (v, g, u), 2 x 8 B written (u, v)
       + 8 B interleaved copy + 8 B cell size."""
-    from dreamplace_b200.dct2_fft2 import gemm_flops
+    from dreamplace_b200.electric_potential import poisson_flops
     d, ep = design, eng.ep
     n_s = d.num_movable_nodes + d.num_filler_nodes
     M, N = ep.num_bins_x, ep.num_bins_y
     P, E, n = d.num_pins, d.num_nets, d.num_nodes
     return {"density_scatter": (32.0 * n_s + 16.0 * M * N, "hbm"),
-            "poisson_gemms": (gemm_flops(M, N, eng.prec, 4), "tensor" if eng.prec else "fp32"),
+            "poisson_gemms": (poisson_flops(M, N, eng.prec), "tensor" if eng.prec else "fp32"),
             "field_gather": (40.0 * n_s + 8.0 * M * N, "hbm"),
             "wa_forward": (28.0 * P + 10.0 * E + 8.0 * n, "hbm"),
             "assemble_precondition": (8.0 * P + 64.0 * n, "hbm"),

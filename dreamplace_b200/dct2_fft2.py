@@ -16,7 +16,6 @@ fp64).  ``precision`` picks the arithmetic: ``fp32`` (SIMT, the plain form),
 ``tf32``, ``bf16`` or ``split_bf16`` (hi*hi + hi*lo + lo*hi, fp32 accumulation).
 The matrices are built in fp64 and rounded once.
 """
-import math
 
 import numpy as np
 import torch
@@ -199,7 +198,3 @@ def gemm_flops(M, N, prec, transforms):
     """Algorithmic flops of ``transforms`` 2-D transforms at M x N (2 GEMMs each)."""
     k = 3 if prec == 3 else 1
     return transforms * k * 2.0 * M * N * (M + N)
-
-
-def _unused():  # keep math import used by type checkers
-    return math.pi

@@ -47,6 +47,13 @@ def spectral_tables(M, N, wv_scale, device):
     return _SPECTRAL_CACHE[key]
 
 
+def poisson_flops(M, N, precision):
+    """Algorithmic GEMM flops of one poisson_solve: rho -> a (one 2-D transform)
+    and a -> (Ex, Ey) (two 2-D transforms), x3 for split-BF16."""
+    k = 3 if precision_code(precision) == 3 else 1
+    return 3 * k * 2.0 * M * N * (M + N)
+
+
 def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
     """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
 
