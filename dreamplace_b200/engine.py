@@ -163,6 +163,7 @@ class GPEngine(object):
         self.kernels_launched = 0  # this library's kernels, graph replays included
         self.pool = None
         self.graph_key = None
+        self._metrics_ready = None
         self.trials = 0
         self.last_energy = None
         self._quad_c = 0.0
@@ -484,7 +485,9 @@ class GPEngine(object):
             self.graphs[key] = g
         return g
 
-    def _run(self, p):
+    def _launch(self, p):
+        """Enqueue one trial (graph replay) and the read-back of its metrics on the
+        current stream."""
         if self.use_graphs:
             self._graph(p).replay()
             self.kernels_launched += self.graph_kernels[p]
@@ -493,10 +496,20 @@ class GPEngine(object):
             self._body(p)
             self.kernels_launched += C.launch_count() - before
         self.metrics_host.copy_(self.metrics, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        if self._metrics_ready is None:
+            self._metrics_ready = torch.cuda.Event()
+        self._metrics_ready.record()
+
+    def _collect(self):
+        """Wait for the last launched trial and return its metrics."""
+        self._metrics_ready.synchronize()
         if self.piece_events is not None:
             self._collect_pieces()
         return self.metrics_host.numpy().copy()
+
+    def _run(self, p):
+        self._launch(p)
+        return self._collect()
 
     def _check_graph_key(self):
         """Refresh the device copy of (density factor, quadratic penalty
@@ -523,6 +536,17 @@ class GPEngine(object):
     def step(self):
         """One GP iteration: evaluation at v_k, then Nesterov trials until accepted
         (<= 10).  Returns (hpwl, overflow / total movable area, max_density, objective, trials)."""
+        gen = self.step_gen()
+        try:
+            while True:
+                next(gen)
+        except StopIteration as stop:
+            return stop.value
+
+    def step_gen(self):
+        """step() as a generator: it yields once, right after the first trial is
+        enqueued, so a driver of several designs can enqueue theirs (on their own
+        streams) before this one waits for its metrics."""
         self._check_graph_key()
         if self.use_graphs and len(self.graphs) < 2:
             self.prepare_graphs()
@@ -530,7 +554,9 @@ class GPEngine(object):
         if self.sort_interval > 0 and self.iterations % self.sort_interval == 0:
             self.refresh_order(self.V[p])
         self.iterations += 1
-        mh = self._run(p)
+        self._launch(p)
+        yield
+        mh = self._collect()
         hpwl, ovf, maxd = mh[M_HPWL], mh[M_OVF], mh[M_MAXD]
         trials = 1
         while mh[M_ACCEPT] == 0.0 and trials < 10:

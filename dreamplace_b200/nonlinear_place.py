@@ -109,12 +109,22 @@ class _EngineStepper(object):
         self.lr = self.eng.initial_learning_rate(lr0)
 
     def step(self, first):
+        gen = self.step_gen(first)
+        try:
+            while True:
+                next(gen)
+        except StopIteration as stop:
+            return stop.value
+
+    def step_gen(self, first):
+        """step() as a generator that yields once the iteration's first trial is
+        enqueued (see GPEngine.step_gen)."""
         e = self.eng
         if first:
             e.move_boundary(e.V[e.parity])
             e.initialize_density_weight()
             e.start_optimizer(self.lr)
-        h, o, md, obj, trials = e.step()
+        h, o, md, obj, trials = yield from e.step_gen()
         return h, o, md, obj
 
     def position(self):
@@ -139,6 +149,18 @@ class NonLinearPlace(nn.Module):
         self.op_collections = build_ops(params, design, self.data_collections)
 
     def __call__(self, params=None, design=None, max_iterations=None, callback=None):
+        gen = self.run_gen(params, design, max_iterations, callback)
+        try:
+            while True:
+                next(gen)
+        except StopIteration as stop:
+            return stop.value
+
+    def run_gen(self, params=None, design=None, max_iterations=None, callback=None):
+        """The GP loop as a generator: with the graph engine it yields once per
+        iteration, after enqueuing the iteration's first trial, so that a batch
+        driver can interleave several designs (each on its own stream); the
+        return value is __call__'s."""
         params = params or self.params
         design = design or self.design
         torch.manual_seed(params.random_seed)
@@ -205,7 +227,10 @@ class NonLinearPlace(nn.Module):
                         stop_placement = True
                         logger.error("possible DIVERGENCE detected, roll back to the best position recorded")
                     t0 = time.time()
-                    h, o, md, obj = stepper.step(iteration == 0)
+                    if hasattr(stepper, "step_gen"):
+                        h, o, md, obj = yield from stepper.step_gen(iteration == 0)
+                    else:
+                        h, o, md, obj = stepper.step(iteration == 0)
                     cur = EvalMetrics(iteration, h, o, md, obj)
                     lsub.append(cur)
                     if best["metric"] is None or best["metric"].overflow > o:

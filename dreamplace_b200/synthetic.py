@@ -354,9 +354,3 @@ def config4(seed=1):
     """50k cells at 256x256 bins (finite-difference check design)."""
     return scaled(50_000, num_bins=256, seed=seed, name="config4")
 
-
-def batch_designs(count=64, seed=1, lo=5000, hi=200000):
-    """Batched-placement set: movable counts log-uniform in [lo, hi]."""
-    rng = np.random.RandomState(seed)
-    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).astype(np.int64)
-    return [scaled(int(c), seed=seed * 1000 + i, name=f"batch{i}") for i, c in enumerate(counts)]

@@ -44,3 +44,16 @@ def test_initial_positions_reference_rule():
     assert abs(pos[:m].mean() - 1500) < 1 and pos[:m].std() < 5
     assert np.all(pos[d.num_physical_nodes:n] <= d.xh - d.node_size_x[-1])
     assert np.array_equal(pos[m:d.num_physical_nodes], d.node_x[m:])
+
+
+def test_batch_partition_and_bins():
+    """Batched placement: every design lands on exactly one rank; bins follow
+    the nearest power of two of sqrt(cells), clamped to 64..512."""
+    from dreamplace_b200 import batch
+    for world in (1, 2, 3, 8):
+        seen = sorted(i for r in range(world) for i in batch.assign(64, r, world))
+        assert seen == list(range(64))
+    assert batch.bins_for(5000) == 64 and batch.bins_for(20000) == 128 and batch.bins_for(200000) == 512
+    ds = batch.batch_set(3, seed=2, lo=5000, hi=8000)
+    assert [d.name for d in ds] == ["batch0", "batch1", "batch2"]
+    assert all(5000 <= d.num_movable_nodes <= 8000 and d.num_bins_x == 64 for d in ds)
