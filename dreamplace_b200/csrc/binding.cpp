@@ -553,18 +553,25 @@ void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::
                         cur_stream()));
 }
 
-std::vector<at::Tensor> plan_net_lanes(at::Tensor netpin_start_cpu) {
+std::vector<at::Tensor> plan_net_lanes(at::Tensor netpin_start_cpu, c10::optional<at::Tensor> net_order_cpu) {
   TORCH_CHECK(!netpin_start_cpu.is_cuda() && netpin_start_cpu.scalar_type() == at::kInt,
               "netpin_start must be int32 on CPU");
   auto ns = netpin_start_cpu.contiguous();
   const int num_nets = ns.numel() - 1;
+  at::Tensor order;
+  if (net_order_cpu.has_value()) {
+    order = net_order_cpu->contiguous();
+    TORCH_CHECK(!order.is_cuda() && order.scalar_type() == at::kInt && order.numel() == num_nets,
+                "net_order must be int32 on CPU with one entry per net");
+  }
+  const int* op = order.defined() ? order.data_ptr<int>() : nullptr;
   int groups = 0, slots = 0;
-  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, &groups, &slots, nullptr, nullptr, nullptr, nullptr));
+  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, op, &groups, &slots, nullptr, nullptr, nullptr, nullptr));
   auto opt = ns.options();
   auto deg = at::empty({groups}, opt), base = at::empty({groups}, opt);
   auto net = at::empty({32 * (int64_t)groups}, opt), slot = at::empty({slots}, opt);
-  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, &groups, &slots, deg.data_ptr<int>(), base.data_ptr<int>(),
-                            net.data_ptr<int>(), slot.data_ptr<int>()));
+  DP_CALL(dp_plan_net_lanes(ns.data_ptr<int>(), num_nets, op, &groups, &slots, deg.data_ptr<int>(),
+                            base.data_ptr<int>(), net.data_ptr<int>(), slot.data_ptr<int>()));
   return {deg, base, net, slot};
 }
 
@@ -650,7 +657,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("assemble_precondition_step", &assemble_precondition_step);
   m.def("plan_net_chunks", &plan_net_chunks);
   m.def("wa_chunk_forward", &wa_chunk_forward);
-  m.def("plan_net_lanes", &plan_net_lanes);
+  m.def("plan_net_lanes", &plan_net_lanes, py::arg("netpin_start_cpu"), py::arg("net_order_cpu") = py::none());
   m.def("wa_lanes_forward", &wa_lanes_forward);
   m.def("hpwl_lanes", &hpwl_lanes);
   m.def("hpwl_chunk", &hpwl_chunk);

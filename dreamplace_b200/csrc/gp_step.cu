@@ -17,6 +17,7 @@
 //    and both step-size norms (fp64) are two streaming passes over the
 //    position / gradient vectors, and a one-thread kernel finishes the step
 //    size, the backtracking test and the momentum scalars on the device.
+#include <vector>
 #include <climits>
 #include "reduce.cuh"
 
@@ -291,53 +292,84 @@ __global__ void __launch_bounds__(256) precondition_norms_kernel(
 // g'[i] = (wirelength pin sum of node i, nodes < num_movable) + (force of node i,
 // movable and filler nodes, read from order space through inv_order); then
 // g' /= max(1, pws + lambda*area), and the fp64 step-size norms as above.
-__global__ void __launch_bounds__(256) assemble_precondition_kernel(
+// One block per tile of kAsmNodes consecutive nodes.  The tile's movable pins
+// form one contiguous node-CSR range; the block gathers it kAsmPins at a time
+// into shared memory (kAsmPins / 256 independent gathers per thread, all in
+// flight together), then each thread folds its own node's staged pins in pin
+// order, so the sums are those of the sequential per-node loop.
+constexpr int kAsmNodes = 256;
+constexpr int kAsmPins = 2048;
+
+__global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
     const float2* __restrict__ gnode, const int* __restrict__ node_start, const float* __restrict__ wl_scale_p,
     const float2* __restrict__ force_o, const int* __restrict__ inv_order, int num_movable, int num_filler,
     const float* __restrict__ pws, const float* __restrict__ area, const float* __restrict__ lam_p, int num_nodes,
     const float* __restrict__ v_new, const float* __restrict__ v, const float* __restrict__ g,
     float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index) {
+  __shared__ int s_start[kAsmNodes + 1];
+  __shared__ float2 s_q[kAsmPins];
   const float lam = *lam_p;
   const float ws = *wl_scale_p;
+  const int t = threadIdx.x;
   double dv = 0.0, dg = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
+  for (int n0 = blockIdx.x * kAsmNodes; n0 < num_nodes; n0 += gridDim.x * kAsmNodes) {
+    const int i = n0 + t;
+    const bool valid = i < num_nodes;
+    // the node's own loads first: independent of the pin gather below
+    float2 f = make_float2(0.f, 0.f);
+    float pw = 0.f, ar = 0.f, vnx = 0.f, vny = 0.f, vx = 0.f, vy = 0.f, gx0 = 0.f, gy0 = 0.f;
+    if (valid) {
+      if (i < num_movable || i >= num_nodes - num_filler) f = force_o[__ldg(inv_order + i)];
+      pw = __ldg(pws + i);
+      ar = __ldg(area + i);
+      vnx = __ldcs(v_new + i);
+      vny = __ldcs(v_new + i + num_nodes);
+      vx = __ldcs(v + i);
+      vy = __ldcs(v + i + num_nodes);
+      gx0 = __ldcs(g + i);
+      gy0 = __ldcs(g + i + num_nodes);
+    }
     float sx = 0.f, sy = 0.f;
-    if (i < num_movable) {
-      const int k1 = node_start[i + 1];
-      // four pins at a time: their loads are issued together, the sum keeps
-      // the pin order
-      for (int k = node_start[i]; k < k1; k += 4) {
-        float2 q[4];
+    const int m_cnt = min(num_movable - n0, kAsmNodes);  // movable nodes of the tile (block-uniform)
+    if (m_cnt > 0) {
+      // m_cnt + 1 offsets (up to kAsmNodes + 1: one more than the threads)
+      if (t < m_cnt) s_start[t] = __ldg(node_start + n0 + t);
+      if (t == 0) s_start[m_cnt] = __ldg(node_start + n0 + m_cnt);
+      __syncthreads();
+      const int p0 = s_start[0], p1 = s_start[m_cnt];
+      const int my0 = t < m_cnt ? s_start[t] : 0, my1 = t < m_cnt ? s_start[t + 1] : 0;
+      for (int c0 = p0; c0 < p1; c0 += kAsmPins) {
+        float2 q[kAsmPins / kAsmNodes];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          q[t] = make_float2(0.f, 0.f);
-          if (k + t < k1) q[t] = grad_index ? gnode[__ldcs(grad_index + k + t)] : __ldcs(gnode + k + t);
+        for (int j = 0; j < kAsmPins / kAsmNodes; ++j) {
+          const int k = c0 + j * kAsmNodes + t;
+          q[j] = make_float2(0.f, 0.f);
+          if (k < p1) q[j] = grad_index ? gnode[__ldcs(grad_index + k)] : __ldcs(gnode + k);
         }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          if (k + t < k1) {
-            sx = fadd(sx, fmul(q[t].x, ws));
-            sy = fadd(sy, fmul(q[t].y, ws));
-          }
+        for (int j = 0; j < kAsmPins / kAsmNodes; ++j) s_q[j * kAsmNodes + t] = q[j];
+        __syncthreads();
+        const int ka = max(my0, c0), kb = min(my1, c0 + kAsmPins);
+        for (int k = ka; k < kb; ++k) {
+          const float2 w = s_q[k - c0];
+          sx = fadd(sx, fmul(w.x, ws));
+          sy = fadd(sy, fmul(w.y, ws));
         }
+        __syncthreads();  // s_q is refilled by the next chunk
       }
     }
-    float fx = 0.f, fy = 0.f;
-    if (i < num_movable || i >= num_nodes - num_filler) {
-      const float2 f = force_o[inv_order[i]];
-      fx = f.x;
-      fy = f.y;
+    if (valid) {
+      const float p = fmaxf(fadd(pw, fmul(lam, ar)), 1.0f);
+      const float gx = __fdiv_rn(fadd(sx, f.x), p);
+      const float gy = __fdiv_rn(fadd(sy, f.y), p);
+      __stcs(g_new + i, gx);
+      __stcs(g_new + i + num_nodes, gy);
+      const double a1 = (double)vnx - (double)vx, a2 = (double)vny - (double)vy;
+      const double b1 = (double)gx - (double)gx0, b2 = (double)gy - (double)gy0;
+      dv += a1 * a1 + a2 * a2;
+      dg += b1 * b1 + b2 * b2;
     }
-    const float p = fmaxf(fadd(pws[i], fmul(lam, area[i])), 1.0f);
-    const float gx = __fdiv_rn(fadd(sx, fx), p);
-    const float gy = __fdiv_rn(fadd(sy, fy), p);
-    const int j = i + num_nodes;
-    g_new[i] = gx;
-    g_new[j] = gy;
-    const double a1 = (double)v_new[i] - (double)v[i], a2 = (double)v_new[j] - (double)v[j];
-    const double b1 = (double)gx - (double)g[i], b2 = (double)gy - (double)g[j];
-    dv += a1 * a1 + a2 * a2;
-    dg += b1 * b1 + b2 * b2;
+    __syncthreads();  // s_start is rewritten by the next tile
   }
   block_partial2(dv, dg, partials);
 }
@@ -855,10 +887,10 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   DP_REQUIRE(num_nodes > 0 && num_movable >= 0 && num_filler >= 0 && num_movable + num_filler <= num_nodes,
              "dp_assemble_precondition_step: bad node counts");
   cudaStream_t s = as_stream(stream);
-  int blocks = grid_for(num_nodes, 256, 4);
+  int blocks = grid_for(num_nodes, kAsmNodes, 4);
   if (blocks > DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
-  assemble_precondition_kernel<<<blocks, 256, 0, s>>>(
+  assemble_precondition_kernel<<<blocks, kAsmNodes, 0, s>>>(
       reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
       inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index);
   int rc = check_launch("dp_assemble_precondition_step");
@@ -1110,16 +1142,26 @@ __global__ void __launch_bounds__(256, 3) wa_lane_kernel(LaneArgs A, double* __r
 
 }  // namespace dpb
 
-extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int* num_groups, int* num_lane_slots,
-                                 int* group_deg, int* group_base, int* group_net, int* lane_slot) {
+extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, const int* net_order_host,
+                                 int* num_groups, int* num_lane_slots, int* group_deg, int* group_base,
+                                 int* group_net, int* lane_slot) {
   using namespace dpb;
   DP_REQUIRE(netpin_start_host && num_groups && num_lane_slots && num_nets >= 0, "dp_plan_net_lanes: bad arguments");
+  if (net_order_host) {  // must be a permutation: every net planned exactly once
+    std::vector<unsigned char> seen(num_nets, 0);
+    for (int t = 0; t < num_nets; ++t) {
+      const int e = net_order_host[t];
+      DP_REQUIRE(e >= 0 && e < num_nets && !seen[e], "dp_plan_net_lanes: net_order is not a permutation");
+      seen[e] = 1;
+    }
+  }
   const bool fill = group_deg && group_base && group_net && lane_slot;
   int g = 0;
   long long base = 0;
   for (int d = 1; d <= kLaneDeg; ++d) {
     int in_group = 0;
-    for (int e = 0; e < num_nets; ++e) {
+    for (int t = 0; t < num_nets; ++t) {
+      const int e = net_order_host ? net_order_host[t] : t;
       const int s0 = netpin_start_host[e];
       if (netpin_start_host[e + 1] - s0 != d) continue;
       if (in_group == 0) {
@@ -1145,7 +1187,8 @@ extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int
       base += 32 * d;
     }
   }
-  for (int e = 0; e < num_nets; ++e) {
+  for (int t = 0; t < num_nets; ++t) {
+    const int e = net_order_host ? net_order_host[t] : t;
     const int s0 = netpin_start_host[e], d = netpin_start_host[e + 1] - s0;
     if (d <= kLaneDeg) continue;
     if (fill) {

@@ -20,6 +20,9 @@ is summed in the spectral domain by the second launch's epilogue,
   sum_xy rho IDCT2(a winv) = M N sum_uv w_u w_v winv_uv a_uv^2 (w_0 = 1/2),
 so the potential map is never formed.
 Backward: the hand-written adjoint ``-electric_force`` (reference :219-275).
+With ``recompute_field`` the forward runs only the first two launches (the
+energy) and keeps the normalised density map; the backward repeats the solve
+for the field maps, so no field map is held between forward and backward.
 """
 import logging
 import math
@@ -54,16 +57,13 @@ def poisson_flops(M, N, precision):
     return 3 * k * 2.0 * M * N * (M + N)
 
 
-def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
-    """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
-
-    Returns (field_map_x, field_map_y, energy_f64[1]); energy is zero when
-    ``fast_mode``.  Four GEMM launches, see the module docstring."""
-    prec = precision_code(precision)
+def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy):
+    """G1 and G2 of the solve: the two spectral operands a*wx, a*wy [M, N];
+    when ``energy`` (f64[1]) is given the G2 epilogue adds the energy to it."""
     M, N = rho.shape
     dev = rho.device
-    cM, chM, shM = transform_matrices(M, prec, dev)
-    cN, chN, shN = transform_matrices(N, prec, dev)
+    cM = transform_matrices(M, prec, dev)[0]
+    cN = transform_matrices(N, prec, dev)[0]
     # G1: T1^T = (rho C_N^T)^T, [N, M]
     t1 = Operand((N, M), prec, dev)
     g1 = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=1.0, ldc=M)
@@ -77,12 +77,11 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
     # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy  [M, N]; the energy
     # sum(rho * IDCT2(a*winv)) = MN sum w_u w_v winv a^2 is summed in the same
     # epilogue, so the potential map is never formed
-    energy = torch.zeros(1, dtype=torch.float64, device=dev)
     spec = [Operand((M, N), prec, dev) for _ in range(2)]
     g2 = dict(lda=M, ldb=M, epilogue=EPI_SPECTRAL, alpha=4.0 / (M * N), ldc=N,
               wv_scale=float(bin_size_x / bin_size_y),
               spec_weights=spectral_tables(M, N, float(bin_size_x / bin_size_y), dev))
-    if not fast_mode:
+    if energy is not None:
         g2["energy"] = energy
     cM.as_a(g2)
     t1.as_b(g2)
@@ -93,6 +92,29 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
             g2["sp%d_hi" % i] = s.hi
             g2["sp%d_lo" % i] = s.lo
     C.transform_gemm(prec, M, N, M, [g2])
+    return spec
+
+
+def poisson_energy(rho, bin_size_x, bin_size_y, precision):
+    """Energy (f64[1]) of a normalised density map without the field maps:
+    G1 and G2 only (two launches)."""
+    energy = torch.zeros(1, dtype=torch.float64, device=rho.device)
+    _poisson_spectral(rho, bin_size_x, bin_size_y, precision_code(precision), energy)
+    return energy
+
+
+def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
+    """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
+
+    Returns (field_map_x, field_map_y, energy_f64[1]); energy is zero when
+    ``fast_mode``.  Four GEMM launches, see the module docstring."""
+    prec = precision_code(precision)
+    M, N = rho.shape
+    dev = rho.device
+    _, chM, shM = transform_matrices(M, prec, dev)
+    _, chN, shN = transform_matrices(N, prec, dev)
+    energy = torch.zeros(1, dtype=torch.float64, device=dev)
+    spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy)
     # G3: U^T = (A R^T)^T for the x field (R = Ch_N) and the y field (Sh_N)
     rights = [chN, shN]
     us = [Operand((N, M), prec, dev) for _ in spec]
@@ -252,7 +274,7 @@ class ElectricPotentialFunction(Function):
                 num_filler_impacted_bins_y, deterministic_flag, sorted_node_map, exact_expkM=None,
                 exact_expkN=None, inv_wu2_plus_wv2=None, wu_by_wu2_plus_wv2_half=None,
                 wv_by_wu2_plus_wv2_half=None, dct2=None, idct2=None, idct_idxst=None, idxst_idct=None,
-                fast_mode=True, precision="fp32"):
+                fast_mode=True, precision="fp32", recompute_field=False):
         density_map = ElectricDensityMapFunction.forward(
             pos, node_size_x_clamped, node_size_y_clamped, offset_x, offset_y, ratio, bin_center_x,
             bin_center_y, initial_density_map, target_density, xl, yl, xh, yh, bin_size_x, bin_size_y,
@@ -268,10 +290,17 @@ class ElectricPotentialFunction(Function):
         ctx.sorted_node_map = sorted_node_map
         ctx.pos = pos
         density_map.mul_(1.0 / (bin_size_x * bin_size_y))
-        ex, ey, energy = poisson_solve(density_map, bin_size_x, bin_size_y, precision, fast_mode)
-        ctx.field_map_x = ex
-        ctx.field_map_y = ey
+        ctx.precision = precision
         ctx.density_map = density_map
+        if recompute_field:
+            # keep only rho; the backward recomputes the field maps
+            energy = torch.zeros(1, dtype=torch.float64, device=pos.device) if fast_mode else \
+                poisson_energy(density_map, bin_size_x, bin_size_y, precision)
+            ctx.field_map_x = ctx.field_map_y = None
+        else:
+            ex, ey, energy = poisson_solve(density_map, bin_size_x, bin_size_y, precision, fast_mode)
+            ctx.field_map_x = ex
+            ctx.field_map_y = ey
         if fast_mode:
             return torch.zeros(1, dtype=pos.dtype, device=pos.device)
         return energy.to(pos.dtype).view([])
@@ -282,11 +311,14 @@ class ElectricPotentialFunction(Function):
         sxc, syc, ox, oy, ratio, bcx, bcy = ctx.node
         xl, yl, xh, yh, bsx, bsy, nm, nf = ctx.geom
         g = grad_pos.reshape(1).to(torch.float32)
-        output = C.electric_force(g, nbx, nby, a, b, c, d, ctx.field_map_x.view([-1]), ctx.field_map_y.view([-1]),
+        fx, fy = ctx.field_map_x, ctx.field_map_y
+        if fx is None:
+            fx, fy, _ = poisson_solve(ctx.density_map, bsx, bsy, ctx.precision, True)
+        output = C.electric_force(g, nbx, nby, a, b, c, d, fx.view([-1]), fy.view([-1]),
                                   ctx.pos, sxc, syc, ox, oy, ratio, bcx, bcy, float(xl), float(yl), float(xh),
                                   float(yh), float(bsx), float(bsy), int(nm), int(nf),
                                   int(bool(ctx.deterministic_flag)), ctx.sorted_node_map, -1.0)
-        return (output,) + (None,) * 38
+        return (output,) + (None,) * 39
 
 
 class ElectricPotential(ElectricOverflow):
@@ -295,7 +327,8 @@ class ElectricPotential(ElectricOverflow):
     def __init__(self, node_size_x, node_size_y, bin_center_x, bin_center_y, target_density, xl, yl, xh, yh,
                  bin_size_x, bin_size_y, num_movable_nodes, num_terminals, num_filler_nodes, padding,
                  deterministic_flag, sorted_node_map, movable_macro_mask=None, fast_mode=False, region_id=None,
-                 fence_regions=None, node2fence_region_map=None, placedb=None, precision="fp32"):
+                 fence_regions=None, node2fence_region_map=None, placedb=None, precision="fp32",
+                 recompute_field=False):
         if region_id is not None or fence_regions is not None:
             raise NotImplementedError("fence-region electric fields are not supported by dreamplace_b200")
         super().__init__(node_size_x=node_size_x, node_size_y=node_size_y, bin_center_x=bin_center_x,
@@ -306,6 +339,9 @@ class ElectricPotential(ElectricOverflow):
                          movable_macro_mask=movable_macro_mask)
         self.fast_mode = fast_mode
         self.precision = precision_code(precision)
+        # True: the forward keeps only the normalised density map and the
+        # backward recomputes the field maps (less memory held between the two)
+        self.recompute_field = recompute_field
         self.region_id = None
         self.fence_regions = None
 
@@ -335,7 +371,8 @@ class ElectricPotential(ElectricOverflow):
                 self.num_movable_impacted_bins_x, self.num_movable_impacted_bins_y,
                 self.num_filler_impacted_bins_x, self.num_filler_impacted_bins_y, self.deterministic_flag,
                 self.sorted_node_map, self.exact_expkM, self.exact_expkN, None, None, None, self.dct2,
-                self.idct2, self.idct_idxst, self.idxst_idct, self.fast_mode, self.precision)
+                self.idct2, self.idct_idxst, self.idxst_idct, self.fast_mode, self.precision,
+                self.recompute_field)
         density_map = self._density_map(pos, 0)
         bin_area = self.bin_size_x * self.bin_size_y
         out = C.density_overflow(density_map, float(self.target_density * bin_area), float(bin_area))

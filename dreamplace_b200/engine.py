@@ -68,7 +68,9 @@ class GPEngine(object):
         self.gnode = torch.empty(2 * P, dtype=torch.float32, device=dev)
         # lane-per-net plan: nets of degree <= 8 grouped 32 at a time by degree,
         # pin arrays gathered into the transposed lane-slot order
-        g_deg, g_base, g_net, l_slot = C.plan_net_lanes(self.netpin_start.cpu())
+        self.net_order = getattr(params, "net_order", "locality")
+        order = self._net_locality_order() if self.net_order == "locality" else None
+        g_deg, g_base, g_net, l_slot = C.plan_net_lanes(self.netpin_start.cpu(), order)
         self.group_deg, self.group_base, self.group_net = g_deg.to(dev), g_base.to(dev), g_net.to(dev)
         ls = l_slot.to(dev).long()
         real = ls >= 0
@@ -167,6 +169,25 @@ class GPEngine(object):
         self.trials = 0
         self.last_energy = None
         self._quad_c = 0.0
+
+    def _net_locality_order(self):
+        """Nets ordered by the median node index of their pins (CPU int32
+        permutation for the lane planner).  Nets whose pins sit on nearby nodes
+        then share lane groups and neighbouring lane slots, so the WA kernel's
+        position gathers and the assembly's gradient gather stay local; the
+        median ignores a net's few far-away pins."""
+        ns = self.netpin_start.long()
+        num_nets = ns.numel() - 1
+        deg = ns[1:] - ns[:-1]
+        if num_nets == 0 or int(ns[-1]) == 0:
+            return None
+        span = int(self.design.num_nodes) + 1
+        net_of_slot = torch.repeat_interleave(torch.arange(num_nets, device=ns.device), deg)
+        key = torch.sort(net_of_slot * span + self.slot_node.long()).values
+        mid = (ns[:-1] + deg // 2).clamp(max=key.numel() - 1)
+        median = key[mid] - torch.arange(num_nets, device=ns.device) * span
+        median = torch.where(deg > 0, median, torch.zeros_like(median))
+        return torch.argsort(median, stable=True).to(torch.int32).cpu()
 
     # ---------------------------------------------------------------- pieces
     def _build_records(self):

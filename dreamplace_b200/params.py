@@ -1,6 +1,7 @@
 """Global-placement parameters with the reference's defaults
 (dreamplace/params.json; dreamplace/Params.py:19-34, 119-138), restricted to
-the keys the global-placement hot path reads, plus ``dct_precision``."""
+the keys the global-placement hot path reads, plus ``dct_precision`` and
+``recompute_field``."""
 import copy
 import json
 
@@ -29,6 +30,9 @@ DEFAULTS = {
     "dtype": "float32",
     # Poisson-solve arithmetic of this implementation: fp32 | tf32 | bf16 | split_bf16
     "dct_precision": "split_bf16",
+    # autograd path: 1 keeps only the density map between the electric
+    # potential's forward and backward and recomputes the field maps there
+    "recompute_field": 0,
 }
 
 

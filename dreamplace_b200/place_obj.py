@@ -222,7 +222,7 @@ class PlaceObj(nn.Module):
             num_terminals=design.num_terminals, num_filler_nodes=design.num_filler_nodes, padding=0,
             deterministic_flag=params.deterministic_flag, sorted_node_map=data.sorted_node_map,
             movable_macro_mask=data.movable_macro_mask, fast_mode=bool(params.RePlAce_skip_energy_flag),
-            precision=params.dct_precision)
+            precision=params.dct_precision, recompute_field=bool(getattr(params, "recompute_field", 0)))
 
     def initialize_density_weight(self, params, design):
         """lambda0 = density_weight * |grad WL|_1 / |grad D|_1 (reference PlaceObj.py:767-825)."""

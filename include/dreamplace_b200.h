@@ -399,15 +399,19 @@ int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const fl
                   const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
                   const float* net_weights, const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
 /* Lane-per-net plan (host): nets of degree 1..8 grouped 32 at a time by degree,
- * in net order within a degree; each larger net a group of its own.  Call with
+ * in the order net_order_host gives (a permutation of the nets; NULL: net
+ * index order) within a degree; each larger net a group of its own.  The
+ * order only places the nets in memory: ordering nets by where their pins
+ * live in the node arrays makes the pin-position gathers and the gradient
+ * gather of the assembly local.  Call with
  * NULL group_deg / group_base / group_net / lane_slot to get *num_groups and
  * *num_lane_slots, then with buffers of those sizes (group_net: 32 per group).
  * Group g of degree d <= 8 stores pin j of lane l at lane slot
  * group_base[g] + 32 j + l; a larger net stores its pins contiguously from
  * group_base[g].  lane_slot maps lane slots to pin slots (flat_netpin order),
  * -1 for padding; group_net holds net ids, -1 for padding lanes. */
-int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, int* num_groups, int* num_lane_slots,
-                      int* group_deg, int* group_base, int* group_net, int* lane_slot);
+int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, const int* net_order_host, int* num_groups,
+                      int* num_lane_slots, int* group_deg, int* group_base, int* group_net, int* lane_slot);
 /* WA forward over a lane plan: one warp per group, one lane per net (degree
  * <= 8, pins in registers, the reference's per-net loops in pin order) or the
  * whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the

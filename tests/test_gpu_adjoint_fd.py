@@ -205,3 +205,28 @@ def test_density_adjoint_against_fd_and_reference(setup):
     assert cos > 0.9, cos
     assert abs(scale - 1.0) < 0.25, scale
     del base
+
+
+@pytest.mark.parametrize("precision", ["fp32", "split_bf16"])
+def test_recomputed_field_matches_stored(setup, precision):
+    """recompute_field=True (forward keeps only rho, backward repeats the
+    solve) gives the stored-field gradient bit for bit and the same energy."""
+    from dreamplace_b200.electric_potential import ElectricPotential
+    d, pos_np, _ = setup
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    m = d.num_movable_nodes
+    sorted_map = t(np.argsort(d.node_size_x[:m], kind="stable").astype(np.int32))
+    out = []
+    for recompute in (False, True):
+        op = ElectricPotential(t(d.node_size_x), t(d.node_size_y), t(d.bin_centers(d.xl, d.xh, d.bin_size_x)),
+                               t(d.bin_centers(d.yl, d.yh, d.bin_size_y)), d.target_density, d.xl, d.yl, d.xh,
+                               d.yh, d.bin_size_x, d.bin_size_y, m, d.num_terminals, d.num_filler_nodes, 0, True,
+                               sorted_map, fast_mode=False, precision=precision, recompute_field=recompute)
+        pos = t(pos_np).requires_grad_(True)
+        energy = op(pos)
+        energy.backward()
+        out.append((float(energy), pos.grad.clone()))
+    (e0, g0), (e1, g1) = out
+    assert torch.equal(g0, g1)
+    assert abs(e0 - e1) <= 1e-6 * abs(e0), (e0, e1)

@@ -411,6 +411,51 @@ def test_ordered_force_and_fused_assembly(C, golden):
     np.testing.assert_allclose(st_got[:8].cpu().numpy(), st_ref[:8].cpu().numpy(), rtol=1e-12)
 
 
+def test_fused_assembly_long_pin_ranges(C):
+    """The assembly's staged gather on node tiles whose pins overflow one
+    shared-memory chunk (nodes of up to 5000 pins, ranges crossing chunk
+    edges, nodes without pins, fixed nodes between movable and filler ones):
+    bit-exact with the separate pin-sum and precondition kernels."""
+    rng = np.random.RandomState(11)
+    m, nfix, nf = 3000, 40, 700
+    n = m + nfix + nf
+    deg = rng.randint(0, 7, size=n)
+    deg[rng.choice(m, 12, replace=False)] = rng.randint(1500, 5000, size=12)
+    deg[m:m + nfix] = rng.randint(0, 20, size=nfix)
+    deg[m + nfix:] = 0
+    start = np.zeros(n + 1, np.int64)
+    np.cumsum(deg, out=start[1:])
+    P = int(start[-1])
+    node_start = dev(start.astype(np.int32))
+    gnode = dev(rng.standard_normal(2 * P).astype(np.float32))
+    grad = torch.tensor([0.37], device="cuda")
+    pws = dev(rng.uniform(0, 5, n).astype(np.float32))
+    area = dev(rng.uniform(0, 400, n).astype(np.float32))
+    lam = torch.tensor([1e-2], device="cuda")
+    v = dev(rng.standard_normal(2 * n).astype(np.float32))
+    v_new = v + dev(rng.standard_normal(2 * n).astype(np.float32))
+    g_old = dev(rng.standard_normal(2 * n).astype(np.float32))
+    inv = dev(rng.permutation(m + nf).astype(np.int32))
+    inv_full = torch.zeros(n, dtype=torch.int32, device="cuda")
+    inv_full[:m] = inv[:m]
+    inv_full[m + nfix:] = inv[m:]
+    force_o = dev(rng.standard_normal(2 * (m + nf)).astype(np.float32))
+    fo = force_o.view(-1, 2)
+    exp = torch.zeros(2 * n, device="cuda")
+    mov_or_fill = torch.cat([torch.arange(m), torch.arange(m + nfix, n)]).cuda()
+    exp[mov_or_fill] = fo[inv_full[mov_or_fill].long(), 0]
+    exp[n + mov_or_fill] = fo[inv_full[mov_or_fill].long(), 1]
+    C.node_pin_sum(gnode, node_start, grad, m, 1, exp)
+    st_ref = torch.zeros(8 + 2 * 1280, dtype=torch.float64, device="cuda")
+    C.precondition_step_size(exp, g_old, v_new, v, pws, area, lam, st_ref)
+    st_got = torch.zeros_like(st_ref)
+    got = torch.empty(2 * n, device="cuda")
+    C.assemble_precondition_step(gnode, node_start, grad, force_o, inv_full, m, nf, pws, area, lam, v_new, v, g_old,
+                                 got, st_got, None)
+    assert torch.equal(got, exp)
+    np.testing.assert_allclose(st_got[:8].cpu().numpy(), st_ref[:8].cpu().numpy(), rtol=1e-12)
+
+
 def test_ordered_split_scatter(C):
     """Two maps from one pass (movable prefix, all cells): bit-exact with two
     separate fixed-point scatters; fp32 within atomic-order tolerance."""
@@ -450,8 +495,9 @@ def test_ordered_split_scatter(C):
             torch.testing.assert_close(full, exp_full, rtol=1e-4, atol=tol)
 
 
-def lane_inputs(C, d):
-    """Slot (flat_netpin) arrays, node-CSR positions and the lane plan of a design."""
+def lane_inputs(C, d, net_order=None):
+    """Slot (flat_netpin) arrays, node-CSR positions and the lane plan of a design
+    (nets placed in ``net_order``, a permutation; None: index order)."""
     P = d.num_pins
     fnp = d.flat_net2pin_map.astype(np.int64)
     slot_of_pin = np.empty(P, np.int64)
@@ -459,7 +505,9 @@ def lane_inputs(C, d):
     node_slots = slot_of_pin[d.flat_node2pin_map]
     csr_pos = np.empty(P, np.int64)
     csr_pos[node_slots] = np.arange(P)
-    g_deg, g_base, g_net, l_slot = C.plan_net_lanes(torch.from_numpy(d.flat_net2pin_start_map.astype(np.int32)))
+    g_deg, g_base, g_net, l_slot = C.plan_net_lanes(torch.from_numpy(d.flat_net2pin_start_map.astype(np.int32)),
+                                                    None if net_order is None else
+                                                    torch.from_numpy(net_order.astype(np.int32)))
     ls = l_slot.numpy().astype(np.int64)
     real = ls >= 0
     ls = np.where(real, ls, 0)
@@ -511,3 +559,26 @@ def test_wa_lanes_against_reference(C, golden, weighted):
     alone = torch.zeros(1280, dtype=torch.float64, device="cuda")
     C.hpwl_lanes(xy, *plan, dev(weights), mask, alone)
     assert alone[0].item() == hp[0].item()  # same plan, same summation order
+
+
+def test_wa_lanes_net_order_invariant(C, golden):
+    """The planner's net order only moves nets in memory: every pin gradient
+    is bit-identical under a shuffled order (each net's loops run the same),
+    the fp64 totals agree to rounding."""
+    g = golden("design_small.npz")
+    d = small_design()
+    n, P = d.num_nodes, d.num_pins
+    xy = pack_xy(g["pos"].astype(np.float32), n)
+    mask = dev(g["net_mask"])
+    inv_gamma = torch.tensor([float(g["inv_gamma"])], device="cuda")
+    out = []
+    for order in (None, np.random.RandomState(3).permutation(d.num_nets)):
+        plan, ln_csr, csr_pos, slot_of_pin, _ = lane_inputs(C, d, order)
+        wl = torch.zeros(1280, dtype=torch.float64, device="cuda")
+        hp = torch.zeros(1280, dtype=torch.float64, device="cuda")
+        gnode = torch.empty(2 * P, device="cuda")
+        C.wa_lanes_forward(xy, *plan[:3], *plan[3:], ln_csr, None, mask, inv_gamma, wl, gnode, mask, hp)
+        out.append((gnode.cpu().numpy().reshape(-1, 2)[csr_pos[slot_of_pin]], wl[0].item(), hp[0].item()))
+    (g0, w0, h0), (g1, w1, h1) = out
+    assert np.array_equal(g0, g1)
+    assert math.isclose(w0, w1, rel_tol=1e-12) and math.isclose(h0, h1, rel_tol=1e-12)
