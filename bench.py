@@ -317,11 +317,12 @@ def kernel_roofline(placer, design, peaks, reps=20):
     eng = placer.stepper.eng
     ep = eng.ep
     work = piece_work(design, eng)
-    p = eng.parity
-    q = 1 - p
+    p = eng.slot
+    q = eng.next_slot(p)
     v, g = eng.V[p], eng.G[p]
     vn, gn = eng.V[q], eng.G[q]
-    saved = eng.state.clone()
+    torch.cuda.synchronize()  # the iteration enqueued ahead writes the slot after q
+    saved = eng.S[p].clone()
     t = {}
     t["density_scatter"] = _graph_time(lambda: eng.scatter_maps(v, eng.O[q]), reps)
     rho = eng.dmap.mul(1.0 / (ep.bin_size_x * ep.bin_size_y))
@@ -331,7 +332,7 @@ def kernel_roofline(placer, design, peaks, reps=20):
     t["wa_forward"] = _graph_time(lambda: eng.wirelength(v, eng.H[q]), reps)
     t["assemble_precondition"] = _graph_time(lambda: eng.assemble(v, g, vn, gn), reps)
     t["nesterov_trial"] = _graph_time(lambda: eng.nesterov_trial_only(p), reps)
-    eng.state.copy_(saved)
+    eng.S[p].copy_(saved)
     return {k: (t[k],) + work[k] for k in t}
 
 

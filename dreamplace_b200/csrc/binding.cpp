@@ -397,6 +397,40 @@ void precondition_step_size(at::Tensor g_new, at::Tensor g, at::Tensor v_new, at
 
 void nesterov_advance(at::Tensor state) { DP_CALL(dp_nesterov_advance(ptr<double>(state), cur_stream())); }
 
+void iteration_head(at::Tensor state_prev, at::Tensor state_new, at::Tensor sched_prev, at::Tensor sched_new,
+                    at::Tensor hpwl_k, at::Tensor overflow_k, at::Tensor weights_prev, at::Tensor weights_new,
+                    double base_gamma, double total_area, double ref_hpwl, double lower, double upper,
+                    c10::optional<at::Tensor> gate) {
+  TORCH_CHECK(state_prev.scalar_type() == at::kDouble && state_new.scalar_type() == at::kDouble &&
+                  sched_prev.scalar_type() == at::kDouble && sched_new.scalar_type() == at::kDouble &&
+                  hpwl_k.scalar_type() == at::kDouble && overflow_k.scalar_type() == at::kDouble,
+              "iteration_head: state, sched and metrics must be float64");
+  TORCH_CHECK(state_prev.numel() >= DP_NESTEROV_STATE_DOUBLES && state_new.numel() >= DP_NESTEROV_STATE_DOUBLES &&
+                  sched_prev.numel() >= 2 && sched_new.numel() >= 2 && weights_prev.numel() >= 3 &&
+                  weights_new.numel() >= 3,
+              "iteration_head: buffers too small");
+  CHECK_F32(weights_prev); CHECK_F32(weights_new);
+  DP_CALL(dp_iteration_head(ptr<double>(state_prev), ptr<double>(state_new), ptr<double>(sched_prev),
+                            ptr<double>(sched_new), ptr<double>(hpwl_k), ptr<double>(overflow_k),
+                            ptr<float>(weights_prev), ptr<float>(weights_new), base_gamma, total_area, ref_hpwl,
+                            lower, upper, gate.has_value() ? ptr<int>(*gate) : nullptr, cur_stream()));
+}
+
+// the installed gate word must stay alive while graphs captured with it exist
+void set_trial_gate(c10::optional<at::Tensor> gate) {
+  if (gate.has_value()) {
+    CHECK_I32(*gate);
+    TORCH_CHECK(gate->is_cuda(), "trial gate must be a CUDA tensor");
+  }
+  DP_CALL(dp_set_trial_gate(gate.has_value() ? ptr<int>(*gate) : nullptr));
+}
+
+void trial_gate(at::Tensor gate, c10::optional<at::Tensor> accept_prev) {
+  CHECK_I32(gate);
+  DP_CALL(dp_trial_gate(ptr<int>(gate), accept_prev.has_value() ? ptr<double>(*accept_prev) : nullptr,
+                        cur_stream()));
+}
+
 void objective_finish(at::Tensor wl, at::Tensor energy, at::Tensor density_weight, at::Tensor factor_quad,
                       at::Tensor obj, at::Tensor grad_scale) {
   CHECK_F32(factor_quad);
@@ -645,6 +679,12 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("nesterov_trial", &nesterov_trial);
   m.def("precondition_step_size", &precondition_step_size);
   m.def("nesterov_advance", &nesterov_advance);
+  m.def("iteration_head", &iteration_head, py::arg("state_prev"), py::arg("state_new"), py::arg("sched_prev"),
+        py::arg("sched_new"), py::arg("hpwl_k"), py::arg("overflow_k"), py::arg("weights_prev"),
+        py::arg("weights_new"), py::arg("base_gamma"), py::arg("total_area"), py::arg("ref_hpwl"), py::arg("lower"),
+        py::arg("upper"), py::arg("gate") = py::none());
+  m.def("set_trial_gate", &set_trial_gate);
+  m.def("trial_gate", &trial_gate, py::arg("gate"), py::arg("accept_prev") = py::none());
   m.def("pack_xy", &pack_xy);
   m.def("objective_finish", &objective_finish);
   m.def("density_map_into", &density_map_into);

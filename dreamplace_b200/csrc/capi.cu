@@ -6,6 +6,13 @@ namespace dpb {
 
 static thread_local char g_err[1024] = "";
 static std::atomic<uint64_t> g_launches{0};
+static const int* g_trial_gate = nullptr;
+
+const int* trial_gate() { return g_trial_gate; }
+
+__global__ void trial_gate_kernel(int* gate, const double* accept_prev) {
+  *gate = accept_prev ? (*accept_prev == 0.0 ? 1 : 0) : 0;
+}
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -32,5 +39,14 @@ int launch_finish_sum(double* buf, int count, float* out_f32, cudaStream_t s) {
 }  // namespace dpb
 
 extern "C" const char* dp_last_error(void) { return dpb::g_err; }
+extern "C" int dp_set_trial_gate(const int* gate) {
+  dpb::g_trial_gate = gate;
+  return DP_OK;
+}
+extern "C" int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t stream) {
+  DP_REQUIRE(gate, "dp_trial_gate: null gate");
+  dpb::trial_gate_kernel<<<1, 1, 0, dpb::as_stream(stream)>>>(gate, accept_prev);
+  return dpb::check_launch("dp_trial_gate");
+}
 extern "C" int dp_version(void) { return 1; }
 extern "C" uint64_t dp_launch_count(void) { return dpb::g_launches.load(std::memory_order_relaxed); }

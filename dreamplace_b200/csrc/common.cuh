@@ -20,6 +20,13 @@ constexpr int kNumSMs = 148;  // B200
 void set_error(const char* fmt, ...);
 void count_launch(int n = 1);
 
+// Trial gate (dp_set_trial_gate): the device word that the heavy kernels of a
+// GP trial receive while a gate is installed on the host; such a kernel returns
+// at once when the word is non-zero (a trial enqueued ahead whose predecessor
+// was rejected, to be enqueued again).  nullptr when no gate is installed.
+const int* trial_gate();
+__device__ __forceinline__ bool gate_closed(const int* gate) { return gate != nullptr && *gate != 0; }
+
 inline cudaStream_t as_stream(dp_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
 inline int check_launch(const char* what) {

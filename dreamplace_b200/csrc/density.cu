@@ -171,7 +171,9 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
                                                                         const float4* __restrict__ rec4,
                                                                         const float* __restrict__ ratio_o, int count,
                                                                         float fx_scale, float* map_f32,
-                                                                        unsigned long long* map_fx) {
+                                                                        unsigned long long* map_fx,
+                                                                        const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   extern __shared__ __align__(16) unsigned char tile_raw[];
   using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
   Acc* tile = reinterpret_cast<Acc*>(tile_raw);
@@ -384,7 +386,8 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
 }
 
 __global__ void gather_order_xy_kernel(const float2* __restrict__ xy, const int* __restrict__ order, int count,
-                                       float2* __restrict__ xy_o) {
+                                       float2* __restrict__ xy_o, const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
     xy_o[idx] = xy[order[idx]];
 }
@@ -411,7 +414,9 @@ __global__ void fixed_to_float_kernel(const long long* fixed, const float* init,
   }
 }
 
-__global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n4) {
+__global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n4,
+                            const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x)
     dst[i] = src[i];
 }
@@ -419,7 +424,7 @@ __global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__
 static int copy_map(const float* src, float* dst, int n, cudaStream_t s) {
   if (src == dst) return DP_OK;
   if ((n & 3) == 0 && ((uintptr_t)src & 15) == 0 && ((uintptr_t)dst & 15) == 0) {
-    copy_kernel<<<grid_for(n / 4, 256), 256, 0, s>>>((const float4*)src, (float4*)dst, n / 4);
+    copy_kernel<<<grid_for(n / 4, 256), 256, 0, s>>>((const float4*)src, (float4*)dst, n / 4, trial_gate());
     return check_launch("copy_map");
   }
   cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
@@ -561,7 +566,9 @@ __global__ void overflow_kernel(const float* __restrict__ map, int n, double tar
 // reduces its overflow sum and maximum as overflow_kernel does.
 __global__ void first_map_kernel(const long long* __restrict__ fixed, const float* __restrict__ init,
                                  double inv_scale, float* first, float* __restrict__ copy_to, int n,
-                                 double target_area, double* partials, unsigned* maxkey) {
+                                 double target_area, double* partials, unsigned* maxkey,
+                                 const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   double s = 0.0;
   float m = -INFINITY;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -747,7 +754,7 @@ extern "C" int dp_gather_order_xy(const float* xy, const int* order, int count, 
   DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)xy_o & 7) == 0, "dp_gather_order_xy: misaligned xy / xy_o");
   if (count == 0) return DP_OK;
   gather_order_xy_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
-      reinterpret_cast<const float2*>(xy), order, count, reinterpret_cast<float2*>(xy_o));
+      reinterpret_cast<const float2*>(xy), order, count, reinterpret_cast<float2*>(xy_o), trial_gate());
   return check_launch("dp_gather_order_xy");
 }
 
@@ -794,10 +801,11 @@ int scatter_range_r(const OrderedScatter& o, int begin, int end, int determinist
   if (deterministic)
     window_scatter_kernel<true, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
         o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits),
-        nullptr, reinterpret_cast<unsigned long long*>(scratch));
+        nullptr, reinterpret_cast<unsigned long long*>(scratch), trial_gate());
   else
     window_scatter_kernel<false, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr);
+        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr,
+        trial_gate());
   return check_launch("dp_density_map_ordered scatter");
 }
 
@@ -898,7 +906,8 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4
     if (overflow_out) {
       cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
       first_map_kernel<<<blocks, 256, 0, o.s>>>((const long long*)scratch, init, ldexp(1.0, -fraction_bits),
-                                                 out_first, nullptr, nbins, target_area, overflow_out + 3, maxslot);
+                                                 out_first, nullptr, nbins, target_area, overflow_out + 3, maxslot,
+                                                 trial_gate());
       rc = check_launch("dp_density_map_ordered_split first map");
       if (rc) return rc;
       overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
@@ -919,7 +928,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4
   if (overflow_out) {
     cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
     first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, nbins, target_area,
-                                               overflow_out + 3, maxslot);
+                                               overflow_out + 3, maxslot, trial_gate());
     rc = check_launch("dp_density_map_ordered_split first map");
     if (rc) return rc;
     overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,

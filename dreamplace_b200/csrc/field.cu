@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) electric_force_records_kernel(
     const float* __restrict__ grad_pos, int nbx, int nby, const float* __restrict__ ex, const float* __restrict__ ey,
     const float2* __restrict__ xy_o, const float4* __restrict__ rec4,
     const float* __restrict__ ratio_o, int count, float xl, float yl, float bsx, float bsy, float ibx, float iby,
-    float scale, float2* __restrict__ force_o) {
+    float scale, float2* __restrict__ force_o, const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   const float g = grad_pos[0];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
     const float4 r4 = __ldcs(rec4 + idx);
@@ -133,7 +134,7 @@ extern "C" int dp_electric_force_ordered(const float* grad_pos, int nbx, int nby
   if (count == 0) return DP_OK;
   electric_force_records_kernel<<<grid_for(count, 256, 16), 256, 0, as_stream(stream)>>>(
       grad_pos, nbx, nby, ex, ey, reinterpret_cast<const float2*>(xy_o), reinterpret_cast<const float4*>(rec4),
-      ratio_o, count, xl, yl, bsx, bsy, ibx, iby, scale, reinterpret_cast<float2*>(force_o));
+      ratio_o, count, xl, yl, bsx, bsy, ibx, iby, scale, reinterpret_cast<float2*>(force_o), trial_gate());
   return check_launch("dp_electric_force_ordered");
 }
 

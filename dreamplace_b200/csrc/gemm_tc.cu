@@ -161,7 +161,10 @@ struct TcConfig {
 
 template <int PREC, int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcBatch batch, int M,
-                                                                 int N, int K) {
+                                                                 int N, int K, const int* __restrict__ gate) {
+  // a closed trial gate (dp_set_trial_gate): every thread of every CTA returns
+  // before any barrier, TMEM allocation or copy is set up
+  if (gate_closed(gate)) return;
   using Cfg = TcConfig<PREC, BN, STAGES>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -361,7 +364,7 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
     configured = true;
   }
   dim3 grid(ceil_div(N, BN), ceil_div(M, TC_BM), count);
-  kern<<<grid, TC_THREADS, Cfg::kSmemBytes, s>>>(batch, M, N, K);
+  kern<<<grid, TC_THREADS, Cfg::kSmemBytes, s>>>(batch, M, N, K, trial_gate());
   return check_launch("dp_transform_gemm(tcgen05)");
 }
 

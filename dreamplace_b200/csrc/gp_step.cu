@@ -237,7 +237,9 @@ __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* 
                                       const double* __restrict__ st, const float* __restrict__ sx,
                                       const float* __restrict__ sy, float xl, float yl, float xh, float yh,
                                       int num_nodes, int num_movable, int num_filler,
-                                      const int* __restrict__ inv_order, float2* __restrict__ xy_o) {
+                                      const int* __restrict__ inv_order, float2* __restrict__ xy_o,
+                                      const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   const float alpha = (float)st[NS_ALPHA];
   const float coef = (float)st[NS_COEF];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
@@ -305,7 +307,9 @@ __global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
     const float2* __restrict__ force_o, const int* __restrict__ inv_order, int num_movable, int num_filler,
     const float* __restrict__ pws, const float* __restrict__ area, const float* __restrict__ lam_p, int num_nodes,
     const float* __restrict__ v_new, const float* __restrict__ v, const float* __restrict__ g,
-    float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index) {
+    float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index,
+    const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   __shared__ int s_start[kAsmNodes + 1];
   __shared__ float2 s_q[kAsmPins];
   const float lam = *lam_p;
@@ -496,7 +500,7 @@ extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u,
   if (num_nodes == 0) return DP_OK;
   nesterov_trial_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
       v, g, u, u_new, v_new, reinterpret_cast<float2*>(xy_new), state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable,
-      num_filler, inv_order, reinterpret_cast<float2*>(xy_order));
+      num_filler, inv_order, reinterpret_cast<float2*>(xy_order), trial_gate());
   return check_launch("dp_nesterov_trial");
 }
 
@@ -527,6 +531,71 @@ extern "C" int dp_nesterov_advance(double* state, dp_stream_t stream) {
   DP_REQUIRE(state, "dp_nesterov_advance: null state");
   nesterov_advance_kernel<<<1, 1, 0, as_stream(stream)>>>(state);
   return check_launch("dp_nesterov_advance");
+}
+
+// What the GP loop does on the host between iteration k and k+1, on the
+// device, so that iteration k+1 can be enqueued before the host has read
+// iteration k's metrics:
+//  * Nesterov: the scalars of iteration k (after its last trial) are copied
+//    to iteration k+1's state and advanced (a_k <- a_{k+1}, coef);
+//  * density weight (RePlAce HPWL mode, dreamplace/PlaceObj.py:833-851): with
+//    f = k + 1 iterations done, for f > 1
+//      mu = upper * max(0.9999^f, 0.98)                         if hpwl_k < hpwl_{k-1}
+//      mu = upper * min(max(upper^(-(hpwl_k - hpwl_{k-1}) / ref_hpwl), lower), upper)  otherwise
+//    lambda <- lambda * (float)mu;
+//  * gamma (dreamplace/PlaceObj.py:901-915): gamma = base_gamma *
+//    10^((ovf_k / total_area - 0.1) * 20 / 9 - 1), rounded to float, and its
+//    reciprocal (the WA kernel's scalar).
+// sched = {k, hpwl_{k-1}}; weights = {lambda, gamma, 1 / gamma}.
+__global__ void iteration_head_kernel(const double* __restrict__ st_prev, double* __restrict__ st_new,
+                                      const double* __restrict__ sched_prev, double* __restrict__ sched_new,
+                                      const double* __restrict__ hpwl_k, const double* __restrict__ ovf_k,
+                                      const float* __restrict__ w_prev, float* __restrict__ w_new, double base_gamma,
+                                      double total_area, double ref_hpwl, double lower, double upper, int* gate) {
+  // the previous trial was rejected: this iteration was enqueued ahead and is
+  // void; its gated kernels return at once
+  if (gate) *gate = st_prev[NS_ACCEPT] == 0.0 ? 1 : 0;
+  for (int i = 0; i < DP_NESTEROV_STATE_DOUBLES; ++i) st_new[i] = st_prev[i];
+  const double a = st_new[NS_A_NEXT];
+  st_new[NS_A] = a;
+  const double an = (1.0 + sqrt(4.0 * a * a + 1.0)) / 2.0;
+  st_new[NS_A_NEXT] = an;
+  st_new[NS_COEF] = (a - 1.0) / an;
+  const double f = sched_prev[0] + 1.0;
+  const double hp = hpwl_k[0];
+  float lam = w_prev[0];
+  if (f > 1.0) {
+    const double delta = hp - sched_prev[1];
+    double mu;
+    if (delta < 0.0)
+      mu = upper * fmax(pow(0.9999, f), 0.98);
+    else
+      mu = upper * fmin(fmax(pow(upper, -delta / ref_hpwl), lower), upper);
+    lam = fmul(lam, (float)mu);
+  }
+  sched_new[0] = f;
+  sched_new[1] = hp;
+  const double t = (ovf_k[0] / total_area - 0.1) * 20.0 / 9.0 - 1.0;
+  const float gamma = (float)(base_gamma * pow(10.0, t));
+  w_new[0] = lam;
+  w_new[1] = gamma;
+  w_new[2] = __fdiv_rn(1.0f, gamma);
+}
+
+extern "C" int dp_iteration_head(const double* state_prev, double* state_new, const double* sched_prev,
+                                 double* sched_new, const double* hpwl_k, const double* overflow_k,
+                                 const float* weights_prev, float* weights_new, double base_gamma, double total_area,
+                                 double ref_hpwl, double lower, double upper, int* gate, dp_stream_t stream) {
+  DP_REQUIRE(state_prev && state_new && sched_prev && sched_new && hpwl_k && overflow_k && weights_prev &&
+                 weights_new,
+             "dp_iteration_head: null pointer argument");
+  DP_REQUIRE(state_prev != state_new && sched_prev != sched_new && weights_prev != weights_new,
+             "dp_iteration_head: the previous and the new iteration need separate buffers");
+  DP_REQUIRE(total_area > 0.0 && ref_hpwl > 0.0, "dp_iteration_head: total_area and ref_hpwl must be positive");
+  iteration_head_kernel<<<1, 1, 0, as_stream(stream)>>>(state_prev, state_new, sched_prev, sched_new, hpwl_k,
+                                                        overflow_k, weights_prev, weights_new, base_gamma,
+                                                        total_area, ref_hpwl, lower, upper, gate);
+  return check_launch("dp_iteration_head");
 }
 
 // ============================================================== warp-per-chunk WA / HPWL
@@ -892,7 +961,8 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
   assemble_precondition_kernel<<<blocks, kAsmNodes, 0, s>>>(
       reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
-      inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index);
+      inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index,
+      trial_gate());
   int rc = check_launch("dp_assemble_precondition_step");
   if (rc) return rc;
   nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
@@ -1109,7 +1179,9 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
 
 template <bool kGrad>
 __global__ void __launch_bounds__(256, 3) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
-                                                      double* __restrict__ hpwl_partials) {
+                                                      double* __restrict__ hpwl_partials,
+                                                      const int* __restrict__ gate) {
+  if (gate_closed(gate)) return;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1212,9 +1284,9 @@ static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, doub
   int blocks = A.num_groups > 0 ? ceil_div((long long)A.num_groups * 32, 256) : 1;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   if (grad)
-    wa_lane_kernel<true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr);
+    wa_lane_kernel<true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr, trial_gate());
   else
-    wa_lane_kernel<false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr);
+    wa_lane_kernel<false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
   int rc = check_launch(grad ? "dp_wa_lanes_forward" : "dp_hpwl_lanes");
   if (rc) return rc;
   if (grad && hpwl_f64) {

@@ -10,13 +10,18 @@ re-organised for the GPU:
   density gradient (scaled by lambda on the device) and the WA backward fused
   with the pin -> node sum accumulating the wirelength gradient on top;
 * the Nesterov trial point, move-boundary clamp, preconditioner and the fp64
-  step-size estimate run as fused kernels on ping-pong buffers (v, u, g for
-  step k and k+1), so an accepted step swaps a parity bit instead of copying;
+  step-size estimate run as fused kernels on three rotating slots of (v, u, g)
+  buffers, so an accepted step advances a slot index instead of copying;
 * one Nesterov trial is one CUDA graph replay; the trial's WA forward also
   sums the HPWL of the trial point and its scatter also yields the
   movable-only map, so the evaluation of v_k (HPWL, overflow) reported at
   iteration k was computed when v_k was produced; the host reads a handful of
-  fp64 scalars once per trial and makes the loop decisions.
+  fp64 scalars once per trial and makes the loop decisions;
+* the loop's between-iteration work (Nesterov advance, density-weight and
+  gamma updates) runs on the device at the head of the next iteration's graph,
+  so iteration k+1 is enqueued before the host has read iteration k: the host
+  loop runs while the GPU computes, and iteration k+1 is enqueued again only
+  when k needed a retry or the host changed what k+1 reads.
 """
 import math
 
@@ -30,6 +35,7 @@ from .electric_potential import poisson_solve
 NS_ALPHA, NS_A, NS_A_NEXT, NS_COEF, NS_ACC_DV, NS_ACC_DG, NS_ALPHA_NEW, NS_ACCEPT = range(8)
 NESTEROV_STATE = 8
 REDUCE_DOUBLES = 1280
+NSLOT = 3
 # metric slots
 M_HPWL, M_OVF, M_MAXD, M_ACCEPT, M_ALPHA, M_OBJ, M_WL, M_ENERGY = range(8)
 # pieces of one Nesterov trial, in launch order
@@ -91,40 +97,48 @@ class GPEngine(object):
         ep = ops.density_op
         self.ep = ep
         self.ovf_op = ops.density_overflow_op
-        # ping-pong state
+        # iteration slots: slot s holds v_k, u_k, g_k of an iteration (and its
+        # interleaved / visiting-order position copies, the HPWL and overflow
+        # of v_k, the optimizer scalars, the density weight and gamma); a trial
+        # reads slot s and writes slot s + 1 (mod 3).  Three slots let
+        # iteration k+1 be enqueued while iteration k may still be retried.
         pos = data.pos[0]
-        self.V = [pos.data.clone(), torch.empty_like(pos.data)]
-        self.U = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
-        self.G = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
-        # interleaved (x, y) copies of V[0], V[1] for the gather kernels
-        self.XY = [torch.empty_like(pos.data), torch.empty_like(pos.data)]
-        self._xy_of = {self.V[0].data_ptr(): self.XY[0], self.V[1].data_ptr(): self.XY[1]}
+        self.V = [pos.data.clone()] + [torch.empty_like(pos.data) for _ in range(NSLOT - 1)]
+        self.U = [torch.empty_like(pos.data) for _ in range(NSLOT)]
+        self.G = [torch.empty_like(pos.data) for _ in range(NSLOT)]
+        # interleaved (x, y) copies of the positions for the gather kernels
+        self.XY = [torch.empty_like(pos.data) for _ in range(NSLOT)]
+        self._xy_of = {self.V[i].data_ptr(): self.XY[i] for i in range(NSLOT)}
         # the same positions for the scattered cells, in visiting order (written
         # by the trial kernel; gathered after a pack or a re-sort)
         ns = d.num_movable_nodes + d.num_filler_nodes
-        self.XYO = [torch.empty(2 * ns, dtype=torch.float32, device=dev),
-                    torch.empty(2 * ns, dtype=torch.float32, device=dev)]
-        self._xyo_of = {self.V[0].data_ptr(): self.XYO[0], self.V[1].data_ptr(): self.XYO[1]}
+        self.XYO = [torch.empty(2 * ns, dtype=torch.float32, device=dev) for _ in range(NSLOT)]
+        self._xyo_of = {self.V[i].data_ptr(): self.XYO[i] for i in range(NSLOT)}
         self.tmp = torch.empty_like(pos.data)
         f64 = dict(dtype=torch.float64, device=dev)
         # optimizer scalars + fixed-order reduction scratch (include/dreamplace_b200.h)
-        self.state = torch.zeros(NESTEROV_STATE + 2 * REDUCE_DOUBLES, **f64)
+        self.S = [torch.zeros(NESTEROV_STATE + 2 * REDUCE_DOUBLES, **f64) for _ in range(NSLOT)]
+        # {iteration index, HPWL of the previous iteration} and {lambda, gamma,
+        # 1 / gamma} of the iteration in each slot (dp_iteration_head)
+        self.sched = [torch.zeros(2, **f64) for _ in range(NSLOT)]
+        self.weights = [torch.zeros(3, dtype=torch.float32, device=dev) for _ in range(NSLOT)]
         self.wl64_buf = torch.zeros(REDUCE_DOUBLES, **f64)
         self.wl64 = self.wl64_buf[0:1]
         self.obj64 = torch.zeros(1, **f64)
-        # metrics of v_k and v_{k+1} by parity: the HPWL rides along the trial's
-        # WA forward and the movable-only map (overflow) along its scatter, so
-        # the evaluation of v_k is already on the device when iteration k starts
-        self.H = [torch.zeros(REDUCE_DOUBLES, **f64), torch.zeros(REDUCE_DOUBLES, **f64)]
-        self.O = [torch.zeros(REDUCE_DOUBLES, **f64), torch.zeros(REDUCE_DOUBLES, **f64)]
-        self.metrics = torch.zeros(8, **f64)
-        self.metrics_host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
+        # metrics of v_k by slot: the HPWL rides along the WA forward of the trial
+        # that produced v_k and the movable-only map (overflow) along its
+        # scatter, so the evaluation of v_k is on the device when iteration k starts
+        self.H = [torch.zeros(REDUCE_DOUBLES, **f64) for _ in range(NSLOT)]
+        self.O = [torch.zeros(REDUCE_DOUBLES, **f64) for _ in range(NSLOT)]
+        self.metrics = [torch.zeros(8, **f64) for _ in range(NSLOT)]
+        self.metrics_host = [torch.zeros(8, dtype=torch.float64, pin_memory=True) for _ in range(NSLOT)]
+        self.ready = [None] * NSLOT
         self.grad_scale = torch.zeros(1, dtype=torch.float32, device=dev)
         # (density factor, quadratic penalty coefficient) read by the objective
         # kernel on the device, so the captured graphs follow their changes
         self.factor_quad = torch.tensor([1.0, 0.0], dtype=torch.float32, device=dev)
         self.one = torch.ones(1, dtype=torch.float32, device=dev)
-        self.inv_gamma = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.inv_gamma = torch.zeros(1, dtype=torch.float32, device=dev)  # set-up evaluations (model gamma)
         self.dmap = torch.empty(ep.num_bins_x, ep.num_bins_y, dtype=torch.float32, device=dev)
         self.omap = torch.empty_like(self.dmap)
         self.ovf_area = float(self.ovf_op.bin_size_x * self.ovf_op.bin_size_y)
@@ -152,20 +166,42 @@ class GPEngine(object):
         # inside the captured graph); piece_query selects the pieces whose
         # durations are accumulated after each trial
         self.piece_events = None
+        self._mark_slot = 0
         self.piece_query = set(PIECES)
         self.piece_ms = {k: 0.0 for k in PIECES}
         self.piece_n = {k: 0 for k in PIECES}
         if getattr(params, "time_pieces", False):
-            self.piece_events = {k: (torch.cuda.Event(enable_timing=True, external=True),
-                                     torch.cuda.Event(enable_timing=True, external=True)) for k in PIECES}
+            # one set per slot: the trial of the next slot may record its own
+            # while this slot's durations are read
+            self.piece_events = [{k: (torch.cuda.Event(enable_timing=True, external=True),
+                                      torch.cuda.Event(enable_timing=True, external=True)) for k in PIECES}
+                                 for _ in range(NSLOT)]
         self.iterations = 0
-        self.parity = 0
+        self.slot = 0
+        # the iteration whose first trial is already enqueued (None: none)
+        self.enqueued = None
+        # enqueue iteration k+1 right behind iteration k's first trial, before the
+        # host has read k's metrics (the GP loop's between-iteration work runs on
+        # the device, dp_iteration_head); needs the loop's default schedule of one
+        # Nesterov step per density-weight and per gamma update
+        gp = params.global_place_stages[0]
+        self.schedule_ok = int(gp.get("Lsub_iteration", 1)) == 1 and \
+            int(gp.get("Llambda_density_weight_iteration", 1)) == 1
+        if not self.schedule_ok:
+            raise ValueError("the graph engine runs the default schedule (Lsub_iteration = "
+                             "Llambda_density_weight_iteration = 1); use gp_engine='autograd' for others")
+        self.speculate = bool(getattr(params, "speculate", True)) and use_graphs
+        # trial gate word (dp_set_trial_gate): written by each trial graph's
+        # first kernel; a trial enqueued ahead of a rejected one skips its work
+        self.gate = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.head_scalars = (float(model.base_gamma(params, d)), float(d.total_movable_node_area),
+                             float(params.RePlAce_ref_hpwl), float(params.RePlAce_LOWER_PCOF),
+                             float(params.RePlAce_UPPER_PCOF))
         self.graphs = {}
         self.graph_kernels = {}
         self.kernels_launched = 0  # this library's kernels, graph replays included
         self.pool = None
         self.graph_key = None
-        self._metrics_ready = None
         self.trials = 0
         self.last_energy = None
         self._quad_c = 0.0
@@ -238,16 +274,18 @@ class GPEngine(object):
         C.pack_xy(v, self.xy(v))
         C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
 
-    def wirelength(self, v, hpwl_out=None):
+    def wirelength(self, v, hpwl_out=None, inv_gamma=None):
         """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
-        net weight) in node-CSR order in self.gnode; with hpwl_out, the HPWL of v from the
-        same pin reads."""
+        net weight) in self.gnode; with hpwl_out, the HPWL of v from the same pin reads.
+        inv_gamma: device scalar 1/gamma (default: from the model's gamma)."""
         dc = self.data
-        self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
+        if inv_gamma is None:
+            self.inv_gamma.copy_(1.0 / self.model.gamma.reshape(1))
+            inv_gamma = self.inv_gamma
         C.wa_lanes_forward(self.xy(v), self.group_deg, self.group_base, self.group_net, self.ln_node, self.ln_offx,
                            self.ln_offy, self.ln_csr if self.lane_of_csr is None else None, dc.net_weights,
                            dc.net_mask_ignore_large_degrees,
-                           self.inv_gamma, self.wl64_buf, self.gnode,
+                           inv_gamma, self.wl64_buf, self.gnode,
                            dc.net_mask_all if hpwl_out is not None else None, hpwl_out)
 
     def wl_grad_into(self, g, accumulate):
@@ -284,13 +322,15 @@ class GPEngine(object):
                                  self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
                                  float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
 
-    def assemble(self, v, g, v_new, g_new):
+    def assemble(self, v, g, v_new, g_new, s=None):
         """Preconditioned gradient at v_new into g_new (pin sum + force) and the fp64
-        step-size norms against (v, g)."""
+        step-size norms against (v, g), with the density weight and optimizer
+        scalars of slot s (default: the current slot)."""
         d = self.design
+        s = self.slot if s is None else s
         C.assemble_precondition_step(self.gnode, self.node_start, self.one, self.force_o, self.inv_order,
                                      d.num_movable_nodes, d.num_filler_nodes, self._pws(), self.data.node_areas,
-                                     self.model.density_weight, v_new, v, g, g_new, self.state, self.lane_of_csr)
+                                     self.weights[s][0:1], v_new, v, g, g_new, self.S[s], self.lane_of_csr)
 
     def density_grad_into(self, v, ex, ey, scale_t, g):
         ep = self.ep
@@ -318,17 +358,20 @@ class GPEngine(object):
 
     def precondition(self, g, v_ref, g_ref, v_new):
         C.precondition_step_size(g, g_ref, v_new, v_ref, self._pws(), self.data.node_areas,
-                                 self.model.density_weight, self.state)
+                                 self.model.density_weight, self.S[self.slot])
 
-    def objective_and_step(self, v, g, v_new, g_new, q_new):
+    def objective_and_step(self, v, g, v_new, g_new, s):
         """The trial's objective at v_new and its preconditioned gradient into g_new,
-        with the fp64 step-size norms against (v, g): the field force is gathered
-        in visiting order and assembled per node together with the wirelength pin
-        sum, the preconditioner and the norms (one pass over the nodes).  The
-        HPWL and overflow of v_new land in the parity-q_new metric buffers."""
-        m, ep, d = self.model, self.ep, self.design
+        with the fp64 step-size norms against (v, g) into slot s's scalars: the
+        field force is gathered in visiting order and assembled per node together
+        with the wirelength pin sum, the preconditioner and the norms (one pass
+        over the nodes).  The HPWL and overflow of v_new land in the metric
+        buffers of slot s + 1."""
+        ep = self.ep
+        q_new = (s + 1) % NSLOT
+        w = self.weights[s]
         self._mark("wa_forward", 0)
-        self.wirelength(v_new, self.H[q_new])
+        self.wirelength(v_new, self.H[q_new], w[2:3])
         self._mark("wa_forward", 1)
         self._mark("density_scatter", 0)
         self.scatter_maps(v_new, self.O[q_new])
@@ -337,23 +380,23 @@ class GPEngine(object):
         self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
         ex, ey, energy = poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
         self._mark("poisson_gemms", 1)
-        C.objective_finish(self.wl64, energy, m.density_weight, self.factor_quad, self.obj64, self.grad_scale)
+        C.objective_finish(self.wl64, energy, w[0:1], self.factor_quad, self.obj64, self.grad_scale)
         self._mark("field_gather", 0)
         self.field_force(v_new, ex, ey)
         self._mark("field_gather", 1)
         self._mark("assemble_precondition", 0)
-        self.assemble(v, g, v_new, g_new)
+        self.assemble(v, g, v_new, g_new, s)
         self._mark("assemble_precondition", 1)
         self.last_energy = energy
         return energy
 
     def _mark(self, piece, which):
         if self.piece_events is not None:
-            self.piece_events[piece][which].record()
+            self.piece_events[self._mark_slot][piece][which].record()
 
-    def _collect_pieces(self):
+    def _collect_pieces(self, s):
         for k in self.piece_query:
-            a, b = self.piece_events[k]
+            a, b = self.piece_events[s][k]
             self.piece_ms[k] += a.elapsed_time(b)
             self.piece_n[k] += 1
 
@@ -381,7 +424,7 @@ class GPEngine(object):
         C.move_boundary_forward(v, self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl),
                                 float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes)
         self.pack(v)
-        for q in (0, 1):
+        for q in range(NSLOT):
             if v.data_ptr() == self.V[q].data_ptr():
                 self.evaluate(q)
 
@@ -408,7 +451,7 @@ class GPEngine(object):
 
     def initialize_density_weight(self):
         """lambda0 = density_weight * |grad WL|_1 / |grad D|_1 (PlaceObj.initialize_density_weight)."""
-        v = self.V[self.parity]
+        v = self.V[self.slot]
         self.wirelength(v)
         self.wl_grad_into(self.tmp, False)
         wl_norm = self.tmp.double().abs().sum()
@@ -423,136 +466,181 @@ class GPEngine(object):
 
     def start_optimizer(self, lr):
         """First optimizer step's set-up: g_k at v_k, g_k_1 at v_k - lr g_k, alpha_k."""
-        p = self.parity
+        p = self.slot
         v, g, u = self.V[p], self.G[p], self.U[p]
         self._plain_objective()
         self.obj_and_raw_grad(v, g)
         self.precondition(g, v, g, v)
         u.copy_(v)
-        x1, g1 = self.V[1 - p], self.G[1 - p]
+        x1, g1 = self.V[(p + 1) % NSLOT], self.G[(p + 1) % NSLOT]
         torch.sub(v, g, alpha=lr, out=x1)
         self.pack(x1)
         self.obj_and_raw_grad(x1, g1)
         self.precondition(g1, v, g, x1)
         alpha = float((torch.dist(v.double(), x1.double()) / torch.dist(g.double(), g1.double())).item())
-        C.nesterov_init(self.state, alpha)
+        C.nesterov_init(self.S[p], alpha)
+        # iteration 0's density weight and gamma come from the model (the set-up
+        # above); later iterations' from dp_iteration_head
+        m = self.model
+        self.weights[p].copy_(torch.cat([m.density_weight.reshape(1).float(), m.gamma.reshape(1).float(),
+                                         (1.0 / m.gamma.reshape(1)).float()]))
+        self.sched[p].zero_()
+        self.enqueued = None
         return alpha
 
+    def sync_model(self):
+        """Copy the current iteration's density weight and gamma (kept on the
+        device by the trial graphs) into the model's tensors."""
+        m, w = self.model, self.weights[self.slot]
+        with torch.no_grad():
+            m.density_weight.copy_(w[0:1].reshape(m.density_weight.shape))
+            m.gamma.copy_(w[1].reshape(m.gamma.shape))
+
     # ---------------------------------------------------------------- iteration
-    def _trial(self, p):
+    def _trial(self, s, head=False):
+        """One Nesterov trial from slot s into slot s + 1.  head: the first trial
+        of an iteration k >= 1, preceded by the loop's between-iteration work on
+        the device (advance, density weight, gamma from slot s - 1)."""
         d = self.design
-        v, g, u = self.V[p], self.G[p], self.U[p]
-        vn, gn, un = self.V[1 - p], self.G[1 - p], self.U[1 - p]
+        t = (s + 1) % NSLOT
+        self._mark_slot = s
+        gate = self.gate if self.use_graphs else None
+        if head:
+            r = (s - 1) % NSLOT
+            C.iteration_head(self.S[r], self.S[s], self.sched[r], self.sched[s], self.H[r][0:1], self.O[r][0:1],
+                             self.weights[r], self.weights[s], *self.head_scalars, gate=gate)
+        elif gate is not None:
+            C.trial_gate(gate)
+        v, g, u = self.V[s], self.G[s], self.U[s]
+        vn, gn, un = self.V[t], self.G[t], self.U[t]
+        st = self.S[s]
         self._mark("nesterov_trial", 0)
         scatter_write = self.xyo_mode == "trial"
-        C.nesterov_trial(v, g, u, un, vn, self.XY[1 - p], self.state, self.data.node_size_x, self.data.node_size_y,
+        C.nesterov_trial(v, g, u, un, vn, self.XY[t], st, self.data.node_size_x, self.data.node_size_y,
                          float(d.xl), float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes,
-                         self.inv_order if scatter_write else None, self.XYO[1 - p] if scatter_write else None)
+                         self.inv_order if scatter_write else None, self.XYO[t] if scatter_write else None)
         if not scatter_write:
-            C.gather_order_xy(self.XY[1 - p], self.order, self.order.numel(), self.XYO[1 - p])
+            C.gather_order_xy(self.XY[t], self.order, self.order.numel(), self.XYO[t])
         self._mark("nesterov_trial", 1)
-        energy = self.objective_and_step(v, g, vn, gn, 1 - p)
+        energy = self.objective_and_step(v, g, vn, gn, s)
         # HPWL / overflow of v_k (computed when v_k was the trial point), then the trial's scalars
-        torch.cat([self.H[p][0:1], self.O[p][0:2], self.state[NS_ACCEPT:NS_ACCEPT + 1],
-                   self.state[NS_ALPHA:NS_ALPHA + 1], self.obj64, self.wl64, energy.reshape(1)], out=self.metrics)
+        torch.cat([self.H[s][0:1], self.O[s][0:2], st[NS_ACCEPT:NS_ACCEPT + 1], st[NS_ALPHA:NS_ALPHA + 1],
+                   self.obj64, self.wl64, energy.reshape(1)], out=self.metrics[s])
 
-    def nesterov_trial_only(self, p):
+    def nesterov_trial_only(self, s):
         """The trial-point kernel alone (used for per-kernel timing)."""
         d = self.design
-        C.nesterov_trial(self.V[p], self.G[p], self.U[p], self.U[1 - p], self.V[1 - p], self.XY[1 - p], self.state,
+        t = (s + 1) % NSLOT
+        C.nesterov_trial(self.V[s], self.G[s], self.U[s], self.U[t], self.V[t], self.XY[t], self.S[s],
                          self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
-                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes, self.inv_order, self.XYO[1 - p])
+                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes, self.inv_order, self.XYO[t])
 
-    def _body(self, p):
+    def _body(self, s, head):
         # v_k was clamped into the die when it was produced (trial kernel, or
         # move_boundary + pack at the start / after a rollback), so the
         # reference's per-iteration move_boundary(pos) is the identity here,
         # and its evaluation (HPWL, overflow) was computed with it
-        self._trial(p)
+        self._trial(s, head)
 
-    def _graph(self, p, warm=True):
-        key = p
+    def _graph(self, s, head, warm=True):
+        key = (s, head)
         g = self.graphs.get(key)
         if g is None:
             if warm:
-                # warm-up on a side stream.  Only the body of the current parity
-                # may run here: it writes the step-k+1 buffers, which hold nothing
-                # yet, and the optimizer scalars, which are restored.
-                assert p == self.parity, "graph warm-up must run at the current parity"
-                s = torch.cuda.Stream()
-                s.wait_stream(torch.cuda.current_stream())
-                with torch.cuda.stream(s):
-                    saved = self.state.clone()
-                    self._body(p)
-                    self.state.copy_(saved)
-                torch.cuda.current_stream().wait_stream(s)
+                # warm-up on a side stream.  Only the head-less body of the
+                # current slot may run here: it writes the next slot's buffers,
+                # which hold nothing yet, and the slot's optimizer scalars, which
+                # are restored.
+                assert s == self.slot and not head, "graph warm-up must run the current slot without head"
+                st = torch.cuda.Stream()
+                st.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(st):
+                    saved = self.S[s].clone()
+                    self._body(s, head)
+                    self.S[s].copy_(saved)
+                torch.cuda.current_stream().wait_stream(st)
             # captured on a side stream with capture_begin / capture_end (the
             # torch.cuda.graph context would also run gc and empty the
             # allocator cache, which costs a stall inside the GP loop)
             g = torch.cuda.CUDAGraph()
             before = C.launch_count()
-            s = torch.cuda.Stream()
-            s.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(s):
+            st = torch.cuda.Stream()
+            st.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(st):
                 g.capture_begin(pool=self.pool)
+                C.set_trial_gate(self.gate)
                 try:
-                    self._body(p)
+                    self._body(s, head)
                 finally:
+                    C.set_trial_gate(None)
                     g.capture_end()
-            torch.cuda.current_stream().wait_stream(s)
+            torch.cuda.current_stream().wait_stream(st)
             self.graph_kernels[key] = C.launch_count() - before
             if self.pool is None:
                 self.pool = g.pool()
             self.graphs[key] = g
         return g
 
-    def _launch(self, p):
-        """Enqueue one trial (graph replay) and the read-back of its metrics on the
-        current stream."""
+    def _launch(self, s, head):
+        """Enqueue one trial from slot s (graph replay) and the read-back of its
+        metrics on the current stream."""
         if self.use_graphs:
-            self._graph(p).replay()
-            self.kernels_launched += self.graph_kernels[p]
+            self._graph(s, head).replay()
+            self.kernels_launched += self.graph_kernels[(s, head)]
         else:
             before = C.launch_count()
-            self._body(p)
+            self._body(s, head)
             self.kernels_launched += C.launch_count() - before
-        self.metrics_host.copy_(self.metrics, non_blocking=True)
-        if self._metrics_ready is None:
-            self._metrics_ready = torch.cuda.Event()
-        self._metrics_ready.record()
+        self.metrics_host[s].copy_(self.metrics[s], non_blocking=True)
+        if self.ready[s] is None:
+            self.ready[s] = torch.cuda.Event()
+        self.ready[s].record()
 
-    def _collect(self):
-        """Wait for the last launched trial and return its metrics."""
-        self._metrics_ready.synchronize()
+    def _collect(self, s):
+        """Wait for the last trial launched from slot s and return its metrics."""
+        self.ready[s].synchronize()
         if self.piece_events is not None:
-            self._collect_pieces()
-        return self.metrics_host.numpy().copy()
+            self._collect_pieces(s)
+        return self.metrics_host[s].numpy().copy()
 
-    def _run(self, p):
-        self._launch(p)
-        return self._collect()
+    def _run(self, s, head=False):
+        self._launch(s, head)
+        return self._collect(s)
+
+    def _enqueue_first(self, k, s):
+        """Enqueue the first trial of iteration k (input slot s), with the
+        visiting-order refresh that iteration starts with."""
+        if self.sort_interval > 0 and k % self.sort_interval == 0:
+            self.refresh_order(self.V[s])
+        self._launch(s, k > 0)
+        self.enqueued = k
 
     def _check_graph_key(self):
         """Refresh the device copy of (density factor, quadratic penalty
-        coefficient) when the GP loop changed them (no recapture needed)."""
+        coefficient) when the GP loop changed them (no recapture needed); an
+        iteration enqueued ahead with the old values is enqueued again."""
         m = self.model
         key = (float(m.density_factor), bool(m.quad_penalty))
         if key != self.graph_key:
             self._quad_c = float(m.quad_penalty_coeff.item()) if m.quad_penalty else 0.0
             self.factor_quad.copy_(torch.tensor([key[0], self._quad_c], dtype=torch.float32))
             self.graph_key = key
+            self.enqueued = None
 
     def prepare_graphs(self):
-        """Capture the trial graph of both parities up front, so no capture happens
-        inside a timed or latency-sensitive window."""
+        """Capture the trial graphs of every slot (first trial with the
+        between-iteration head, and retry) up front, so no capture happens inside
+        a timed or latency-sensitive window."""
         if not self.use_graphs:
             return
         self._check_graph_key()
-        p = self.parity
-        # one warm-up (current parity) initialises every lazy resource; the
-        # other parity is captured without running
-        self._graph(p)
-        self._graph(1 - p, warm=False)
+        s = self.slot
+        # one warm-up (current slot, no head) initialises every lazy resource;
+        # the other graphs are captured without running
+        self._graph(s, False)
+        for q in range(NSLOT):
+            for head in (False, True):
+                self._graph(q, head, warm=False)
 
     def step(self):
         """One GP iteration: evaluation at v_k, then Nesterov trials until accepted
@@ -565,35 +653,63 @@ class GPEngine(object):
             return stop.value
 
     def step_gen(self):
-        """step() as a generator: it yields once, right after the first trial is
-        enqueued, so a driver of several designs can enqueue theirs (on their own
-        streams) before this one waits for its metrics."""
+        """step() as a generator: it yields once, right after the iteration's
+        first trial is enqueued, so a driver of several designs can enqueue theirs
+        (on their own streams) before this one waits for its metrics.
+
+        With speculation the first trial of iteration k+1 is enqueued behind
+        iteration k's before the host waits: its head does on the device what the
+        host loop does between iterations, so the GPU never waits for the host.
+        It is enqueued again when iteration k needed a retry, or the host changed
+        the density factor or the position after reading iteration k."""
         self._check_graph_key()
-        if self.use_graphs and len(self.graphs) < 2:
+        if self.use_graphs and len(self.graphs) < 2 * NSLOT:
             self.prepare_graphs()
-        p = self.parity
-        if self.sort_interval > 0 and self.iterations % self.sort_interval == 0:
-            self.refresh_order(self.V[p])
-        self.iterations += 1
-        self._launch(p)
+        s = self.slot
+        k = self.iterations
+        if self.enqueued != k:
+            self._enqueue_first(k, s)
+        if self.speculate:
+            self._enqueue_first(k + 1, (s + 1) % NSLOT)
         yield
-        mh = self._collect()
+        mh = self._collect(s)
         hpwl, ovf, maxd = mh[M_HPWL], mh[M_OVF], mh[M_MAXD]
         trials = 1
         while mh[M_ACCEPT] == 0.0 and trials < 10:
-            mh = self._run(p)
+            # the iteration enqueued ahead saw the rejection (its gate closed);
+            # enqueue it again behind the retry
+            self._launch(s, False)
+            if self.speculate:
+                self._enqueue_first(k + 1, (s + 1) % NSLOT)
+            else:
+                self.enqueued = None
+            mh = self._collect(s)
             trials += 1
-        C.nesterov_advance(self.state)
-        self.kernels_launched += 1
-        self.parity = 1 - p
+        if mh[M_ACCEPT] == 0.0:
+            # out of trials: the loop moves on with the last one, so the next
+            # iteration must run (not see a rejection)
+            self.S[s][NS_ACCEPT].fill_(1.0)
+            self.enqueued = None
+        self.iterations = k + 1
+        self.slot = (s + 1) % NSLOT
         self.trials += trials
         return (float(hpwl), float(ovf) / self.design.total_movable_node_area, float(maxd), float(mh[M_OBJ]), trials)
 
+    @property
+    def parity(self):
+        """The current slot (the iteration's input buffers)."""
+        return self.slot
+
+    def next_slot(self, s):
+        return (s + 1) % NSLOT
+
     def current_position(self):
-        return self.V[self.parity]
+        return self.V[self.slot]
 
     def set_position(self, t):
-        """Overwrite v_k (divergence rollback), clamped into the die."""
-        v = self.V[self.parity]
+        """Overwrite v_k (divergence rollback), clamped into the die; an
+        iteration enqueued ahead from the old v_k is enqueued again."""
+        v = self.V[self.slot]
         v.copy_(t)
         self.move_boundary(v)
+        self.enqueued = None

@@ -127,6 +127,11 @@ class _EngineStepper(object):
         h, o, md, obj, trials = yield from e.step_gen()
         return h, o, md, obj
 
+    device_updates = True
+
+    def sync_model(self):
+        self.eng.sync_model()
+
     def position(self):
         return self.eng.current_position()
 
@@ -175,6 +180,9 @@ class NonLinearPlace(nn.Module):
         else:
             stepper = _EngineStepper(self, model, params, design, gp["learning_rate"], mode == "graph")
         self.stepper = stepper
+        # the graph engine applies the density-weight and gamma updates itself,
+        # on the device at the start of the next iteration (the same formulas)
+        device_updates = getattr(stepper, "device_updates", False)
         base_gamma = model.base_gamma(params, design)
         ref_hpwl = params.RePlAce_ref_hpwl
         lower, upper = params.RePlAce_LOWER_PCOF, params.RePlAce_UPPER_PCOF
@@ -261,16 +269,20 @@ class NonLinearPlace(nn.Module):
                         mu = upper * max(math.pow(0.9999, float(flat_llambda)), 0.98)
                     else:
                         mu = upper * min(max(math.pow(upper, -delta / ref_hpwl), lower), upper)
-                    with torch.no_grad():
-                        model.density_weight.mul_(mu)
+                    if not device_updates:
+                        with torch.no_grad():
+                            model.density_weight.mul_(mu)
                 if self._llambda_stop(params, llam):
                     break
             # gamma = base * 10^((overflow - 0.1) * 20/9 - 1) (dreamplace/PlaceObj.py:901-915)
             coef = math.pow(10, (llam[-1][-1].overflow - 0.1) * 20 / 9 - 1)
-            with torch.no_grad():
-                model.gamma.fill_(base_gamma * coef)
+            if not device_updates:
+                with torch.no_grad():
+                    model.gamma.fill_(base_gamma * coef)
             if self._lgamma_stop(params, design, Lgamma_step, all_metrics, best) or stop_placement:
                 break
+        if device_updates:
+            stepper.sync_model()
         with torch.no_grad():
             self.pos[0].data.copy_(stepper.position())
         self.metrics = all_metrics

@@ -374,6 +374,31 @@ int dp_assemble_precondition_step(const float* grad_node_order, const int* node_
                                   dp_stream_t stream);
 /* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
 int dp_nesterov_advance(double* state, dp_stream_t stream);
+/* The GP loop's work between iteration k and k+1 (dreamplace/NonLinearPlace.py
+ * main loop; dreamplace/PlaceObj.py:833-851 update_density_weight in RePlAce
+ * HPWL mode, :901-915 update_gamma), on the device: state_new <- state_prev's
+ * scalars, advanced (dp_nesterov_advance); sched = {k, HPWL of iteration k-1}
+ * (fp64[2]) becomes {k + 1, hpwl_k[0]}; weights = {lambda, gamma, 1/gamma}
+ * (float[3]): with f = k + 1, lambda <- lambda * (float)mu for f > 1,
+ * mu = upper * max(0.9999^f, 0.98) when HPWL fell, else
+ * upper * min(max(upper^(-(hpwl_k - hpwl_{k-1}) / ref_hpwl), lower), upper);
+ * gamma = (float)(base_gamma * 10^((overflow_k[0] / total_area - 0.1) * 20 / 9 - 1)).
+ * Lets iteration k+1 be enqueued before the host reads iteration k.  gate
+ * (optional): set to 1 when state_prev's last trial was rejected (the
+ * iteration was enqueued ahead and is void), else 0 (dp_set_trial_gate). */
+int dp_iteration_head(const double* state_prev, double* state_new, const double* sched_prev, double* sched_new,
+                      const double* hpwl_k, const double* overflow_k, const float* weights_prev,
+                      float* weights_new, double base_gamma, double total_area, double ref_hpwl, double lower,
+                      double upper, int* gate, dp_stream_t stream);
+/* Trial gate.  dp_set_trial_gate installs a device word (NULL removes it):
+ * the kernels of the trial pieces launched while it is installed (the trial
+ * point, position gather, WA, density scatter, operand preparation, transform
+ * GEMMs, field gather, assembly) receive it and return at once when it holds a
+ * non-zero value at run time.  Meant for CUDA-graph capture of a trial that is
+ * enqueued ahead of the decision it depends on.  dp_trial_gate sets the word:
+ * 1 when accept_prev is given and *accept_prev == 0, else 0. */
+int dp_set_trial_gate(const int* gate);
+int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t stream);
 /* Host planner: packs nets, in order, into chunks of at most max_pins pins (a
  * larger net is a chunk of its own).  chunk_net_host [num_nets + 1] receives the
  * first net of each chunk followed by num_nets; *num_chunks their count. */

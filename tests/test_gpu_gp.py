@@ -80,3 +80,95 @@ def test_trial_metrics_match_direct_evaluation(design):
                       np.ones(d.num_nets, np.uint8), d.net_weights)
     ref = ref[0] if isinstance(ref, tuple) else ref
     assert abs(h_trial - ref) <= 1e-6 * ref
+
+
+def test_iteration_head_matches_host_loop():
+    """dp_iteration_head against the host loop's formulas (NonLinearPlace
+    density-weight update in RePlAce HPWL mode, gamma update, Nesterov advance):
+    HPWL up and down, both clamps of mu, the first iteration (no update)."""
+    import math
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dreamplace_b200._native import C
+    base_gamma, area, ref, lower, upper = 4.0 * 46.875, 2.5e6, 350000.0, 0.95, 1.05
+    cases = [(0, 1.0e6, 9.0e5, 0.9), (1, 1.0e6, 9.0e5, 0.5), (7, 1.0e6, 1.1e6, 0.3), (12, 1.0e6, 1.0e6 + 1e9, 0.12),
+             (30, 2.0e6, 2.0e6 + 1.0, 0.07), (400, 5.0e5, 4.0e5, 0.2)]
+    for k, hp_prev, hp, ovf in cases:
+        st_prev = torch.zeros(8 + 2 * 1280, dtype=torch.float64, device="cuda")
+        st_prev[0:4] = torch.tensor([0.3, 2.5, 3.1, 0.4], dtype=torch.float64)
+        st_new = torch.zeros_like(st_prev)
+        sched_prev = torch.tensor([float(k), hp_prev], dtype=torch.float64, device="cuda")
+        sched_new = torch.zeros(2, dtype=torch.float64, device="cuda")
+        w_prev = torch.tensor([1.7e-4, 20.0, 0.05], dtype=torch.float32, device="cuda")
+        w_new = torch.zeros(3, dtype=torch.float32, device="cuda")
+        hpk = torch.tensor([hp], dtype=torch.float64, device="cuda")
+        ovk = torch.tensor([ovf * area], dtype=torch.float64, device="cuda")
+        C.iteration_head(st_prev, st_new, sched_prev, sched_new, hpk, ovk, w_prev, w_new, base_gamma, area, ref,
+                         lower, upper)
+        # the host loop (nonlinear_place.py run_gen)
+        f = k + 1
+        lam = torch.tensor([1.7e-4], dtype=torch.float32)
+        if f > 1:
+            delta = hp - hp_prev
+            if delta < 0:
+                mu = upper * max(math.pow(0.9999, float(f)), 0.98)
+            else:
+                mu = upper * min(max(math.pow(upper, -delta / ref), lower), upper)
+            lam.mul_(mu)
+        gamma = torch.zeros((), dtype=torch.float32).fill_(base_gamma * math.pow(10, ((ovf * area) / area - 0.1) * 20 / 9 - 1))
+        w = w_new.cpu()
+        assert w[0].item() == lam.item(), (k, w[0].item(), lam.item())
+        assert w[1].item() == gamma.item()
+        assert w[2].item() == (1.0 / gamma.reshape(1)).item()
+        a = 3.1
+        an = (1.0 + math.sqrt(4.0 * a * a + 1.0)) / 2.0
+        got = st_new[0:4].cpu().tolist()
+        assert got == [0.3, a, an, (a - 1.0) / an]
+        assert sched_new.cpu().tolist() == [float(f), hp]
+
+
+def test_speculative_iterations_match_serial(design):
+    """Iteration k+1 enqueued ahead of the host (speculate) gives the serial
+    loop's trajectory bit for bit in deterministic mode, retries included."""
+    traj = {}
+    for spec in (False, True):
+        t = []
+        p = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision="fp32",
+                   deterministic_flag=1, speculate=spec)
+        placer, res = place(design, p, max_iterations=120, callback=lambda it, m: t.append((m.hpwl, m.overflow)))
+        traj[spec] = (t, placer.stepper.eng.trials, placer.pos[0].detach().cpu())
+    (t0, n0, p0), (t1, n1, p1) = traj[False], traj[True]
+    assert n0 == n1 and n0 > 120  # some iterations needed a retry
+    assert t0 == t1
+    assert torch.equal(p0, p1)
+
+
+def test_trial_gate_skips_gated_kernels():
+    """Launches made while a trial gate is installed return at once when the
+    word is set, and run when it is clear; dp_trial_gate sets it from an
+    accept flag; launches after removal ignore the word."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dreamplace_b200._native import C
+    n = 1000
+    xy = torch.arange(2 * n, dtype=torch.float32, device="cuda")
+    order = torch.arange(n - 1, -1, -1, dtype=torch.int32, device="cuda")
+    gate = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rejected = torch.zeros(1, dtype=torch.float64, device="cuda")
+    accepted = torch.ones(1, dtype=torch.float64, device="cuda")
+    out = torch.full((2 * n,), -1.0, device="cuda")
+    C.set_trial_gate(gate)
+    try:
+        C.trial_gate(gate, rejected)
+        C.gather_order_xy(xy, order, n, out)
+        assert gate.item() == 1 and bool((out == -1.0).all())
+        C.trial_gate(gate, accepted)
+        C.gather_order_xy(xy, order, n, out)
+        assert gate.item() == 0
+        assert torch.equal(out.view(-1, 2), xy.view(-1, 2)[order.long()])
+        C.trial_gate(gate, rejected)
+    finally:
+        C.set_trial_gate(None)
+    out.fill_(-1.0)
+    C.gather_order_xy(xy, order, n, out)  # gate removed: runs although the word is set
+    assert gate.item() == 1 and torch.equal(out.view(-1, 2), xy.view(-1, 2)[order.long()])
