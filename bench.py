@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host round-trip run (profiling)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the per-kernel timing (profiling)")
+    ap.add_argument("--no-speculate", action="store_true",
+                    help="enqueue each GP iteration after the host read the previous one (profiling: no trial is "
+                         "enqueued ahead and voided)")
     return ap.parse_args()
 
 
@@ -181,11 +184,11 @@ def replica_value(steps, world, ms_max):
 class TimedRun(object):
     """Runs the GP loop and times iterations [warmup, warmup + steps) with CUDA events."""
 
-    def __init__(self, design, precision, world, e2e=False, time_pieces=False):
+    def __init__(self, design, precision, world, e2e=False, time_pieces=False, speculate=True):
         from dreamplace_b200.nonlinear_place import NonLinearPlace
         from dreamplace_b200.params import Params
         self.params = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision=precision,
-                             deterministic_flag=0, time_pieces=time_pieces)
+                             deterministic_flag=0, time_pieces=time_pieces, speculate=speculate)
         self.dominant = None
         self.dominant_ms = None
         self.design = design
@@ -548,7 +551,8 @@ def main():
     peaks = load_peaks()
     W, K = max(args.warmup, 3), args.steps
     clocks = ClockSampler(local) if rank == 0 else None
-    run = TimedRun(design, args.precision, world, time_pieces=not args.no_roofline)
+    spec = not args.no_speculate
+    run = TimedRun(design, args.precision, world, time_pieces=not args.no_roofline, speculate=spec)
     ms = run.run(W, K, clocks=clocks)
     clk = clocks.stop() if clocks else None
     ms = max_over_ranks(ms, world)
@@ -557,7 +561,7 @@ def main():
     # end-to-end through the public API with a host round trip per step
     e2e = None
     if not args.no_e2e:
-        run_e2e = TimedRun(design, args.precision, world, e2e=True)
+        run_e2e = TimedRun(design, args.precision, world, e2e=True, speculate=spec)
         ms_e2e = max_over_ranks(run_e2e.run(W, K), world)
         e2e = {"value": round(replica_value(K, world, ms_e2e), 3), "unit": UNIT,
                "h2d_bytes_per_step": run_e2e.h2d, "d2h_bytes_per_step": run_e2e.d2h}
@@ -570,7 +574,7 @@ def main():
                               "trials of the timed region")
     plain = None
     if not args.no_plain and args.precision != "fp32":
-        prun = TimedRun(design, "fp32", world)
+        prun = TimedRun(design, "fp32", world, speculate=spec)
         pms = max_over_ranks(prun.run(W, K), world)
         pval = world * K / (pms / 1000.0)
         h_ours = run.placer.metrics[-1][-1][-1]._host[0]
