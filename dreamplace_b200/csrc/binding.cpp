@@ -431,12 +431,14 @@ void trial_gate(at::Tensor gate, c10::optional<at::Tensor> accept_prev) {
                         cur_stream()));
 }
 
-void objective_finish(at::Tensor wl, at::Tensor energy, at::Tensor density_weight, at::Tensor factor_quad,
-                      at::Tensor obj, at::Tensor grad_scale) {
+void objective_finish(c10::optional<at::Tensor> wl, at::Tensor energy, at::Tensor density_weight,
+                      at::Tensor factor_quad, c10::optional<at::Tensor> obj, c10::optional<at::Tensor> grad_scale) {
   CHECK_F32(factor_quad);
   TORCH_CHECK(factor_quad.numel() >= 2, "factor_quad holds (density_factor, quad_c)");
-  DP_CALL(dp_objective_finish(ptr<double>(wl), ptr<double>(energy), ptr<float>(density_weight),
-                              ptr<float>(factor_quad), ptr<double>(obj), ptr<float>(grad_scale), cur_stream()));
+  DP_CALL(dp_objective_finish(wl.has_value() ? ptr<double>(*wl) : nullptr, ptr<double>(energy),
+                              ptr<float>(density_weight), ptr<float>(factor_quad),
+                              obj.has_value() ? ptr<double>(*obj) : nullptr,
+                              grad_scale.has_value() ? ptr<float>(*grad_scale) : nullptr, cur_stream()));
 }
 
 // density scatter into a caller-owned map (no allocation; graph friendly)

@@ -36,6 +36,21 @@ int launch_finish_sum(double* buf, int count, float* out_f32, cudaStream_t s) {
   return check_launch("finish_sum");
 }
 
+// two independent fixed-order reductions of `count` partials in one launch
+__global__ void finish_sum2_kernel(double* a, double* b, int count) {
+  double ra = finish_sum(a + 1, count);
+  double rb = finish_sum(b + 1, count);
+  if (threadIdx.x == 0) {
+    a[0] = ra;
+    b[0] = rb;
+  }
+}
+
+int launch_finish_sum2(double* a, double* b, int count, cudaStream_t s) {
+  finish_sum2_kernel<<<1, kReduceThreads, 0, s>>>(a, b, count);
+  return check_launch("finish_sum2");
+}
+
 }  // namespace dpb
 
 extern "C" const char* dp_last_error(void) { return dpb::g_err; }

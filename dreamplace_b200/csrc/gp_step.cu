@@ -419,9 +419,9 @@ __global__ void objective_finish_kernel(const double* wl, const double* energy, 
   double lam = (double)density_factor * (double)density_weight[0];
   double d = energy[0];
   double dp = quad_c > 0.f ? d * (1.0 + (double)quad_c * d) : d;
-  obj[0] = wl[0] + lam * dp;
+  if (obj) obj[0] = wl[0] + lam * dp;
   double dd = quad_c > 0.f ? 1.0 + 2.0 * (double)quad_c * d : 1.0;
-  grad_scale[0] = (float)(lam * dd);
+  if (grad_scale) grad_scale[0] = (float)(lam * dd);
 }
 
 }  // namespace dpb
@@ -430,7 +430,8 @@ using namespace dpb;
 
 extern "C" int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
                                    const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream) {
-  DP_REQUIRE(wl && energy && density_weight && factor_quad && obj && grad_scale, "dp_objective_finish: null pointer");
+  DP_REQUIRE(energy && density_weight && factor_quad && (obj || grad_scale) && (!obj || wl),
+             "dp_objective_finish: null pointer");
   objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, factor_quad, obj, grad_scale);
   return check_launch("dp_objective_finish");
 }
@@ -1289,10 +1290,8 @@ static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, doub
     wa_lane_kernel<false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
   int rc = check_launch(grad ? "dp_wa_lanes_forward" : "dp_hpwl_lanes");
   if (rc) return rc;
-  if (grad && hpwl_f64) {
-    rc = launch_finish_sum(hpwl_f64, blocks, nullptr, s);
-    if (rc) return rc;
-  }
+  // the WA total and the HPWL (same fixed-order reduction each) in one launch
+  if (grad && hpwl_f64) return launch_finish_sum2(out_f64, hpwl_f64, blocks, s);
   return launch_finish_sum(out_f64, blocks, nullptr, s);
 }
 

@@ -49,6 +49,7 @@ __device__ __forceinline__ double finish_sum(const double* partials, int count) 
 __global__ void finish_sum_kernel(double* buf, int count, float* out_f32);
 
 int launch_finish_sum(double* buf, int count, float* out_f32, cudaStream_t s);
+int launch_finish_sum2(double* a, double* b, int count, cudaStream_t s);
 
 // the largest grid a reduction may use (partials must fit in DP_REDUCE_DOUBLES - 1)
 constexpr int kMaxReduceBlocks = DP_REDUCE_DOUBLES - 1;

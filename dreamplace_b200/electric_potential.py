@@ -57,16 +57,17 @@ def poisson_flops(M, N, precision):
     return 3 * k * 2.0 * M * N * (M + N)
 
 
-def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy):
+def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy, rho_scale=1.0):
     """G1 and G2 of the solve: the two spectral operands a*wx, a*wy [M, N];
-    when ``energy`` (f64[1]) is given the G2 epilogue adds the energy to it."""
+    when ``energy`` (f64[1]) is given the G2 epilogue adds the energy to it.
+    The solve runs on rho * rho_scale (the scale is G1's alpha)."""
     M, N = rho.shape
     dev = rho.device
     cM = transform_matrices(M, prec, dev)[0]
     cN = transform_matrices(N, prec, dev)[0]
     # G1: T1^T = (rho C_N^T)^T, [N, M]
     t1 = Operand((N, M), prec, dev)
-    g1 = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=1.0, ldc=M)
+    g1 = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=float(rho_scale), ldc=M)
     if prec == 0:
         g1["a_hi"] = rho
     else:
@@ -103,18 +104,20 @@ def poisson_energy(rho, bin_size_x, bin_size_y, precision):
     return energy
 
 
-def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False):
+def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False, rho_scale=1.0):
     """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
 
     Returns (field_map_x, field_map_y, energy_f64[1]); energy is zero when
-    ``fast_mode``.  Four GEMM launches, see the module docstring."""
+    ``fast_mode``.  Four GEMM launches, see the module docstring.  With
+    rho_scale the map is normalised inside the first GEMM (its alpha): a
+    density map and rho_scale = 1 / bin area give the solve of rho."""
     prec = precision_code(precision)
     M, N = rho.shape
     dev = rho.device
     _, chM, shM = transform_matrices(M, prec, dev)
     _, chN, shN = transform_matrices(N, prec, dev)
     energy = torch.zeros(1, dtype=torch.float64, device=dev)
-    spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy)
+    spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy, rho_scale)
     # G3: U^T = (A R^T)^T for the x field (R = Ch_N) and the y field (Sh_N)
     rights = [chN, shN]
     us = [Operand((N, M), prec, dev) for _ in spec]

@@ -370,6 +370,9 @@ class GPEngine(object):
         ep = self.ep
         q_new = (s + 1) % NSLOT
         w = self.weights[s]
+        # (the WA forward was also run on a second stream beside the density
+        # chain: its kernels and the scatter's, or the GEMMs', slow each other
+        # down by about what they would overlap, ~1% net, so it runs in line)
         self._mark("wa_forward", 0)
         self.wirelength(v_new, self.H[q_new], w[2:3])
         self._mark("wa_forward", 1)
@@ -377,8 +380,9 @@ class GPEngine(object):
         self.scatter_maps(v_new, self.O[q_new])
         self._mark("density_scatter", 1)
         self._mark("poisson_gemms", 0)
-        self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
-        ex, ey, energy = poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
+        # rho = D / bin area is applied as the first GEMM's alpha
+        ex, ey, energy = poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode),
+                                       1.0 / (ep.bin_size_x * ep.bin_size_y))
         self._mark("poisson_gemms", 1)
         C.objective_finish(self.wl64, energy, w[0:1], self.factor_quad, self.obj64, self.grad_scale)
         self._mark("field_gather", 0)

@@ -461,7 +461,9 @@ int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node
 /* obj = wl + lambda_eff * D (1 + c D), lambda_eff = factor_quad[0] *
  * density_weight, c = factor_quad[1] (0: no quadratic penalty);
  * grad_scale = d obj / d D.  All operands live on the device, so a captured
- * graph follows changes of the density factor and penalty. */
+ * graph follows changes of the density factor and penalty.  Either output may
+ * be NULL (wl may be NULL with obj): grad_scale needs only the energy, so the
+ * field gather can start before the wirelength is summed. */
 int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
                         const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream);
 
