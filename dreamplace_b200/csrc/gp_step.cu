@@ -294,15 +294,16 @@ __global__ void __launch_bounds__(256) precondition_norms_kernel(
 // g'[i] = (wirelength pin sum of node i, nodes < num_movable) + (force of node i,
 // movable and filler nodes, read from order space through inv_order); then
 // g' /= max(1, pws + lambda*area), and the fp64 step-size norms as above.
-// One block per tile of kAsmNodes consecutive nodes.  The tile's movable pins
-// form one contiguous node-CSR range; the block gathers it kAsmPins at a time
-// into shared memory (kAsmPins / 256 independent gathers per thread, all in
-// flight together), then each thread folds its own node's staged pins in pin
-// order, so the sums are those of the sequential per-node loop.
-constexpr int kAsmNodes = 256;
-constexpr int kAsmPins = 2048;
+// One warp per tile of 32 consecutive nodes; the warps of a block work on
+// independent tiles, so no block barrier sits inside the loop.  The tile's
+// movable pins form one contiguous node-CSR range, gathered kAsmWarpPins at a
+// time (8 independent gathers per lane, through grad_index) into the warp's
+// shared buffer; each lane then folds its own node's staged pins in pin order,
+// so the sums are those of the sequential per-node loop.
+constexpr int kAsmThreads = 256;
+constexpr int kAsmWarpPins = 256;
 
-__global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
+__global__ void __launch_bounds__(kAsmThreads, 4) assemble_precondition_kernel(
     const float2* __restrict__ gnode, const int* __restrict__ node_start, const float* __restrict__ wl_scale_p,
     const float2* __restrict__ force_o, const int* __restrict__ inv_order, int num_movable, int num_filler,
     const float* __restrict__ pws, const float* __restrict__ area, const float* __restrict__ lam_p, int num_nodes,
@@ -310,15 +311,35 @@ __global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
     float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index,
     const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
-  __shared__ int s_start[kAsmNodes + 1];
-  __shared__ float2 s_q[kAsmPins];
+  __shared__ float2 s_q[kAsmThreads / 32][kAsmWarpPins];
   const float lam = *lam_p;
   const float ws = *wl_scale_p;
-  const int t = threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  float2* q_s = s_q[threadIdx.x >> 5];
+  const int warp = (blockIdx.x * kAsmThreads + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kAsmThreads) >> 5;
   double dv = 0.0, dg = 0.0;
-  for (int n0 = blockIdx.x * kAsmNodes; n0 < num_nodes; n0 += gridDim.x * kAsmNodes) {
-    const int i = n0 + t;
+  // the tile's pin offsets are loaded one tile ahead
+  int nx0 = 0, nx1 = 0;
+  {
+    const int i = warp * 32 + lane;
+    if (warp * 32 < num_movable && i < num_movable) {  // node_start holds an entry past the last movable node
+      nx0 = __ldg(node_start + i);
+      nx1 = __ldg(node_start + i + 1);
+    }
+  }
+  for (int n0 = warp * 32; n0 < num_nodes; n0 += nwarps * 32) {  // warp-uniform
+    const int i = n0 + lane;
     const bool valid = i < num_nodes;
+    const int my0 = nx0, my1 = nx1;
+    {
+      const int inext = n0 + nwarps * 32 + lane;
+      nx0 = nx1 = 0;
+      if (inext < num_movable) {
+        nx0 = __ldg(node_start + inext);
+        nx1 = __ldg(node_start + inext + 1);
+      }
+    }
     // the node's own loads first: independent of the pin gather below
     float2 f = make_float2(0.f, 0.f);
     float pw = 0.f, ar = 0.f, vnx = 0.f, vny = 0.f, vx = 0.f, vy = 0.f, gx0 = 0.f, gy0 = 0.f;
@@ -334,32 +355,28 @@ __global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
       gy0 = __ldcs(g + i + num_nodes);
     }
     float sx = 0.f, sy = 0.f;
-    const int m_cnt = min(num_movable - n0, kAsmNodes);  // movable nodes of the tile (block-uniform)
+    const int m_cnt = min(num_movable - n0, 32);  // movable nodes of the tile (warp-uniform)
     if (m_cnt > 0) {
-      // m_cnt + 1 offsets (up to kAsmNodes + 1: one more than the threads)
-      if (t < m_cnt) s_start[t] = __ldg(node_start + n0 + t);
-      if (t == 0) s_start[m_cnt] = __ldg(node_start + n0 + m_cnt);
-      __syncthreads();
-      const int p0 = s_start[0], p1 = s_start[m_cnt];
-      const int my0 = t < m_cnt ? s_start[t] : 0, my1 = t < m_cnt ? s_start[t + 1] : 0;
-      for (int c0 = p0; c0 < p1; c0 += kAsmPins) {
-        float2 q[kAsmPins / kAsmNodes];
+      const int p0 = __shfl_sync(0xffffffffu, my0, 0);
+      const int p1 = __shfl_sync(0xffffffffu, my1, m_cnt - 1);
+      for (int c0 = p0; c0 < p1; c0 += kAsmWarpPins) {
+        float2 q[kAsmWarpPins / 32];
 #pragma unroll
-        for (int j = 0; j < kAsmPins / kAsmNodes; ++j) {
-          const int k = c0 + j * kAsmNodes + t;
+        for (int j = 0; j < kAsmWarpPins / 32; ++j) {
+          const int k = c0 + 32 * j + lane;
           q[j] = make_float2(0.f, 0.f);
           if (k < p1) q[j] = grad_index ? gnode[__ldcs(grad_index + k)] : __ldcs(gnode + k);
         }
 #pragma unroll
-        for (int j = 0; j < kAsmPins / kAsmNodes; ++j) s_q[j * kAsmNodes + t] = q[j];
-        __syncthreads();
-        const int ka = max(my0, c0), kb = min(my1, c0 + kAsmPins);
+        for (int j = 0; j < kAsmWarpPins / 32; ++j) q_s[32 * j + lane] = q[j];
+        __syncwarp();
+        const int ka = max(my0, c0), kb = min(my1, c0 + kAsmWarpPins);
         for (int k = ka; k < kb; ++k) {
-          const float2 w = s_q[k - c0];
+          const float2 w = q_s[k - c0];
           sx = fadd(sx, fmul(w.x, ws));
           sy = fadd(sy, fmul(w.y, ws));
         }
-        __syncthreads();  // s_q is refilled by the next chunk
+        __syncwarp();  // q_s is refilled by the next chunk or tile
       }
     }
     if (valid) {
@@ -373,7 +390,6 @@ __global__ void __launch_bounds__(kAsmNodes, 4) assemble_precondition_kernel(
       dv += a1 * a1 + a2 * a2;
       dg += b1 * b1 + b2 * b2;
     }
-    __syncthreads();  // s_start is rewritten by the next tile
   }
   block_partial2(dv, dg, partials);
 }
@@ -957,10 +973,10 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   DP_REQUIRE(num_nodes > 0 && num_movable >= 0 && num_filler >= 0 && num_movable + num_filler <= num_nodes,
              "dp_assemble_precondition_step: bad node counts");
   cudaStream_t s = as_stream(stream);
-  int blocks = grid_for(num_nodes, kAsmNodes, 4);
+  int blocks = grid_for(num_nodes, kAsmThreads, 4);
   if (blocks > DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
-  assemble_precondition_kernel<<<blocks, kAsmNodes, 0, s>>>(
+  assemble_precondition_kernel<<<blocks, kAsmThreads, 0, s>>>(
       reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
       inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index,
       trial_gate());
