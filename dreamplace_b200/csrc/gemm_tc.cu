@@ -3,7 +3,7 @@
 // C[m,n] = sum_k A[m,k] * B[n,k], A and B K-contiguous in global memory.
 // One CTA computes a 128 x BN tile (BN = 64 or 128): TMA (128-byte swizzle, no multicast)
 // stages A and B k-blocks into a STAGES-deep shared-memory ring, one thread
-// issues tcgen05.mma (M=128, N=BN) into a TMEM accumulator, and all four
+// issues tcgen05.mma (M=128, N=BN) into a TMEM accumulator, and all eight
 // warps read the accumulator back with tcgen05.ld for the fused epilogue
 // (transposed operand store with bf16 hi/lo split, spectral scaling, fp32
 // field store, or the energy dot product; epilogue.cuh).
@@ -25,7 +25,7 @@ namespace dpb {
 __device__ int g_tc_status = 0;
 
 constexpr int TC_BM = 128;
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;  // 8 warps: producer, MMA issuer, and all 8 in the epilogue
 constexpr long long kWaitBudgetCycles = 4000000000ll;  // ~2 s at 2 GHz
 
 struct TcBatch {
@@ -258,10 +258,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     float* stage = reinterpret_cast<float*>(tiles);
     constexpr int kRowPitch = BN + 4;     // stage[m][n] for row-major outputs
     constexpr int kColPitch = TC_BM + 4;  // stage[n][m] for STORE_T
-    const int r_acc = warp * 32 + lane;   // accumulator row = TMEM lane
-    const uint32_t row_addr = tmem_base + ((uint32_t)(warp * 32) << 16);
+    // a warp reads the TMEM lane quarter (warp % 4) it may access, and half of
+    // the columns (warp / 4)
+    const int quarter = warp & 3, half = warp >> 2;
+    const int r_acc = quarter * 32 + lane;  // accumulator row = TMEM lane
+    const uint32_t row_addr = tmem_base + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll 1
-    for (int c = 0; c < BN; c += 16) {
+    for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 16) {
       float v[16];
       tmem_ld16(row_addr + (uint32_t)c, v);
       if (trans) {
