@@ -545,6 +545,8 @@ class GPEngine(object):
         # reference's per-iteration move_boundary(pos) is the identity here,
         # and its evaluation (HPWL, overflow) was computed with it
         self._trial(s, head)
+        # the metrics' read-back is part of the trial (a copy node in the graph)
+        self.metrics_host[s].copy_(self.metrics[s], non_blocking=True)
 
     def _graph(self, s, head, warm=True):
         key = (s, head)
@@ -595,7 +597,6 @@ class GPEngine(object):
             before = C.launch_count()
             self._body(s, head)
             self.kernels_launched += C.launch_count() - before
-        self.metrics_host[s].copy_(self.metrics[s], non_blocking=True)
         if self.ready[s] is None:
             self.ready[s] = torch.cuda.Event()
         self.ready[s].record()

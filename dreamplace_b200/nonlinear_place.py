@@ -220,6 +220,13 @@ class NonLinearPlace(nn.Module):
             if len(x) < window:
                 return False
             x = x[-window:]
+            # plain floats decide unless the ratio is within rounding of the
+            # threshold, where numpy's mean (the reference's) decides
+            total = sum(x)
+            if total > 0.0:
+                r = (max(x) - min(x)) / (total / window)
+                if abs(r - threshold) > 1e-9 * threshold:
+                    return r < threshold
             return (np.max(x) - np.min(x)) / np.mean(x) < threshold
 
         for Lgamma_step in range(model.Lgamma_iteration):
