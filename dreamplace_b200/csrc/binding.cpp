@@ -475,13 +475,18 @@ void build_cell_records(at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor 
 void density_map_ordered_into(at::Tensor xy_o, at::Tensor rec4, at::Tensor ratio_o, int count,
                               c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh, double bsx,
                               double bsy, int nbx, int nby, int deterministic, c10::optional<at::Tensor> scratch,
-                              at::Tensor out) {
+                              at::Tensor out, c10::optional<at::Tensor> order) {
   CHECK_FLAT(xy_o); CHECK_F32(xy_o); CHECK_F32(rec4);
+  if (order.has_value()) {
+    CHECK_I32(*order);
+    TORCH_CHECK(order->numel() >= count, "density_map_ordered_into: order shorter than count");
+  }
   TORCH_CHECK(2 * count <= xy_o.numel() && 4 * count <= rec4.numel() && count <= ratio_o.numel(),
               "density_map_ordered_into: buffers smaller than count");
   TORCH_CHECK(out.numel() == (int64_t)nbx * nby, "density_map_ordered_into: output is not num_bins_x*num_bins_y");
   TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
-  DP_CALL(dp_density_map_ordered(ptr<float>(xy_o), ptr<float>(rec4), ptr<float>(ratio_o), count,
+  DP_CALL(dp_density_map_ordered(ptr<float>(xy_o), (const int*)ovp(order), ptr<float>(rec4), ptr<float>(ratio_o),
+                                 count,
                                  (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy), nbx, nby,
                                  deterministic, fraction_bits(xl, yl, xh, yh), (int64_t*)ovp(scratch),
                                  ptr<float>(out), cur_stream()));
@@ -491,7 +496,12 @@ void density_map_ordered_split(at::Tensor xy_o, at::Tensor rec4, at::Tensor rati
                                int count, c10::optional<at::Tensor> init, double xl, double yl, double xh, double yh,
                                double bsx, double bsy, int nbx, int nby, int deterministic,
                                c10::optional<at::Tensor> scratch, at::Tensor out_first, at::Tensor out_all,
-                               double target_area, double bin_area, c10::optional<at::Tensor> overflow_out) {
+                               double target_area, double bin_area, c10::optional<at::Tensor> overflow_out,
+                               c10::optional<at::Tensor> order) {
+  if (order.has_value()) {
+    CHECK_I32(*order);
+    TORCH_CHECK(order->numel() >= count, "density_map_ordered_split: order shorter than count");
+  }
   TORCH_CHECK(!overflow_out.has_value() || (overflow_out->scalar_type() == at::kDouble &&
                                             overflow_out->numel() >= DP_REDUCE_DOUBLES),
               "overflow_out needs DP_REDUCE_DOUBLES doubles");
@@ -501,7 +511,8 @@ void density_map_ordered_split(at::Tensor xy_o, at::Tensor rec4, at::Tensor rati
   TORCH_CHECK(out_first.numel() == (int64_t)nbx * nby && out_all.numel() == out_first.numel(),
               "density_map_ordered_split: outputs are not num_bins_x*num_bins_y");
   TORCH_CHECK(!deterministic || scratch.has_value(), "deterministic mode needs the int64 scratch map");
-  DP_CALL(dp_density_map_ordered_split(ptr<float>(xy_o), ptr<float>(rec4), ptr<float>(ratio_o),
+  DP_CALL(dp_density_map_ordered_split(ptr<float>(xy_o), (const int*)ovp(order), ptr<float>(rec4),
+                                       ptr<float>(ratio_o),
                                        num_first, count, (const float*)ovp(init), xl, yl, xh, yh, bsx, bsy,
                                        inv_f(bsx), inv_f(bsy), nbx, nby, deterministic, fraction_bits(xl, yl, xh, yh),
                                        (int64_t*)ovp(scratch), ptr<float>(out_first), ptr<float>(out_all),
@@ -510,12 +521,17 @@ void density_map_ordered_split(at::Tensor xy_o, at::Tensor rec4, at::Tensor rati
 
 void electric_force_ordered(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at::Tensor xy_o, at::Tensor rec4,
                             at::Tensor ratio_o, int count, double xl, double yl, double bsx, double bsy, int nbx,
-                            int nby, double scale, at::Tensor force_o) {
+                            int nby, double scale, at::Tensor force_o, c10::optional<at::Tensor> order) {
   CHECK_FLAT(xy_o); CHECK_F32(force_o);
+  if (order.has_value()) {
+    CHECK_I32(*order);
+    TORCH_CHECK(order->numel() >= count, "electric_force_ordered: order shorter than count");
+  }
   TORCH_CHECK(2 * count <= xy_o.numel() && 4 * count <= rec4.numel() && 2 * count <= force_o.numel(),
               "electric_force_ordered: buffers smaller than count");
   TORCH_CHECK(ex.numel() == (int64_t)nbx * nby && ey.numel() == ex.numel(), "electric_force_ordered: field map size");
   DP_CALL(dp_electric_force_ordered(ptr<float>(grad_scale), nbx, nby, ptr<float>(ex), ptr<float>(ey), ptr<float>(xy_o),
+                                    (const int*)ovp(order),
                                     ptr<float>(rec4), ptr<float>(ratio_o), count, xl, yl, bsx, bsy,
                                     inv_f(bsx), inv_f(bsy), (float)scale, ptr<float>(force_o), cur_stream()));
 }
@@ -691,11 +707,21 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("objective_finish", &objective_finish);
   m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);
-  m.def("density_map_ordered_into", &density_map_ordered_into);
+  m.def("density_map_ordered_into", &density_map_ordered_into, py::arg("xy_o"), py::arg("rec4"), py::arg("ratio_o"),
+        py::arg("count"), py::arg("init"), py::arg("xl"), py::arg("yl"), py::arg("xh"), py::arg("yh"), py::arg("bsx"),
+        py::arg("bsy"), py::arg("nbx"), py::arg("nby"), py::arg("deterministic"), py::arg("scratch"), py::arg("out"),
+        py::arg("order") = py::none());
   m.def("build_cell_records", &build_cell_records);
   m.def("gather_order_xy", &gather_order_xy);
-  m.def("density_map_ordered_split", &density_map_ordered_split);
-  m.def("electric_force_ordered", &electric_force_ordered);
+  m.def("density_map_ordered_split", &density_map_ordered_split, py::arg("xy_o"), py::arg("rec4"),
+        py::arg("ratio_o"), py::arg("num_first"), py::arg("count"), py::arg("init"), py::arg("xl"), py::arg("yl"),
+        py::arg("xh"), py::arg("yh"), py::arg("bsx"), py::arg("bsy"), py::arg("nbx"), py::arg("nby"),
+        py::arg("deterministic"), py::arg("scratch"), py::arg("out_first"), py::arg("out_all"),
+        py::arg("target_area"), py::arg("bin_area"), py::arg("overflow_out"), py::arg("order") = py::none());
+  m.def("electric_force_ordered", &electric_force_ordered, py::arg("grad_scale"), py::arg("ex"), py::arg("ey"),
+        py::arg("xy_o"), py::arg("rec4"), py::arg("ratio_o"), py::arg("count"), py::arg("xl"), py::arg("yl"),
+        py::arg("bsx"), py::arg("bsy"), py::arg("nbx"), py::arg("nby"), py::arg("scale"), py::arg("force_o"),
+        py::arg("order") = py::none());
   m.def("assemble_precondition_step", &assemble_precondition_step);
   m.def("plan_net_chunks", &plan_net_chunks);
   m.def("wa_chunk_forward", &wa_chunk_forward);

@@ -168,6 +168,7 @@ __device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0,
 template <bool kFixed, int kRadixBits>
 __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a, int sort_cells,
                                                                         const float2* __restrict__ xy_o,
+                                                                        const int* __restrict__ order,
                                                                         const float4* __restrict__ rec4,
                                                                         const float* __restrict__ ratio_o, int count,
                                                                         float fx_scale, float* map_f32,
@@ -193,7 +194,8 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_ker
     nx[c] = ny[c] = sxs[c] = sys[c] = rr[c] = 0.f;
     if (idx < count) {
       const float4 r4 = __ldg(rec4 + idx);
-      const float2 p = __ldg(xy_o + idx);
+      // positions in visiting order, or in node order read through the order
+      const float2 p = order ? __ldg(xy_o + __ldg(order + idx)) : __ldg(xy_o + idx);
       sxs[c] = r4.x;
       sys[c] = r4.y;
       nx[c] = fadd(p.x, r4.z);
@@ -777,7 +779,8 @@ namespace {
 
 struct OrderedScatter {
   TriangleArgs a;
-  const float2* xy_o;
+  const float2* xy_o;  // visiting order, or node order when `order` is given
+  const int* order;
   const float4* rec4;
   const float* ratio_o;
   cudaStream_t s;
@@ -800,11 +803,13 @@ int scatter_range_r(const OrderedScatter& o, int begin, int end, int determinist
   const int blocks = ceil_div(count, kWsCells);
   if (deterministic)
     window_scatter_kernel<true, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits),
+        o.a, sort_cells, o.order ? o.xy_o : o.xy_o + begin, o.order ? o.order + begin : nullptr, o.rec4 + begin,
+        o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits),
         nullptr, reinterpret_cast<unsigned long long*>(scratch), trial_gate());
   else
     window_scatter_kernel<false, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, sort_cells, o.xy_o + begin, o.rec4 + begin, o.ratio_o + begin, count, 0.f, out, nullptr,
+        o.a, sort_cells, o.order ? o.xy_o : o.xy_o + begin, o.order ? o.order + begin : nullptr, o.rec4 + begin,
+        o.ratio_o + begin, count, 0.f, out, nullptr,
         trial_gate());
   return check_launch("dp_density_map_ordered scatter");
 }
@@ -831,7 +836,8 @@ int start_map(const float* init, float* out, int nbins, cudaStream_t s) {
   return DP_OK;
 }
 
-int ordered_setup(const char* who, const float* xy_o, const float* rec4, const float* ratio_o, int count, float xl,
+int ordered_setup(const char* who, const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
+                  int count, float xl,
                   float yl, float bsx, float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
                   int fraction_bits, int64_t* scratch, dp_stream_t stream, OrderedScatter& o) {
   DP_REQUIRE(xy_o && rec4 && ratio_o, "%s: null pointer", who);
@@ -844,6 +850,7 @@ int ordered_setup(const char* who, const float* xy_o, const float* rec4, const f
   o.a.xl = xl; o.a.yl = yl; o.a.bsx = bsx; o.a.bsy = bsy; o.a.inv_bsx = ibx; o.a.inv_bsy = iby;
   o.a.num_bins_x = nbx; o.a.num_bins_y = nby;
   o.xy_o = reinterpret_cast<const float2*>(xy_o);
+  o.order = order;
   o.rec4 = reinterpret_cast<const float4*>(rec4);
   o.ratio_o = ratio_o;
   o.s = as_stream(stream);
@@ -854,12 +861,13 @@ int ordered_setup(const char* who, const float* xy_o, const float* rec4, const f
 
 // Order-driven scatter (see window_scatter_kernel): cells 0..count of the
 // visiting order, positions (xy_o) and attributes (rec4, ratio_o) in that order.
-extern "C" int dp_density_map_ordered(const float* xy_o, const float* rec4, const float* ratio_o, int count,
+extern "C" int dp_density_map_ordered(const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
+                                      int count,
                                       const float* init, float xl, float yl, float xh, float yh, float bsx,
                                       float bsy, float ibx, float iby, int nbx, int nby, int deterministic,
                                       int fraction_bits, int64_t* scratch, float* out, dp_stream_t stream) {
   OrderedScatter o;
-  int rc = ordered_setup("dp_density_map_ordered", xy_o, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx, nby,
+  int rc = ordered_setup("dp_density_map_ordered", xy_o, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx, nby,
                          deterministic, fraction_bits, scratch, stream, o);
   if (rc) return rc;
   DP_REQUIRE(out, "dp_density_map_ordered: null output");
@@ -884,13 +892,14 @@ extern "C" int dp_density_map_ordered(const float* xy_o, const float* rec4, cons
 // scatter of all cells can take.  Only the first range gets the block-local
 // sort (the second one is the engine's fillers, spread about one per bin, for
 // which runs of equal start bins stay short anyway).
-extern "C" int dp_density_map_ordered_split(const float* xy_o, const float* rec4, const float* ratio_o, int num_first, int count, const float* init,
+extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order, const float* rec4,
+                                            const float* ratio_o, int num_first, int count, const float* init,
                                             float xl, float yl, float xh, float yh, float bsx, float bsy, float ibx,
                                             float iby, int nbx, int nby, int deterministic, int fraction_bits,
                                             int64_t* scratch, float* out_first, float* out_all, double target_area,
                                             double bin_area, double* overflow_out, dp_stream_t stream) {
   OrderedScatter o;
-  int rc = ordered_setup("dp_density_map_ordered_split", xy_o, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx,
+  int rc = ordered_setup("dp_density_map_ordered_split", xy_o, order, rec4, ratio_o, count, xl, yl, bsx, bsy, ibx, iby, nbx,
                          nby, deterministic, fraction_bits, scratch, stream, o);
   if (rc) return rc;
   DP_REQUIRE(out_first && out_all && out_first != out_all, "dp_density_map_ordered_split: bad outputs");

@@ -59,19 +59,20 @@ __global__ void zero_range_kernel(float* a, int begin, int end, float* b) {
 constexpr int kForceWin = 4;  // standard cells cover at most 4 x 4 bins
 
 // Field gather over cells in visiting order (engine path): attributes from the
-// per-cell records, positions from xy_o (both in visiting order); the force pair is written in order
+// per-cell records, positions from xy_o (both in visiting order, or xy_o in
+// node order read through `order`); the force pair is written in order
 // space, force_o[idx] = scale * grad * ratio * sum(px py E), for the gradient
 // assembly kernel to pick up per node.
 __global__ void __launch_bounds__(256) electric_force_records_kernel(
     const float* __restrict__ grad_pos, int nbx, int nby, const float* __restrict__ ex, const float* __restrict__ ey,
-    const float2* __restrict__ xy_o, const float4* __restrict__ rec4,
+    const float2* __restrict__ xy_o, const int* __restrict__ order, const float4* __restrict__ rec4,
     const float* __restrict__ ratio_o, int count, float xl, float yl, float bsx, float bsy, float ibx, float iby,
     float scale, float2* __restrict__ force_o, const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
   const float g = grad_pos[0];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
     const float4 r4 = __ldcs(rec4 + idx);
-    const float2 p = __ldg(xy_o + idx);
+    const float2 p = order ? __ldg(xy_o + __ldg(order + idx)) : __ldg(xy_o + idx);
     const float sx = r4.x, sy = r4.y;
     const float nx = fadd(p.x, r4.z);
     const float ny = fadd(p.y, r4.w);
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(256) electric_force_records_kernel(
 using namespace dpb;
 
 extern "C" int dp_electric_force_ordered(const float* grad_pos, int nbx, int nby, const float* ex, const float* ey,
-                                         const float* xy_o, const float* rec4, const float* ratio_o,
+                                         const float* xy_o, const int* order, const float* rec4,
+                                         const float* ratio_o,
                                          int count, float xl, float yl, float bsx, float bsy, float ibx, float iby,
                                          float scale, float* force_o, dp_stream_t stream) {
   DP_REQUIRE(grad_pos && ex && ey && xy_o && rec4 && ratio_o && force_o,
@@ -133,7 +135,7 @@ extern "C" int dp_electric_force_ordered(const float* grad_pos, int nbx, int nby
              "dp_electric_force_ordered: misaligned xy_o / rec4 / force_o");
   if (count == 0) return DP_OK;
   electric_force_records_kernel<<<grid_for(count, 256, 16), 256, 0, as_stream(stream)>>>(
-      grad_pos, nbx, nby, ex, ey, reinterpret_cast<const float2*>(xy_o), reinterpret_cast<const float4*>(rec4),
+      grad_pos, nbx, nby, ex, ey, reinterpret_cast<const float2*>(xy_o), order, reinterpret_cast<const float4*>(rec4),
       ratio_o, count, xl, yl, bsx, bsy, ibx, iby, scale, reinterpret_cast<float2*>(force_o), trial_gate());
   return check_launch("dp_electric_force_ordered");
 }

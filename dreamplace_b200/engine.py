@@ -58,16 +58,12 @@ class GPEngine(object):
         self.slot_node = data.pin2node_map[fnp].to(torch.int32).contiguous()
         self.slot_offx = data.pin_offset_x[fnp].contiguous()
         self.slot_offy = data.pin_offset_y[fnp].contiguous()
-        self.slot_net = data.pin2net_map[fnp].to(torch.int32).contiguous()
         slot_of_pin = torch.empty(P, dtype=torch.int64, device=dev)
         slot_of_pin[fnp] = torch.arange(P, device=dev)
         self.node_slots = slot_of_pin[data.flat_node2pin_map.long()].to(torch.int32).contiguous()
         self.node_start = data.flat_node2pin_start_map
         self.netpin_start = data.flat_net2pin_start_map
-        # warp-per-chunk WA / HPWL: nets packed into <= 32-pin chunks; the WA
-        # gradient lands at each pin's position in node-CSR order
-        self.chunk_net = C.plan_net_chunks(self.netpin_start.cpu(), 32).to(dev)
-        self.chunk_pin = self.netpin_start[self.chunk_net.long()].contiguous()
+        # each pin's position in node-CSR order (where the assembly reads its gradient)
         csr_pos = torch.empty(P, dtype=torch.int64, device=dev)
         csr_pos[self.node_slots.long()] = torch.arange(P, device=dev)
         self.csr_pos = csr_pos.to(torch.int32)
@@ -159,9 +155,13 @@ class GPEngine(object):
         self.force_o = torch.empty(2 * count, dtype=torch.float32, device=dev)
         self._build_records()
         self.sort_interval = int(getattr(params, "sort_interval", 50))
-        # how the trial point reaches the visiting-order copy: "gather" (a
-        # gather kernel after the trial) or "trial" (scattered writes in it)
+        # how the scatter and the field gather read the trial point: "gather"
+        # (a visiting-order copy gathered after the trial), "trial" (the copy
+        # written by scattered stores in the trial kernel) or "order" (no copy:
+        # the kernels read the node-order positions through the order)
         self.xyo_mode = getattr(params, "xyo_mode", "gather")
+        if self.xyo_mode not in ("gather", "trial", "order"):
+            raise ValueError("xyo_mode must be 'gather', 'trial' or 'order'")
         # optional per-piece device timing of the trial (CUDA events recorded
         # inside the captured graph); piece_query selects the pieces whose
         # durations are accumulated after each trial
@@ -234,10 +234,11 @@ class GPEngine(object):
     def _density(self, v, num_filler, out):
         ep = self.ep
         count = ep.num_movable_nodes + (num_filler if num_filler else 0)
-        C.density_map_ordered_into(self.xyo(v), self.rec4, self.ratio_o, count,
+        xy_o, order = self._cells_xy(v)
+        C.density_map_ordered_into(xy_o, self.rec4, self.ratio_o, count,
                                    ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl), float(ep.xh),
                                    float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y), ep.num_bins_x,
-                                   ep.num_bins_y, int(self.det), self.scratch, out)
+                                   ep.num_bins_y, int(self.det), self.scratch, out, order=order)
 
     def refresh_order(self, v):
         """Sort movable and filler cells by the bin where their stretched footprint
@@ -260,7 +261,8 @@ class GPEngine(object):
                 of = torch.sort(key[n - nf:]).indices.to(torch.int32).add_(n - nf)
                 self.order[nm:].copy_(of)
             self._build_records()
-            C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
+            if self.xyo_mode != "order":
+                C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
 
     def xy(self, v):
         return self._xy_of[v.data_ptr()]
@@ -268,11 +270,20 @@ class GPEngine(object):
     def xyo(self, v):
         return self._xyo_of[v.data_ptr()]
 
+    def _cells_xy(self, v):
+        """(positions, order) for the scatter and the field gather: the
+        visiting-order copy, or (xyo_mode "order") the node-order interleaved
+        copy read through the visiting order."""
+        if self.xyo_mode == "order":
+            return self.xy(v), self.order
+        return self.xyo(v), None
+
     def pack(self, v):
         """Refresh the interleaved and the visiting-order copies of a position buffer
         written outside the trial kernel."""
         C.pack_xy(v, self.xy(v))
-        C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
+        if self.xyo_mode != "order":
+            C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))
 
     def wirelength(self, v, hpwl_out=None, inv_gamma=None):
         """WA forward at node positions v: fp64 total in self.wl64, per-pin gradient (times the
@@ -298,11 +309,12 @@ class GPEngine(object):
         """One scatter of v: the movable-only map (self.omap) and the movable +
         filler map (self.dmap); (overflow, max density) of v into ovf_out."""
         ep = self.ep
-        C.density_map_ordered_split(self.xyo(v), self.rec4, self.ratio_o, ep.num_movable_nodes,
+        xy_o, order = self._cells_xy(v)
+        C.density_map_ordered_split(xy_o, self.rec4, self.ratio_o, ep.num_movable_nodes,
                                     self.order.numel(), ep.initial_density_map.view(-1), float(ep.xl), float(ep.yl),
                                     float(ep.xh), float(ep.yh), float(ep.bin_size_x), float(ep.bin_size_y),
                                     ep.num_bins_x, ep.num_bins_y, int(self.det), self.scratch, self.omap.view(-1),
-                                    self.dmap.view(-1), self.ovf_target, self.ovf_area, ovf_out)
+                                    self.dmap.view(-1), self.ovf_target, self.ovf_area, ovf_out, order=order)
 
     def density_energy(self, v, ovf_out=None):
         """Density map, Poisson solve; returns (ex, ey, energy_f64[1]).  With ovf_out,
@@ -318,9 +330,10 @@ class GPEngine(object):
     def field_force(self, v, ex, ey):
         """Field force of every movable and filler cell, in visiting order (self.force_o)."""
         ep = self.ep
-        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), self.xyo(v), self.rec4,
+        xy_o, order = self._cells_xy(v)
+        C.electric_force_ordered(self.grad_scale, ex.view(-1), ey.view(-1), xy_o, self.rec4,
                                  self.ratio_o, self.order.numel(), float(ep.xl), float(ep.yl), float(ep.bin_size_x),
-                                 float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o)
+                                 float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y, -1.0, self.force_o, order=order)
 
     def assemble(self, v, g, v_new, g_new, s=None):
         """Preconditioned gradient at v_new into g_new (pin sum + force) and the fp64
@@ -523,7 +536,7 @@ class GPEngine(object):
         C.nesterov_trial(v, g, u, un, vn, self.XY[t], st, self.data.node_size_x, self.data.node_size_y,
                          float(d.xl), float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes,
                          self.inv_order if scatter_write else None, self.XYO[t] if scatter_write else None)
-        if not scatter_write:
+        if self.xyo_mode == "gather":
             C.gather_order_xy(self.XY[t], self.order, self.order.numel(), self.XYO[t])
         self._mark("nesterov_trial", 1)
         energy = self.objective_and_step(v, g, vn, gn, s)

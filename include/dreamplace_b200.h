@@ -131,8 +131,10 @@ int dp_gather_order_xy(const float* xy, const int* order, int count, float* xy_o
  * accumulate in registers (bin box <= 16 bins) or a shared-memory tile over
  * their bin box before touching global memory, so a spatial order turns most
  * global atomics into local ones.  deterministic != 0: int64 fixed point
- * (scratch_fixed [num_bins] required). */
-int dp_density_map_ordered(const float* xy_o, const float* rec4, const float* ratio_o,
+ * (scratch_fixed [num_bins] required).  order (optional): the visiting order
+ * itself; then xy_o holds the positions in node order and cell idx is read at
+ * xy_o[order[idx]], so no visiting-order copy of the positions is needed. */
+int dp_density_map_ordered(const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
                            int count, const float* initial_density_map,
                            float xl, float yl, float xh, float yh,
                            float bin_size_x, float bin_size_y,
@@ -146,8 +148,10 @@ int dp_density_map_ordered(const float* xy_o, const float* rec4, const float* ra
  * movable + filler map (Poisson input) of one position, so each cell is
  * scattered once.  Deterministic: both maps bit-exact with separate scatters.
  * overflow_out (optional, DP_REDUCE_DOUBLES doubles): dp_density_overflow of
- * out_first with target_area and bin_area, computed in the same pass. */
-int dp_density_map_ordered_split(const float* xy_o, const float* rec4, const float* ratio_o, int num_first, int count, const float* initial_density_map,
+ * out_first with target_area and bin_area, computed in the same pass.
+ * order: as dp_density_map_ordered. */
+int dp_density_map_ordered_split(const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
+                                 int num_first, int count, const float* initial_density_map,
                                  float xl, float yl, float xh, float yh,
                                  float bin_size_x, float bin_size_y,
                                  float inv_bin_size_x, float inv_bin_size_y,
@@ -212,9 +216,10 @@ int dp_electric_force(const float* grad_pos, int num_bins_x, int num_bins_y,
 
 /* Field gather of the cells 0..count of a visiting order (records as
  * dp_build_cell_records, positions in the same order in xy_o); force_o[2*idx..2*idx+1] = scale * grad_pos[0] *
- * ratio * sum(px py E), in the CPU op's per-cell order without contraction. */
+ * ratio * sum(px py E), in the CPU op's per-cell order without contraction.
+ * order: as dp_density_map_ordered. */
 int dp_electric_force_ordered(const float* grad_pos, int num_bins_x, int num_bins_y,
-                              const float* field_map_x, const float* field_map_y, const float* xy_o,
+                              const float* field_map_x, const float* field_map_y, const float* xy_o, const int* order,
                               const float* rec4, const float* ratio_o, int count,
                               float xl, float yl, float bin_size_x, float bin_size_y,
                               float inv_bin_size_x, float inv_bin_size_y, float scale, float* force_o,

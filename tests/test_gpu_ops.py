@@ -493,6 +493,27 @@ def test_ordered_split_scatter(C):
             tol = 1e-4 * float(exp_full.abs().max())
             torch.testing.assert_close(first, exp_first, rtol=1e-4, atol=tol)
             torch.testing.assert_close(full, exp_full, rtol=1e-4, atol=tol)
+        # node-order positions read through the order: the same maps and overflow
+        first2, full2 = torch.empty(nb, device="cuda"), torch.empty(nb, device="cuda")
+        ovf2 = torch.zeros(1280, dtype=torch.float64, device="cuda")
+        C.density_map_ordered_split(xy, rec4, ratio_o, m, len(order), init, *geo, det, scratch if det else None,
+                                    first2, full2, 0.9 * ba, ba, ovf2, order=dev(order))
+        if det:
+            assert torch.equal(first2, first) and torch.equal(full2, full) and torch.equal(ovf2[:2], ovf[:2])
+        else:
+            tol = 1e-4 * float(full.abs().max())
+            torch.testing.assert_close(full2, full, rtol=1e-4, atol=tol)
+    # the field gather through the order equals the gather from the ordered copy
+    fx = dev(np.random.RandomState(5).standard_normal(nb).astype(np.float32))
+    fy = dev(np.random.RandomState(6).standard_normal(nb).astype(np.float32))
+    grad = torch.tensor([0.5], device="cuda")
+    fo1 = torch.empty(2 * len(order), device="cuda")
+    fo2 = torch.empty_like(fo1)
+    C.electric_force_ordered(grad, fx, fy, order_xy(C, xy, order), rec4, ratio_o, len(order), d.xl, d.yl,
+                             d.bin_size_x, d.bin_size_y, d.num_bins_x, d.num_bins_y, -1.0, fo1)
+    C.electric_force_ordered(grad, fx, fy, xy, rec4, ratio_o, len(order), d.xl, d.yl, d.bin_size_x, d.bin_size_y,
+                             d.num_bins_x, d.num_bins_y, -1.0, fo2, order=dev(order))
+    assert torch.equal(fo1, fo2)
 
 
 def lane_inputs(C, d, net_order=None):
