@@ -172,3 +172,17 @@ def test_trial_gate_skips_gated_kernels():
     out.fill_(-1.0)
     C.gather_order_xy(xy, order, n, out)  # gate removed: runs although the word is set
     assert gate.item() == 1 and torch.equal(out.view(-1, 2), xy.view(-1, 2)[order.long()])
+
+
+@pytest.mark.parametrize("xyo_mode,wa_grad_order", [("order", "lane"), ("trial", "lane"), ("gather", "csr")])
+def test_engine_layout_options_give_the_same_trajectory(design, xyo_mode, wa_grad_order):
+    """The engine's layout options (how the scatter reads the trial point, where
+    the WA gradient is written) change no arithmetic: deterministic runs give
+    the default layout's trajectory bit for bit."""
+    def traj(**kw):
+        t = []
+        p = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision="fp32",
+                   deterministic_flag=1, **kw)
+        place(design, p, max_iterations=40, callback=lambda it, m: t.append((m.hpwl, m.overflow, m.objective)))
+        return t
+    assert traj(xyo_mode=xyo_mode, wa_grad_order=wa_grad_order) == traj()
