@@ -67,10 +67,14 @@ class BatchPlacer(object):
         latencies = []
         last = [None] * n
         active = list(range(n))
-        while active:
-            still = []
-            for i in active:
-                with torch.cuda.stream(streams[i]):
+        home = torch.cuda.current_stream()
+        try:
+            while active:
+                still = []
+                for i in active:
+                    # set_stream, not a stream context: the context's current-stream
+                    # lookups cost more host time than a small design's iteration
+                    torch.cuda.set_stream(streams[i])
                     try:
                         next(gens[i])
                         now = time.perf_counter()
@@ -80,7 +84,9 @@ class BatchPlacer(object):
                         still.append(i)
                     except StopIteration as stop:
                         results[i] = stop.value
-            active = still
+                active = still
+        finally:
+            torch.cuda.set_stream(home)
         torch.cuda.synchronize()
         return results, latencies
 
