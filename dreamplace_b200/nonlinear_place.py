@@ -196,10 +196,8 @@ class NonLinearPlace(nn.Module):
         flat_llambda = 0
         self.iteration_times = []
 
-        def check_divergence(window=50, threshold=0.05):
-            if len(divergence_list) < window or best["metric"] is None:
-                return False
-            x = np.array(divergence_list[-window:])
+        def divergence_numpy(xs, threshold):
+            x = np.array(xs)
             overflow_mean = np.mean(x[:, 1])
             overflow_diff = np.sum(np.maximum(0, np.sign(x[1:, 1] - x[:-1, 1]))) / (x.shape[0] - 1)
             overflow_range = np.max(x[:, 1]) - np.min(x[:, 1])
@@ -213,6 +211,34 @@ class NonLinearPlace(nn.Module):
                 if overflow_range / overflow_mean < threshold:
                     return True
                 if overflow_diff > 0.6:
+                    return True
+            return False
+
+        def check_divergence(window=50, threshold=0.05):
+            if len(divergence_list) < window or best["metric"] is None:
+                return False
+            xs = divergence_list[-window:]
+            # plain floats decide every comparison that is not within rounding
+            # of its bound; otherwise numpy's means (the reference's) decide
+            ov = [p[1] for p in xs]
+            n = len(ov)
+            overflow_mean = sum(ov) / n
+            wl_mean = sum(p[0] for p in xs) / n
+            bh, bo = best["metric"].hpwl, best["metric"].overflow
+            wl_ratio = (wl_mean - bh) / bh
+            overflow_ratio = (overflow_mean - max(params.stop_overflow, bo)) / bo
+            rng_ratio = (max(ov) - min(ov)) / overflow_mean if overflow_mean != 0.0 else None
+            close = lambda a, b: abs(a - b) <= 1e-9 * max(abs(a), abs(b))  # noqa: E731
+            if rng_ratio is None or close(wl_ratio, threshold * 1.2) or close(overflow_ratio, threshold) or \
+                    close(rng_ratio, threshold):
+                return divergence_numpy(xs, threshold)
+            if wl_ratio > threshold * 1.2:
+                if overflow_ratio > threshold:
+                    return True
+                if rng_ratio < threshold:
+                    return True
+                ups = sum(1 for a, b in zip(ov, ov[1:]) if b > a)
+                if ups / (n - 1) > 0.6:
                     return True
             return False
 
