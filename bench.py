@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split_bf16")
-    ap.add_argument("--design", default="config2", choices=["config1", "config2"])
+    ap.add_argument("--design", default="cells_2m", choices=["cells_10k", "cells_2m"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
@@ -62,7 +62,7 @@ def parse():
 
 def make_design(name):
     from dreamplace_b200 import synthetic
-    return synthetic.config2() if name == "config2" else synthetic.config1()
+    return synthetic.cells_2m() if name == "cells_2m" else synthetic.cells_10k()
 
 
 # ------------------------------------------------------------------ clocks

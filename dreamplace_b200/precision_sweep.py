@@ -138,7 +138,7 @@ def main(argv=None):
     if not torch.cuda.is_available():
         raise SystemExit("precision_sweep needs a CUDA device")
     precision_code("split_bf16")
-    design = synthetic.config1()
+    design = synthetic.cells_10k()
     snaps = snapshots(design, [int(x) for x in args.iterations.split(",")])
     sweep_sizes(design, snaps, [int(x) for x in args.sizes.split(",")])
     if args.gp:

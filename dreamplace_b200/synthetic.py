@@ -4,12 +4,12 @@ The reference reads designs through its C++ ``place_io`` (Bookshelf/LEF/DEF);
 no benchmark files exist on this machine, so designs are generated from a seed
 with the shapes, sizes and distributions of the hot-path workloads:
 
-* ``config1``  - 3000x3000 die, 250 rows of height 12, 10,000 movable cells of
+* ``cells_10k``  - 3000x3000 die, 250 rows of height 12, 10,000 movable cells of
   width U{2..32}, 50 fixed macros with sides U[60,300], 10,200 nets of degree
   2+Geometric(0.45) truncated at 50, 128x128 bins.
-* ``config2``  - 2.1M movable cells of width round(exp(U[ln1,ln40])), 1,000
+* ``cells_2m``   - 2.1M movable cells of width round(exp(U[ln1,ln40])), 1,000
   macros, 2.2M nets, square die sized for 70% utilisation, 1024x1024 bins.
-* ``scaled``   - the same generator at any cell count (config 4 / config 5).
+* ``scaled``     - the same generator at any cell count (``cells_50k``, batched designs).
 
 Pins are numbered in net order, as the reference's Bookshelf reader numbers
 them while reading the ``.nets`` file; 70% of a net's pins come from a
@@ -272,7 +272,7 @@ def _finish_from_arrays(name, xl, yl, xh, yh, row_height, mov_w, mov_h, mac_x, m
         extra={"filler_size": (filler_w, filler_h), "cell_utilization": cell_utilization})
 
 
-def config1(seed=1):
+def cells_10k(seed=1):
     """The CPU-runnable parity design (10k cells, 128x128 bins)."""
     rng = np.random.RandomState(seed)
     xl, yl, xh, yh, rh = 0.0, 0.0, 3000.0, 3000.0, 12.0
@@ -280,7 +280,7 @@ def config1(seed=1):
     mov_w = rng.randint(2, 33, size=m).astype(np.float32)
     mov_h = np.full(m, rh, dtype=np.float32)
     mx, my, mw, mh = _place_macros(rng, 50, 60, 300, xl, yl, xh, yh, rh)
-    return _finish("config1", seed, xl, yl, xh, yh, rh, mov_w, mov_h, mx, my, mw, mh,
+    return _finish("cells10k", seed, xl, yl, xh, yh, rh, mov_w, mov_h, mx, my, mw, mh,
                    10200, 128, 1.0, rng)
 
 
@@ -344,13 +344,13 @@ def scaled(num_movable, num_nets=None, num_macros=None, num_bins=None, seed=1, u
                    xs, ys, mac_w, mac_h, num_nets, num_bins, 1.0, rng)
 
 
-def config2(seed=1):
+def cells_2m(seed=1):
     """The op-level / full-GP scale design: 2.1M cells, 2.2M nets, 1024x1024 bins."""
     return scaled(2_100_000, num_nets=2_200_000, num_macros=1000, num_bins=1024, seed=seed,
-                  name="config2")
+                  name="cells2100k")
 
 
-def config4(seed=1):
+def cells_50k(seed=1):
     """50k cells at 256x256 bins (finite-difference check design)."""
-    return scaled(50_000, num_bins=256, seed=seed, name="config4")
+    return scaled(50_000, num_bins=256, seed=seed, name="cells50k")
 

@@ -6,7 +6,7 @@ from dreamplace_b200 import bookshelf, synthetic
 
 
 def test_round_trip(tmp_path):
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     aux = bookshelf.write_bookshelf(d, str(tmp_path))
     r = bookshelf.read_bookshelf(aux, num_bins=d.num_bins_x)
     assert (r.num_movable_nodes, r.num_terminals, r.num_nets, r.num_pins) == \

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def design():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    return synthetic.config1()
+    return synthetic.cells_10k()
 
 
 def run(design, engine, precision, iters=None, deterministic=0):

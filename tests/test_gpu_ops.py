@@ -102,7 +102,7 @@ def test_density_map_fp32(C, golden):
 def test_density_map_clustered_start(C):
     """All movable cells at the die centre (GP iteration 0): the warp-combined
     atomics must still produce the oracle's integer map exactly."""
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     pos = d.initial_positions()
     sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
     fx = C.density_map_fixed_point(dev(pos), sxc, syc, ox, oy, ratio, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
@@ -180,7 +180,7 @@ def test_wa_unit_golden(C, golden):
 
 
 def test_move_boundary_and_pws(C):
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     pos = d.initial_positions()
     pos[:100] = -50.0
     pos[d.num_nodes:d.num_nodes + 100] = 1e5
@@ -264,7 +264,7 @@ def test_density_map_exact_against_reference(C):
     if ref is None:
         pytest.skip("reference density_map_cpp not built")
     from dreamplace_b200.placement_ops import DensityMap
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     pos = d.initial_positions()
     rng = np.random.RandomState(5)
     m = d.num_movable_nodes

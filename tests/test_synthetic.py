@@ -4,8 +4,8 @@ import numpy as np
 from dreamplace_b200 import synthetic
 
 
-def test_config1_shapes():
-    d = synthetic.config1()
+def test_10k_design_shapes():
+    d = synthetic.cells_10k()
     assert d.num_movable_nodes == 10000 and d.num_terminals == 50
     assert d.num_nets == 10200 and d.num_bins_x == 128
     deg = np.diff(d.flat_net2pin_start_map)
@@ -38,7 +38,7 @@ def test_csr_consistency():
 
 
 def test_initial_positions_reference_rule():
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     pos = d.initial_positions()
     n, m = d.num_nodes, d.num_movable_nodes
     assert abs(pos[:m].mean() - 1500) < 1 and pos[:m].std() < 5

@@ -26,7 +26,7 @@ def test_noalloc_scatter_matches_scratch_entry_point():
         pytest.skip("no CUDA device")
     lib = ctypes.CDLL(LIB)
     lib.dp_last_error.restype = ctypes.c_char_p
-    d = synthetic.config1()
+    d = synthetic.cells_10k()
     pos_np = d.initial_positions()
     rng = np.random.RandomState(4)
     n, m = d.num_nodes, d.num_movable_nodes
