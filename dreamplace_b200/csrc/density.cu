@@ -131,12 +131,12 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
 // flushes its own window and adds only its own bins.  The fixed-point map is
 // independent of the summation order, so the deterministic result does not
 // depend on the visiting order or the tiling.
-constexpr int kWin = 4;
+constexpr int kWin = 3;
 constexpr int kWsThreads = 256;
 constexpr int kWsCellsPerLane = 4;
 constexpr int kWsWarpCells = 32 * kWsCellsPerLane;
 constexpr int kWsCells = kWsThreads * kWsCellsPerLane;
-constexpr int kWsSmemBytes = 32 * 1024;
+constexpr int kWsSmemBytes = 24 * 1024;
 
 template <typename Acc>
 __device__ __forceinline__ void add_to(Acc* tile, float* map_f32, unsigned long long* map_fx, bool use_tile, int slot,
@@ -166,7 +166,7 @@ __device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0,
 }
 
 template <bool kFixed, int kRadixBits>
-__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 3) window_scatter_kernel(TriangleArgs a, int sort_cells,
+__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_kernel(TriangleArgs a, int sort_cells,
                                                                         const float2* __restrict__ xy_o,
                                                                         const int* __restrict__ order,
                                                                         const float4* __restrict__ rec4,

@@ -128,7 +128,7 @@ int dp_gather_order_xy(const float* xy, const int* order, int count, float* xy_o
  * initial_density_map (NULL = zeros); positions (xy_o, interleaved) and
  * records (rec4, ratio_o) are both stored in that order.  Same
  * arithmetic as dp_density_map_f32 / _fx64.  Blocks of consecutive cells
- * accumulate in registers (bin box <= 16 bins) or a shared-memory tile over
+ * accumulate in registers (3 x 3-bin windows) or a shared-memory tile over
  * their bin box before touching global memory, so a spatial order turns most
  * global atomics into local ones.  deterministic != 0: int64 fixed point
  * (scratch_fixed [num_bins] required).  order (optional): the visiting order
