@@ -56,7 +56,7 @@ __global__ void zero_range_kernel(float* a, int begin, int end, float* b) {
   }
 }
 
-constexpr int kForceWin = 4;  // standard cells cover at most 4 x 4 bins
+constexpr int kForceWin = 3;  // almost every stretched cell covers at most 3 x 3 bins
 
 // Field gather over cells in visiting order (engine path): attributes from the
 // per-cell records, positions from xy_o (both in visiting order, or xy_o in
