@@ -1194,8 +1194,10 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
   }
 }
 
+// 4 blocks of 256 per SM: the 64-register cap spills a few words of the
+// 5..8-pin paths to L1, and still measures faster than 3 blocks without spills
 template <bool kGrad>
-__global__ void __launch_bounds__(256, 3) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
+__global__ void __launch_bounds__(256, 4) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
                                                       double* __restrict__ hpwl_partials,
                                                       const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
