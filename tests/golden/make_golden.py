@@ -15,7 +15,23 @@ Fixtures (all float32 unless noted):
   spread positions through electric_potential_cpp (density_map fp32 and
   deterministic, fixed_density_map, electric_force from the reference's own
   field maps), weighted_average_wirelength_cpp_merged, hpwl_cpp, pin_pos_cpp.
+* ``ep_unit.npz`` -- the case of the reference's
+  unittest/ops/electric_potential_unittest.py (1 movable + 83 fixed cells,
+  1024 x 1024 bins; its arrays are read from that file with ``ast``) in
+  float32: fixed and density maps, energy, force, and the field maps in a
+  window around the movable cell.
+* ``dct_unit.npz`` -- the 4 x 8 inputs of the reference's
+  unittest/ops/dct_unittest.py (seed 10) through dct2_fft2_cpp.
+* ``wa_edge.npz`` -- a netlist of edge-case nets (degree 1, full and partial
+  lane groups of degrees 2..8, degrees up to 300, coincident pins, exp
+  underflow, masked nets, net weights) through pin_pos_cpp,
+  weighted_average_wirelength_cpp_merged and hpwl_cpp.
+
+``python tests/golden/make_golden.py [fixture ...]`` regenerates the named
+fixtures (default: all).  The reference checkout is read from
+``$DREAMPLACE_REFERENCE`` (default /root/reference).
 """
+import ast
 import math
 import os
 import sys
@@ -170,11 +186,194 @@ def design_small():
     np.savez_compressed(os.path.join(HERE, "design_small.npz"), **res)
 
 
+# ---------------------------------------------------------------- reference unit-test cases
+REF = os.environ.get("DREAMPLACE_REFERENCE", "/root/reference")
+
+
+def reference_test_literals(relpath, func):
+    """The literal assignments (numbers, and ``np.array([...])`` lists with an
+    optional ``.astype``) of one test function of a reference unit-test file,
+    read with ``ast`` when the fixture is generated."""
+    tree = ast.parse(open(os.path.join(REF, relpath)).read())
+    fn = next(n for n in ast.walk(tree) if isinstance(n, ast.FunctionDef) and n.name == func)
+    out = {}
+    for st in fn.body:
+        if not (isinstance(st, ast.Assign) and len(st.targets) == 1 and isinstance(st.targets[0], ast.Name)):
+            continue
+        v = st.value
+        if isinstance(v, ast.Call) and isinstance(v.func, ast.Attribute) and v.func.attr == "astype":
+            v = v.func.value
+        if isinstance(v, ast.Call) and isinstance(v.func, ast.Attribute) and v.func.attr == "array" and v.args:
+            v = v.args[0]
+        try:
+            out[st.targets[0].id] = ast.literal_eval(v)
+        except ValueError:
+            pass
+    return out
+
+
+def bin_centers(lo, hi, size, n):
+    c = np.zeros(n, np.float32)
+    for i in range(n):
+        bl = lo + i * size
+        c[i] = (bl + min(bl + size, hi)) / 2
+    return c
+
+
+def ep_unit():
+    """The reference's electric-potential unit test case
+    (unittest/ops/electric_potential_unittest.py, test_densityOverflowRandom):
+    one movable cell and 83 fixed cells (one of them as wide as the die) on a
+    16728 x 11424 die starting at y = 6, 1024 x 1024 bins, target density 0.7,
+    here in float32.  Field maps are kept only in a window around the movable
+    cell (the bins its force reads)."""
+    ep = need("electric_potential_cpp")
+    dct = need("dct2_fft2_cpp")
+    a = reference_test_literals("unittest/ops/electric_potential_unittest.py", "test_densityOverflowRandom")
+    xx, yy = np.array(a["xx"], np.float32), np.array(a["yy"], np.float32)
+    sxn, syn = np.array(a["node_size_x"], np.float32), np.array(a["node_size_y"], np.float32)
+    n, m = len(xx), int(a["num_movable_nodes"])
+    nt, nf = n - m, 0
+    xl, yl, xh, yh = (float(a[k]) for k in ("xl", "yl", "xh", "yh"))
+    M, N = int(a["num_bins_x"]), int(a["num_bins_y"])
+    target = float(a["target_density"])
+    bsx, bsy = (xh - xl) / M, (yh - yl) / N
+    bcx, bcy = bin_centers(xl, xh, bsx, M), bin_centers(yl, yh, bsy, N)
+    pos = np.concatenate([xx, yy]).astype(np.float32)
+    sx, sy = t(sxn), t(syn)
+    sxc = sx.clamp(min=bsx * math.sqrt(2))
+    syc = sy.clamp(min=bsy * math.sqrt(2))
+    ox = (sx - sxc).mul(0.5)
+    oy = (sy - syc).mul(0.5)
+    ratio = sx * sy / (sxc * syc)
+    tpos = t(pos)
+    res = dict(pos=pos, node_size_x=sxn, node_size_y=syn, num_movable=m, num_terminals=nt,
+               geometry=np.array([xl, yl, xh, yh], np.float64), bins=np.array([M, N]), target_density=target)
+    for det in (0, 1):
+        fixed = ep.fixed_density_map(tpos, sx, sy, t(bcx), t(bcy), xl, yl, xh, yh, bsx, bsy, m, nt, M, N, 0, 0, det)
+        res["fixed_map_det%d" % det] = fixed.numpy().copy()
+        dm = ep.density_map(tpos, sxc, syc, ox, oy, ratio, t(bcx), t(bcy), fixed.mul(target), target, xl, yl, xh,
+                            yh, bsx, bsy, m, nf, 0, M, N, 0, 0, 0, 0, det)
+        res["density_map_det%d" % det] = dm.numpy().copy()
+    rho = t(res["density_map_det1"]).view(M, N).clone().mul_(1.0 / (bsx * bsy))
+    expkM, expkN = oracle_expk(M), oracle_expk(N)
+    buf = torch.empty(M, N // 2 + 1, 2)
+    auv = torch.empty(M, N)
+    dct.dct2_fft2(rho, expkM, expkN, auv, buf, 1)
+    wu = torch.arange(M, dtype=torch.float32).mul(2 * np.pi / M).view([M, 1])
+    wv = torch.arange(N, dtype=torch.float32).mul(2 * np.pi / N).view([1, N]).mul_(bsx / bsy)
+    w2 = wu.pow(2) + wv.pow(2)
+    w2[0, 0] = 1.0
+    inv = 1.0 / w2
+    inv[0, 0] = 0.0
+    ex, ey, phi = torch.empty(M, N), torch.empty(M, N), torch.empty(M, N)
+    dct.idxst_idct(auv.mul(wu.mul(inv).mul_(0.5)), expkM, expkN, ex, buf, 1)
+    dct.idct_idxst(auv.mul(wv.mul(inv).mul_(0.5)), expkM, expkN, ey, buf, 1)
+    dct.idct2_fft2(auv.mul(inv), expkM, expkN, phi, buf, 1)
+    res["energy"] = np.float32((phi * rho).sum().item())
+    force = ep.electric_force(torch.ones(1), M, N, 0, 0, 0, 0, ex.view(-1), ey.view(-1), tpos, sxc, syc, ox, oy,
+                              ratio, t(bcx), t(bcy), xl, yl, xh, yh, bsx, bsy, m, nf)
+    res["force"] = (-force).numpy().copy()
+    # window of bins around the movable cells' stretched footprints, 4 bins of margin
+    xs = pos[:m] + ox.numpy()[:m]
+    ys = pos[n:n + m] + oy.numpy()[:m]
+    k0 = max(int(np.floor((xs.min() - xl) / bsx)) - 4, 0)
+    k1 = min(int(np.ceil((xs.max() + sxc.numpy()[:m].max() - xl) / bsx)) + 4, M)
+    h0 = max(int(np.floor((ys.min() - yl) / bsy)) - 4, 0)
+    h1 = min(int(np.ceil((ys.max() + syc.numpy()[:m].max() - yl) / bsy)) + 4, N)
+    res["field_window"] = np.array([k0, k1, h0, h1])
+    res["field_x_window"] = ex[k0:k1, h0:h1].numpy().copy()
+    res["field_y_window"] = ey[k0:k1, h0:h1].numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "ep_unit.npz"), **res)
+
+
+def dct_unit():
+    """The reference's 2-D transform unit-test inputs (unittest/ops/dct_unittest.py
+    test_dct2Random and the inverse tests: seed 10, 4 x 8; U[0, 10) for DCT2,
+    integers 0..9 for the inverse transforms), in float32, through
+    dct2_fft2_cpp's four transforms."""
+    d = need("dct2_fft2_cpp")
+    M, N = 4, 8
+    torch.manual_seed(10)
+    x = torch.empty(M, N, dtype=torch.float32).uniform_(0, 10.0)
+    torch.manual_seed(10)
+    xi = torch.empty(M, N, dtype=torch.int32).random_(0, 10).float()
+    res = {"x": x.numpy().copy(), "x_int": xi.numpy().copy()}
+    expkM, expkN = oracle_expk(M), oracle_expk(N)
+    for name in ("dct2_fft2", "idct2_fft2", "idct_idxst", "idxst_idct"):
+        src = x if name == "dct2_fft2" else xi
+        out = torch.empty(M, N)
+        buf = torch.empty(M, N // 2 + 1, 2)
+        getattr(d, name)(src.contiguous(), expkM, expkN, out, buf, 1)
+        res[name] = out.numpy().copy()
+    np.savez_compressed(os.path.join(HERE, "dct_unit.npz"), **res)
+
+
+def wa_edge():
+    """Nets the synthetic designs do not have: degree 1 (unmasked, as the
+    reference's mask keeps them), full and partial groups of every degree
+    2..8, degrees 9..300, all pins of a net on one point, a net spread far
+    beyond gamma (exp underflow), masked nets; random net weights.  Pins sit
+    on shared nodes with offsets; the reference ops see the pin positions."""
+    wa = need("weighted_average_wirelength_cpp_merged")
+    hp = need("hpwl_cpp")
+    pp = need("pin_pos_cpp")
+    rng = np.random.RandomState(21)
+    degrees = [d for d in range(1, 9) for _ in range(37)] + [9, 12, 16, 31, 32, 33, 40, 64, 65, 150, 300]
+    degrees = list(rng.permutation(degrees)) + [5, 9]  # the last two: coincident and far-spread
+    E = len(degrees)
+    P = int(sum(degrees))
+    n = P // 3
+    pin2node = rng.randint(0, n, size=P).astype(np.int32)
+    offx = rng.uniform(0, 4, size=P).astype(np.float32)
+    offy = rng.uniform(0, 4, size=P).astype(np.float32)
+    node_x = rng.uniform(0, 1000, size=n).astype(np.float32)
+    node_y = rng.uniform(0, 1000, size=n).astype(np.float32)
+    flat = rng.permutation(P).astype(np.int32)  # pins of a net are not consecutive ids
+    start = np.concatenate([[0], np.cumsum(degrees)]).astype(np.int32)
+    # coincident net: every pin on one node, zero offsets
+    cpins = flat[start[E - 2]:start[E - 1]]
+    pin2node[cpins] = pin2node[cpins[0]]
+    offx[cpins] = 0
+    offy[cpins] = 0
+    # far-spread net: its own nodes, x from 0 to 1e5
+    fpins = flat[start[E - 1]:start[E]]
+    fnodes = np.arange(n - len(fpins), n)
+    pin2node[fpins] = fnodes
+    node_x[fnodes] = np.linspace(0, 1e5, len(fpins)).astype(np.float32)
+    pin2net = np.zeros(P, np.int32)
+    for e in range(E):
+        pin2net[flat[start[e]:start[e + 1]]] = e
+    mask = np.ones(E, np.uint8)
+    mask[::7] = 0
+    mask[E - 2:] = 1
+    weights = rng.uniform(0.5, 2.0, size=E).astype(np.float32)
+    pos = np.concatenate([node_x, node_y]).astype(np.float32)
+    order = np.argsort(pin2node, kind="stable").astype(np.int32)  # node -> pin CSR
+    node_start = np.concatenate([[0], np.cumsum(np.bincount(pin2node, minlength=n))]).astype(np.int32)
+    pin = pp.forward(t(pos), t(offx), t(offy), t(pin2node.astype(np.int64)), t(order), t(node_start))
+    gamma = 8.0
+    inv_gamma = torch.tensor([1.0 / gamma], dtype=torch.float32)
+    wl, gi = wa.forward(pin, t(flat), t(start), t(pin2net), t(weights), t(mask), inv_gamma)
+    grad = wa.backward(torch.ones(1), pin, gi.clone(), t(flat), t(start), t(pin2net), t(weights), t(mask),
+                       inv_gamma)
+    hmask = (np.diff(start) >= 2).astype(np.uint8)
+    h = hp.forward(pin, t(flat), t(start), t(weights), t(hmask))
+    np.savez_compressed(os.path.join(HERE, "wa_edge.npz"), pos=pos, pin2node=pin2node, pin_offset_x=offx,
+                        pin_offset_y=offy, flat_node2pin=order, node_start=node_start, flat_netpin=flat,
+                        netpin_start=start, pin2net=pin2net, net_mask=mask, net_weights=weights,
+                        hpwl_mask=hmask, gamma=np.float32(gamma), pin_pos=pin.numpy().copy(),
+                        wl=np.float32(wl.item()), grad_intermediate=gi.numpy().copy(), grad=grad.numpy().copy(),
+                        hpwl=np.float32(h.item()))
+
+
+FIXTURES = {"wa_unit": wa_unit, "dct_small": dct_small, "design_small": design_small, "ep_unit": ep_unit,
+            "dct_unit": dct_unit, "wa_edge": wa_edge}
+
 if __name__ == "__main__":
     torch.set_num_threads(1)
-    wa_unit()
-    dct_small()
-    design_small()
+    for name in sys.argv[1:] or list(FIXTURES):
+        FIXTURES[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

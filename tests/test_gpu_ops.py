@@ -10,6 +10,7 @@ import torch
 
 import oracle
 from dreamplace_b200 import synthetic
+from golden_cases import ep_unit_case, wa_cancellation_scale, wa_edge_netlist, window_to_map
 
 pytestmark = pytest.mark.gpu
 
@@ -603,3 +604,127 @@ def test_wa_lanes_net_order_invariant(C, golden):
     (g0, w0, h0), (g1, w1, h1) = out
     assert np.array_equal(g0, g1)
     assert math.isclose(w0, w1, rel_tol=1e-12) and math.isclose(h0, h1, rel_tol=1e-12)
+
+
+def test_reference_ep_unit_case(C, golden):
+    """The reference's own electric-potential unit-test case (one movable cell,
+    83 fixed cells of which one spans the die width, die from y = 6, bins of
+    16.34 x 11.16): fixed and density maps and the force bit-exact against the
+    reference CPU op; the Poisson solve with non-square bins against the fp64
+    oracle; the ElectricPotential module against the reference's energy and
+    gradient.  The gradient bar follows from the field bar: the cell's force
+    sums the field over its area, so |dF| <= 2 * tol * max|E| * area."""
+    from dreamplace_b200.electric_potential import ElectricPotential, poisson_solve
+    g = golden("ep_unit.npz")
+    d = ep_unit_case(g)
+    M, N, nm, nt = d.num_bins_x, d.num_bins_y, d.num_movable_nodes, d.num_terminals
+    geo = (d.xl, d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y)
+    pos = dev(g["pos"])
+    sx, sy, sxc, syc, ox, oy, ratio = stretched_t(d)
+    bcx, bcy = dev(d.bcx), dev(d.bcy)
+    snm = dev(np.arange(nm, dtype=np.int32))
+    for det in (0, 1):
+        fixed = C.fixed_density_map(pos, sx, sy, bcx, bcy, *geo, nm, nt, M, N, 0, 0, det)
+        init = fixed.mul(d.target_density).view(-1)
+        dm = C.density_map(pos, sxc, syc, ox, oy, ratio, init, init, init, d.target_density, *geo, nm, 0, 0, M, N,
+                           0, 0, 0, 0, det, snm)
+        ref_fixed, ref_dm = (g["%s_det%d" % (k, det)].reshape(-1) for k in ("fixed_map", "density_map"))
+        if det:
+            assert np.array_equal(fixed.cpu().numpy().reshape(-1), ref_fixed)
+            assert np.array_equal(dm.cpu().numpy().reshape(-1), ref_dm)
+        else:
+            np.testing.assert_allclose(fixed.cpu().numpy().reshape(-1), ref_fixed, rtol=1e-5, atol=1e-3)
+            np.testing.assert_allclose(dm.cpu().numpy().reshape(-1), ref_dm, rtol=1e-5, atol=1e-3)
+    ex = dev(window_to_map(g, "field_x_window", M, N)).view(-1)
+    ey = dev(window_to_map(g, "field_y_window", M, N)).view(-1)
+    force = C.electric_force(torch.ones(1, device="cuda"), M, N, 0, 0, 0, 0, ex, ey, pos, sxc, syc, ox, oy, ratio,
+                             pos, pos, *geo, nm, 0, 1, snm, -1.0)
+    assert np.array_equal(force.cpu().numpy(), g["force"])
+    dmap = g["density_map_det1"].reshape(M, N)
+    rex, rey, renergy = oracle.poisson(dmap, d.bin_size_x, d.bin_size_y)
+    emax = max(np.max(np.abs(rex)), np.max(np.abs(rey)))
+    area = float(d.node_size_x[0] * d.node_size_y[0])
+    for precision in ("fp32", "split_bf16"):
+        tol = FIELD_TOL[precision]
+        rho = dev(dmap).mul_(1.0 / (d.bin_size_x * d.bin_size_y))
+        fx, fy, energy = poisson_solve(rho, d.bin_size_x, d.bin_size_y, precision)
+        for got, ref in ((fx, rex), (fy, rey)):
+            assert np.max(np.abs(got.cpu().numpy() - ref)) <= tol * np.max(np.abs(ref)), precision
+        assert abs(float(energy.item()) - renergy) <= 10 * tol * abs(renergy)
+        p = dev(g["pos"]).requires_grad_(True)
+        op = ElectricPotential(sx, sy, bcx, bcy, d.target_density, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+                               d.bin_size_y, nm, nt, 0, 0, True, snm, precision=precision)
+        e = op(p)
+        assert math.isclose(float(e.item()), float(g["energy"]), rel_tol=10 * tol), precision
+        e.backward()
+        err = np.max(np.abs(p.grad.cpu().numpy() - g["force"]))
+        assert err <= 2 * tol * emax * area, (precision, err)
+        assert np.count_nonzero(p.grad.cpu().numpy()) == 2 * nm
+    assert C.tc_status() == 0
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32"])
+def test_transforms_reference_unit_inputs(C, golden, precision):
+    """The 4 x 8 inputs of the reference's transform unit tests against the
+    reference's dct2_fft2 op (bf16 operands need rows of 16 bytes, i.e. map
+    sides that are multiples of 8)."""
+    from dreamplace_b200 import dct2_fft2 as dct
+    g = golden("dct_unit.npz")
+    for cls, name, key in ((dct.DCT2, "dct2_fft2", "x"), (dct.IDCT2, "idct2_fft2", "x_int"),
+                           (dct.IDCT_IDXST, "idct_idxst", "x_int"), (dct.IDXST_IDCT, "idxst_idct", "x_int")):
+        got = cls(precision=precision)(dev(g[key])).cpu().numpy()
+        ref = g[name]
+        assert np.max(np.abs(got - ref)) <= FIELD_TOL[precision] * np.max(np.abs(ref)), (name, precision)
+    assert C.tc_status() == 0
+
+
+def test_wa_edge_nets(C, golden):
+    """Edge-case nets against the reference's merged WA and HPWL ops: degree-1
+    nets (kept by the mask, zero wirelength and gradient), partial lane groups
+    of every degree 2..8, warp nets of degree 9..300, coincident pins, a net
+    spread far beyond gamma (exp underflow), masked and weighted nets; through
+    the drop-in op and through the engine's lane kernel.  With pins hundreds of
+    gamma apart the gradient is a small difference of large terms, so the bar
+    on each pin is relative to those terms (wa_cancellation_scale): CUDA's and
+    glibc's expf differ by an ulp here and there, which moves such a gradient
+    by ~2e-7 of the scale (measured on the CPU with a one-ulp perturbation)."""
+    g = golden("wa_edge.npz")
+    d = wa_edge_netlist(g)
+    P, n = d.num_pins, d.num_nodes
+    pin = dev(g["pin_pos"])
+    flat, start, p2n = dev(g["flat_netpin"]), dev(g["netpin_start"]), dev(g["pin2net"])
+    w, mask = dev(g["net_weights"]), dev(g["net_mask"])
+    ig = float(np.float32(1.0) / g["gamma"])
+    inv_gamma = torch.tensor([ig], device="cuda")
+    assert np.array_equal(C.pin_pos_forward(dev(g["pos"]), dev(g["pin_offset_x"]), dev(g["pin_offset_y"]),
+                                            dev(g["pin2node"])).cpu().numpy(), g["pin_pos"])
+    scale = wa_cancellation_scale(g["pin_pos"], g["flat_netpin"], g["netpin_start"], g["net_mask"], ig)
+    w_pin2 = np.tile(g["net_weights"][g["pin2net"]], 2)
+
+    def check(got, ref, weight=1.0):
+        bar = 1e-6 + 1e-5 * np.abs(ref) + 4e-6 * scale * weight
+        assert np.all(np.abs(got - ref) <= bar), float(np.max(np.abs(got - ref) - bar))
+
+    wl, gi = C.wa_merged_forward(pin, flat, start, p2n, w, mask, inv_gamma)
+    assert math.isclose(float(wl.item()), float(g["wl"]), rel_tol=1e-5)
+    check(gi.cpu().numpy(), g["grad_intermediate"])
+    out = C.wa_merged_backward(torch.ones(1, device="cuda"), pin, gi.clone(), flat, start, p2n, w, mask, inv_gamma,
+                               None)
+    check(out.cpu().numpy(), g["grad"], w_pin2)
+    deg = np.diff(g["netpin_start"])
+    one = g["flat_netpin"][g["netpin_start"][:-1][deg == 1]]
+    assert not np.any(gi.cpu().numpy()[np.r_[one, P + one]])  # degree-1 nets: zero gradient
+    h = C.hpwl_forward(pin, flat, start, w, dev(g["hpwl_mask"]))
+    assert math.isclose(float(h.item()), float(g["hpwl"]), rel_tol=1e-6)
+    # the engine's lane kernel (node positions + pin offsets, lane groups by degree)
+    plan, ln_csr, csr_pos, slot_of_pin, g_deg = lane_inputs(C, d)
+    assert set(range(1, 9)) <= set(g_deg.tolist()) and g_deg.max() == 300
+    xy = pack_xy(g["pos"], n)
+    wl2 = torch.zeros(1280, dtype=torch.float64, device="cuda")
+    hp = torch.zeros(1280, dtype=torch.float64, device="cuda")
+    gnode = torch.empty(2 * P, device="cuda")
+    C.wa_lanes_forward(xy, *plan, ln_csr, w, mask, inv_gamma, wl2, gnode, dev(g["hpwl_mask"]), hp)
+    got = gnode.cpu().numpy().reshape(-1, 2)[csr_pos[slot_of_pin]]
+    check(np.concatenate([got[:, 0], got[:, 1]]), g["grad_intermediate"] * w_pin2, w_pin2)
+    assert math.isclose(float(wl2[0].item()), float(g["wl"]), rel_tol=1e-5)
+    assert math.isclose(float(hp[0].item()), float(g["hpwl"]), rel_tol=1e-6)

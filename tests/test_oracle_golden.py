@@ -5,6 +5,7 @@ import numpy as np
 
 import oracle
 from dreamplace_b200 import synthetic
+from golden_cases import ep_unit_case, window_to_map
 
 
 def small_design():
@@ -91,3 +92,65 @@ def test_pins_nets(golden):
     deg = np.diff(d.flat_net2pin_start_map)
     h = oracle.hpwl(pin, d.flat_net2pin_map, d.flat_net2pin_start_map, (deg >= 2).astype(np.uint8), d.net_weights)
     assert math.isclose(h, float(g["hpwl"]), rel_tol=1e-5)
+
+
+def test_ep_unit_case_oracle(golden):
+    """The reference's own electric-potential unit-test case (one movable cell,
+    83 fixed cells of which one spans the die width, die starting at y = 6,
+    non-power-of-two bin sizes): maps and force bit-exact, Poisson energy within
+    the fp32 FFT's rounding."""
+    g = golden("ep_unit.npz")
+    d = ep_unit_case(g)
+    xl, yl, xh, yh, M, N = d.xl, d.yl, d.xh, d.yh, d.num_bins_x, d.num_bins_y
+    bsx, bsy, n, m, nt = d.bin_size_x, d.bin_size_y, d.num_nodes, d.num_movable_nodes, d.num_terminals
+    bcx, bcy = d.bcx, d.bcy
+    s = oracle.stretched(g["node_size_x"], g["node_size_y"], bsx, bsy)
+    for det in (False, True):
+        fixed = oracle.fixed_density_map(g["pos"], g["node_size_x"], g["node_size_y"], bcx, bcy, n, m, nt, M, N, xl,
+                                         yl, xh, yh, bsx, bsy, deterministic=det)
+        ref_fixed = g["fixed_map_det%d" % int(det)].reshape(-1)
+        init = (fixed * np.float32(float(g["target_density"]))).astype(np.float32)
+        dm, _ = oracle.triangle_density_map(g["pos"], *s, n, m, 0, M, N, xl, yl, xh, yh, bsx, bsy, initial=init,
+                                            deterministic=det)
+        ref_dm = g["density_map_det%d" % int(det)].reshape(-1)
+        if det:
+            assert np.array_equal(fixed.reshape(-1), ref_fixed) and np.array_equal(dm, ref_dm)
+        else:
+            np.testing.assert_allclose(fixed.reshape(-1), ref_fixed, rtol=1e-5, atol=1e-3)
+            np.testing.assert_allclose(dm, ref_dm, rtol=1e-5, atol=1e-3)
+    ex, ey = window_to_map(g, "field_x_window", M, N), window_to_map(g, "field_y_window", M, N)
+    f = oracle.electric_force(ex.reshape(-1), ey.reshape(-1), g["pos"], *s, n, m, 0, M, N, xl, yl, bsx, bsy)
+    assert np.array_equal(f, g["force"])
+    assert np.count_nonzero(f) == 2 * m  # fixed cells get no force
+    oex, oey, energy = oracle.poisson(g["density_map_det1"].reshape(M, N), bsx, bsy)
+    k0, k1, h0, h1 = (int(v) for v in g["field_window"])
+    for got, ref in ((oex[k0:k1, h0:h1], g["field_x_window"]), (oey[k0:k1, h0:h1], g["field_y_window"])):
+        assert np.max(np.abs(got - ref)) <= 1e-4 * np.max(np.abs(ref))
+    assert math.isclose(energy, float(g["energy"]), rel_tol=1e-4)
+
+
+def test_dct_unit_oracle(golden):
+    """The 4 x 8 inputs of the reference's transform unit tests."""
+    g = golden("dct_unit.npz")
+    for name, f, x in (("dct2_fft2", oracle.dct2, g["x"]), ("idct2_fft2", oracle.idct2, g["x_int"]),
+                       ("idct_idxst", oracle.idct_idxst, g["x_int"]), ("idxst_idct", oracle.idxst_idct, g["x_int"])):
+        ref = g[name].astype(np.float64)
+        assert np.max(np.abs(f(x) - ref)) <= 2e-6 * max(1.0, np.max(np.abs(ref))), name
+
+
+def test_wa_edge_nets_oracle(golden):
+    """Degree-1 nets, partial lane groups, degrees up to 300, coincident pins,
+    exp underflow, masked and weighted nets: the C restatement against the
+    reference's pin_pos, merged WA and HPWL ops."""
+    g = golden("wa_edge.npz")
+    n = len(g["pos"]) // 2
+    pin = oracle.pin_pos(g["pos"], g["pin_offset_x"], g["pin_offset_y"], g["pin2node"], n)
+    assert np.array_equal(pin, g["pin_pos"])
+    wl, partial, grad = oracle.wa_merged(pin, g["flat_netpin"], g["netpin_start"], g["net_mask"], g["net_weights"],
+                                         float(np.float32(1.0) / g["gamma"]))
+    assert math.isclose(wl, float(g["wl"]), rel_tol=1e-6)
+    np.testing.assert_allclose(grad, g["grad_intermediate"], rtol=1e-6, atol=1e-6)
+    deg = np.diff(g["netpin_start"])
+    assert deg.min() == 1 and deg.max() == 300 and np.all(partial[(deg == 1)] == 0)
+    h = oracle.hpwl(pin, g["flat_netpin"], g["netpin_start"], g["hpwl_mask"], g["net_weights"])
+    assert math.isclose(h, float(g["hpwl"]), rel_tol=1e-6)
