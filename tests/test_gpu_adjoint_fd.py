@@ -226,7 +226,7 @@ def test_recomputed_field_matches_stored(setup, precision):
         pos = t(pos_np).requires_grad_(True)
         energy = op(pos)
         energy.backward()
-        out.append((float(energy), pos.grad.clone()))
+        out.append((float(energy.detach()), pos.grad.clone()))
     (e0, g0), (e1, g1) = out
     assert torch.equal(g0, g1)
     assert abs(e0 - e1) <= 1e-6 * abs(e0), (e0, e1)

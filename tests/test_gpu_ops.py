@@ -728,3 +728,87 @@ def test_wa_edge_nets(C, golden):
     check(np.concatenate([got[:, 0], got[:, 1]]), g["grad_intermediate"] * w_pin2, w_pin2)
     assert math.isclose(float(wl2[0].item()), float(g["wl"]), rel_tol=1e-5)
     assert math.isclose(float(hp[0].item()), float(g["hpwl"]), rel_tol=1e-6)
+
+
+def test_boundary_and_wide_cells(C):
+    """Cells on, across and beyond every die edge and corner, movable cells 5
+    and 9 bins wide and 6 bins tall (the per-bin paths of the window scatter
+    and of the field gather), fillers across the edge, a filler-only pass and
+    an empty pass: the order-driven scatter's integer map and the field
+    gather's force bit-exact with the oracle (which clamps bin ranges as the
+    reference CPU op does)."""
+    d = synthetic.scaled(3000, num_bins=64, seed=7, name="edge_cells")
+    n, m, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+    bsx, bsy = d.bin_size_x, d.bin_size_y
+    sx, sy = d.node_size_x.copy(), d.node_size_y.copy()
+    sx[:50] = 5 * bsx
+    sx[50:100] = 9 * bsx
+    sy[100:150] = 6 * bsy
+    d.node_size_x, d.node_size_y = sx.astype(np.float32), sy.astype(np.float32)
+    rng = np.random.RandomState(4)
+    pos = d.initial_positions().astype(np.float64)
+    pos[:m] = rng.uniform(d.xl, d.xh, m)
+    pos[n:n + m] = rng.uniform(d.yl, d.yh, m)
+    X, Y = pos[:n], pos[n:]
+    X[150:200] = d.xl
+    Y[200:250] = d.yl
+    X[250:300] = d.xh - sx[250:300]
+    Y[300:350] = d.yh - sy[300:350]
+    X[350:400] = d.xl - 0.5 * sx[350:400]
+    X[400:450] = d.xh - 0.3 * sx[400:450]
+    Y[450:500] = d.yl - 0.7 * sy[450:500]
+    Y[500:550] = d.yh - 0.2 * sy[500:550]
+    X[550:600] = d.xl - 10 * bsx
+    X[600:650] = d.xh + 3 * bsx
+    X[650:700], Y[650:700] = d.xl - 0.5 * sx[650:700], d.yh - 0.5 * sy[650:700]
+    X[700:750], Y[700:750] = d.xh - 0.5 * sx[700:750], d.yl - 0.5 * sy[700:750]
+    X[0:20] = d.xh - 2 * bsx  # wide cells across the right edge
+    Y[100:120] = d.yl - 2 * bsy  # tall cells across the bottom edge
+    f0 = n - nf
+    X[f0:f0 + 50] = d.xh - 0.5 * sx[f0:f0 + 50]
+    Y[f0 + 50:f0 + 100] = d.yh - 0.5 * sy[f0 + 50:f0 + 100]
+    pos = pos.astype(np.float32)
+    s = oracle.stretched(d.node_size_x, d.node_size_y, bsx, bsy)
+    geo = (d.xl, d.yl, d.xh, d.yh, bsx, bsy, d.num_bins_x, d.num_bins_y)
+    nb = d.num_bins_x * d.num_bins_y
+    xy = pack_xy(pos, n)
+    idx = np.r_[0:m, f0:n].astype(np.int32)
+    fx = dev(np.random.RandomState(5).standard_normal(nb).astype(np.float32))
+    fy = dev(np.random.RandomState(6).standard_normal(nb).astype(np.float32))
+    ref_force = oracle.electric_force(fx.cpu().numpy(), fy.cpu().numpy(), pos, *s, n, m, nf, d.num_bins_x,
+                                      d.num_bins_y, d.xl, d.yl, bsx, bsy)
+    cases = (("all", idx, m), ("fillers", idx[m:], 0), ("empty", idx, 0))
+    for name, order, num_mov in cases:
+        if name == "all":
+            order = np.r_[spatial_order(d, pos, idx[:m]), spatial_order(d, pos, idx[m:])].astype(np.int32)
+        count = 0 if name == "empty" else len(order)
+        ref_map, ref_fx = oracle.triangle_density_map(pos, *s, n, num_mov, nf if count else 0, d.num_bins_x,
+                                                      d.num_bins_y, d.xl, d.yl, d.xh, d.yh, bsx, bsy,
+                                                      deterministic=True)
+        rec4, ratio_o, _ = records(C, d, order)
+        out = torch.empty(nb, device="cuda")
+        scratch = torch.empty(nb, dtype=torch.int64, device="cuda")
+        C.density_map_ordered_into(order_xy(C, xy, order), rec4, ratio_o, count, None, *geo, 1, scratch, out)
+        assert np.array_equal(scratch.cpu().numpy(), ref_fx), name
+        assert np.array_equal(out.cpu().numpy(), ref_map), name
+        if count:
+            force_o = torch.empty(2 * len(order), device="cuda")
+            C.electric_force_ordered(torch.ones(1, device="cuda"), fx, fy, order_xy(C, xy, order), rec4, ratio_o,
+                                     count, d.xl, d.yl, bsx, bsy, d.num_bins_x, d.num_bins_y, -1.0, force_o)
+            fo = force_o.cpu().numpy().reshape(-1, 2)
+            assert np.array_equal(fo[:, 0], ref_force[order]), name
+            assert np.array_equal(fo[:, 1], ref_force[n + order]), name
+    # the drop-in ops (node order, thread per cell) on the same cells
+    _, _, sxc, syc, ox, oy, ratio = stretched_t(d)
+    tpos = dev(pos)
+    ref_map, ref_fx = oracle.triangle_density_map(pos, *s, n, m, nf, d.num_bins_x, d.num_bins_y, d.xl, d.yl, d.xh,
+                                                  d.yh, bsx, bsy, deterministic=True)
+    fxm = C.density_map_fixed_point(tpos, sxc, syc, ox, oy, ratio, d.xl, d.yl, d.xh, d.yh, bsx, bsy, m, nf,
+                                    d.num_bins_x, d.num_bins_y, sorted_map(d))
+    assert np.array_equal(fxm.cpu().numpy(), ref_fx)
+    force = C.electric_force(torch.ones(1, device="cuda"), d.num_bins_x, d.num_bins_y, 0, 0, 0, 0, fx, fy, tpos, sxc,
+                             syc, ox, oy, ratio, tpos, tpos, d.xl, d.yl, d.xh, d.yh, bsx, bsy, m, nf, 1,
+                             sorted_map(d), -1.0)
+    assert np.array_equal(force.cpu().numpy(), ref_force)
+    # the cells entirely outside the die contribute nothing and feel no force
+    assert not np.any(ref_force[np.r_[550:650]])
