@@ -20,6 +20,9 @@ Fixtures (all float32 unless noted):
   1024 x 1024 bins; its arrays are read from that file with ``ast``) in
   float32: fixed and density maps, energy, force, and the field maps in a
   window around the movable cell.
+* ``ep_options.npz`` -- the 3,000-cell design through the reference
+  module's options (movable-macro mask at target density 0.8, padding 2,
+  overflow mode), composed from electric_potential_cpp and dct2_fft2_cpp.
 * ``dct_unit.npz`` -- the 4 x 8 inputs of the reference's
   unittest/ops/dct_unittest.py (seed 10) through dct2_fft2_cpp.
 * ``wa_edge.npz`` -- a netlist of edge-case nets (degree 1, full and partial
@@ -367,8 +370,78 @@ def wa_edge():
                         hpwl=np.float32(h.item()))
 
 
+def ep_options():
+    """The seeded 3,000-cell design through the reference module's options,
+    composed from the reference ops as dreamplace/ops/electric_potential/
+    electric_overflow.py:162-278 and electric_potential.py:52-217 do:
+    target density 0.8 with a movable-macro mask (ratio := target density for
+    the 40 largest movable cells), padding 2 (padding bins filled with
+    target x bin area), deterministic maps; the energy, the force, and the
+    overflow mode (movable cells only)."""
+    ep = need("electric_potential_cpp")
+    dct = need("dct2_fft2_cpp")
+    d = synthetic.scaled(3000, num_bins=64, seed=7, name="golden_small")
+    pos = np.load(os.path.join(HERE, "design_small.npz"))["pos"]
+    n, m, nt, nf = d.num_nodes, d.num_movable_nodes, d.num_terminals, d.num_filler_nodes
+    M = N = d.num_bins_x
+    bsx, bsy = d.bin_size_x, d.bin_size_y
+    target, padding = 0.8, 2
+    bcx = d.bin_centers(d.xl, d.xh, bsx)
+    bcy = d.bin_centers(d.yl, d.yh, bsy)
+    sx, sy = t(d.node_size_x), t(d.node_size_y)
+    sxc = sx.clamp(min=bsx * math.sqrt(2))
+    syc = sy.clamp(min=bsy * math.sqrt(2))
+    ox = (sx - sxc).mul(0.5)
+    oy = (sy - syc).mul(0.5)
+    ratio = sx * sy / (sxc * syc)
+    area = d.node_size_x[:m] * d.node_size_y[:m]
+    macro = np.zeros(m, bool)
+    macro[np.argsort(-area, kind="stable")[:40]] = True
+    ratio[:m][t(macro)] = target
+    pad = torch.ones(M, N, dtype=torch.bool)
+    pad[padding:M - padding, padding:N - padding] = False
+    tpos = t(pos)
+    init = ep.fixed_density_map(tpos, sx, sy, t(bcx), t(bcy), d.xl, d.yl, d.xh, d.yh, bsx, bsy, m, nt, M, N, 0, 0,
+                                1).mul(target)
+
+    def dmap(num_filler):
+        out = ep.density_map(tpos, sxc, syc, ox, oy, ratio, t(bcx), t(bcy), init, target, d.xl, d.yl, d.xh, d.yh,
+                             bsx, bsy, m, num_filler, padding, M, N, 0, 0, 0, 0, 1).view(M, N)
+        out.masked_fill_(pad, target * bsx * bsy)
+        return out
+
+    dm = dmap(nf)
+    res = dict(macro_mask=macro.astype(np.uint8), target_density=target, padding=padding,
+               density_map=dm.numpy().copy())
+    rho = dm.clone().mul_(1.0 / (bsx * bsy))
+    expkM, expkN = oracle_expk(M), oracle_expk(N)
+    buf = torch.empty(M, N // 2 + 1, 2)
+    auv = torch.empty(M, N)
+    dct.dct2_fft2(rho, expkM, expkN, auv, buf, 1)
+    wu = torch.arange(M, dtype=torch.float32).mul(2 * np.pi / M).view([M, 1])
+    wv = torch.arange(N, dtype=torch.float32).mul(2 * np.pi / N).view([1, N]).mul_(bsx / bsy)
+    w2 = wu.pow(2) + wv.pow(2)
+    w2[0, 0] = 1.0
+    inv = 1.0 / w2
+    inv[0, 0] = 0.0
+    ex, ey, phi = torch.empty(M, N), torch.empty(M, N), torch.empty(M, N)
+    dct.idxst_idct(auv.mul(wu.mul(inv).mul_(0.5)), expkM, expkN, ex, buf, 1)
+    dct.idct_idxst(auv.mul(wv.mul(inv).mul_(0.5)), expkM, expkN, ey, buf, 1)
+    dct.idct2_fft2(auv.mul(inv), expkM, expkN, phi, buf, 1)
+    res.update(field_x=ex.numpy().copy(), field_y=ey.numpy().copy(), energy=np.float32((phi * rho).sum().item()))
+    force = ep.electric_force(torch.ones(1), M, N, 0, 0, 0, 0, ex.view(-1), ey.view(-1), tpos, sxc, syc, ox, oy,
+                              ratio, t(bcx), t(bcy), d.xl, d.yl, d.xh, d.yh, bsx, bsy, m, nf)
+    res["force"] = (-force).numpy().copy()
+    om = dmap(0)
+    bin_area = bsx * bsy
+    res["overflow_map"] = om.numpy().copy()
+    res["overflow"] = np.float32((om - target * bin_area).clamp_(min=0.0).sum().item())
+    res["max_density"] = np.float32(om.max().item() / bin_area)
+    np.savez_compressed(os.path.join(HERE, "ep_options.npz"), **res)
+
+
 FIXTURES = {"wa_unit": wa_unit, "dct_small": dct_small, "design_small": design_small, "ep_unit": ep_unit,
-            "dct_unit": dct_unit, "wa_edge": wa_edge}
+            "dct_unit": dct_unit, "wa_edge": wa_edge, "ep_options": ep_options}
 
 if __name__ == "__main__":
     torch.set_num_threads(1)

@@ -812,3 +812,45 @@ def test_boundary_and_wide_cells(C):
     assert np.array_equal(force.cpu().numpy(), ref_force)
     # the cells entirely outside the die contribute nothing and feel no force
     assert not np.any(ref_force[np.r_[550:650]])
+
+
+def test_electric_potential_options(C, golden):
+    """The reference module's options against the reference ops composed as
+    its module does (ep_options.npz): movable-macro ratios at target density
+    0.8 and padding 2 give the same density map bit for bit (deterministic),
+    the energy and gradient of the fp32 solve; fast_mode returns zero energy
+    and the same gradient bit for bit; overflow mode and the ElectricOverflow
+    module (movable cells only) give the reference's overflow and max density."""
+    from dreamplace_b200.electric_potential import ElectricOverflow, ElectricPotential
+    g = golden("ep_options.npz")
+    d = small_design()
+    pos_np = golden("design_small.npz")["pos"]
+    target, padding = float(g["target_density"]), int(g["padding"])
+    mask = dev(g["macro_mask"]).bool()
+    bcx, bcy = dev(d.bin_centers(d.xl, d.xh, d.bin_size_x)), dev(d.bin_centers(d.yl, d.yh, d.bin_size_y))
+    args = (dev(d.node_size_x), dev(d.node_size_y), bcx, bcy, target, d.xl, d.yl, d.xh, d.yh, d.bin_size_x,
+            d.bin_size_y, d.num_movable_nodes, d.num_terminals)
+    grads = []
+    for fast in (False, True):
+        op = ElectricPotential(*args, d.num_filler_nodes, padding, True, sorted_map(d), movable_macro_mask=mask,
+                               fast_mode=fast, precision="fp32")
+        p = dev(pos_np).requires_grad_(True)
+        e = op(p)
+        if fast:
+            assert float(e.item()) == 0.0
+        else:
+            assert math.isclose(float(e.item()), float(g["energy"]), rel_tol=1e-4)
+            dm = op._density_map(p.detach(), d.num_filler_nodes)
+            assert np.array_equal(dm.cpu().numpy(), g["density_map"])
+        e.backward()
+        grads.append(p.grad.clone())
+        ovf, mx = op(p.detach(), mode="overflow")
+        assert math.isclose(float(ovf), float(g["overflow"]), rel_tol=1e-5)
+        assert math.isclose(float(mx), float(g["max_density"]), rel_tol=1e-6)
+    ref = g["force"]
+    assert np.max(np.abs(grads[0].cpu().numpy() - ref)) <= 1e-4 * np.max(np.abs(ref))
+    assert torch.equal(grads[0], grads[1])
+    ov = ElectricOverflow(*args, 0, padding, True, sorted_map(d), movable_macro_mask=mask)
+    ovf, mx = ov(dev(pos_np))
+    assert math.isclose(float(ovf.item()), float(g["overflow"]), rel_tol=1e-5)
+    assert math.isclose(float(mx.item()), float(g["max_density"]), rel_tol=1e-6)

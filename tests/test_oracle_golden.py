@@ -154,3 +154,38 @@ def test_wa_edge_nets_oracle(golden):
     assert deg.min() == 1 and deg.max() == 300 and np.all(partial[(deg == 1)] == 0)
     h = oracle.hpwl(pin, g["flat_netpin"], g["netpin_start"], g["hpwl_mask"], g["net_weights"])
     assert math.isclose(h, float(g["hpwl"]), rel_tol=1e-6)
+
+
+def test_ep_options_oracle(golden):
+    """The reference module's options on the 3,000-cell design (movable-macro
+    ratio at target density 0.8, padding 2): density map and force bit-exact
+    with the oracle, overflow and max density as the reference computes them."""
+    g = golden("ep_options.npz")
+    d = small_design()
+    pos = golden("design_small.npz")["pos"]
+    n, m, nf, M, N = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes, d.num_bins_x, d.num_bins_y
+    target, padding = float(g["target_density"]), int(g["padding"])
+    sxc, syc, ox, oy, ratio = _stretched(d)
+    ratio = ratio.copy()
+    ratio[:m][g["macro_mask"].astype(bool)] = np.float32(target)
+    bcx = d.bin_centers(d.xl, d.xh, d.bin_size_x)
+    bcy = d.bin_centers(d.yl, d.yh, d.bin_size_y)
+    fixed = oracle.fixed_density_map(pos, d.node_size_x, d.node_size_y, bcx, bcy, n, m, d.num_terminals, M, N, d.xl,
+                                     d.yl, d.xh, d.yh, d.bin_size_x, d.bin_size_y, deterministic=True)
+    init = (fixed * np.float32(target)).astype(np.float32)
+    pad = np.ones((M, N), bool)
+    pad[padding:M - padding, padding:N - padding] = False
+    fill = np.float32(target * d.bin_size_x * d.bin_size_y)
+    for key, num_filler in (("density_map", nf), ("overflow_map", 0)):
+        dm, _ = oracle.triangle_density_map(pos, sxc, syc, ox, oy, ratio, n, m, num_filler, M, N, d.xl, d.yl, d.xh,
+                                            d.yh, d.bin_size_x, d.bin_size_y, initial=init, deterministic=True)
+        dm = dm.reshape(M, N)
+        dm[pad] = fill
+        assert np.array_equal(dm, g[key]), key
+    f = oracle.electric_force(g["field_x"].reshape(-1), g["field_y"].reshape(-1), pos, sxc, syc, ox, oy, ratio, n, m,
+                              nf, M, N, d.xl, d.yl, d.bin_size_x, d.bin_size_y)
+    assert np.array_equal(f, g["force"])
+    om = g["overflow_map"].astype(np.float64)
+    ba = d.bin_size_x * d.bin_size_y
+    assert math.isclose(np.clip(om - target * ba, 0, None).sum(), float(g["overflow"]), rel_tol=1e-5)
+    assert math.isclose(om.max() / ba, float(g["max_density"]), rel_tol=1e-6)
