@@ -670,6 +670,17 @@ void node_pin_sum(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor 
 
 uint64_t launch_count() { return dp_launch_count(); }
 
+// Launches an instantiated CUDA graph (torch.cuda.CUDAGraph.raw_cuda_graph_exec)
+// on a stream (raw handle): the replay of a captured GP trial without
+// torch's per-replay bookkeeping, which only serves graphs that draw random
+// numbers (these do not).
+void graph_launch(int64_t graph_exec, int64_t stream) {
+  TORCH_CHECK(graph_exec != 0, "graph_launch: null graph");
+  cudaError_t e = cudaGraphLaunch(reinterpret_cast<cudaGraphExec_t>(graph_exec),
+                                  reinterpret_cast<cudaStream_t>(stream));
+  TORCH_CHECK(e == cudaSuccess, "graph_launch: ", cudaGetErrorString(e));
+}
+
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.doc() = "dreamplace_b200 native ops (sm_100a) over the C ABI";
   m.def("density_map", &density_map);
@@ -690,6 +701,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("move_boundary_forward", &move_boundary_forward);
   m.def("pws_forward", &pws_forward);
   m.def("launch_count", &launch_count);
+  m.def("graph_launch", &graph_launch);
   m.def("wa_slot_forward", &wa_slot_forward);
   m.def("wa_node_backward", &wa_node_backward);
   m.def("hpwl_slot", &hpwl_slot);

@@ -88,9 +88,12 @@ class Operand:
 
     @classmethod
     def from_tensor(cls, x, prec, scale=1.0):
-        op = cls(tuple(x.shape), prec, x.device)
-        C.prepare_operand(prec, x.contiguous(), float(scale), op.f32, op.hi, op.lo)
-        return op
+        return cls(tuple(x.shape), prec, x.device).fill(x, scale)
+
+    def fill(self, x, scale=1.0):
+        """Stores scale * x (fp32, this operand's shape) in this operand's format."""
+        C.prepare_operand(self.prec, x.contiguous(), float(scale), self.f32, self.hi, self.lo)
+        return self
 
     @property
     def main(self):

@@ -57,19 +57,45 @@ def poisson_flops(M, N, precision):
     return 3 * k * 2.0 * M * N * (M + N)
 
 
-def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy, rho_scale=1.0):
+class PoissonWorkspace(object):
+    """The intermediate operands and outputs of one M x N solve in one
+    precision, allocated once: a caller that solves repeatedly on one stream
+    (the GP engine, inside its captured trials) passes it to poisson_solve,
+    which then allocates nothing.  The returned field maps and energy are the
+    workspace's own buffers, overwritten by the next solve."""
+
+    def __init__(self, M, N, prec, device):
+        self.key = (M, N, prec)
+        self.rho = Operand((M, N), prec, device) if prec != 0 else None
+        self.t1 = Operand((N, M), prec, device)
+        self.spec = [Operand((M, N), prec, device) for _ in range(2)]
+        self.us = [Operand((N, M), prec, device) for _ in range(2)]
+        self.ex = torch.empty(M, N, dtype=torch.float32, device=device)
+        self.ey = torch.empty(M, N, dtype=torch.float32, device=device)
+        self.energy = torch.zeros(1, dtype=torch.float64, device=device)
+
+    def check(self, M, N, prec):
+        if self.key != (M, N, prec):
+            raise ValueError("poisson workspace is for %s, not %s" % (self.key, (M, N, prec)))
+        return self
+
+
+def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy, rho_scale=1.0, ws=None):
     """G1 and G2 of the solve: the two spectral operands a*wx, a*wy [M, N];
     when ``energy`` (f64[1]) is given the G2 epilogue adds the energy to it.
-    The solve runs on rho * rho_scale (the scale is G1's alpha)."""
+    The solve runs on rho * rho_scale (the scale is G1's alpha).  With a
+    PoissonWorkspace ``ws`` the operands are the workspace's."""
     M, N = rho.shape
     dev = rho.device
     cM = transform_matrices(M, prec, dev)[0]
     cN = transform_matrices(N, prec, dev)[0]
     # G1: T1^T = (rho C_N^T)^T, [N, M]
-    t1 = Operand((N, M), prec, dev)
+    t1 = ws.t1 if ws is not None else Operand((N, M), prec, dev)
     g1 = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=float(rho_scale), ldc=M)
     if prec == 0:
         g1["a_hi"] = rho
+    elif ws is not None:
+        ws.rho.fill(rho).as_a(g1)
     else:
         Operand.from_tensor(rho, prec).as_a(g1)
     cN.as_b(g1)
@@ -78,7 +104,7 @@ def _poisson_spectral(rho, bin_size_x, bin_size_y, prec, energy, rho_scale=1.0):
     # G2: a = 4/(MN) C_M T1 -> spectral operands a*wx, a*wy  [M, N]; the energy
     # sum(rho * IDCT2(a*winv)) = MN sum w_u w_v winv a^2 is summed in the same
     # epilogue, so the potential map is never formed
-    spec = [Operand((M, N), prec, dev) for _ in range(2)]
+    spec = ws.spec if ws is not None else [Operand((M, N), prec, dev) for _ in range(2)]
     g2 = dict(lda=M, ldb=M, epilogue=EPI_SPECTRAL, alpha=4.0 / (M * N), ldc=N,
               wv_scale=float(bin_size_x / bin_size_y),
               spec_weights=spectral_tables(M, N, float(bin_size_x / bin_size_y), dev))
@@ -104,23 +130,29 @@ def poisson_energy(rho, bin_size_x, bin_size_y, precision):
     return energy
 
 
-def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False, rho_scale=1.0):
+def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False, rho_scale=1.0, ws=None):
     """Field maps and energy of a normalised density map ``rho`` [M, N] (fp32).
 
     Returns (field_map_x, field_map_y, energy_f64[1]); energy is zero when
     ``fast_mode``.  Four GEMM launches, see the module docstring.  With
     rho_scale the map is normalised inside the first GEMM (its alpha): a
-    density map and rho_scale = 1 / bin area give the solve of rho."""
+    density map and rho_scale = 1 / bin area give the solve of rho.  With a
+    PoissonWorkspace ``ws`` nothing is allocated and the results are the
+    workspace's buffers."""
     prec = precision_code(precision)
     M, N = rho.shape
     dev = rho.device
     _, chM, shM = transform_matrices(M, prec, dev)
     _, chN, shN = transform_matrices(N, prec, dev)
-    energy = torch.zeros(1, dtype=torch.float64, device=dev)
-    spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy, rho_scale)
+    if ws is not None:
+        ws.check(M, N, prec)
+        energy = ws.energy.zero_()
+    else:
+        energy = torch.zeros(1, dtype=torch.float64, device=dev)
+    spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy, rho_scale, ws)
     # G3: U^T = (A R^T)^T for the x field (R = Ch_N) and the y field (Sh_N)
     rights = [chN, shN]
-    us = [Operand((N, M), prec, dev) for _ in spec]
+    us = ws.us if ws is not None else [Operand((N, M), prec, dev) for _ in spec]
     g3 = []
     for s, r, u in zip(spec, rights, us):
         d = dict(lda=N, ldb=N, epilogue=EPI_STORE_T, alpha=1.0, ldc=M)
@@ -130,8 +162,11 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False, rho_s
         g3.append(d)
     C.transform_gemm(prec, M, N, N, g3)
     # G4: Ex = 4 Sh_M Ux, Ey = 4 Ch_M Uy
-    ex = torch.empty(M, N, dtype=torch.float32, device=dev)
-    ey = torch.empty(M, N, dtype=torch.float32, device=dev)
+    if ws is not None:
+        ex, ey = ws.ex, ws.ey
+    else:
+        ex = torch.empty(M, N, dtype=torch.float32, device=dev)
+        ey = torch.empty(M, N, dtype=torch.float32, device=dev)
     g4 = [shM.as_a(us[0].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ex))),
           chM.as_a(us[1].as_b(dict(lda=M, ldb=M, epilogue=EPI_STORE, alpha=4.0, ldc=N, out_f32=ey)))]
     C.transform_gemm(prec, M, N, M, g4)

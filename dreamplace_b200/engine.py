@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from ._native import C, precision_code
-from .electric_potential import poisson_solve
+from .electric_potential import PoissonWorkspace, poisson_solve
 
 # device scalar slots of the optimizer state (gp_step.cu)
 NS_ALPHA, NS_A, NS_A_NEXT, NS_COEF, NS_ACC_DV, NS_ACC_DG, NS_ALPHA_NEW, NS_ACCEPT = range(8)
@@ -145,6 +145,9 @@ class GPEngine(object):
         self.det = bool(params.deterministic_flag)
         self.scratch = torch.empty(ep.num_bins_x * ep.num_bins_y, dtype=torch.int64, device=dev) if self.det else None
         self.prec = precision_code(ep.precision)
+        # the Poisson solve's operands and outputs, allocated once: every trial
+        # (eager or captured) of this design solves on its one stream
+        self.poisson_ws = PoissonWorkspace(ep.num_bins_x, ep.num_bins_y, self.prec, dev)
         # spatial visiting order of the scattered cells (movable block, then filler
         # block), refreshed every `sort_interval` iterations
         nm, nf = d.num_movable_nodes, d.num_filler_nodes
@@ -201,8 +204,15 @@ class GPEngine(object):
                              float(params.RePlAce_ref_hpwl), float(params.RePlAce_LOWER_PCOF),
                              float(params.RePlAce_UPPER_PCOF))
         self.graphs = {}
+        self.graph_exec = {}  # raw cudaGraphExec_t of each captured trial
         self.graph_kernels = {}
         self.kernels_launched = 0  # this library's kernels, graph replays included
+        # best position so far (the GP loop's divergence rollback target): the
+        # slot that holds it and the buffer it is copied into before that slot
+        # is overwritten; a newer best usually supersedes it first, so most
+        # improvements cost no copy
+        self.best_slot = None
+        self.best_buf = None
         self.pool = None
         self.graph_key = None
         self.trials = 0
@@ -328,7 +338,8 @@ class GPEngine(object):
         else:
             self.scatter_maps(v, ovf_out)
         self.dmap.mul_(1.0 / (ep.bin_size_x * ep.bin_size_y))
-        return poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode))
+        return poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode),
+                             ws=self.poisson_ws)
 
     def field_force(self, v, ex, ey):
         """Field force of every movable and filler cell, in visiting order (self.force_o)."""
@@ -398,7 +409,7 @@ class GPEngine(object):
         self._mark("poisson_gemms", 0)
         # rho = D / bin area is applied as the first GEMM's alpha
         ex, ey, energy = poisson_solve(self.dmap, ep.bin_size_x, ep.bin_size_y, self.prec, bool(ep.fast_mode),
-                                       1.0 / (ep.bin_size_x * ep.bin_size_y))
+                                       1.0 / (ep.bin_size_x * ep.bin_size_y), self.poisson_ws)
         self._mark("poisson_gemms", 1)
         C.objective_finish(self.wl64, energy, w[0:1], self.factor_quad, self.obj64, self.grad_scale)
         self._mark("field_gather", 0)
@@ -601,13 +612,17 @@ class GPEngine(object):
             if self.pool is None:
                 self.pool = g.pool()
             self.graphs[key] = g
+            self.graph_exec[key] = g.raw_cuda_graph_exec()
         return g
 
     def _launch(self, s, head):
         """Enqueue one trial from slot s (graph replay) and the read-back of its
         metrics on the current stream."""
+        if self.best_slot == (s + 1) % NSLOT:
+            self.flush_best()  # the trial overwrites the best position's slot
         if self.use_graphs:
-            self._graph(s, head).replay()
+            self._graph(s, head)
+            C.graph_launch(self.graph_exec[(s, head)], torch._C._cuda_getCurrentRawStream(self._dev_index))
             self.kernels_launched += self.graph_kernels[(s, head)]
         else:
             before = C.launch_count()
@@ -736,9 +751,27 @@ class GPEngine(object):
     def current_position(self):
         return self.V[self.slot]
 
+    def mark_best(self, buf=None):
+        """Record the current position as the best one.  It is copied into
+        ``buf`` (allocated when None) on the stream right before a trial
+        overwrites its slot, or by flush_best; returns ``buf``."""
+        if buf is None:
+            buf = torch.empty_like(self.V[self.slot])
+        self.best_buf = buf
+        self.best_slot = self.slot
+        return buf
+
+    def flush_best(self):
+        """Complete a pending best-position copy (stream-ordered)."""
+        if self.best_slot is not None:
+            self.best_buf.copy_(self.V[self.best_slot])
+            self.best_slot = None
+        return self.best_buf
+
     def set_position(self, t):
         """Overwrite v_k (divergence rollback), clamped into the die; an
         iteration enqueued ahead from the old v_k is enqueued again."""
+        self.flush_best()
         v = self.V[self.slot]
         v.copy_(t)
         self.move_boundary(v)

@@ -138,6 +138,12 @@ class _EngineStepper(object):
     def set_position(self, t):
         self.eng.set_position(t)
 
+    def record_best(self, buf):
+        return self.eng.mark_best(buf)
+
+    def best_position(self):
+        return self.eng.flush_best()
+
 
 class NonLinearPlace(nn.Module):
     """Global placement of one design on one GPU."""
@@ -264,6 +270,8 @@ class NonLinearPlace(nn.Module):
                 for Lsub_step in range(model.Lsub_iteration):
                     if (params.stop_overflow * 1.1 < overflow_list[-1] < params.stop_overflow * 4
                             and check_divergence(50, overflow_list[-1])):
+                        if hasattr(stepper, "best_position"):
+                            stepper.best_position()  # completes a pending copy into best["pos"]
                         stepper.set_position(best["pos"])
                         stop_placement = True
                         logger.error("possible DIVERGENCE detected, roll back to the best position recorded")
@@ -276,7 +284,10 @@ class NonLinearPlace(nn.Module):
                     lsub.append(cur)
                     if best["metric"] is None or best["metric"].overflow > o:
                         best["metric"] = cur
-                        if best["pos"] is None:
+                        if hasattr(stepper, "record_best"):
+                            # copied on the device only before its slot is reused
+                            best["pos"] = stepper.record_best(best["pos"])
+                        elif best["pos"] is None:
                             best["pos"] = stepper.position().clone()
                         else:
                             best["pos"].copy_(stepper.position())

@@ -186,3 +186,39 @@ def test_engine_layout_options_give_the_same_trajectory(design, xyo_mode, wa_gra
         place(design, p, max_iterations=40, callback=lambda it, m: t.append((m.hpwl, m.overflow, m.objective)))
         return t
     assert traj(xyo_mode=xyo_mode, wa_grad_order=wa_grad_order) == traj()
+
+
+def test_best_position_copied_before_its_slot_is_reused(design):
+    """The GP loop's best position is copied lazily: a newer best supersedes a
+    pending copy, a pending copy is made on the stream before a trial
+    overwrites the slot holding it, and the divergence rollback
+    (set_position) completes it first."""
+    p = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision="fp32", deterministic_flag=1)
+    placer, _ = place(design, p, max_iterations=10)
+    eng = placer.stepper.eng
+
+    def step():
+        g = eng.step_gen()
+        next(g)
+        try:
+            next(g)
+        except StopIteration:
+            pass
+
+    step()
+    first = eng.current_position().clone()
+    buf = eng.mark_best(None)
+    step()
+    second = eng.current_position().clone()
+    assert eng.mark_best(buf) is buf  # supersedes the first best before any copy
+    for _ in range(4):
+        step()  # the trials write every slot, the second best's included
+    torch.cuda.synchronize()
+    assert eng.best_slot is None
+    assert torch.equal(buf, second) and not torch.equal(buf, first)
+    step()
+    third = eng.current_position().clone()
+    eng.mark_best(buf)
+    eng.set_position(buf)  # completes the pending copy, then restores from it
+    torch.cuda.synchronize()
+    assert torch.equal(buf, third) and torch.equal(eng.current_position(), third)
