@@ -11,8 +11,9 @@ Across GPUs the designs are partitioned (design i goes to rank i mod world);
 ranks exchange nothing but their results at the end.
 
 Usage: python -m dreamplace_b200.batch [--designs 64] [--seed 1] [--sequential]
-  [--max-iterations N]; prints one JSON line (designs/s, per-design iteration
-  latency p50 / p99, and the same for the sequential loop with --sequential).
+  [--max-iterations N] [--repeat 2]; prints one JSON line (designs/s,
+  per-design iteration latency p50 / p99 of the last batched pass, the first
+  pass's time, and the same for the sequential loop with --sequential).
 """
 import argparse
 import json
@@ -116,6 +117,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--max-iterations", type=int, default=None)
     ap.add_argument("--sequential", action="store_true", help="also time the single-design loop")
+    ap.add_argument("--repeat", type=int, default=2,
+                    help="batched passes over the same designs; the last one is reported (the first also "
+                         "pays the process's one-time set-up, reported as batched_first_pass_*)")
     args = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("batch placement needs a CUDA device")
@@ -130,11 +134,21 @@ def main(argv=None):
     mine = [designs_all[i] for i in assign(len(designs_all), rank, world)]
     out = {"designs": len(designs_all), "designs_on_rank": len(mine), "world": world,
            "cells": int(sum(d.num_movable_nodes for d in mine))}
-    bp = BatchPlacer(mine)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res, lat = bp.run(args.max_iterations)
-    out.update(summary("batched", mine, res, lat, time.perf_counter() - t0))
+    for r in range(max(args.repeat, 1)):
+        # each pass places the same designs with new placers; the first also
+        # pays the process's one-time costs (kernel loading, the caching
+        # allocator's device allocations), later ones run as a service
+        # placing batch after batch would
+        bp = BatchPlacer(mine)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res, lat = bp.run(args.max_iterations)
+        seconds = time.perf_counter() - t0
+        if r == 0 and args.repeat > 1:
+            out["batched_first_pass_seconds"] = round(seconds, 3)
+            out["batched_first_pass_designs_per_s"] = round(len(mine) / seconds, 3)
+        del bp
+    out.update(summary("batched", mine, res, lat, seconds))
     if args.sequential:
         seq = BatchPlacer(mine)
         torch.cuda.synchronize()
