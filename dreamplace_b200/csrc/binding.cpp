@@ -334,35 +334,6 @@ static void* ovp(const c10::optional<at::Tensor>& t) {
   return (t.has_value() && t->defined() && t->numel() > 0) ? t->data_ptr() : nullptr;
 }
 
-void wa_slot_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
-                     at::Tensor netpin_start, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
-                     at::Tensor inv_gamma, at::Tensor wl_f64, at::Tensor grad_slot) {
-  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(slot_node); CHECK_F32(grad_slot);
-  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble, "wl_f64 must be float64");
-  DP_CALL(dp_wa_slot_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                             ptr<float>(slot_offy), ptr<int>(netpin_start), netpin_start.numel() - 1,
-                             (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<float>(inv_gamma),
-                             ptr<double>(wl_f64), ptr<float>(grad_slot), slot_node.numel(), cur_stream()));
-}
-
-void wa_node_backward(at::Tensor grad_slot, at::Tensor node_slots, at::Tensor node_start, at::Tensor slot_net,
-                      c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor grad_pos,
-                      int num_movable, int accumulate, at::Tensor grad_out) {
-  CHECK_F32(grad_slot); CHECK_F32(grad_out); CHECK_F32(grad_pos);
-  DP_CALL(dp_wa_node_backward(ptr<float>(grad_slot), grad_slot.numel() / 2, ptr<int>(node_slots),
-                              ptr<int>(node_start), ptr<int>(slot_net), (const float*)ovp(net_weights),
-                              net_mask.data_ptr<uint8_t>(), ptr<float>(grad_pos), num_movable, grad_out.numel() / 2,
-                              accumulate, ptr<float>(grad_out), cur_stream()));
-}
-
-void hpwl_slot(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
-               at::Tensor netpin_start, c10::optional<at::Tensor> net_weights, at::Tensor net_mask, at::Tensor out) {
-  TORCH_CHECK(out.scalar_type() == at::kDouble, "out must be float64");
-  DP_CALL(dp_hpwl_slot(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                       ptr<float>(slot_offy), ptr<int>(netpin_start), netpin_start.numel() - 1,
-                       (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<double>(out), cur_stream()));
-}
-
 void nesterov_init(at::Tensor state, double alpha) { DP_CALL(dp_nesterov_init(ptr<double>(state), alpha, cur_stream())); }
 
 void nesterov_trial(at::Tensor v, at::Tensor g, at::Tensor u, at::Tensor u_new, at::Tensor v_new,
@@ -394,8 +365,6 @@ void precondition_step_size(at::Tensor g_new, at::Tensor g, at::Tensor v_new, at
                                     ptr<float>(pws), ptr<float>(area), ptr<float>(lam), g_new.numel() / 2,
                                     ptr<double>(state), cur_stream()));
 }
-
-void nesterov_advance(at::Tensor state) { DP_CALL(dp_nesterov_advance(ptr<double>(state), cur_stream())); }
 
 void iteration_head(at::Tensor state_prev, at::Tensor state_new, at::Tensor sched_prev, at::Tensor sched_new,
                     at::Tensor hpwl_k, at::Tensor overflow_k, at::Tensor weights_prev, at::Tensor weights_new,
@@ -439,26 +408,6 @@ void objective_finish(c10::optional<at::Tensor> wl, at::Tensor energy, at::Tenso
                               ptr<float>(density_weight), ptr<float>(factor_quad),
                               obj.has_value() ? ptr<double>(*obj) : nullptr,
                               grad_scale.has_value() ? ptr<float>(*grad_scale) : nullptr, cur_stream()));
-}
-
-// density scatter into a caller-owned map (no allocation; graph friendly)
-void density_map_into(at::Tensor pos, at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio,
-                      at::Tensor init, double xl, double yl, double xh, double yh, double bsx, double bsy,
-                      int num_movable, int num_filler, int nbx, int nby, c10::optional<at::Tensor> sorted_node_map,
-                      int deterministic, c10::optional<at::Tensor> scratch, at::Tensor out) {
-  const int* snm = (const int*)ovp(sorted_node_map);
-  int n = pos.numel() / 2;
-  if (deterministic) {
-    TORCH_CHECK(scratch.has_value(), "deterministic mode needs the int64 scratch map");
-    DP_CALL(dp_density_map_fx64(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
-                                ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
-                                num_movable, num_filler, nbx, nby, snm, fraction_bits(xl, yl, xh, yh),
-                                ptr<int64_t>(*scratch), ptr<float>(out), cur_stream()));
-  } else {
-    DP_CALL(dp_density_map_f32(ptr<float>(pos), n, ptr<float>(sx), ptr<float>(sy), ptr<float>(ox), ptr<float>(oy),
-                               ptr<float>(ratio), ptr<float>(init), xl, yl, xh, yh, bsx, bsy, inv_f(bsx), inv_f(bsy),
-                               num_movable, num_filler, nbx, nby, snm, ptr<float>(out), cur_stream()));
-  }
 }
 
 void build_cell_records(at::Tensor sx, at::Tensor sy, at::Tensor ox, at::Tensor oy, at::Tensor ratio,
@@ -566,45 +515,6 @@ void electric_force_into(at::Tensor grad_scale, at::Tensor ex, at::Tensor ey, at
                             num_filler, (const int*)ovp(sorted_node_map), (float)scale, ptr<float>(out), cur_stream()));
 }
 
-at::Tensor plan_net_chunks(at::Tensor netpin_start_cpu, int max_pins) {
-  TORCH_CHECK(!netpin_start_cpu.is_cuda() && netpin_start_cpu.scalar_type() == at::kInt, "netpin_start must be int32 on CPU");
-  auto ns = netpin_start_cpu.contiguous();
-  int num_nets = ns.numel() - 1;
-  auto out = at::empty({num_nets + 1}, ns.options());
-  int count = 0;
-  DP_CALL(dp_plan_net_chunks(ns.data_ptr<int>(), num_nets, max_pins, out.data_ptr<int>(), &count));
-  return out.narrow(0, 0, count + 1).clone();
-}
-
-void wa_chunk_forward(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy,
-                      at::Tensor slot_net, at::Tensor chunk_pin, c10::optional<at::Tensor> net_weights,
-                      at::Tensor net_mask, at::Tensor inv_gamma, at::Tensor csr_pos, at::Tensor wl_f64,
-                      at::Tensor grad_node_order, c10::optional<at::Tensor> hpwl_mask,
-                      c10::optional<at::Tensor> hpwl_f64) {
-  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(chunk_pin); CHECK_I32(csr_pos); CHECK_F32(grad_node_order);
-  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
-  TORCH_CHECK(!hpwl_f64.has_value() || (hpwl_mask.has_value() && hpwl_f64->scalar_type() == at::kDouble &&
-                                        hpwl_f64->numel() >= DP_REDUCE_DOUBLES),
-              "hpwl_f64 needs hpwl_mask and DP_REDUCE_DOUBLES doubles");
-  DP_CALL(dp_wa_chunk_forward(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                              ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(chunk_pin), chunk_pin.numel() - 1,
-                              (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<float>(inv_gamma),
-                              ptr<int>(csr_pos), ptr<double>(wl_f64), ptr<float>(grad_node_order), slot_node.numel(),
-                              hpwl_mask.has_value() ? hpwl_mask->data_ptr<uint8_t>() : nullptr,
-                              (double*)ovp(hpwl_f64), cur_stream()));
-}
-
-void hpwl_chunk(at::Tensor pos, at::Tensor slot_node, at::Tensor slot_offx, at::Tensor slot_offy, at::Tensor slot_net,
-                at::Tensor chunk_pin, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
-                at::Tensor out_f64) {
-  CHECK_I32(chunk_pin);
-  TORCH_CHECK(out_f64.scalar_type() == at::kDouble && out_f64.numel() >= DP_REDUCE_DOUBLES, "out_f64 too small");
-  DP_CALL(dp_hpwl_chunk(ptr<float>(pos), pos.numel() / 2, ptr<int>(slot_node), ptr<float>(slot_offx),
-                        ptr<float>(slot_offy), ptr<int>(slot_net), ptr<int>(chunk_pin), chunk_pin.numel() - 1,
-                        (const float*)ovp(net_weights), net_mask.data_ptr<uint8_t>(), ptr<double>(out_f64),
-                        cur_stream()));
-}
-
 std::vector<at::Tensor> plan_net_lanes(at::Tensor netpin_start_cpu, c10::optional<at::Tensor> net_order_cpu) {
   TORCH_CHECK(!netpin_start_cpu.is_cuda() && netpin_start_cpu.scalar_type() == at::kInt,
               "netpin_start must be int32 on CPU");
@@ -702,13 +612,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("pws_forward", &pws_forward);
   m.def("launch_count", &launch_count);
   m.def("graph_launch", &graph_launch);
-  m.def("wa_slot_forward", &wa_slot_forward);
-  m.def("wa_node_backward", &wa_node_backward);
-  m.def("hpwl_slot", &hpwl_slot);
   m.def("nesterov_init", &nesterov_init);
   m.def("nesterov_trial", &nesterov_trial);
   m.def("precondition_step_size", &precondition_step_size);
-  m.def("nesterov_advance", &nesterov_advance);
   m.def("iteration_head", &iteration_head, py::arg("state_prev"), py::arg("state_new"), py::arg("sched_prev"),
         py::arg("sched_new"), py::arg("hpwl_k"), py::arg("overflow_k"), py::arg("weights_prev"),
         py::arg("weights_new"), py::arg("base_gamma"), py::arg("total_area"), py::arg("ref_hpwl"), py::arg("lower"),
@@ -717,7 +623,6 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("trial_gate", &trial_gate, py::arg("gate"), py::arg("accept_prev") = py::none());
   m.def("pack_xy", &pack_xy);
   m.def("objective_finish", &objective_finish);
-  m.def("density_map_into", &density_map_into);
   m.def("density_overflow_into", &density_overflow_into);
   m.def("density_map_ordered_into", &density_map_ordered_into, py::arg("xy_o"), py::arg("rec4"), py::arg("ratio_o"),
         py::arg("count"), py::arg("init"), py::arg("xl"), py::arg("yl"), py::arg("xh"), py::arg("yh"), py::arg("bsx"),
@@ -735,12 +640,9 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("bsx"), py::arg("bsy"), py::arg("nbx"), py::arg("nby"), py::arg("scale"), py::arg("force_o"),
         py::arg("order") = py::none());
   m.def("assemble_precondition_step", &assemble_precondition_step);
-  m.def("plan_net_chunks", &plan_net_chunks);
-  m.def("wa_chunk_forward", &wa_chunk_forward);
   m.def("plan_net_lanes", &plan_net_lanes, py::arg("netpin_start_cpu"), py::arg("net_order_cpu") = py::none());
   m.def("wa_lanes_forward", &wa_lanes_forward);
   m.def("hpwl_lanes", &hpwl_lanes);
-  m.def("hpwl_chunk", &hpwl_chunk);
   m.def("node_pin_sum", &node_pin_sum);
   m.def("electric_force_into", &electric_force_into);
   m.def("version", &dp_version);

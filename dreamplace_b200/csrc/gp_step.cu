@@ -39,181 +39,6 @@ __device__ __forceinline__ void block_partial2(double a, double b, double* parti
   }
 }
 
-// ---------------------------------------------------------------- WA fused
-// Nets of degree <= kWaCache keep their pin coordinates and the four
-// exponentials per pin in registers between the three passes (max/min, sums,
-// gradient), so the gather and expf run once per pin; larger nets re-read.
-// The arithmetic is the same either way.
-constexpr int kWaCache = 6;
-
-__global__ void __launch_bounds__(256) wa_slot_forward_kernel(
-    const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ slot_node,
-    const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ netpin_start,
-    int num_nets, const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
-    const float* __restrict__ inv_gamma_p, double* __restrict__ partials, float* __restrict__ gx,
-    float* __restrict__ gy) {
-  const float inv_gamma = *inv_gamma_p;
-  double contrib = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
-    const int b = netpin_start[i], e = netpin_start[i + 1];
-    const int deg = e - b;
-    if (!net_mask[i]) {
-      for (int j = b; j < e; ++j) {
-        gx[j] = 0.f;
-        gy[j] = 0.f;
-      }
-      continue;
-    }
-    float cx[kWaCache], cy[kWaCache];
-    float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
-#pragma unroll
-    for (int q = 0; q < kWaCache; ++q) {
-      if (q < deg) {
-        const int n = slot_node[b + q];
-        cx[q] = fadd(slot_offx[b + q], x[n]);
-        cy[q] = fadd(slot_offy[b + q], y[n]);
-        x_max = fmaxf(cx[q], x_max);
-        x_min = fminf(cx[q], x_min);
-        y_max = fmaxf(cy[q], y_max);
-        y_min = fminf(cy[q], y_min);
-      }
-    }
-    for (int j = b + kWaCache; j < e; ++j) {
-      const int n = slot_node[j];
-      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-      x_max = fmaxf(xx, x_max);
-      x_min = fminf(xx, x_min);
-      y_max = fmaxf(yy, y_max);
-      y_min = fminf(yy, y_min);
-    }
-    float ex[kWaCache], enx[kWaCache], ey[kWaCache], eny[kWaCache];
-    float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
-#pragma unroll
-    for (int q = 0; q < kWaCache; ++q) {
-      if (q < deg) {
-        ex[q] = expf(fmul(fsub(cx[q], x_max), inv_gamma));
-        enx[q] = expf(fmul(fsub(x_min, cx[q]), inv_gamma));
-        xe_p = fadd(xe_p, fmul(cx[q], ex[q]));
-        xe_n = fadd(xe_n, fmul(cx[q], enx[q]));
-        e_p = fadd(e_p, ex[q]);
-        e_n = fadd(e_n, enx[q]);
-        ey[q] = expf(fmul(fsub(cy[q], y_max), inv_gamma));
-        eny[q] = expf(fmul(fsub(y_min, cy[q]), inv_gamma));
-        ye_p = fadd(ye_p, fmul(cy[q], ey[q]));
-        ye_n = fadd(ye_n, fmul(cy[q], eny[q]));
-        f_p = fadd(f_p, ey[q]);
-        f_n = fadd(f_n, eny[q]);
-      }
-    }
-    for (int j = b + kWaCache; j < e; ++j) {
-      const int n = slot_node[j];
-      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-      const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
-      xe_p = fadd(xe_p, fmul(xx, a1));
-      xe_n = fadd(xe_n, fmul(xx, a2));
-      e_p = fadd(e_p, a1);
-      e_n = fadd(e_n, a2);
-      const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
-      ye_p = fadd(ye_p, fmul(yy, a3));
-      ye_n = fadd(ye_n, fmul(yy, a4));
-      f_p = fadd(f_p, a3);
-      f_n = fadd(f_n, a4);
-    }
-    const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                          __fdiv_rn(ye_n, f_n));
-    contrib += (double)(net_weights ? fmul(wl, net_weights[i]) : wl);
-    const float b_x = __fdiv_rn(inv_gamma, e_p);
-    const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
-    const float b_nx = __fdiv_rn(-inv_gamma, e_n);
-    const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
-    const float b_y = __fdiv_rn(inv_gamma, f_p);
-    const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
-    const float b_ny = __fdiv_rn(-inv_gamma, f_n);
-    const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
-#pragma unroll
-    for (int q = 0; q < kWaCache; ++q) {
-      if (q < deg) {
-        gx[b + q] = fsub(fmul(fadd(a_x, fmul(b_x, cx[q])), ex[q]), fmul(fadd(a_nx, fmul(b_nx, cx[q])), enx[q]));
-        gy[b + q] = fsub(fmul(fadd(a_y, fmul(b_y, cy[q])), ey[q]), fmul(fadd(a_ny, fmul(b_ny, cy[q])), eny[q]));
-      }
-    }
-    for (int j = b + kWaCache; j < e; ++j) {
-      const int n = slot_node[j];
-      const float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-      const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
-      gx[j] = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
-      const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
-      gy[j] = fsub(fmul(fadd(a_y, fmul(b_y, yy)), a3), fmul(fadd(a_ny, fmul(b_ny, yy)), a4));
-    }
-  }
-  block_partial(contrib, partials);
-}
-
-// node grad (+)= sum over the node's pins, in flat_node2pin order, of
-// (gi * g) * w_net  -- zero for nodes >= num_movable (all their pins are masked)
-__global__ void wa_node_backward_kernel(const float* __restrict__ gx, const float* __restrict__ gy,
-                                        const int* __restrict__ node_slots, const int* __restrict__ node_start,
-                                        const int* __restrict__ slot_net, const float* __restrict__ net_weights,
-                                        const unsigned char* __restrict__ net_mask, const float* __restrict__ grad_p,
-                                        int num_movable, int num_nodes, int accumulate, float* __restrict__ out_x,
-                                        float* __restrict__ out_y) {
-  const float g = *grad_p;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
-    float sx = 0.f, sy = 0.f;
-    if (i < num_movable) {
-      for (int k = node_start[i]; k < node_start[i + 1]; ++k) {
-        int s = node_slots[k];
-        float vx = fmul(gx[s], g), vy = fmul(gy[s], g);
-        if (net_weights) {
-          int net = slot_net[s];
-          if (net_mask[net]) {
-            float w = net_weights[net];
-            vx = fmul(vx, w);
-            vy = fmul(vy, w);
-          }
-        }
-        sx = fadd(sx, vx);
-        sy = fadd(sy, vy);
-      }
-    }
-    if (accumulate) {
-      out_x[i] = fadd(sx, out_x[i]);
-      out_y[i] = fadd(sy, out_y[i]);
-    } else {
-      out_x[i] = sx;
-      out_y[i] = sy;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(256) hpwl_slot_kernel(const float* __restrict__ x, const float* __restrict__ y,
-                                                        const int* __restrict__ slot_node,
-                                                        const float* __restrict__ slot_offx,
-                                                        const float* __restrict__ slot_offy,
-                                                        const int* __restrict__ netpin_start, int num_nets,
-                                                        const float* __restrict__ net_weights,
-                                                        const unsigned char* __restrict__ net_mask,
-                                                        double* __restrict__ partials) {
-  double c = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
-    if (net_mask[i]) {
-      float max_x = -FLT_MAX, min_x = FLT_MAX, max_y = -FLT_MAX, min_y = FLT_MAX;
-      for (int j = netpin_start[i]; j < netpin_start[i + 1]; ++j) {
-        int n = slot_node[j];
-        float xx = fadd(slot_offx[j], x[n]), yy = fadd(slot_offy[j], y[n]);
-        min_x = fminf(min_x, xx);
-        max_x = fmaxf(max_x, xx);
-        min_y = fminf(min_y, yy);
-        max_y = fmaxf(max_y, yy);
-      }
-      float h = fsub(fadd(fsub(max_x, min_x), max_y), min_y);
-      if (net_weights) h = fmul(h, net_weights[i]);
-      c += (double)h;
-    }
-  }
-  block_partial(c, partials);
-}
-
 // ---------------------------------------------------------------- Nesterov
 // Device scalars of the optimizer (one array of doubles):
 enum {
@@ -407,15 +232,6 @@ __global__ void nesterov_finish_kernel(double* st, const double* partials, int c
   st[NS_ALPHA] = an;  // the reference copies alpha_{k+1} into alpha_k after every trial
 }
 
-// called once per accepted step: a_k <- a_{k+1}; a_{k+2}, coef for the next step
-__global__ void nesterov_advance_kernel(double* st) {
-  double a = st[NS_A_NEXT];
-  st[NS_A] = a;
-  double an = (1.0 + sqrt(4.0 * a * a + 1.0)) / 2.0;
-  st[NS_A_NEXT] = an;
-  st[NS_COEF] = (a - 1.0) / an;
-}
-
 __global__ void nesterov_init_kernel(double* st, double alpha) {
   st[NS_ALPHA] = alpha;
   st[NS_A] = 1.0;
@@ -450,54 +266,6 @@ extern "C" int dp_objective_finish(const double* wl, const double* energy, const
              "dp_objective_finish: null pointer");
   objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, factor_quad, obj, grad_scale);
   return check_launch("dp_objective_finish");
-}
-
-extern "C" int dp_wa_slot_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
-                                  const float* slot_offy, const int* netpin_start, int num_nets,
-                                  const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
-                                  double* wl_f64, float* grad_slot, int num_slots, dp_stream_t stream) {
-  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && netpin_start && net_mask && inv_gamma && wl_f64 &&
-                 grad_slot,
-             "dp_wa_slot_forward: null pointer argument");
-  cudaStream_t s = as_stream(stream);
-  int blocks = grid_for(num_nets, 256, 8);
-  double* partials = wl_f64 + 1;
-  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  wa_slot_forward_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
-                                               num_nets, net_weights, net_mask, inv_gamma, partials, grad_slot,
-                                               grad_slot + num_slots);
-  int rc = check_launch("dp_wa_slot_forward");
-  if (rc) return rc;
-  return launch_finish_sum(wl_f64, blocks, nullptr, s);
-}
-
-extern "C" int dp_wa_node_backward(const float* grad_slot, int num_slots, const int* node_slots,
-                                   const int* node_start, const int* slot_net, const float* net_weights,
-                                   const unsigned char* net_mask, const float* grad_pos, int num_movable,
-                                   int num_nodes, int accumulate, float* grad_out, dp_stream_t stream) {
-  DP_REQUIRE(grad_slot && node_slots && node_start && grad_pos && grad_out, "dp_wa_node_backward: null pointer");
-  DP_REQUIRE(!net_weights || (slot_net && net_mask), "dp_wa_node_backward: net weights need slot_net and net_mask");
-  if (num_nodes == 0) return DP_OK;
-  wa_node_backward_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
-      grad_slot, grad_slot + num_slots, node_slots, node_start, slot_net, net_weights, net_mask, grad_pos,
-      num_movable, num_nodes, accumulate, grad_out, grad_out + num_nodes);
-  return check_launch("dp_wa_node_backward");
-}
-
-extern "C" int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
-                            const float* slot_offy, const int* netpin_start, int num_nets, const float* net_weights,
-                            const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
-  DP_REQUIRE(pos && slot_node && slot_offx && slot_offy && netpin_start && net_mask && out_f64,
-             "dp_hpwl_slot: null pointer argument");
-  cudaStream_t s = as_stream(stream);
-  int blocks = grid_for(num_nets, 256, 8);
-  double* partials = out_f64 + 1;
-  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  hpwl_slot_kernel<<<blocks, 256, 0, s>>>(pos, pos + num_nodes, slot_node, slot_offx, slot_offy, netpin_start,
-                                         num_nets, net_weights, net_mask, partials);
-  int rc = check_launch("dp_hpwl_slot");
-  if (rc) return rc;
-  return launch_finish_sum(out_f64, blocks, nullptr, s);
 }
 
 extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream) {
@@ -542,12 +310,6 @@ extern "C" int dp_precondition_step_size(float* g_new, const float* g, const flo
   if (rc) return rc;
   nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
   return check_launch("dp_precondition_step_size finish");
-}
-
-extern "C" int dp_nesterov_advance(double* state, dp_stream_t stream) {
-  DP_REQUIRE(state, "dp_nesterov_advance: null state");
-  nesterov_advance_kernel<<<1, 1, 0, as_stream(stream)>>>(state);
-  return check_launch("dp_nesterov_advance");
 }
 
 // What the GP loop does on the host between iteration k and k+1, on the
@@ -615,234 +377,16 @@ extern "C" int dp_iteration_head(const double* state_prev, double* state_new, co
   return check_launch("dp_iteration_head");
 }
 
-// ============================================================== warp-per-chunk WA / HPWL
-// Nets are packed (in order) into chunks of at most 32 pins (host planner
-// dp_plan_net_chunks); a net with more than 32 pins is a chunk of its own.
-// One warp per chunk, one lane per pin: the pin gather is issued by all
-// lanes at once, and every per-net max / min / sum is a segmented shuffle
-// reduction over the lanes of that net (log2(32) steps), so no lane waits on
-// another net's degree.  The WA gradient is written to the pin's position in
-// node-CSR order (csr_pos), which makes the pin -> node sum of the backward a
-// contiguous streaming read.
+// ============================================================== warp reductions, pin sums
 namespace dpb {
 
-struct SegInfo {
-  int end;      // last lane of this lane's net within the warp
-  int head;     // first lane of this lane's net within the warp
-  int longest;  // pins of the largest net in the warp (uniform)
-};
-
-// Tree reduction over the lanes of each net, towards its head lane; only as
-// many halving steps as the largest net of the warp needs (a chunk of ~3-pin
-// nets takes 2-3 steps instead of 5), then the head's value is broadcast.
-// N values go together: the N shuffles of a step are independent, so their
-// latencies overlap.
-template <int N, typename Op>
-__device__ __forceinline__ void seg_reduce_n(float (&v)[N], const SegInfo& sg, int lane, Op op) {
-  for (int o = 1; o < sg.longest; o <<= 1) {
-    float u[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) u[i] = __shfl_down_sync(0xffffffffu, v[i], o);
-    if (lane + o <= sg.end) {
-#pragma unroll
-      for (int i = 0; i < N; ++i) v[i] = op(v[i], u[i]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, v[i], sg.head);
-}
-
-struct MaxOp { __device__ float operator()(float a, float b) const { return fmaxf(a, b); } };
-struct MinOp { __device__ float operator()(float a, float b) const { return fminf(a, b); } };
-struct AddOp { __device__ float operator()(float a, float b) const { return fadd(a, b); } };
-
+// max (kind 0), min (kind 1) or sum (kind 2) over the warp's 32 lanes, in every lane
 __device__ __forceinline__ float warp_all(float v, int kind) {
   for (int o = 16; o > 0; o >>= 1) {
     float u = __shfl_xor_sync(0xffffffffu, v, o);
     v = kind == 0 ? fmaxf(v, u) : kind == 1 ? fminf(v, u) : fadd(v, u);
   }
   return v;
-}
-
-// per-lane segment info from the lane's net id (net ids of a chunk are
-// non-decreasing across lanes); lanes past the chunk get net = INT_MAX
-__device__ __forceinline__ SegInfo segment_of(int net, int lane) {
-  unsigned same = __match_any_sync(0xffffffffu, net);
-  SegInfo sg;
-  sg.head = __ffs(same) - 1;
-  sg.end = 31 - __clz(same);
-  // lanes past the chunk (net == INT_MAX) never need their values reduced
-  sg.longest = (int)__reduce_max_sync(0xffffffffu, net == INT_MAX ? 1u : (unsigned)(sg.end - sg.head + 1));
-  return sg;
-}
-
-template <bool kGrad>
-__global__ void __launch_bounds__(256) wa_chunk_kernel(
-    const float2* __restrict__ xy, const int* __restrict__ slot_node,
-    const float* __restrict__ slot_offx, const float* __restrict__ slot_offy, const int* __restrict__ slot_net,
-    const int* __restrict__ chunk_pin, int num_chunks,
-    const float* __restrict__ net_weights, const unsigned char* __restrict__ net_mask,
-    const float* __restrict__ inv_gamma_p, const int* __restrict__ csr_pos, double* __restrict__ partials,
-    float2* __restrict__ gnode, const unsigned char* __restrict__ hpwl_mask, double* __restrict__ hpwl_partials) {
-  const float inv_gamma = kGrad ? *inv_gamma_p : 0.f;
-  // HPWL riding along the WA forward (hpwl_partials != NULL): the same per-net
-  // value and the same per-thread accumulation order as the kGrad = false pass
-  double hcontrib = 0.0;
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  double contrib = 0.0;
-  for (int c = warp; c < num_chunks; c += nwarps) {
-    const int s0 = chunk_pin[c], s1 = chunk_pin[c + 1];
-    const int np = s1 - s0;
-    if (np <= 32) {
-      const bool valid = lane < np;
-      const int s = s0 + lane;
-      const int net = valid ? __ldcs(slot_net + s) : INT_MAX;
-      int cur_csr = 0;
-      float xx = 0.f, yy = 0.f;
-      if (valid) {
-        const float2 p = xy[__ldcs(slot_node + s)];
-        xx = fadd(__ldcs(slot_offx + s), p.x);
-        yy = fadd(__ldcs(slot_offy + s), p.y);
-        if (kGrad) cur_csr = __ldcs(csr_pos + s);
-      }
-      const SegInfo sg = segment_of(net, lane);
-      const bool on = valid && net_mask[net];
-      // max and min in one pass: min(x) = -max(-x) exactly
-      float ext[4] = {valid ? xx : -FLT_MAX, valid ? -xx : -FLT_MAX, valid ? yy : -FLT_MAX, valid ? -yy : -FLT_MAX};
-      seg_reduce_n<4>(ext, sg, lane, MaxOp());
-      const float x_max = ext[0], x_min = -ext[1], y_max = ext[2], y_min = -ext[3];
-      if (kGrad && hpwl_partials && valid && lane == sg.head && hpwl_mask[net]) {
-        float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
-        if (net_weights) h = fmul(h, net_weights[net]);
-        hcontrib += (double)h;
-      }
-      if (!kGrad) {  // HPWL
-        if (on && lane == sg.head) {
-          float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
-          if (net_weights) h = fmul(h, net_weights[net]);
-          contrib += (double)h;
-        }
-        continue;
-      }
-      float ex = 0.f, enx = 0.f, ey = 0.f, eny = 0.f;
-      if (on) {
-        ex = expf(fmul(fsub(xx, x_max), inv_gamma));
-        enx = expf(fmul(fsub(x_min, xx), inv_gamma));
-        ey = expf(fmul(fsub(yy, y_max), inv_gamma));
-        eny = expf(fmul(fsub(y_min, yy), inv_gamma));
-      }
-      float sums[8] = {ex, enx, fmul(xx, ex), fmul(xx, enx), ey, eny, fmul(yy, ey), fmul(yy, eny)};
-      seg_reduce_n<8>(sums, sg, lane, AddOp());
-      const float e_p = sums[0], e_n = sums[1], xe_p = sums[2], xe_n = sums[3];
-      const float f_p = sums[4], f_n = sums[5], ye_p = sums[6], ye_n = sums[7];
-      if (!valid) continue;
-      float gxv = 0.f, gyv = 0.f;
-      if (on) {
-        const float w = net_weights ? net_weights[net] : 1.0f;
-        if (lane == sg.head) {
-          const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                                __fdiv_rn(ye_n, f_n));
-          contrib += (double)(net_weights ? fmul(wl, w) : wl);
-        }
-        const float b_x = __fdiv_rn(inv_gamma, e_p);
-        const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
-        const float b_nx = __fdiv_rn(-inv_gamma, e_n);
-        const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
-        const float b_y = __fdiv_rn(inv_gamma, f_p);
-        const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
-        const float b_ny = __fdiv_rn(-inv_gamma, f_n);
-        const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
-        gxv = fsub(fmul(fadd(a_x, fmul(b_x, xx)), ex), fmul(fadd(a_nx, fmul(b_nx, xx)), enx));
-        gyv = fsub(fmul(fadd(a_y, fmul(b_y, yy)), ey), fmul(fadd(a_ny, fmul(b_ny, yy)), eny));
-        if (net_weights) {  // the backward's net-weight factor, folded in
-          gxv = fmul(gxv, w);
-          gyv = fmul(gyv, w);
-        }
-      }
-      __stcs(gnode + cur_csr, make_float2(gxv, gyv));
-    } else {
-      // one net with more than 32 pins: lanes stride over its pins
-      const int net = slot_net[s0];
-      const bool on = net_mask[net];
-      float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
-      for (int s = s0 + lane; s < s1; s += 32) {
-        const float2 p = xy[slot_node[s]];
-        const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
-        x_max = fmaxf(x_max, xx);
-        x_min = fminf(x_min, xx);
-        y_max = fmaxf(y_max, yy);
-        y_min = fminf(y_min, yy);
-      }
-      x_max = warp_all(x_max, 0);
-      x_min = warp_all(x_min, 1);
-      y_max = warp_all(y_max, 0);
-      y_min = warp_all(y_min, 1);
-      if (kGrad && hpwl_partials && lane == 0 && hpwl_mask[net]) {
-        float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
-        if (net_weights) h = fmul(h, net_weights[net]);
-        hcontrib += (double)h;
-      }
-      if (!kGrad) {
-        if (on && lane == 0) {
-          float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
-          if (net_weights) h = fmul(h, net_weights[net]);
-          contrib += (double)h;
-        }
-        continue;
-      }
-      float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
-      for (int s = s0 + lane; s < s1; s += 32) {
-        const float2 p = xy[slot_node[s]];
-        const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
-        const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
-        const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
-        xe_p = fadd(xe_p, fmul(xx, a1));
-        xe_n = fadd(xe_n, fmul(xx, a2));
-        e_p = fadd(e_p, a1);
-        e_n = fadd(e_n, a2);
-        ye_p = fadd(ye_p, fmul(yy, a3));
-        ye_n = fadd(ye_n, fmul(yy, a4));
-        f_p = fadd(f_p, a3);
-        f_n = fadd(f_n, a4);
-      }
-      xe_p = warp_all(xe_p, 2); xe_n = warp_all(xe_n, 2); e_p = warp_all(e_p, 2); e_n = warp_all(e_n, 2);
-      ye_p = warp_all(ye_p, 2); ye_n = warp_all(ye_n, 2); f_p = warp_all(f_p, 2); f_n = warp_all(f_n, 2);
-      const float w = net_weights ? net_weights[net] : 1.0f;
-      if (on && lane == 0) {
-        const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                              __fdiv_rn(ye_n, f_n));
-        contrib += (double)(net_weights ? fmul(wl, w) : wl);
-      }
-      const float b_x = __fdiv_rn(inv_gamma, e_p);
-      const float a_x = (float)((1.0 - (double)fmul(b_x, xe_p)) / (double)e_p);
-      const float b_nx = __fdiv_rn(-inv_gamma, e_n);
-      const float a_nx = (float)((1.0 - (double)fmul(b_nx, xe_n)) / (double)e_n);
-      const float b_y = __fdiv_rn(inv_gamma, f_p);
-      const float a_y = (float)((1.0 - (double)fmul(b_y, ye_p)) / (double)f_p);
-      const float b_ny = __fdiv_rn(-inv_gamma, f_n);
-      const float a_ny = (float)((1.0 - (double)fmul(b_ny, ye_n)) / (double)f_n);
-      for (int s = s0 + lane; s < s1; s += 32) {
-        float gxv = 0.f, gyv = 0.f;
-        if (on) {
-          const float2 p = xy[slot_node[s]];
-          const float xx = fadd(slot_offx[s], p.x), yy = fadd(slot_offy[s], p.y);
-          const float a1 = expf(fmul(fsub(xx, x_max), inv_gamma)), a2 = expf(fmul(fsub(x_min, xx), inv_gamma));
-          const float a3 = expf(fmul(fsub(yy, y_max), inv_gamma)), a4 = expf(fmul(fsub(y_min, yy), inv_gamma));
-          gxv = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
-          gyv = fsub(fmul(fadd(a_y, fmul(b_y, yy)), a3), fmul(fadd(a_ny, fmul(b_ny, yy)), a4));
-          if (net_weights) {
-            gxv = fmul(gxv, w);
-            gyv = fmul(gyv, w);
-          }
-        }
-        gnode[csr_pos[s]] = make_float2(gxv, gyv);
-      }
-    }
-  }
-  block_partial(contrib, partials);
-  if (kGrad && hpwl_partials) block_partial(hcontrib, hpwl_partials);
 }
 
 // node grad (+)= grad_pos[0] * sum of its pins' (weighted) gradients, which
@@ -872,81 +416,6 @@ __global__ void node_sum_kernel(const float2* __restrict__ gnode, const int* __r
 }
 
 }  // namespace dpb
-
-extern "C" int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
-                                  int* num_chunks) {
-  DP_REQUIRE(netpin_start_host && chunk_net_host && num_chunks && max_pins > 0, "dp_plan_net_chunks: bad arguments");
-  int c = 0;
-  int e = 0;
-  while (e < num_nets) {
-    chunk_net_host[c++] = e;
-    int pins = netpin_start_host[e + 1] - netpin_start_host[e];
-    ++e;
-    if (pins <= max_pins) {
-      while (e < num_nets && pins + (netpin_start_host[e + 1] - netpin_start_host[e]) <= max_pins) {
-        pins += netpin_start_host[e + 1] - netpin_start_host[e];
-        ++e;
-      }
-    }
-  }
-  chunk_net_host[c] = num_nets;
-  *num_chunks = c;
-  return DP_OK;
-}
-
-static int launch_chunks(bool grad, const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                         const float* slot_offy, const int* slot_net, const int* chunk_pin,
-                         int num_chunks, const float* net_weights, const unsigned char* net_mask,
-                         const float* inv_gamma, const int* csr_pos, double* out_f64, float* gnode, int num_slots,
-                         const unsigned char* hpwl_mask, double* hpwl_f64, cudaStream_t s) {
-  using namespace dpb;
-  int blocks = num_chunks > 0 ? ceil_div((long long)num_chunks * 32, 256) : 1;
-  if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  const float2* p2 = reinterpret_cast<const float2*>(xy);
-  if (grad)
-    wa_chunk_kernel<true><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, chunk_pin,
-                                                num_chunks, net_weights, net_mask, inv_gamma, csr_pos,
-                                                out_f64 + 1, reinterpret_cast<float2*>(gnode), hpwl_mask,
-                                                hpwl_f64 ? hpwl_f64 + 1 : nullptr);
-  else
-    wa_chunk_kernel<false><<<blocks, 256, 0, s>>>(p2, slot_node, slot_offx, slot_offy, slot_net, chunk_pin,
-                                                 num_chunks, net_weights, net_mask, nullptr, nullptr,
-                                                 out_f64 + 1, nullptr, nullptr, nullptr);
-  int rc = check_launch(grad ? "dp_wa_chunk_forward" : "dp_hpwl_chunk");
-  if (rc) return rc;
-  if (grad && hpwl_f64) {
-    rc = launch_finish_sum(hpwl_f64, blocks, nullptr, s);
-    if (rc) return rc;
-  }
-  return launch_finish_sum(out_f64, blocks, nullptr, s);
-}
-
-extern "C" int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                                   const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
-                                   const float* net_weights,
-                                   const unsigned char* net_mask, const float* inv_gamma, const int* csr_pos,
-                                   double* wl_f64, float* grad_node_order, int num_slots,
-                                   const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream) {
-  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && chunk_pin && net_mask && inv_gamma && csr_pos &&
-                 wl_f64 && grad_node_order,
-             "dp_wa_chunk_forward: null pointer argument");
-  DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)grad_node_order & 7) == 0,
-             "dp_wa_chunk_forward: xy and grad_node_order must be 8-byte aligned");
-  DP_REQUIRE(!hpwl_f64 || hpwl_mask, "dp_wa_chunk_forward: hpwl_f64 needs hpwl_mask");
-  return launch_chunks(true, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, chunk_pin, num_chunks, net_weights, net_mask, inv_gamma, csr_pos, wl_f64, grad_node_order, num_slots,
-                       hpwl_mask, hpwl_f64, dpb::as_stream(stream));
-}
-
-extern "C" int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                             const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
-                             const float* net_weights,
-                             const unsigned char* net_mask, double* out_f64, dp_stream_t stream) {
-  DP_REQUIRE(xy && slot_node && slot_offx && slot_offy && slot_net && chunk_pin && net_mask && out_f64,
-             "dp_hpwl_chunk: null pointer argument");
-  DP_REQUIRE(((uintptr_t)xy & 7) == 0, "dp_hpwl_chunk: xy must be 8-byte aligned");
-  return launch_chunks(false, xy, num_nodes, slot_node, slot_offx, slot_offy, slot_net, chunk_pin, num_chunks, net_weights, net_mask, nullptr, nullptr, out_f64, nullptr, 0, nullptr, nullptr,
-                       dpb::as_stream(stream));
-}
 
 extern "C" int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start,
                                const float* grad_pos, int num_movable, int num_nodes, int accumulate, float* grad_out,

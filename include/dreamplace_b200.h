@@ -320,32 +320,7 @@ int dp_pin_weight_sum(const float* net_weights, const int* flat_nodepin,
                       int num_physical_nodes, int num_nodes, float* node_weights,
                       dp_stream_t stream);
 
-/* ---- fused global-placement iteration (engine path) -------------------------
- * "Slots" are pin positions in flat_netpin order: slot_node[j] =
- * pin2node[flat_netpin[j]], slot_offx/y[j] = pin offsets of that pin.
- * dp_wa_slot_forward = pin_pos + WA merged forward of the reference
- * (pin_pos/src/pin_pos_cuda_kernel.cu:11-27 + weighted_average_wirelength/src/
- * weighted_average_wirelength_cuda_merged_kernel.cu:15-85): per-slot gradient
- * grad_slot [2*num_slots] and the fp64 total.  wl_f64 holds DP_REDUCE_DOUBLES
- * doubles: [0] receives the total, the rest is scratch for the fixed-order
- * (run-to-run reproducible) reduction. */
-int dp_wa_slot_forward(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
-                       const float* slot_offy, const int* netpin_start, int num_nets,
-                       const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
-                       double* wl_f64, float* grad_slot, int num_slots, dp_stream_t stream);
-/* WA backward + pin_pos backward (weighted_average_wirelength.py:197-213 +
- * pin_pos/src/pin_pos_cuda_kernel.cu:50-74): grad_out[node] (+)= sum over the
- * node's pins, in flat_node2pin order (node_slots = slot of each pin), of
- * grad_slot * grad_pos[0] * w_net; nodes >= num_movable get 0 (pin mask). */
-int dp_wa_node_backward(const float* grad_slot, int num_slots, const int* node_slots,
-                        const int* node_start, const int* slot_net, const float* net_weights,
-                        const unsigned char* net_mask, const float* grad_pos, int num_movable,
-                        int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
-/* HPWL through the slot gather (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64 holds
- * DP_REDUCE_DOUBLES doubles, [0] receives the fp64 total. */
-int dp_hpwl_slot(const float* pos, int num_nodes, const int* slot_node, const float* slot_offx,
-                 const float* slot_offy, const int* netpin_start, int num_nets, const float* net_weights,
-                 const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
+/* ---- fused global-placement iteration (engine path) ------------------------- */
 /* Nesterov step of NesterovAcceleratedGradientOptimizer.step_nobb
  * (dreamplace/NesterovAcceleratedGradientOptimizer.py:65-166) on device
  * scalars state[DP_NESTEROV_STATE_DOUBLES + 2 * DP_REDUCE_DOUBLES] (fp64):
@@ -377,12 +352,10 @@ int dp_assemble_precondition_step(const float* grad_node_order, const int* node_
                                   const float* lambda_, int num_nodes, const float* v_new, const float* v,
                                   const float* g, float* g_new, double* state, const int* grad_index,
                                   dp_stream_t stream);
-/* after an accepted step: a_k <- a_{k+1}, next a_{k+1} and coef */
-int dp_nesterov_advance(double* state, dp_stream_t stream);
 /* The GP loop's work between iteration k and k+1 (dreamplace/NonLinearPlace.py
  * main loop; dreamplace/PlaceObj.py:833-851 update_density_weight in RePlAce
  * HPWL mode, :901-915 update_gamma), on the device: state_new <- state_prev's
- * scalars, advanced (dp_nesterov_advance); sched = {k, HPWL of iteration k-1}
+ * scalars, advanced (a_k <- a_{k+1}, next a_{k+1} and coef); sched = {k, HPWL of iteration k-1}
  * (fp64[2]) becomes {k + 1, hpwl_k[0]}; weights = {lambda, gamma, 1/gamma}
  * (float[3]): with f = k + 1, lambda <- lambda * (float)mu for f > 1,
  * mu = upper * max(0.9999^f, 0.98) when HPWL fell, else
@@ -404,30 +377,6 @@ int dp_iteration_head(const double* state_prev, double* state_new, const double*
  * 1 when accept_prev is given and *accept_prev == 0, else 0. */
 int dp_set_trial_gate(const int* gate);
 int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t stream);
-/* Host planner: packs nets, in order, into chunks of at most max_pins pins (a
- * larger net is a chunk of its own).  chunk_net_host [num_nets + 1] receives the
- * first net of each chunk followed by num_nets; *num_chunks their count. */
-int dp_plan_net_chunks(const int* netpin_start_host, int num_nets, int max_pins, int* chunk_net_host,
-                       int* num_chunks);
-/* WA forward, one warp per net chunk (max_pins = 32), one lane per pin; per-net
- * reductions are segmented warp shuffles.  chunk_pin [num_chunks + 1]: first
- * pin slot of each chunk (netpin_start at the chunk's first net, see
- * dp_plan_net_chunks), then the pin count.  Node positions come interleaved
- * (xy [2 * num_nodes], see dp_pack_xy).  The per-pin gradient, times the net
- * weight, is written as an (x, y) pair at csr_pos[slot] (the pin's position in
- * node-CSR order) of grad_node_order [2 * num_slots]; masked nets write 0.
- * wl_f64: DP_REDUCE_DOUBLES doubles.  hpwl_f64 (optional, DP_REDUCE_DOUBLES
- * doubles): the HPWL of the same pins under hpwl_mask, equal to dp_hpwl_chunk's
- * result (same per-net values, same summation order), from the same pin reads. */
-int dp_wa_chunk_forward(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                        const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
-                        const float* net_weights, const unsigned char* net_mask, const float* inv_gamma,
-                        const int* csr_pos, double* wl_f64, float* grad_node_order, int num_slots,
-                        const unsigned char* hpwl_mask, double* hpwl_f64, dp_stream_t stream);
-/* HPWL with the same chunking (hpwl/src/hpwl_cuda_kernel.cu:10-39); out_f64: DP_REDUCE_DOUBLES */
-int dp_hpwl_chunk(const float* xy, int num_nodes, const int* slot_node, const float* slot_offx,
-                  const float* slot_offy, const int* slot_net, const int* chunk_pin, int num_chunks,
-                  const float* net_weights, const unsigned char* net_mask, double* out_f64, dp_stream_t stream);
 /* Lane-per-net plan (host): nets of degree 1..8 grouped 32 at a time by degree,
  * in the order net_order_host gives (a permutation of the nets; NULL: net
  * index order) within a degree; each larger net a group of its own.  The
@@ -447,8 +396,12 @@ int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, const int* net
  * whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the
  * pin arrays gathered to lane-slot order (ln_csr: the pin's position in
  * node-CSR order, where its gradient is written; NULL writes the gradient of
- * lane slot p at p).  Outputs as dp_wa_chunk_forward; hpwl_f64 (optional)
- * equals dp_hpwl_lanes on the same plan. */
+ * lane slot p at p).  The per-pin gradient, times the net weight, is written
+ * as an (x, y) pair into grad_node_order; masked nets write 0.  wl_f64 holds
+ * DP_REDUCE_DOUBLES doubles: [0] receives the fp64 total, the rest is scratch
+ * for the fixed-order (run-to-run reproducible) reduction.  hpwl_f64
+ * (optional, DP_REDUCE_DOUBLES doubles): the HPWL of the same pins under
+ * hpwl_mask, equal to dp_hpwl_lanes on the same plan. */
 int dp_wa_lanes_forward(const float* xy, const int* group_deg, const int* group_base, const int* group_net,
                         int num_groups, const int* ln_node, const float* ln_offx, const float* ln_offy,
                         const int* ln_csr, const float* net_weights, const unsigned char* net_mask,
