@@ -769,7 +769,11 @@ extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, con
 
 static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, double* hpwl_f64, cudaStream_t s) {
   using namespace dpb;
+  // one wave: the launch bounds keep 4 blocks of 256 resident per SM, and the
+  // warps stride over the groups, so a larger grid only adds a partial last
+  // wave (at 1279 blocks, a third wave of 95)
   int blocks = A.num_groups > 0 ? ceil_div((long long)A.num_groups * 32, 256) : 1;
+  if (blocks > kNumSMs * 4) blocks = kNumSMs * 4;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   if (grad)
     wa_lane_kernel<true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr, trial_gate());
