@@ -165,16 +165,36 @@ __device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0,
       }
 }
 
+// Cells [b0, b1) of the visiting order (blocked-sorted when sort0, added to
+// map0) and [b1, b2) (sorted when sort1, added to map1) in one launch: the
+// first ceil((b1 - b0) / kWsCells) blocks take the first range, so the
+// second range's blocks fill the first's last wave.
+struct WsRanges {
+  int b0, b1, b2;
+  int sort0, sort1;
+  float* map0_f32;
+  float* map1_f32;
+  unsigned long long* map0_fx;
+  unsigned long long* map1_fx;
+};
+
 template <bool kFixed, int kRadixBits>
-__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_kernel(TriangleArgs a, int sort_cells,
+__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_kernel(TriangleArgs a, WsRanges rg,
                                                                         const float2* __restrict__ xy_o,
                                                                         const int* __restrict__ order,
                                                                         const float4* __restrict__ rec4,
-                                                                        const float* __restrict__ ratio_o, int count,
-                                                                        float fx_scale, float* map_f32,
-                                                                        unsigned long long* map_fx,
+                                                                        const float* __restrict__ ratio_o,
+                                                                        float fx_scale,
                                                                         const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
+  const int nb0 = (rg.b1 - rg.b0 + kWsCells - 1) / kWsCells;
+  const bool second = (int)blockIdx.x >= nb0;
+  const int begin = second ? rg.b1 : rg.b0;
+  const int count = second ? rg.b2 : rg.b1;  // end of this block's range
+  const int sort_cells = second ? rg.sort1 : rg.sort0;
+  float* const map_f32 = second ? rg.map1_f32 : rg.map0_f32;
+  unsigned long long* const map_fx = second ? rg.map1_fx : rg.map0_fx;
+  const int bid = second ? (int)blockIdx.x - nb0 : (int)blockIdx.x;
   extern __shared__ __align__(16) unsigned char tile_raw[];
   using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
   Acc* tile = reinterpret_cast<Acc*>(tile_raw);
@@ -184,7 +204,7 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_ker
   // each warp takes kWsWarpCells consecutive cells, each lane kWsCellsPerLane
   // consecutive ones, so cells of one window start bin (sorted together) meet
   // in one lane's running window and then in neighbouring lanes
-  const int wbase = blockIdx.x * kWsCells + warp * kWsWarpCells;
+  const int wbase = begin + bid * kWsCells + warp * kWsWarpCells;
   float nx[kWsCellsPerLane], ny[kWsCellsPerLane], sxs[kWsCellsPerLane], sys[kWsCellsPerLane], rr[kWsCellsPerLane];
   int bk0 = INT_MAX, bk1 = INT_MIN, bh0 = INT_MAX, bh1 = INT_MIN;
   unsigned live = 0;
@@ -566,9 +586,13 @@ __global__ void overflow_kernel(const float* __restrict__ map, int n, double tar
 // First map of the split scatter: converts it from fixed point (fixed != NULL)
 // or reads it, optionally copies it to copy_to (start of the second map), and
 // reduces its overflow sum and maximum as overflow_kernel does.
+// The movable-only map (from the fixed-point sums, or as scattered) with its
+// overflow partials and max (when partials is given), and the full map:
+// copy_to = first, or copy_to += first when add_to_copy (copy_to then holds
+// the fillers' own map).
 __global__ void first_map_kernel(const long long* __restrict__ fixed, const float* __restrict__ init,
-                                 double inv_scale, float* first, float* __restrict__ copy_to, int n,
-                                 double target_area, double* partials, unsigned* maxkey,
+                                 double inv_scale, float* first, float* __restrict__ copy_to, int add_to_copy,
+                                 int n, double target_area, double* partials, unsigned* maxkey,
                                  const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
   double s = 0.0;
@@ -581,11 +605,12 @@ __global__ void first_map_kernel(const long long* __restrict__ fixed, const floa
     } else {
       d = first[i];
     }
-    if (copy_to) copy_to[i] = d;
+    if (copy_to) copy_to[i] = add_to_copy ? fadd(d, copy_to[i]) : d;
     const double over = (double)d - target_area;
     s += over > 0.0 ? over : 0.0;
     m = fmaxf(m, d);
   }
+  if (!partials) return;  // uniform: no overflow wanted
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(maxkey, float_key(m));
   block_partial(s, partials);
@@ -786,10 +811,10 @@ struct OrderedScatter {
   cudaStream_t s;
 };
 
-// adds cells [begin, end) of the visiting order onto out (fp32) or scratch (fixed)
+// adds the cells of rg's two ranges of the visiting order onto their maps
+// (fp32, or the fixed-point scratch maps), in one launch
 template <int kRadixBits>
-int scatter_range_r(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits,
-                    int64_t* scratch, float* out, int sort_cells) {
+int scatter_ranges_r(const OrderedScatter& o, const WsRanges& rg, int deterministic, int fraction_bits) {
   static bool configured = false;
   if (!configured) {
     cudaFuncSetAttribute(window_scatter_kernel<false, kRadixBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -798,25 +823,29 @@ int scatter_range_r(const OrderedScatter& o, int begin, int end, int determinist
                          kWsSmemBytes);
     configured = true;
   }
-  const int count = end - begin;
-  if (count <= 0) return DP_OK;
-  const int blocks = ceil_div(count, kWsCells);
+  const int blocks = ceil_div(rg.b1 - rg.b0, kWsCells) + ceil_div(rg.b2 - rg.b1, kWsCells);
+  if (blocks <= 0) return DP_OK;
   if (deterministic)
     window_scatter_kernel<true, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, sort_cells, o.order ? o.xy_o : o.xy_o + begin, o.order ? o.order + begin : nullptr, o.rec4 + begin,
-        o.ratio_o + begin, count, ldexpf(1.0f, fraction_bits),
-        nullptr, reinterpret_cast<unsigned long long*>(scratch), trial_gate());
+        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, ldexpf(1.0f, fraction_bits), trial_gate());
   else
     window_scatter_kernel<false, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, sort_cells, o.order ? o.xy_o : o.xy_o + begin, o.order ? o.order + begin : nullptr, o.rec4 + begin,
-        o.ratio_o + begin, count, 0.f, out, nullptr,
-        trial_gate());
+        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, 0.f, trial_gate());
   return check_launch("dp_density_map_ordered scatter");
 }
 
+// adds cells [begin, end) of the visiting order onto out (fp32) or scratch (fixed)
 int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits, int64_t* scratch,
                   float* out, int sort_cells = 1) {
-  return scatter_range_r<4>(o, begin, end, deterministic, fraction_bits, scratch, out, sort_cells);
+  if (end <= begin) return DP_OK;
+  WsRanges rg;
+  memset(&rg, 0, sizeof(rg));
+  rg.b0 = begin;
+  rg.b1 = rg.b2 = end;
+  rg.sort0 = sort_cells;
+  rg.map0_f32 = out;
+  rg.map0_fx = reinterpret_cast<unsigned long long*>(scratch);
+  return scatter_ranges_r<4>(o, rg, deterministic, fraction_bits);
 }
 
 int convert_fixed(const int64_t* scratch, const float* init, int fraction_bits, float* out, int nbins,
@@ -915,7 +944,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
     if (overflow_out) {
       cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
       first_map_kernel<<<blocks, 256, 0, o.s>>>((const long long*)scratch, init, ldexp(1.0, -fraction_bits),
-                                                 out_first, nullptr, nbins, target_area, overflow_out + 3, maxslot,
+                                                 out_first, nullptr, 0, nbins, target_area, overflow_out + 3, maxslot,
                                                  trial_gate());
       rc = check_launch("dp_density_map_ordered_split first map");
       if (rc) return rc;
@@ -930,24 +959,35 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
     if (rc) return rc;
     return convert_fixed(scratch, init, fraction_bits, out_all, nbins, o.s);
   }
+  // fp32: both ranges in one launch (the second range's blocks fill the
+  // first's last wave), the first onto out_first = init, the second onto
+  // out_all = 0; then out_all += out_first, with the overflow of out_first
   rc = start_map(init, out_first, nbins, o.s);
   if (rc) return rc;
-  rc = scatter_range(o, 0, num_first, 0, 0, nullptr, out_first);
-  if (rc) return rc;
-  if (overflow_out) {
-    cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
-    first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, nbins, target_area,
-                                               overflow_out + 3, maxslot, trial_gate());
-    rc = check_launch("dp_density_map_ordered_split first map");
-    if (rc) return rc;
-    overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
-                                                          overflow_out + 3, blocks);
-    rc = check_launch("dp_density_map_ordered_split overflow");
-  } else {
-    rc = copy_map(out_first, out_all, nbins, o.s);
+  cudaError_t e = cudaMemsetAsync(out_all, 0, sizeof(float) * nbins, o.s);
+  if (e != cudaSuccess) {
+    set_error("dp_density_map_ordered_split: cudaMemsetAsync: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
   }
+  WsRanges rg;
+  memset(&rg, 0, sizeof(rg));
+  rg.b0 = 0;
+  rg.b1 = num_first;
+  rg.b2 = count;
+  rg.sort0 = 1;  // the movable cells: block-local sort (their order goes stale)
+  rg.sort1 = 0;  // the fillers: about one per bin, runs stay short
+  rg.map0_f32 = out_first;
+  rg.map1_f32 = out_all;
+  rc = scatter_ranges_r<4>(o, rg, 0, 0);
   if (rc) return rc;
-  return scatter_range(o, num_first, count, 0, 0, nullptr, out_all, 0);
+  if (overflow_out) cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
+  first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, 1, nbins, target_area,
+                                             overflow_out ? overflow_out + 3 : nullptr, maxslot, trial_gate());
+  rc = check_launch("dp_density_map_ordered_split first map");
+  if (rc || !overflow_out) return rc;
+  overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
+                                                        overflow_out + 3, blocks);
+  return check_launch("dp_density_map_ordered_split overflow");
 }
 
 // ---------------------------------------------------------------- allocation-free variant
