@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--design", default="cells_2m", choices=["cells_10k", "cells_2m"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-gp", action="store_true",
+                    help="skip the runs of both Poisson-solve forms to the 0.07 overflow stop")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host round-trip run (profiling)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the per-kernel timing (profiling)")
@@ -282,18 +284,20 @@ def _graph_time(fn, reps=20):
 
 
 def piece_work(design, eng):
-    """Algorithmic bytes (or flops) of each piece of one Nesterov trial:
+    """Algorithmic bytes (or flops) of each piece of one Nesterov trial, per
+    launch (n_s scattered cells, P pins, E nets, n nodes, M x N bins):
 
-    * density_scatter: per scattered cell 16 B record + 4 B ratio + 4 B order
-      index + 8 B position; per bin 4 B initial map read, movable-only map
-      written and read back by the fused overflow pass, full map written;
+    * density_scatter: 28 B per scattered cell (16 B record + 4 B ratio + 8 B
+      position); per bin 4 B initial map read and the two maps written (the
+      movable-only map for the overflow and the movable + filler map);
     * poisson_gemms: the GEMM flops of one solve (three 2-D transforms, x3
       for split-BF16; the energy is summed in the spectral domain);
-    * field_gather: per cell the same 32 B as the scatter + 8 B force written;
+    * field_gather: per cell the same 28 B as the scatter + 8 B force written;
       per bin the two field maps read once;
-    * wa_forward (HPWL included): per pin 20 B of pin arrays + 8 B gradient
-      written; per net 4 B start + 2 x 1 B masks + 4 B weight; per node 8 B
-      position;
+    * wa_forward (HPWL included): per pin 12 B of pin arrays (node id, two
+      offsets) + 8 B gradient written; per net 4 B start + 2 x 1 B masks +
+      4 B weight; per node 8 B position (the pins' position gathers hit
+      those 8 B);
     * assemble_precondition: per pin 8 B gradient read; per node 4 B pin
       start + 4 B inverse order + 8 B force + 4 B pin weight sum + 4 B area +
       3 x 8 B (v_new, v, g) read + 8 B written;
@@ -304,10 +308,10 @@ def piece_work(design, eng):
     n_s = d.num_movable_nodes + d.num_filler_nodes
     M, N = ep.num_bins_x, ep.num_bins_y
     P, E, n = d.num_pins, d.num_nets, d.num_nodes
-    return {"density_scatter": (32.0 * n_s + 16.0 * M * N, "hbm"),
+    return {"density_scatter": (28.0 * n_s + 12.0 * M * N, "hbm"),
             "poisson_gemms": (poisson_flops(M, N, eng.prec), "tensor" if eng.prec else "fp32"),
-            "field_gather": (40.0 * n_s + 8.0 * M * N, "hbm"),
-            "wa_forward": (28.0 * P + 10.0 * E + 8.0 * n, "hbm"),
+            "field_gather": (36.0 * n_s + 8.0 * M * N, "hbm"),
+            "wa_forward": (20.0 * P + 10.0 * E + 8.0 * n, "hbm"),
             "assemble_precondition": (8.0 * P + 64.0 * n, "hbm"),
             "nesterov_trial": (64.0 * n, "hbm")}
 
@@ -337,6 +341,40 @@ def kernel_roofline(placer, design, peaks, reps=20):
     t["nesterov_trial"] = _graph_time(lambda: eng.nesterov_trial_only(p), reps)
     eng.S[p].copy_(saved)
     return {k: (t[k],) + work[k] for k in t}
+
+
+def full_gp(design, precision, deterministic):
+    """Global placement of the design to the 0.07 overflow stop (at most 1000
+    iterations) through the public placer; final metrics and wall time."""
+    from dreamplace_b200.nonlinear_place import place
+    from dreamplace_b200.params import Params
+    p = Params(target_density=design.target_density, stop_overflow=0.07, dct_precision=precision,
+               deterministic_flag=int(deterministic))
+    torch.cuda.synchronize()
+    t0 = time.time()
+    placer, res = place(design, p, device="cuda")
+    torch.cuda.synchronize()
+    res["wall_s"] = round(time.time() - t0, 3)
+    res["iter_per_s_wall"] = round(res["iterations"] / res["wall_s"], 2)
+    del placer
+    return res
+
+
+def full_gp_comparison(design, precision):
+    """The metric's HPWL condition: the split-BF16 (or other) form and the
+    plain fp32 form each run to the 0.07 overflow stop; their final HPWLs and
+    the relative difference, in the benchmark's fp32-atomic scatter mode and
+    in deterministic (int64 fixed-point) mode, where the two runs differ only
+    in the Poisson-solve arithmetic."""
+    out = {}
+    for det in (0, 1):
+        a = full_gp(design, precision, det)
+        b = full_gp(design, "fp32", det)
+        key = "deterministic" if det else "fp32_atomic"
+        out[key] = {precision: a, "fp32": b,
+                    "hpwl_rel_diff_final": round(abs(a["hpwl"] - b["hpwl"]) / b["hpwl"], 6)}
+        torch.cuda.empty_cache()
+    return out
 
 
 def roofline_entry(name, ms, work, bound, peaks, timing):
@@ -581,6 +619,18 @@ def main():
         h_plain = prun.placer.metrics[-1][-1][-1]._host[0]
         plain = {"value": round(pval, 3), "ms_per_step": round(pms / K, 3), "speedup": round(value / pval, 3),
                  "hpwl_rel_diff_at_step": round(abs(h_ours - h_plain) / h_plain, 6), "compared_at_iteration": W + K}
+    kernels = {}
+    if pieces:
+        for k, (kms, work, bound) in pieces.items():
+            e = roofline_entry(k, kms, work, bound, peaks, "piece captured alone, replayed 20x")
+            kernels[k] = {"ms": e["ms_per_launch"], "achieved": e["achieved"], "unit": e["unit"], "frac": e["frac"],
+                          "bound": e["bound"], "work_per_launch": work}
+    convergence = None
+    if not args.no_full_gp and args.precision != "fp32":
+        run.placer = None  # free the timed runs' design state first
+        run_e2e = prun = None  # noqa: F841
+        torch.cuda.empty_cache()
+        convergence = full_gp_comparison(design, args.precision)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = cpu_threads()
@@ -604,8 +654,13 @@ def main():
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "kernel_ms": {k: round(v[0], 4) for k, v in pieces.items()},
                 "kernel_ms_timing": "each piece captured alone and replayed 20x after the timed region",
+                "kernels": kernels,
                 "trials_per_step": round(run.trials / max(K, 1), 3),
-                "plain_fp32": plain}
+                "voided_speculative_trials": int(run.trials - K),
+                "plain_fp32": plain,
+                "full_gp_to_overflow_0.07": convergence,
+                "hpwl_rel_diff_final": (convergence["fp32_atomic"]["hpwl_rel_diff_final"]
+                                        if convergence else None)}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -18,6 +18,7 @@
 #include <climits>
 #include <cstdlib>
 #include <mutex>
+#include <cuda.h>
 #include <type_traits>
 #include <cub/block/block_radix_sort.cuh>
 #include "reduce.cuh"
@@ -993,8 +994,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
 // ---------------------------------------------------------------- allocation-free variant
 // Some callers of this library cannot allocate device memory at the point
 // where they place: hosts that reserve the whole GPU up front under a fixed
-// memory budget, code running inside another framework's stream capture
-// (where cudaMalloc is not permitted and may synchronise the device), and
+// memory budget (another allocation would fail or evict their own data), and
 // FFI hosts (Go / Java / JavaScript bindings) that never link the CUDA
 // allocator.  dp_density_map_fx64_noalloc serves them: the deterministic
 // scatter's int64 scratch map lives in the file-scope device array below, of
@@ -1003,8 +1003,41 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
 static __device__ __align__(256) unsigned long long g_noalloc_fixed_map[DP_NOALLOC_MAX_BINS];
 
 // Host code may not use g_noalloc_fixed_map as an address: the symbol names a
-// host-side stand-in.  The device address is looked up once per device, with
-// that device current, and cached.
+// host-side stand-in.  The device address belongs to the CUDA context that
+// loaded this library's module on the device, so it is looked up with that
+// device current and cached per device together with the context's unique ID
+// (cuCtxGetId, never reused within a process).  A call under another context
+// -- the primary context re-created after cudaDeviceReset, or a context the
+// host made itself with the driver API -- looks the address up again.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+
+static int current_context_id(unsigned long long* id) {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PfnCtxGetId>(f);
+  });
+  DP_REQUIRE(get_current && get_id, "dp_density_map_fx64_noalloc: the driver offers no cuCtxGetCurrent / cuCtxGetId");
+  *id = 0;  // 0: no context is current on this thread
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return DP_OK;
+  if (get_id(ctx, id) != CUDA_SUCCESS) {
+    set_error("dp_density_map_fx64_noalloc: cuCtxGetId failed");
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}
+
 static int noalloc_scratch_address(int64_t** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -1014,17 +1047,28 @@ static int noalloc_scratch_address(int64_t** out) {
   }
   constexpr int kMaxDevices = 64;
   DP_REQUIRE(dev >= 0 && dev < kMaxDevices, "dp_density_map_fx64_noalloc: device ordinal %d out of range", dev);
+  unsigned long long ctx_id = 0;
+  int rc = current_context_id(&ctx_id);
+  if (rc) return rc;
   static void* addr[kMaxDevices] = {};
+  static unsigned long long addr_ctx[kMaxDevices] = {};
   static std::mutex mu;
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
+  if (!addr[dev] || ctx_id == 0 || addr_ctx[dev] != ctx_id) {
+    // (with no context current, this runtime call makes the device's primary
+    // context current; its ID is read afterwards)
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_fixed_map);
     if (e != cudaSuccess || !p) {
       set_error("dp_density_map_fx64_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
       return DP_ERR_CUDA;
     }
+    if (ctx_id == 0) {
+      rc = current_context_id(&ctx_id);
+      if (rc) return rc;
+    }
     addr[dev] = p;
+    addr_ctx[dev] = ctx_id;
   }
   *out = static_cast<int64_t*>(addr[dev]);
   return DP_OK;

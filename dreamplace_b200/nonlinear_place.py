@@ -5,7 +5,8 @@ Mirrors the reference's ``NonLinearPlace.__call__`` for the default flow
 loops Lgamma / Llambda / Lsub with their stop criteria, per-iteration HPWL and
 overflow evaluation (dreamplace/EvalMetrics.py:100-141), density-weight and
 gamma updates, best-position tracking, divergence rollback and the plateau
-rule that turns on the quadratic density penalty.
+rule that turns on the quadratic density penalty and, when overflow stays
+above 0.95, injects entropy (shrink towards the centroid plus noise).
 
 Two executions of the same iteration:
 
@@ -294,9 +295,12 @@ class NonLinearPlace(nn.Module):
                     overflow_list.append(o)
                     divergence_list.append([h, o])
                     if iteration - last_perturb_iter > 50 and check_plateau(overflow_list, 15, 0.001):
-                        if overflow_list[-1] > 0.9:
+                        if overflow_list[-1] > 0.9:  # stuck at high overflow
                             model.quad_penalty = True
                             model.density_factor *= 2
+                            if overflow_list[-1] > 0.95:  # stuck at very high overflow
+                                intensity = min(max(40 + (120 - 40) * (overflow_list[-1] - 0.95) * 10, 40), 90)
+                                self._entropy_injection(stepper, design, 0.996, intensity)
                             last_perturb_iter = iteration
                     self.iteration_times.append(time.time() - t0)
                     if callback is not None:
@@ -332,6 +336,31 @@ class NonLinearPlace(nn.Module):
         self.metrics = all_metrics
         self.best = best
         return all_metrics
+
+    @staticmethod
+    def _entropy_injection(stepper, design, shrink_factor, noise_intensity):
+        """Shrink all nodes towards the movable cells' centroid and add Gaussian
+        noise of ``noise_intensity`` layout units, fixed nodes kept in place
+        (reference dreamplace/NonLinearPlace.py:572-606, "random" mode).  The
+        perturbed position replaces v_k; the optimizer state is left as is, as
+        in the reference, whose v_k is the position parameter itself."""
+        d = design
+        n, m, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+        with torch.no_grad():
+            pos = stepper.position().clone()
+            xc = pos[:m].mean()
+            yc = pos[n:n + m].mean()
+            fixed_x = pos[m:n - nf].clone()
+            fixed_y = pos[n + m:2 * n - nf].clone()
+            if shrink_factor != 1:
+                pos[:n] = (pos[:n] - xc) * shrink_factor + xc
+                pos[n:] = (pos[n:] - yc) * shrink_factor + yc
+            if noise_intensity > 0.01:
+                pos.add_(noise_intensity * torch.randn(2 * n, device=pos.device))
+            pos[m:n - nf] = fixed_x
+            pos[n + m:2 * n - nf] = fixed_y
+            stepper.set_position(pos)
+        logger.info("entropy injection: shrink %g, noise intensity %g", shrink_factor, noise_intensity)
 
     @staticmethod
     def _lsub_stop(model, lsub):

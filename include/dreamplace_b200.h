@@ -92,14 +92,16 @@ int dp_density_map_fx64(const float* pos, int num_nodes,
 
 /* No counterpart in the reference.  Same result as dp_density_map_fx64, for
  * callers that cannot allocate device memory (a host that reserved the GPU
- * under a fixed budget, code inside another framework's stream capture where
- * cudaMalloc is not allowed, FFI hosts without the CUDA allocator).  The int64
+ * under a fixed budget, FFI hosts without the CUDA allocator).  The int64
  * scratch map is a built-in device array of DP_NOALLOC_MAX_BINS bins (8 MiB,
  * held by every GPU that loads the library until exit); larger grids are
- * rejected with DP_ERR_INVALID_ARGUMENT.  The first call on a device looks up
- * the array's device address, so make that first call before any stream
- * capture.  All calls share the one array (it keeps the last call's integer
- * map): calls that overlap on the GPU -- different streams or threads -- race. */
+ * rejected with DP_ERR_INVALID_ARGUMENT.  The first call under a CUDA context
+ * looks up the array's device address in that context (and caches it with
+ * the context's ID; a device reset or another context makes the next call
+ * look it up again), so make that first call before any stream capture.  All
+ * calls share the one array (it keeps the last call's integer map; each call
+ * zeroes it before its scatter): calls that overlap on the GPU -- different
+ * streams or threads -- race. */
 int dp_density_map_fx64_noalloc(const float* pos, int num_nodes,
                                 const float* node_size_x_clamped, const float* node_size_y_clamped,
                                 const float* offset_x, const float* offset_y, const float* ratio,

@@ -57,16 +57,34 @@ def wa_cancellation_scale(pin_pos, flat_netpin, netpin_start, net_mask, inv_gamm
     difference of an exponential moves the gradient by ~eps times this scale."""
     P = len(pin_pos) // 2
     T = np.zeros(2 * P)
-    for e in range(len(netpin_start) - 1):
-        if not net_mask[e]:
-            continue
-        pins = flat_netpin[netpin_start[e]:netpin_start[e + 1]]
-        for off in (0, P):
-            x = pin_pos[off + pins].astype(np.float64)
-            ep = np.exp((x - x.max()) * inv_gamma)
-            en = np.exp((x.min() - x) * inv_gamma)
-            b_p, b_n = inv_gamma / ep.sum(), -inv_gamma / en.sum()
-            a_p = (1.0 - b_p * (x * ep).sum()) / ep.sum()
-            a_n = (1.0 - b_n * (x * en).sum()) / en.sum()
-            T[off + pins] = (abs(a_p) + np.abs(b_p * x)) * ep + (abs(a_n) + np.abs(b_n * x)) * en
+    start = np.asarray(netpin_start, np.int64)
+    deg = np.diff(start)
+    live = (np.asarray(net_mask) != 0) & (deg > 0)
+    if not live.any() or P == 0:
+        return T
+    flat = np.asarray(flat_netpin, np.int64)
+    net_of_slot = np.repeat(np.arange(len(deg)), deg)
+    keep = live[net_of_slot]
+    first = start[:-1][live]
+    for off in (0, P):
+        x = pin_pos[off + flat].astype(np.float64)
+        # per-net max / min over each live net's slots (reduceat over the
+        # live nets' starts; slots of dead nets are never read back)
+        xmax = np.maximum.reduceat(x, first)
+        xmin = np.minimum.reduceat(x, first)
+        idx = np.full(len(deg), -1, np.int64)
+        idx[live] = np.arange(live.sum())
+        k = idx[net_of_slot[keep]]
+        xs = x[keep]
+        ep = np.exp((xs - xmax[k]) * inv_gamma)
+        en = np.exp((xmin[k] - xs) * inv_gamma)
+        # segment sums over the kept slots (nets stay contiguous)
+        seg = np.r_[0, np.cumsum(deg[live])[:-1]]
+        s_p, s_n = np.add.reduceat(ep, seg), np.add.reduceat(en, seg)
+        sx_p, sx_n = np.add.reduceat(xs * ep, seg), np.add.reduceat(xs * en, seg)
+        b_p, b_n = inv_gamma / s_p, -inv_gamma / s_n
+        a_p = (1.0 - b_p * sx_p) / s_p
+        a_n = (1.0 - b_n * sx_n) / s_n
+        t = (np.abs(a_p[k]) + np.abs(b_p[k] * xs)) * ep + (np.abs(a_n[k]) + np.abs(b_n[k] * xs)) * en
+        T[off + flat[keep]] = t
     return T

@@ -1,10 +1,11 @@
 """dp_density_map_fx64_noalloc through the C ABI: the allocation-free
 deterministic scatter for callers that cannot allocate device memory
-(fixed-budget hosts, code inside a foreign stream capture, FFI hosts without
-the CUDA allocator).  Its output must equal dp_density_map_fx64's (which takes
-a caller-owned scratch map) bit for bit -- the fixed-point map is exact -- on
-two calls in a row, since every call reuses the same built-in scratch array.
-Runs alone in a fresh process and after the other tests."""
+(fixed-budget hosts, FFI hosts without the CUDA allocator).  Its output must
+equal dp_density_map_fx64's (which takes a caller-owned scratch map) bit for
+bit -- the fixed-point map is exact -- on two calls in a row, since every call
+reuses the same built-in scratch array.  The file is named to be collected
+last; the test passes both in a fresh process
+(``pytest tests/test_zz_no_alloc.py``) and after the other tests."""
 import ctypes
 import math
 import os
