@@ -395,14 +395,18 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_ker
   }
   if (use_tile) {
     __syncthreads();
-    for (int t = threadIdx.x; t < (bk1 - bk0) * H; t += kWsThreads) {
-      const Acc v = tile[t];
-      if (v != (Acc)0) {
-        const int bin = (bk0 + t / H) * nby + bh0 + t % H;
-        if (kFixed)
-          atomicAdd(map_fx + bin, (unsigned long long)v);
-        else
-          atomicAdd(map_f32 + bin, (float)v);
+    // one warp per box row, lanes along the row (no index division)
+    for (int k = warp; k < bk1 - bk0; k += kWsThreads / 32) {
+      const Acc* row = tile + k * H;
+      const int gbase = (bk0 + k) * nby + bh0;
+      for (int h = lane; h < H; h += 32) {
+        const Acc v = row[h];
+        if (v != (Acc)0) {
+          if (kFixed)
+            atomicAdd(map_fx + gbase + h, (unsigned long long)v);
+          else
+            atomicAdd(map_f32 + gbase + h, (float)v);
+        }
       }
     }
   }

@@ -176,6 +176,11 @@ class NonLinearPlace(nn.Module):
         params = params or self.params
         design = design or self.design
         torch.manual_seed(params.random_seed)
+        # the entropy injection's noise comes from a generator of this run, so
+        # designs placed together (interleaved on one GPU) draw the noise they
+        # draw alone
+        noise_gen = torch.Generator(device=self.device)
+        noise_gen.manual_seed(params.random_seed + 1)
         gp = dict(params.global_place_stages[0])
         if max_iterations is not None:
             gp["iteration"] = max_iterations
@@ -300,7 +305,7 @@ class NonLinearPlace(nn.Module):
                             model.density_factor *= 2
                             if overflow_list[-1] > 0.95:  # stuck at very high overflow
                                 intensity = min(max(40 + (120 - 40) * (overflow_list[-1] - 0.95) * 10, 40), 90)
-                                self._entropy_injection(stepper, design, 0.996, intensity)
+                                self._entropy_injection(stepper, design, 0.996, intensity, noise_gen)
                             last_perturb_iter = iteration
                     self.iteration_times.append(time.time() - t0)
                     if callback is not None:
@@ -338,7 +343,7 @@ class NonLinearPlace(nn.Module):
         return all_metrics
 
     @staticmethod
-    def _entropy_injection(stepper, design, shrink_factor, noise_intensity):
+    def _entropy_injection(stepper, design, shrink_factor, noise_intensity, generator=None):
         """Shrink all nodes towards the movable cells' centroid and add Gaussian
         noise of ``noise_intensity`` layout units, fixed nodes kept in place
         (reference dreamplace/NonLinearPlace.py:572-606, "random" mode).  The
@@ -356,7 +361,7 @@ class NonLinearPlace(nn.Module):
                 pos[:n] = (pos[:n] - xc) * shrink_factor + xc
                 pos[n:] = (pos[n:] - yc) * shrink_factor + yc
             if noise_intensity > 0.01:
-                pos.add_(noise_intensity * torch.randn(2 * n, device=pos.device))
+                pos.add_(noise_intensity * torch.randn(2 * n, device=pos.device, generator=generator))
             pos[m:n - nf] = fixed_x
             pos[n + m:2 * n - nf] = fixed_y
             stepper.set_position(pos)

@@ -65,21 +65,17 @@ def wa_cancellation_scale(pin_pos, flat_netpin, netpin_start, net_mask, inv_gamm
     flat = np.asarray(flat_netpin, np.int64)
     net_of_slot = np.repeat(np.arange(len(deg)), deg)
     keep = live[net_of_slot]
-    first = start[:-1][live]
+    idx = np.full(len(deg), -1, np.int64)
+    idx[live] = np.arange(live.sum())
+    k = idx[net_of_slot[keep]]
+    # segments of the live nets' slots (nets stay contiguous among the kept slots)
+    seg = np.r_[0, np.cumsum(deg[live])[:-1]]
     for off in (0, P):
-        x = pin_pos[off + flat].astype(np.float64)
-        # per-net max / min over each live net's slots (reduceat over the
-        # live nets' starts; slots of dead nets are never read back)
-        xmax = np.maximum.reduceat(x, first)
-        xmin = np.minimum.reduceat(x, first)
-        idx = np.full(len(deg), -1, np.int64)
-        idx[live] = np.arange(live.sum())
-        k = idx[net_of_slot[keep]]
-        xs = x[keep]
+        xs = pin_pos[off + flat[keep]].astype(np.float64)
+        xmax = np.maximum.reduceat(xs, seg)
+        xmin = np.minimum.reduceat(xs, seg)
         ep = np.exp((xs - xmax[k]) * inv_gamma)
         en = np.exp((xmin[k] - xs) * inv_gamma)
-        # segment sums over the kept slots (nets stay contiguous)
-        seg = np.r_[0, np.cumsum(deg[live])[:-1]]
         s_p, s_n = np.add.reduceat(ep, seg), np.add.reduceat(en, seg)
         sx_p, sx_n = np.add.reduceat(xs * ep, seg), np.add.reduceat(xs * en, seg)
         b_p, b_n = inv_gamma / s_p, -inv_gamma / s_n
