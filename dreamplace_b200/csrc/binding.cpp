@@ -578,6 +578,63 @@ void node_pin_sum(at::Tensor grad_node_order, at::Tensor node_start, at::Tensor 
                           cur_stream()));
 }
 
+void wa_pins_forward(at::Tensor pin_pos, at::Tensor group_deg, at::Tensor group_base, at::Tensor group_net,
+                     at::Tensor ln_pin, c10::optional<at::Tensor> net_weights, at::Tensor net_mask,
+                     at::Tensor inv_gamma, at::Tensor wl_f64, at::Tensor grad_lane) {
+  CHECK_FLAT(pin_pos); CHECK_F32(pin_pos); CHECK_EVEN(pin_pos); CHECK_I32(group_deg); CHECK_I32(group_base);
+  CHECK_I32(group_net); CHECK_I32(ln_pin); CHECK_F32(grad_lane); CHECK_F32(inv_gamma);
+  TORCH_CHECK(group_net.numel() == 32 * group_deg.numel() && group_base.numel() == group_deg.numel(),
+              "wa_pins_forward: inconsistent plan");
+  TORCH_CHECK(grad_lane.numel() >= 2 * ln_pin.numel(), "wa_pins_forward: grad_lane smaller than the lane slots");
+  TORCH_CHECK(wl_f64.scalar_type() == at::kDouble && wl_f64.numel() >= DP_REDUCE_DOUBLES, "wl_f64 too small");
+  DP_CALL(dp_wa_pins_forward(ptr<float>(pin_pos), pin_pos.numel() / 2, ptr<int>(group_deg), ptr<int>(group_base),
+                             ptr<int>(group_net), group_deg.numel(), ptr<int>(ln_pin), (const float*)ovp(net_weights),
+                             net_mask.data_ptr<uint8_t>(), ptr<float>(inv_gamma), ptr<double>(wl_f64),
+                             ptr<float>(grad_lane), cur_stream()));
+}
+
+at::Tensor wa_pins_backward(at::Tensor grad_lane, at::Tensor lane_of_pin, c10::optional<at::Tensor> pin_mask,
+                            at::Tensor grad_out) {
+  CHECK_F32(grad_lane); CHECK_I32(lane_of_pin); CHECK_F32(grad_out);
+  const int64_t P = lane_of_pin.numel();
+  TORCH_CHECK(!pin_mask.has_value() || (pin_mask->numel() == P && pin_mask->element_size() == 1),
+              "wa_pins_backward: pin_mask must hold one byte per pin");
+  auto out = at::empty({2 * P}, grad_lane.options());
+  DP_CALL(dp_wa_pins_backward(ptr<float>(grad_lane), ptr<int>(lane_of_pin),
+                              pin_mask.has_value() ? (const unsigned char*)pin_mask->data_ptr() : nullptr,
+                              ptr<float>(grad_out), (int)P, ptr<float>(out), cur_stream()));
+  return out;
+}
+
+int64_t order_cells_scratch_bytes(int num_movable, int num_filler, int nbx, int nby) {
+  return (int64_t)dp_order_cells_scratch_bytes(num_movable, num_filler, nbx, nby);
+}
+
+void order_cells_by_bin(at::Tensor pos, at::Tensor ox, at::Tensor oy, int num_movable, int num_filler, double xl,
+                        double yl, double bsx, double bsy, int nbx, int nby, at::Tensor scratch, at::Tensor order) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_EVEN(pos); CHECK_I32(order); CHECK_CUDA_T(scratch); CHECK_CONTIG(scratch);
+  TORCH_CHECK(order.numel() >= num_movable + num_filler, "order_cells_by_bin: order too small");
+  DP_CALL(dp_order_cells_by_bin(ptr<float>(pos), pos.numel() / 2, ptr<float>(ox), ptr<float>(oy), num_movable,
+                                num_filler, xl, yl, inv_f(bsx), inv_f(bsy), nbx, nby, scratch.data_ptr(),
+                                (size_t)scratch.numel() * scratch.element_size(), ptr<int>(order), cur_stream()));
+}
+
+void gather_order_pos(at::Tensor pos, at::Tensor order, int count, at::Tensor xy_o) {
+  CHECK_FLAT(pos); CHECK_F32(pos); CHECK_I32(order); CHECK_F32(xy_o);
+  TORCH_CHECK(order.numel() >= count && xy_o.numel() >= 2 * count, "gather_order_pos: buffers smaller than count");
+  DP_CALL(dp_gather_order_pos(ptr<float>(pos), pos.numel() / 2, ptr<int>(order), count, ptr<float>(xy_o),
+                              cur_stream()));
+}
+
+at::Tensor scatter_pairs_to_nodes(at::Tensor vals_o, at::Tensor order, int count, int num_nodes) {
+  CHECK_F32(vals_o); CHECK_I32(order);
+  TORCH_CHECK(order.numel() >= count && vals_o.numel() >= 2 * count, "scatter_pairs_to_nodes: buffers too small");
+  auto out = at::empty({2 * (int64_t)num_nodes}, vals_o.options());
+  DP_CALL(dp_scatter_pairs_to_nodes(ptr<float>(vals_o), ptr<int>(order), count, num_nodes, ptr<float>(out),
+                                    cur_stream()));
+  return out;
+}
+
 uint64_t launch_count() { return dp_launch_count(); }
 
 // Launches an instantiated CUDA graph (torch.cuda.CUDAGraph.raw_cuda_graph_exec)
@@ -594,6 +651,12 @@ void graph_launch(int64_t graph_exec, int64_t stream) {
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.doc() = "dreamplace_b200 native ops (sm_100a) over the C ABI";
   m.def("density_map", &density_map);
+  m.def("wa_pins_forward", &wa_pins_forward);
+  m.def("wa_pins_backward", &wa_pins_backward);
+  m.def("order_cells_scratch_bytes", &order_cells_scratch_bytes);
+  m.def("order_cells_by_bin", &order_cells_by_bin);
+  m.def("gather_order_pos", &gather_order_pos);
+  m.def("scatter_pairs_to_nodes", &scatter_pairs_to_nodes);
   m.def("density_map_fixed_point", &density_map_fixed_point);
   m.def("fixed_density_map", &fixed_density_map);
   m.def("density_map_exact", &density_map_exact);

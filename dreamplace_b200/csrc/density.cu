@@ -1095,3 +1095,187 @@ extern "C" int dp_density_map_fx64_noalloc(const float* pos, int num_nodes, cons
   return dp_density_map_fx64(pos, num_nodes, sx, sy, ox, oy, ratio, init, xl, yl, xh, yh, bsx, bsy, ibx, iby, nm,
                              nf, nbx, nby, sorted, fraction_bits, scratch, out, stream);
 }
+
+// ---------------------------------------------------------------- visiting order
+// The scattered cells (movable, then fillers) bucketed by the bin where their
+// stretched footprint starts: 16 x 16-bin tiles in serpentine order, bin
+// inside the tile, movable cells before fillers.  A counting sort: one pass
+// computes each cell's bucket and counts the buckets, an exclusive scan turns
+// counts into starts, a second pass places the cells (the order inside a
+// bucket is whatever the atomics give: every visiting order is valid for the
+// scatter and the field gather).
+namespace dpb {
+
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ unsigned cell_bucket(float x, float ox, float lo, float inv_bs, int nbins) {
+  int b = (int)fmul(fsub(fadd(x, ox), lo), inv_bs);
+  return (unsigned)min(max(b, 0), nbins - 1);
+}
+
+__global__ void order_keys_kernel(const float* __restrict__ pos, int num_nodes, const float* __restrict__ ox,
+                                  const float* __restrict__ oy, int nm, int nf, float xl, float yl, float ibx,
+                                  float iby, int nbx, int nby, unsigned tile_buckets, unsigned* __restrict__ keys,
+                                  unsigned* __restrict__ hist) {
+  const int count = nm + nf;
+  const int tiles_y = (nby + 15) >> 4;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int node = i < nm ? i : num_nodes - nf + (i - nm);
+    const unsigned kx = cell_bucket(pos[node], ox[node], xl, ibx, nbx);
+    const unsigned hy = cell_bucket(pos[num_nodes + node], oy[node], yl, iby, nby);
+    const unsigned tx = kx >> 4;
+    unsigned ty = hy >> 4;
+    if (tx & 1u) ty = (unsigned)tiles_y - 1u - ty;
+    const unsigned key = (((tx * (unsigned)tiles_y + ty) << 8) | ((kx & 15u) << 4) | (hy & 15u)) +
+                         (i < nm ? 0u : tile_buckets);
+    keys[i] = key;
+    atomicAdd(hist + key, 1u);
+  }
+}
+
+// exclusive scan of n counts in place: per-block scans with block totals,
+// then the totals (one block), then the totals added back
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* warp_sums, unsigned& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  const unsigned before = warp == 0 ? 0u : warp_sums[warp - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(unsigned* data, int n, unsigned* block_totals) {
+  __shared__ unsigned warp_sums[32];
+  const int i = blockIdx.x * kScanThreads + threadIdx.x;
+  const unsigned v = i < n ? data[i] : 0u;
+  unsigned total;
+  const unsigned ex = block_exclusive_scan(v, warp_sums, total);
+  if (i < n) data[i] = ex;
+  if (threadIdx.x == 0) block_totals[blockIdx.x] = total;
+}
+
+// one block scans the block totals (at most kScanThreads * kScanThreads blocks)
+__global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(unsigned* totals, int nblocks) {
+  __shared__ unsigned warp_sums[32];
+  __shared__ unsigned carry;
+  if (threadIdx.x == 0) carry = 0u;
+  __syncthreads();
+  for (int base = 0; base < nblocks; base += kScanThreads) {
+    const int i = base + threadIdx.x;
+    const unsigned v = i < nblocks ? totals[i] : 0u;
+    unsigned total;
+    const unsigned ex = block_exclusive_scan(v, warp_sums, total);
+    if (i < nblocks) totals[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+}
+
+__global__ void add_block_offsets_kernel(unsigned* data, int n, const unsigned* block_offsets) {
+  const int i = blockIdx.x * kScanThreads + threadIdx.x;
+  if (i < n) data[i] += block_offsets[blockIdx.x];
+}
+
+__global__ void order_place_kernel(const unsigned* __restrict__ keys, int num_nodes, int nm, int nf,
+                                   unsigned* __restrict__ starts, int* __restrict__ order) {
+  const int count = nm + nf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const unsigned slot = atomicAdd(starts + keys[i], 1u);
+    order[slot] = i < nm ? i : num_nodes - nf + (i - nm);
+  }
+}
+
+// xy_o[idx] = (x, y) of node order[idx], from planar positions [x(n) | y(n)]
+__global__ void gather_order_pos_kernel(const float* __restrict__ pos, int num_nodes, const int* __restrict__ order,
+                                        int count, float2* __restrict__ xy_o) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+    const int i = __ldg(order + idx);
+    xy_o[idx] = make_float2(__ldg(pos + i), __ldg(pos + num_nodes + i));
+  }
+}
+
+static unsigned order_tile_buckets(int nbx, int nby) {
+  return (unsigned)(((nbx + 15) >> 4) * ((nby + 15) >> 4)) * 256u;
+}
+
+}  // namespace dpb
+
+extern "C" size_t dp_order_cells_scratch_bytes(int num_movable, int num_filler, int num_bins_x, int num_bins_y) {
+  using namespace dpb;
+  if (num_movable < 0 || num_filler < 0 || num_bins_x <= 0 || num_bins_y <= 0) return 0;
+  const size_t buckets = 2ull * order_tile_buckets(num_bins_x, num_bins_y);
+  const size_t blocks = (buckets + kScanThreads - 1) / kScanThreads;
+  return sizeof(unsigned) * (buckets + blocks + (size_t)num_movable + (size_t)num_filler) + 256;
+}
+
+extern "C" int dp_order_cells_by_bin(const float* pos, int num_nodes, const float* offset_x, const float* offset_y,
+                                     int num_movable, int num_filler, float xl, float yl, float inv_bin_size_x,
+                                     float inv_bin_size_y, int num_bins_x, int num_bins_y, void* scratch,
+                                     size_t scratch_bytes, int* order, dp_stream_t stream) {
+  using namespace dpb;
+  DP_REQUIRE(pos && offset_x && offset_y && scratch && order, "dp_order_cells_by_bin: null pointer argument");
+  DP_REQUIRE(num_movable >= 0 && num_filler >= 0 && num_movable + num_filler <= num_nodes,
+             "dp_order_cells_by_bin: bad node counts");
+  DP_REQUIRE(num_bins_x > 0 && num_bins_y > 0 && num_bins_x <= 65536 && num_bins_y <= 65536,
+             "dp_order_cells_by_bin: bad bin grid %dx%d", num_bins_x, num_bins_y);
+  const size_t need = dp_order_cells_scratch_bytes(num_movable, num_filler, num_bins_x, num_bins_y);
+  DP_REQUIRE(scratch_bytes >= need, "dp_order_cells_by_bin: scratch of %zu bytes, %zu needed", scratch_bytes, need);
+  DP_REQUIRE(((uintptr_t)scratch & 3) == 0, "dp_order_cells_by_bin: scratch must be 4-byte aligned");
+  const int count = num_movable + num_filler;
+  if (count == 0) return DP_OK;
+  cudaStream_t s = as_stream(stream);
+  const unsigned tile_buckets = order_tile_buckets(num_bins_x, num_bins_y);
+  const int buckets = (int)(2u * tile_buckets);
+  const int blocks = (buckets + kScanThreads - 1) / kScanThreads;
+  unsigned* hist = static_cast<unsigned*>(scratch);
+  unsigned* totals = hist + buckets;
+  unsigned* keys = totals + blocks;
+  cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * buckets, s);
+  if (e != cudaSuccess) {
+    set_error("dp_order_cells_by_bin: cudaMemsetAsync: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  order_keys_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(pos, num_nodes, offset_x, offset_y, num_movable,
+                                                            num_filler, xl, yl, inv_bin_size_x, inv_bin_size_y,
+                                                            num_bins_x, num_bins_y, tile_buckets, keys, hist);
+  int rc = check_launch("dp_order_cells_by_bin keys");
+  if (rc) return rc;
+  scan_blocks_kernel<<<blocks, kScanThreads, 0, s>>>(hist, buckets, totals);
+  rc = check_launch("dp_order_cells_by_bin scan");
+  if (rc) return rc;
+  scan_totals_kernel<<<1, kScanThreads, 0, s>>>(totals, blocks);
+  rc = check_launch("dp_order_cells_by_bin scan totals");
+  if (rc) return rc;
+  add_block_offsets_kernel<<<blocks, kScanThreads, 0, s>>>(hist, buckets, totals);
+  rc = check_launch("dp_order_cells_by_bin offsets");
+  if (rc) return rc;
+  order_place_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(keys, num_nodes, num_movable, num_filler, hist, order);
+  return check_launch("dp_order_cells_by_bin place");
+}
+
+extern "C" int dp_gather_order_pos(const float* pos, int num_nodes, const int* order, int count, float* xy_o,
+                                   dp_stream_t stream) {
+  using namespace dpb;
+  DP_REQUIRE(pos && xy_o && (count == 0 || order), "dp_gather_order_pos: null pointer argument");
+  DP_REQUIRE(((uintptr_t)xy_o & 7) == 0, "dp_gather_order_pos: xy_o must be 8-byte aligned");
+  if (count == 0) return DP_OK;
+  gather_order_pos_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+      pos, num_nodes, order, count, reinterpret_cast<float2*>(xy_o));
+  return check_launch("dp_gather_order_pos");
+}

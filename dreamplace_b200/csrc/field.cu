@@ -166,3 +166,34 @@ extern "C" int dp_electric_force(const float* grad_pos, int nbx, int nby, const 
       iby, nm, num_nodes - nf, total, sorted, scale, gx, gy);
   return check_launch("dp_electric_force");
 }
+
+namespace dpb {
+// out[node] = v.x, out[n + node] = v.y for node = order[idx]: values kept in
+// visiting order put back in node order
+__global__ void scatter_pairs_kernel(const float2* __restrict__ vals_o, const int* __restrict__ order, int count,
+                                     int num_nodes, float* __restrict__ out) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+    const int i = __ldg(order + idx);
+    const float2 v = __ldcs(vals_o + idx);
+    out[i] = v.x;
+    out[num_nodes + i] = v.y;
+  }
+}
+}  // namespace dpb
+
+extern "C" int dp_scatter_pairs_to_nodes(const float* vals_o, const int* order, int count, int num_nodes, float* out,
+                                         dp_stream_t stream) {
+  DP_REQUIRE(vals_o && order && out, "dp_scatter_pairs_to_nodes: null pointer argument");
+  DP_REQUIRE(count >= 0 && count <= num_nodes, "dp_scatter_pairs_to_nodes: bad counts");
+  DP_REQUIRE(((uintptr_t)vals_o & 7) == 0, "dp_scatter_pairs_to_nodes: vals_o must be 8-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * 2 * (size_t)num_nodes, s);
+  if (e != cudaSuccess) {
+    set_error("dp_scatter_pairs_to_nodes: cudaMemsetAsync: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  if (count == 0) return DP_OK;
+  scatter_pairs_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(reinterpret_cast<const float2*>(vals_o), order, count,
+                                                               num_nodes, out);
+  return check_launch("dp_scatter_pairs_to_nodes");
+}

@@ -470,7 +470,9 @@ namespace dpb {
 constexpr int kLaneDeg = 8;
 
 struct LaneArgs {
-  const float2* xy;
+  const float2* xy;        // interleaved node positions, or nullptr: planar pin positions below
+  const float* px;         // pin x (planar form: ln_node holds pin ids, no offsets)
+  const float* py;
   const int* group_deg;
   const int* group_base;
   const int* group_net;
@@ -486,6 +488,16 @@ struct LaneArgs {
   float2* gnode;
 };
 
+// position of lane slot p: node position + pin offset, or (planar form) the
+// pin's own position
+template <bool kPins>
+__device__ __forceinline__ float2 lane_xy(const LaneArgs& A, int p) {
+  const int node = __ldcs(A.ln_node + p);
+  if (kPins) return make_float2(A.px[node], A.py[node]);
+  const float2 q = A.xy[node];
+  return make_float2(fadd(__ldcs(A.ln_offx + p), q.x), fadd(__ldcs(A.ln_offy + p), q.y));
+}
+
 // where the gradient of lane slot p goes: its pin's node-CSR position, or p
 // itself (lane-slot order, gathered by the assembly through grad_index)
 __device__ __forceinline__ int grad_slot(const LaneArgs& A, int p) { return A.ln_csr ? __ldcs(A.ln_csr + p) : p; }
@@ -496,16 +508,15 @@ __device__ __forceinline__ float wa_a_term(float b, float xe, float e) {
   return (float)((1.0 - (double)fmul(b, xe)) / (double)e);
 }
 
-template <int D, bool kGrad>
+template <int D, bool kGrad, bool kPins>
 __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, int lane, int net, bool hpwl,
                                          double& contrib, double& hcontrib) {
   float x[D], y[D];
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    const int p = base + 32 * j + lane;
-    const float2 q = A.xy[__ldcs(A.ln_node + p)];
-    x[j] = fadd(__ldcs(A.ln_offx + p), q.x);
-    y[j] = fadd(__ldcs(A.ln_offy + p), q.y);
+    const float2 q = lane_xy<kPins>(A, base + 32 * j + lane);
+    x[j] = q.x;
+    y[j] = q.y;
   }
   float x_max = x[0], x_min = x[0], y_max = y[0], y_min = y[0];
 #pragma unroll
@@ -586,13 +597,13 @@ __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, 
 }
 
 // a net of degree > kLaneDeg: pins base .. base + deg (contiguous), whole warp
-template <bool kGrad>
+template <bool kGrad, bool kPins>
 __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lane, int net, bool hpwl,
                          double& contrib, double& hcontrib) {
   float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
   for (int j = lane; j < deg; j += 32) {
-    const float2 q = A.xy[A.ln_node[base + j]];
-    const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+    const float2 q = lane_xy<kPins>(A, base + j);
+    const float xx = q.x, yy = q.y;
     x_max = fmaxf(x_max, xx);
     x_min = fminf(x_min, xx);
     y_max = fmaxf(y_max, yy);
@@ -620,8 +631,8 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
   float xe_p = 0.f, xe_n = 0.f, e_p = 0.f, e_n = 0.f, ye_p = 0.f, ye_n = 0.f, f_p = 0.f, f_n = 0.f;
   if (on) {
     for (int j = lane; j < deg; j += 32) {
-      const float2 q = A.xy[A.ln_node[base + j]];
-      const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+      const float2 q = lane_xy<kPins>(A, base + j);
+      const float xx = q.x, yy = q.y;
       const float a1 = expf(fmul(fsub(xx, x_max), ig)), a2 = expf(fmul(fsub(x_min, xx), ig));
       const float a3 = expf(fmul(fsub(yy, y_max), ig)), a4 = expf(fmul(fsub(y_min, yy), ig));
       xe_p = fadd(xe_p, fmul(xx, a1));
@@ -648,8 +659,8 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
   for (int j = lane; j < deg; j += 32) {
     float gx = 0.f, gy = 0.f;
     if (on) {
-      const float2 q = A.xy[A.ln_node[base + j]];
-      const float xx = fadd(A.ln_offx[base + j], q.x), yy = fadd(A.ln_offy[base + j], q.y);
+      const float2 q = lane_xy<kPins>(A, base + j);
+      const float xx = q.x, yy = q.y;
       const float a1 = expf(fmul(fsub(xx, x_max), ig)), a2 = expf(fmul(fsub(x_min, xx), ig));
       const float a3 = expf(fmul(fsub(yy, y_max), ig)), a4 = expf(fmul(fsub(y_min, yy), ig));
       gx = fsub(fmul(fadd(a_x, fmul(b_x, xx)), a1), fmul(fadd(a_nx, fmul(b_nx, xx)), a2));
@@ -665,7 +676,7 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
 
 // 4 blocks of 256 per SM: the 64-register cap spills a few words of the
 // 5..8-pin paths to L1, and still measures faster than 3 blocks without spills
-template <bool kGrad>
+template <bool kGrad, bool kPins>
 __global__ void __launch_bounds__(256, 4) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
                                                       double* __restrict__ hpwl_partials,
                                                       const int* __restrict__ gate) {
@@ -679,20 +690,20 @@ __global__ void __launch_bounds__(256, 4) wa_lane_kernel(LaneArgs A, double* __r
   for (int g = warp; g < A.num_groups; g += nwarps) {
     const int deg = A.group_deg[g], base = A.group_base[g];
     if (deg > kLaneDeg) {
-      warp_net<kGrad>(A, ig, base, deg, lane, A.group_net[32 * g], hpwl, contrib, hcontrib);
+      warp_net<kGrad, kPins>(A, ig, base, deg, lane, A.group_net[32 * g], hpwl, contrib, hcontrib);
       continue;
     }
     const int net = A.group_net[32 * g + lane];
     if (net < 0) continue;  // padding lane of the last group of a degree
     switch (deg) {
-      case 1: lane_net<1, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 2: lane_net<2, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 3: lane_net<3, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 4: lane_net<4, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 5: lane_net<5, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 6: lane_net<6, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 7: lane_net<7, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
-      case 8: lane_net<8, kGrad>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 1: lane_net<1, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 2: lane_net<2, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 3: lane_net<3, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 4: lane_net<4, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 5: lane_net<5, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 6: lane_net<6, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 7: lane_net<7, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
+      case 8: lane_net<8, kGrad, kPins>(A, ig, base, lane, net, hpwl, contrib, hcontrib); break;
       default: break;
     }
   }
@@ -775,10 +786,13 @@ static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, doub
   int blocks = A.num_groups > 0 ? ceil_div((long long)A.num_groups * 32, 256) : 1;
   if (blocks > kNumSMs * 4) blocks = kNumSMs * 4;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  if (grad)
-    wa_lane_kernel<true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr, trial_gate());
+  if (grad && A.px)
+    wa_lane_kernel<true, true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
+  else if (grad)
+    wa_lane_kernel<true, false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr,
+                                                       trial_gate());
   else
-    wa_lane_kernel<false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
+    wa_lane_kernel<false, false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
   int rc = check_launch(grad ? "dp_wa_lanes_forward" : "dp_hpwl_lanes");
   if (rc) return rc;
   // the WA total and the HPWL (same fixed-order reduction each) in one launch
@@ -792,6 +806,7 @@ static dpb::LaneArgs lane_args(const float* xy, const int* group_deg, const int*
                                const unsigned char* hpwl_mask, const float* inv_gamma, float* grad_node_order) {
   dpb::LaneArgs A;
   A.xy = reinterpret_cast<const float2*>(xy);
+  A.px = A.py = nullptr;
   A.group_deg = group_deg;
   A.group_base = group_base;
   A.group_net = group_net;
@@ -836,4 +851,54 @@ extern "C" int dp_hpwl_lanes(const float* xy, const int* group_deg, const int* g
   const dpb::LaneArgs A = lane_args(xy, group_deg, group_base, group_net, num_groups, ln_node, ln_offx, ln_offy,
                                     nullptr, net_weights, net_mask, nullptr, nullptr, nullptr);
   return launch_lanes(false, A, out_f64, nullptr, dpb::as_stream(stream));
+}
+
+// ---------------------------------------------------------------- WA on pin positions
+// The lane-per-net WA of dp_wa_lanes_forward reading the pins' own positions
+// (planar [x(P) | y(P)], the layout of the reference op's input), for the
+// drop-in WeightedAverageWirelength: the lane slots hold pin ids.
+extern "C" int dp_wa_pins_forward(const float* pin_pos, int num_pins, const int* group_deg, const int* group_base,
+                                  const int* group_net, int num_groups, const int* ln_pin, const float* net_weights,
+                                  const unsigned char* net_mask, const float* inv_gamma, double* wl_f64,
+                                  float* grad_lane, dp_stream_t stream) {
+  DP_REQUIRE(pin_pos && group_deg && group_base && group_net && ln_pin && net_mask && inv_gamma && wl_f64 && grad_lane,
+             "dp_wa_pins_forward: null pointer argument");
+  DP_REQUIRE(num_pins >= 0 && num_groups >= 0, "dp_wa_pins_forward: bad sizes");
+  DP_REQUIRE(((uintptr_t)grad_lane & 7) == 0, "dp_wa_pins_forward: grad_lane must be 8-byte aligned");
+  dpb::LaneArgs A = lane_args(nullptr, group_deg, group_base, group_net, num_groups, ln_pin, nullptr, nullptr, nullptr,
+                              net_weights, net_mask, nullptr, inv_gamma, grad_lane);
+  A.px = pin_pos;
+  A.py = pin_pos + num_pins;
+  return launch_lanes(true, A, wl_f64, nullptr, dpb::as_stream(stream));
+}
+
+namespace dpb {
+// grad_pin_pos[p] = grad_out * grad_lane[lane_of_pin[p]] (x then y), 0 where pin_mask
+__global__ void wa_pins_backward_kernel(const float2* __restrict__ grad_lane, const int* __restrict__ lane_of_pin,
+                                        const unsigned char* __restrict__ pin_mask, const float* __restrict__ grad_out,
+                                        int num_pins, float* __restrict__ gx, float* __restrict__ gy) {
+  const float g = grad_out[0];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < num_pins; p += gridDim.x * blockDim.x) {
+    float x = 0.f, y = 0.f;
+    if (!(pin_mask && pin_mask[p])) {
+      const float2 v = __ldg(grad_lane + __ldg(lane_of_pin + p));
+      x = fmul(v.x, g);
+      y = fmul(v.y, g);
+    }
+    __stcs(gx + p, x);
+    __stcs(gy + p, y);
+  }
+}
+}  // namespace dpb
+
+extern "C" int dp_wa_pins_backward(const float* grad_lane, const int* lane_of_pin, const unsigned char* pin_mask,
+                                   const float* grad_out, int num_pins, float* grad_pin_pos, dp_stream_t stream) {
+  using namespace dpb;
+  DP_REQUIRE(grad_lane && lane_of_pin && grad_out && grad_pin_pos, "dp_wa_pins_backward: null pointer argument");
+  DP_REQUIRE(((uintptr_t)grad_lane & 7) == 0, "dp_wa_pins_backward: grad_lane must be 8-byte aligned");
+  if (num_pins == 0) return DP_OK;
+  wa_pins_backward_kernel<<<grid_for(num_pins, 256, 8), 256, 0, as_stream(stream)>>>(
+      reinterpret_cast<const float2*>(grad_lane), lane_of_pin, pin_mask, grad_out, num_pins, grad_pin_pos,
+      grad_pin_pos + num_pins);
+  return check_launch("dp_wa_pins_backward");
 }

@@ -20,6 +20,14 @@ is summed in the spectral domain by the second launch's epilogue,
   sum_xy rho IDCT2(a winv) = M N sum_uv w_u w_v winv_uv a_uv^2 (w_0 = 1/2),
 so the potential map is never formed.
 Backward: the hand-written adjoint ``-electric_force`` (reference :219-275).
+
+The modules (``ElectricOverflow``, ``ElectricPotential``) keep a spatial
+visiting order of their cells (``CellOrder``) and run the order-driven kernels
+of the GP engine: the window scatter (block-local sort, 3 x 3-bin register
+windows, shared-memory tiles) and the field gather over per-cell records,
+whose force is put back in node order.  ``ElectricDensityMapFunction`` and
+``ElectricPotentialFunction`` keep the reference's per-cell kernels for
+callers of the Functions themselves.
 With ``recompute_field`` the forward runs only the first two launches (the
 energy) and keeps the normalised density map; the backward repeats the solve
 for the field maps, so no field map is held between forward and backward.
@@ -200,6 +208,53 @@ class ElectricDensityMapFunction(Function):
         return density_map
 
 
+class CellOrder(object):
+    """Spatial visiting order of a module's scattered cells (movable, then
+    fillers) for the order-driven scatter and field gather: the cells bucketed
+    by the bin where their stretched footprint starts (dp_order_cells_by_bin)
+    and their records (stretched sizes, offsets, ratio) in that order.  The
+    order is refreshed every ``interval`` calls of ``positions``; any order is
+    valid (fixed-point maps do not depend on it), a fresh one keeps each
+    scatter block's cells on a compact patch of bins.  A refresh allocates new
+    tensors, so a backward still holding the previous order is unaffected."""
+
+    def __init__(self, op, num_filler_nodes, interval=50):
+        self.op = op
+        self.count = op.num_movable_nodes + num_filler_nodes
+        self.num_filler = num_filler_nodes
+        self.interval = int(interval)
+        self.calls = 0
+        self.order = self.rec4 = self.ratio_o = None
+        self._scratch = None
+
+    def _refresh(self, pos):
+        op = self.op
+        dev = pos.device
+        nm, nf = op.num_movable_nodes, self.num_filler
+        if self._scratch is None:
+            nbytes = C.order_cells_scratch_bytes(nm, nf, op.num_bins_x, op.num_bins_y)
+            self._scratch = torch.empty((nbytes + 3) // 4, dtype=torch.int32, device=dev)
+        order = torch.empty(self.count, dtype=torch.int32, device=dev)
+        C.order_cells_by_bin(pos, op.offset_x, op.offset_y, nm, nf, float(op.xl), float(op.yl),
+                             float(op.bin_size_x), float(op.bin_size_y), op.num_bins_x, op.num_bins_y,
+                             self._scratch, order)
+        rec4 = torch.empty(4 * self.count, dtype=torch.float32, device=dev)
+        ratio_o = torch.empty(self.count, dtype=torch.float32, device=dev)
+        C.build_cell_records(op.node_size_x_clamped, op.node_size_y_clamped, op.offset_x, op.offset_y, op.ratio,
+                             order, self.count, rec4, ratio_o, None)
+        self.order, self.rec4, self.ratio_o = order, rec4, ratio_o
+
+    def positions(self, pos):
+        """The cells' positions in visiting order (interleaved), refreshing the
+        order when due; returns (xy_o, order, rec4, ratio_o)."""
+        if self.order is None or (self.interval > 0 and self.calls % self.interval == 0):
+            self._refresh(pos)
+        self.calls += 1
+        xy_o = torch.empty(2 * self.count, dtype=torch.float32, device=pos.device)
+        C.gather_order_pos(pos, self.order, self.count, xy_o)
+        return xy_o, self.order, self.rec4, self.ratio_o
+
+
 class ElectricOverflow(nn.Module):
     """Overflow / max-density evaluation (reference electric_overflow.py:117-278)."""
 
@@ -261,6 +316,51 @@ class ElectricOverflow(nn.Module):
             self.padding_mask[self.padding:self.num_bins_x - self.padding,
                               self.padding:self.num_bins_y - self.padding] = False
         self.initial_density_map = None
+        self._orders = {}
+        self._fixed_scratch = None
+
+    def cell_order(self, num_filler_nodes):
+        """The visiting order of the movable cells and num_filler_nodes fillers."""
+        o = self._orders.get(num_filler_nodes)
+        if o is None:
+            o = self._orders[num_filler_nodes] = CellOrder(self, num_filler_nodes)
+        return o
+
+    def fixed_scratch(self, device):
+        """The int64 accumulation map of the deterministic scatter (one per module)."""
+        if self._fixed_scratch is None:
+            self._fixed_scratch = torch.empty(self.num_bins_x * self.num_bins_y, dtype=torch.int64, device=device)
+        return self._fixed_scratch
+
+    def ordered_density_map(self, pos, num_filler_nodes):
+        """The density map of the movable cells and num_filler_nodes fillers on
+        the initial map, by the order-driven scatter (window kernel, block-local
+        sort, shared-memory tiles): the same map as ElectricDensityMapFunction
+        (bit for bit in deterministic mode), with the padding bins filled.
+        Returns (density_map [M, N], (xy_o, order, rec4, ratio_o))."""
+        require_cuda(pos, "pos")
+        cells = self.cell_order(num_filler_nodes).positions(pos.view(pos.numel()))
+        xy_o, order, rec4, ratio_o = cells
+        M, N = self.num_bins_x, self.num_bins_y
+        det = int(bool(self.deterministic_flag))
+        scratch = self.fixed_scratch(pos.device) if det else None
+        geo = (float(self.xl), float(self.yl), float(self.xh), float(self.yh), float(self.bin_size_x),
+               float(self.bin_size_y), M, N)
+        out = torch.empty(M * N, dtype=torch.float32, device=pos.device)
+        nm = self.num_movable_nodes
+        count = nm + num_filler_nodes
+        if num_filler_nodes > 0 and nm > 0:
+            # movable cells block-sorted, fillers (about one per bin) not
+            first = torch.empty_like(out)
+            C.density_map_ordered_split(xy_o, rec4, ratio_o, nm, count, self.initial_density_map.view(-1), *geo, det,
+                                        scratch, first, out, 1.0, 1.0, None)
+        else:
+            C.density_map_ordered_into(xy_o, rec4, ratio_o, count, self.initial_density_map.view(-1), *geo, det,
+                                       scratch, out)
+        density_map = out.view(M, N)
+        if self.padding > 0:
+            density_map.masked_fill_(self.padding_mask, self.target_density * self.bin_size_x * self.bin_size_y)
+        return density_map, cells
 
     def compute_initial_density_map(self, pos):
         """Fixed-cell map ×target_density (reference electric_overflow.py:229-258)."""
@@ -292,7 +392,7 @@ class ElectricOverflow(nn.Module):
         """(overflow, max_density) accumulated in fp64, as a [2] float64 tensor."""
         if self.initial_density_map is None:
             self.compute_initial_density_map(pos)
-        density_map = self._density_map(pos, self.num_filler_nodes)
+        density_map, _ = self.ordered_density_map(pos, self.num_filler_nodes)
         bin_area = self.bin_size_x * self.bin_size_y
         return C.density_overflow(density_map, float(self.target_density * bin_area), float(bin_area))
 
@@ -359,6 +459,49 @@ class ElectricPotentialFunction(Function):
         return (output,) + (None,) * 39
 
 
+class ElectricPotentialOrderedFunction(Function):
+    """ElectricPotentialFunction over a visiting order: the order-driven
+    scatter in forward and the order-driven field gather in backward
+    (dp_electric_force_ordered), whose force is put back in node order; the
+    same results as ElectricPotentialFunction (bit for bit in deterministic
+    mode)."""
+
+    @staticmethod
+    def forward(ctx, pos, op, precision, fast_mode, recompute_field):
+        density_map, cells = op.ordered_density_map(pos, op.num_filler_nodes)
+        bsx, bsy = op.bin_size_x, op.bin_size_y
+        density_map.mul_(1.0 / (bsx * bsy))
+        ctx.op, ctx.cells, ctx.precision = op, cells, precision
+        ctx.num_nodes = pos.numel() // 2
+        ctx.density_map = density_map
+        if recompute_field:
+            energy = torch.zeros(1, dtype=torch.float64, device=pos.device) if fast_mode else \
+                poisson_energy(density_map, bsx, bsy, precision)
+            ctx.field_map_x = ctx.field_map_y = None
+        else:
+            ex, ey, energy = poisson_solve(density_map, bsx, bsy, precision, fast_mode)
+            ctx.field_map_x, ctx.field_map_y = ex, ey
+        if fast_mode:
+            return torch.zeros(1, dtype=pos.dtype, device=pos.device)
+        return energy.to(pos.dtype).view([])
+
+    @staticmethod
+    def backward(ctx, grad_pos):
+        op = ctx.op
+        xy_o, order, rec4, ratio_o = ctx.cells
+        count = order.numel()
+        fx, fy = ctx.field_map_x, ctx.field_map_y
+        if fx is None:
+            fx, fy, _ = poisson_solve(ctx.density_map, op.bin_size_x, op.bin_size_y, ctx.precision, True)
+        g = grad_pos.reshape(1).to(torch.float32)
+        force_o = torch.empty(2 * count, dtype=torch.float32, device=g.device)
+        C.electric_force_ordered(g, fx.view(-1), fy.view(-1), xy_o, rec4, ratio_o, count, float(op.xl), float(op.yl),
+                                 float(op.bin_size_x), float(op.bin_size_y), op.num_bins_x, op.num_bins_y, -1.0,
+                                 force_o)
+        output = C.scatter_pairs_to_nodes(force_o, order, count, ctx.num_nodes)
+        return output, None, None, None, None
+
+
 class ElectricPotential(ElectricOverflow):
     """Electrostatic density penalty (reference electric_potential.py:278-553)."""
 
@@ -401,17 +544,9 @@ class ElectricPotential(ElectricOverflow):
             self.idct_idxst = IDCT_IDXST(self.exact_expkM, self.exact_expkN, self.precision)
             self.idxst_idct = IDXST_IDCT(self.exact_expkM, self.exact_expkN, self.precision)
         if mode == "density":
-            return ElectricPotentialFunction.apply(
-                pos, self.node_size_x_clamped, self.node_size_y_clamped, self.offset_x, self.offset_y,
-                self.ratio, self.bin_center_x, self.bin_center_y, self.initial_density_map, self.target_density,
-                self.xl, self.yl, self.xh, self.yh, self.bin_size_x, self.bin_size_y, self.num_movable_nodes,
-                self.num_filler_nodes, self.padding, self.padding_mask, self.num_bins_x, self.num_bins_y,
-                self.num_movable_impacted_bins_x, self.num_movable_impacted_bins_y,
-                self.num_filler_impacted_bins_x, self.num_filler_impacted_bins_y, self.deterministic_flag,
-                self.sorted_node_map, self.exact_expkM, self.exact_expkN, None, None, None, self.dct2,
-                self.idct2, self.idct_idxst, self.idxst_idct, self.fast_mode, self.precision,
-                self.recompute_field)
-        density_map = self._density_map(pos, 0)
+            return ElectricPotentialOrderedFunction.apply(pos, self, self.precision, self.fast_mode,
+                                                          self.recompute_field)
+        density_map, _ = self.ordered_density_map(pos, 0)
         bin_area = self.bin_size_x * self.bin_size_y
         out = C.density_overflow(density_map, float(self.target_density * bin_area), float(bin_area))
         return out[0].float(), out[1].float()

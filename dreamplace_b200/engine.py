@@ -159,6 +159,8 @@ class GPEngine(object):
         self.ratio_o = torch.empty(count, dtype=torch.float32, device=dev)
         self.inv_order = torch.zeros(n, dtype=torch.int32, device=dev)
         self.force_o = torch.empty(2 * count, dtype=torch.float32, device=dev)
+        nbytes = C.order_cells_scratch_bytes(nm, nf, ep.num_bins_x, ep.num_bins_y)
+        self.order_scratch = torch.empty((nbytes + 3) // 4, dtype=torch.int32, device=dev)
         self._build_records()
         self.sort_interval = int(getattr(params, "sort_interval", 50))
         # how the scatter and the field gather read the trial point: "gather"
@@ -259,20 +261,12 @@ class GPEngine(object):
         other), then bin inside the tile.  Each scatter block's cells then cover a
         compact patch of bins, and cells with the same start bin are adjacent."""
         d, ep = self.design, self.ep
-        n, nm, nf = d.num_nodes, d.num_movable_nodes, d.num_filler_nodes
+        nm, nf = d.num_movable_nodes, d.num_filler_nodes
         with torch.no_grad():
-            kx = ((v[:n] + ep.offset_x - ep.xl) * (1.0 / ep.bin_size_x)).clamp_(0, ep.num_bins_x - 1).to(torch.int64)
-            hy = ((v[n:] + ep.offset_y - ep.yl) * (1.0 / ep.bin_size_y)).clamp_(0, ep.num_bins_y - 1).to(torch.int64)
-            tiles_y = (ep.num_bins_y + 15) >> 4
-            tx, ty = kx >> 4, hy >> 4
-            ty = ty + (tx & 1) * (tiles_y - 1 - 2 * ty)
-            # 32-bit keys (tile index * 256 + bin in tile) halve the radix passes
-            key = (((tx * tiles_y + ty) << 8) | ((kx & 15) << 4) | (hy & 15)).to(torch.int32)
-            om = torch.sort(key[:nm]).indices.to(torch.int32)
-            self.order[:nm].copy_(om)
-            if nf:
-                of = torch.sort(key[n - nf:]).indices.to(torch.int32).add_(n - nf)
-                self.order[nm:].copy_(of)
+            # counting sort by start bin (dp_order_cells_by_bin)
+            C.order_cells_by_bin(v, ep.offset_x, ep.offset_y, nm, nf, float(ep.xl), float(ep.yl),
+                                 float(ep.bin_size_x), float(ep.bin_size_y), ep.num_bins_x, ep.num_bins_y,
+                                 self.order_scratch, self.order)
             self._build_records()
             if self.xyo_mode != "order":
                 C.gather_order_xy(self.xy(v), self.order, self.order.numel(), self.xyo(v))

@@ -418,6 +418,46 @@ int dp_hpwl_lanes(const float* xy, const int* group_deg, const int* group_base, 
  * (pin mask of fixed cells) */
 int dp_node_pin_sum(const float* grad_node_order, int num_slots, const int* node_start, const float* grad_pos,
                     int num_movable, int num_nodes, int accumulate, float* grad_out, dp_stream_t stream);
+/* WA merged forward on pin positions (weighted_average_wirelength/src/
+ * weighted_average_wirelength_cuda_merged.cpp:63-118 forward): the lane-plan
+ * kernel of dp_wa_lanes_forward reading pin_pos = [x(num_pins) | y(num_pins)]
+ * (the reference op's input layout); ln_pin holds the pin id of each lane
+ * slot (0 for padding).  grad_lane receives the per-pin gradient times the net
+ * weight as (x, y) pairs in lane-slot order; wl_f64 as in dp_wa_lanes_forward. */
+int dp_wa_pins_forward(const float* pin_pos, int num_pins, const int* group_deg, const int* group_base,
+                       const int* group_net, int num_groups, const int* ln_pin, const float* net_weights,
+                       const unsigned char* net_mask, const float* inv_gamma, double* wl_f64, float* grad_lane,
+                       dp_stream_t stream);
+/* WA merged backward (weighted_average_wirelength_cuda_merged.cpp:121-160 and
+ * weighted_average_wirelength.py:197-213): grad_pin_pos[p] =
+ * grad_out[0] * grad_lane[lane_of_pin[p]] (x block, then y block), 0 where
+ * pin_mask[p] (optional, one byte per pin) is set. */
+int dp_wa_pins_backward(const float* grad_lane, const int* lane_of_pin, const unsigned char* pin_mask,
+                        const float* grad_out, int num_pins, float* grad_pin_pos, dp_stream_t stream);
+/* Visiting order of the scattered cells for the order-driven kernels (no
+ * reference counterpart; the reference visits movable cells through
+ * sorted_node_map, BasicPlace.py:186-188): order[0..num_movable) holds the
+ * movable cells and order[num_movable..) the fillers, each bucketed by the bin
+ * where the stretched footprint starts (pos + offset; 16 x 16-bin tiles in
+ * serpentine order, then the bin inside the tile) by a counting sort; inside
+ * a bucket the order is arbitrary.  scratch: dp_order_cells_scratch_bytes
+ * bytes, 4-byte aligned. */
+size_t dp_order_cells_scratch_bytes(int num_movable, int num_filler, int num_bins_x, int num_bins_y);
+int dp_order_cells_by_bin(const float* pos, int num_nodes, const float* offset_x, const float* offset_y,
+                          int num_movable, int num_filler, float xl, float yl, float inv_bin_size_x,
+                          float inv_bin_size_y, int num_bins_x, int num_bins_y, void* scratch, size_t scratch_bytes,
+                          int* order, dp_stream_t stream);
+/* xy_o[2 idx], xy_o[2 idx + 1] = pos[order[idx]], pos[num_nodes + order[idx]]:
+ * planar node positions gathered into visiting order, interleaved */
+int dp_gather_order_pos(const float* pos, int num_nodes, const int* order, int count, float* xy_o,
+                        dp_stream_t stream);
+/* out = 0 (2 num_nodes floats), then out[order[idx]] = vals_o[2 idx] and
+ * out[num_nodes + order[idx]] = vals_o[2 idx + 1]: pairs kept in visiting
+ * order (e.g. the field force of dp_electric_force_ordered) put back in the
+ * reference's node layout [x(n) | y(n)] */
+int dp_scatter_pairs_to_nodes(const float* vals_o, const int* order, int count, int num_nodes, float* out,
+                              dp_stream_t stream);
+
 /* obj = wl + lambda_eff * D (1 + c D), lambda_eff = factor_quad[0] *
  * density_weight, c = factor_quad[1] (0: no quadratic penalty);
  * grad_scale = d obj / d D.  All operands live on the device, so a captured
