@@ -102,13 +102,59 @@ class BatchPlacer(object):
 
 
 def summary(label, designs, results, latencies, seconds):
+    """designs/s, per-design iteration latency p50 / p99, iterations and the
+    mean final overflow of one pass; a rank without designs reports zeros
+    (and no overflow)."""
+    if not designs:
+        return {label + "_designs_per_s": 0.0, label + "_seconds": 0.0, label + "_iteration_ms_p50": 0.0,
+                label + "_iteration_ms_p99": 0.0, label + "_iterations": 0, label + "_mean_final_overflow": None}
     lat = np.array(latencies) * 1000.0 if latencies else np.zeros(1)
     finals = [r[-1][-1][-1] for r in results]
-    return {label + "_designs_per_s": round(len(designs) / seconds, 3), label + "_seconds": round(seconds, 3),
+    return {label + "_designs_per_s": round(len(designs) / seconds, 3) if seconds > 0 else 0.0,
+            label + "_seconds": round(seconds, 3),
             label + "_iteration_ms_p50": round(float(np.percentile(lat, 50)), 3),
             label + "_iteration_ms_p99": round(float(np.percentile(lat, 99)), 3),
             label + "_iterations": int(sum(f.iteration + 1 for f in finals)),
             label + "_mean_final_overflow": round(float(np.mean([f.overflow for f in finals])), 4)}
+
+
+def place_partition(designs_all, rank, world, run_pass, repeat=1):
+    """The designs of this rank (round robin), placed by run_pass(designs) ->
+    (results, latencies) `repeat` times; the last pass is summarised (the
+    first also pays the process's one-time costs and is reported apart).  A
+    rank without designs places nothing and reports zeros."""
+    mine = [designs_all[i] for i in assign(len(designs_all), rank, world)]
+    out = {"designs": len(designs_all), "designs_on_rank": len(mine), "world": world,
+           "cells": int(sum(d.num_movable_nodes for d in mine))}
+    res, lat, seconds = [], [], 0.0
+    if mine:
+        for r in range(max(repeat, 1)):
+            t0 = time.perf_counter()
+            res, lat = run_pass(mine)
+            seconds = time.perf_counter() - t0
+            if r == 0 and repeat > 1:
+                out["batched_first_pass_seconds"] = round(seconds, 3)
+                out["batched_first_pass_designs_per_s"] = round(len(mine) / seconds, 3)
+    out.update(summary("batched", mine, res, lat, seconds))
+    return out
+
+
+def gather_partition(out, rank, world, num_designs):
+    """Every rank's summary to rank 0 (one all_gather_object, the only
+    collective); rank 0 reports designs/s of the whole job, timed by the
+    slowest rank.  Returns the combined summary on rank 0, this rank's
+    otherwise."""
+    if world == 1:
+        return out
+    import torch.distributed as dist
+    gathered = [None] * world
+    dist.all_gather_object(gathered, out)
+    if rank != 0:
+        return out
+    secs = max(g["batched_seconds"] for g in gathered)
+    return {"designs": num_designs, "world": world,
+            "batched_designs_per_s": round(num_designs / secs, 3) if secs > 0 else 0.0,
+            "slowest_rank_seconds": secs, "per_rank": gathered}
 
 
 def main(argv=None):
@@ -120,6 +166,8 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=2,
                     help="batched passes over the same designs; the last one is reported (the first also "
                          "pays the process's one-time set-up, reported as batched_first_pass_*)")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend for the final exchange of results (multi-rank runs)")
     args = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("batch placement needs a CUDA device")
@@ -129,40 +177,29 @@ def main(argv=None):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=600))
     designs_all = batch_set(args.designs, args.seed)
-    mine = [designs_all[i] for i in assign(len(designs_all), rank, world)]
-    out = {"designs": len(designs_all), "designs_on_rank": len(mine), "world": world,
-           "cells": int(sum(d.num_movable_nodes for d in mine))}
-    for r in range(max(args.repeat, 1)):
-        # each pass places the same designs with new placers; the first also
-        # pays the process's one-time costs (kernel loading, the caching
-        # allocator's device allocations), later ones run as a service
+
+    def run_pass(designs):
+        # each pass places the same designs with new placers, as a service
         # placing batch after batch would
-        bp = BatchPlacer(mine)
+        bp = BatchPlacer(designs)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         res, lat = bp.run(args.max_iterations)
-        seconds = time.perf_counter() - t0
-        if r == 0 and args.repeat > 1:
-            out["batched_first_pass_seconds"] = round(seconds, 3)
-            out["batched_first_pass_designs_per_s"] = round(len(mine) / seconds, 3)
         del bp
-    out.update(summary("batched", mine, res, lat, seconds))
-    if args.sequential:
+        return res, lat
+
+    out = place_partition(designs_all, rank, world, run_pass, args.repeat)
+    mine = [designs_all[i] for i in assign(len(designs_all), rank, world)]
+    if args.sequential and mine:
         seq = BatchPlacer(mine)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res, lat = seq.run_sequential(args.max_iterations)
         out.update(summary("sequential", mine, res, lat, time.perf_counter() - t0))
+    out = gather_partition(out, rank, world, len(designs_all))
     if world > 1:
         import torch.distributed as dist
-        gathered = [None] * world
-        dist.all_gather_object(gathered, out)
-        if rank == 0:
-            secs = max(g["batched_seconds"] for g in gathered)
-            out = {"designs": len(designs_all), "world": world, "batched_designs_per_s": round(len(designs_all) / secs, 3),
-                   "per_rank": gathered}
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -665,6 +665,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("transform_gemm", &transform_gemm);
   m.def("prepare_operand", &prepare_operand);
   m.def("tc_status", &tc_status);
+  m.def("tc_set_wait_budget", [](long long cycles) { DP_CALL(dp_tc_set_wait_budget(cycles)); });
+  m.def("tc_set_skip_loads", [](int skip) { DP_CALL(dp_tc_set_skip_loads(skip)); });
   m.def("spectral_weights", &spectral_weights);
   m.def("wa_merged_forward", &wa_merged_forward);
   m.def("wa_merged_backward", &wa_merged_backward);

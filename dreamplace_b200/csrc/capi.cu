@@ -1,5 +1,9 @@
 // C ABI runtime pieces: per-thread error messages, launch accounting, version.
 #include <stdarg.h>
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "reduce.cuh"
 
 namespace dpb {
@@ -22,6 +26,17 @@ void set_error(const char* fmt, ...) {
 }
 
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+static std::mutex g_smem_mu;
+static std::set<std::pair<const void*, int>> g_smem_opted;
+bool smem_opt_in_done(const void* kernel, int device) {
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  return g_smem_opted.count({kernel, device}) != 0;
+}
+void smem_opt_in_mark(const void* kernel, int device) {
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  g_smem_opted.insert({kernel, device});
+}
 
 __global__ void finish_sum_kernel(double* buf, int count, float* out_f32) {
   double r = finish_sum(buf + 1, count);

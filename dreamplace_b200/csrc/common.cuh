@@ -41,6 +41,33 @@ inline int check_launch(const char* what) {
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Raises a kernel's dynamic shared-memory limit once per device: the
+// attribute applies to the device current when it is set, so a process that
+// launches on several GPUs sets it on each.  Thread-safe; returns DP_OK or
+// DP_ERR_CUDA (message set).
+// whether a kernel's shared-memory limit was already raised on a device, and
+// the record that it was (capi.cu; thread-safe)
+bool smem_opt_in_done(const void* kernel, int device);
+void smem_opt_in_mark(const void* kernel, int device);
+template <typename Kernel>
+int opt_in_smem(Kernel kernel, int bytes, const char* who) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("%s: cudaGetDevice: %s", who, cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  const void* key = reinterpret_cast<const void*>(kernel);
+  if (smem_opt_in_done(key, dev)) return DP_OK;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) {
+    set_error("%s: cudaFuncSetAttribute: %s", who, cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  smem_opt_in_mark(key, dev);
+  return DP_OK;
+}
+
 // grid size for a grid-stride elementwise kernel: a multiple of the SM count
 inline int grid_for(long long n, int threads, int per_sm = 8) {
   long long blocks = (n + threads - 1) / threads;

@@ -820,14 +820,9 @@ struct OrderedScatter {
 // (fp32, or the fixed-point scratch maps), in one launch
 template <int kRadixBits>
 int scatter_ranges_r(const OrderedScatter& o, const WsRanges& rg, int deterministic, int fraction_bits) {
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(window_scatter_kernel<false, kRadixBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kWsSmemBytes);
-    cudaFuncSetAttribute(window_scatter_kernel<true, kRadixBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kWsSmemBytes);
-    configured = true;
-  }
+  int rc = deterministic ? opt_in_smem(window_scatter_kernel<true, kRadixBits>, kWsSmemBytes, "density scatter")
+                         : opt_in_smem(window_scatter_kernel<false, kRadixBits>, kWsSmemBytes, "density scatter");
+  if (rc) return rc;
   const int blocks = ceil_div(rg.b1 - rg.b0, kWsCells) + ceil_div(rg.b2 - rg.b1, kWsCells);
   if (blocks <= 0) return DP_OK;
   if (deterministic)

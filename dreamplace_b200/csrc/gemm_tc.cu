@@ -23,10 +23,14 @@
 namespace dpb {
 
 __device__ int g_tc_status = 0;
+// bound of every mbarrier wait, in SM clock cycles (dp_tc_set_wait_budget)
+__device__ long long g_tc_wait_budget = 4000000000ll;  // ~2 s at 2 GHz
+// test hook (dp_tc_set_skip_loads): the producer issues no copy, so the MMA
+// warp's bounded wait on the first stage runs out and the kernel reports it
+__device__ int g_tc_skip_loads = 0;
 
 constexpr int TC_BM = 128;
 constexpr int TC_THREADS = 256;  // 8 warps: producer, MMA issuer, and all 8 in the epilogue
-constexpr long long kWaitBudgetCycles = 4000000000ll;  // ~2 s at 2 GHz
 
 struct TcBatch {
   CUtensorMap a_hi[3];
@@ -64,9 +68,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // bounded wait; returns false (and records `code`) when the budget runs out
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int code) {
   if (mbar_try_wait(bar, parity)) return true;
-  long long start = clock64();
+  const long long start = clock64();
+  const long long budget = g_tc_wait_budget;
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - start > kWaitBudgetCycles) {
+    if (clock64() - start > budget) {
       atomicCAS(&g_tc_status, 0, code);
       return false;
     }
@@ -202,7 +207,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer ----
-    for (int kb = 0; kb < total_kb; ++kb) {
+    const int skip = g_tc_skip_loads;
+    for (int kb = 0; kb < total_kb && !skip; ++kb) {
       int s = kb % STAGES, round = kb / STAGES;
       if (round > 0 && !mbar_wait(&empty_bar[s], (round - 1) & 1, 1)) break;
       const int kx = kb * Cfg::kBK;
@@ -357,15 +363,8 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
     batch.epi[i] = make_epi(q, PREC, M, N);
   }
   auto kern = tc_gemm_kernel<PREC, BN, STAGES>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::kSmemBytes);
-    if (e != cudaSuccess) {
-      set_error("dp_transform_gemm: cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-      return DP_ERR_CUDA;
-    }
-    configured = true;
-  }
+  int rc_smem = opt_in_smem(kern, Cfg::kSmemBytes, "dp_transform_gemm");
+  if (rc_smem) return rc_smem;
   dim3 grid(ceil_div(N, BN), ceil_div(M, TC_BM), count);
   kern<<<grid, TC_THREADS, Cfg::kSmemBytes, s>>>(batch, M, N, K, trial_gate());
   return check_launch("dp_transform_gemm(tcgen05)");
@@ -415,6 +414,26 @@ extern "C" int dp_tc_status(int* status_out) {
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(dpb::g_tc_status, &zero, sizeof(int));
   if (e != cudaSuccess) {
     dpb::set_error("dp_tc_status: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}
+
+extern "C" int dp_tc_set_wait_budget(long long cycles) {
+  DP_REQUIRE(cycles > 0, "dp_tc_set_wait_budget: the budget must be positive");
+  cudaError_t e = cudaMemcpyToSymbol(dpb::g_tc_wait_budget, &cycles, sizeof(long long));
+  if (e != cudaSuccess) {
+    dpb::set_error("dp_tc_set_wait_budget: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}
+
+extern "C" int dp_tc_set_skip_loads(int skip) {
+  const int v = skip ? 1 : 0;
+  cudaError_t e = cudaMemcpyToSymbol(dpb::g_tc_skip_loads, &v, sizeof(int));
+  if (e != cudaSuccess) {
+    dpb::set_error("dp_tc_set_skip_loads: %s", cudaGetErrorString(e));
     return DP_ERR_CUDA;
   }
   return DP_OK;

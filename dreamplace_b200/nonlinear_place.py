@@ -207,6 +207,7 @@ class NonLinearPlace(nn.Module):
         iteration = 0
         flat_llambda = 0
         self.iteration_times = []
+        self.divergence_iteration = None  # the iteration whose divergence check rolled back, if any
 
         def divergence_numpy(xs, threshold):
             x = np.array(xs)
@@ -280,6 +281,7 @@ class NonLinearPlace(nn.Module):
                             stepper.best_position()  # completes a pending copy into best["pos"]
                         stepper.set_position(best["pos"])
                         stop_placement = True
+                        self.divergence_iteration = iteration
                         logger.error("possible DIVERGENCE detected, roll back to the best position recorded")
                     t0 = time.time()
                     if hasattr(stepper, "step_gen"):

@@ -270,6 +270,16 @@ int dp_spectral_weights(int M, int N, float wv_scale, float* out, dp_stream_t st
  * bounded wait completed; non-zero = a wait expired and the launch returned
  * early).  Synchronises the device. */
 int dp_tc_status(int* status_out);
+/* Bound of every mbarrier wait of the tensor-core kernels, in SM clock cycles
+ * (default 4e9, about 2 s); on expiry a kernel records its status word (see
+ * dp_tc_status), lets what it issued drain, frees its TMEM and returns.
+ * Synchronous; applies to kernels launched afterwards. */
+int dp_tc_set_wait_budget(long long cycles);
+/* Test hook for the bounded waits: while set, the tensor-core kernels' TMA
+ * producer issues no copy, so the MMA warp's wait on the first operand stage
+ * runs out (status 2) and the kernel returns with nothing in flight; the
+ * outputs are then undefined.  Synchronous. */
+int dp_tc_set_skip_loads(int skip);
 
 /* Operand preparation: out = scale * x, written in the operand format of
  * `precision` (fp32, bf16 hi, or bf16 hi+lo). */
