@@ -762,6 +762,39 @@ class GPEngine(object):
             self.best_slot = None
         return self.best_buf
 
+    # ---------------------------------------------------------------- checkpoint
+    _STATE_LISTS = ("V", "U", "G", "XY", "XYO", "S", "sched", "weights", "H", "O", "metrics")
+    _STATE_TENSORS = ("order", "rec4", "ratio_o", "inv_order", "factor_quad", "gate")
+
+    def state_dict(self):
+        """The optimizer and iteration state on the host: the three slots'
+        positions, u, g (and their interleaved / visiting-order copies),
+        optimizer scalars, lambda / gamma, schedule words and metric buffers,
+        the visiting order and its records, and the counters.  The device is
+        synchronised first, so an iteration enqueued ahead has finished."""
+        self.flush_best()
+        torch.cuda.synchronize(self.dev)
+        sd = {k: [t.detach().cpu().clone() for t in getattr(self, k)] for k in self._STATE_LISTS}
+        sd.update({k: getattr(self, k).detach().cpu().clone() for k in self._STATE_TENSORS})
+        sd.update(slot=self.slot, iterations=self.iterations, trials=self.trials, quad_c=self._quad_c)
+        return sd
+
+    def load_state_dict(self, sd):
+        """Restores state_dict() into this engine's own buffers (captured trial
+        graphs keep pointing at them); the next step starts iteration
+        sd["iterations"] from slot sd["slot"], enqueued afresh."""
+        with torch.no_grad():
+            for k in self._STATE_LISTS:
+                for dst, src in zip(getattr(self, k), sd[k]):
+                    dst.copy_(src)
+            for k in self._STATE_TENSORS:
+                getattr(self, k).copy_(sd[k])
+        self.slot, self.iterations, self.trials = int(sd["slot"]), int(sd["iterations"]), int(sd["trials"])
+        self._quad_c = float(sd["quad_c"])
+        self.enqueued = None
+        self.graph_key = None
+        self.best_slot = None
+
     def set_position(self, t):
         """Overwrite v_k (divergence rollback), clamped into the die; an
         iteration enqueued ahead from the old v_k is enqueued again."""

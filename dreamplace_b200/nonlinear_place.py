@@ -95,7 +95,7 @@ class _AutogradStepper(object):
 class _EngineStepper(object):
     """The graph-captured iteration of engine.GPEngine."""
 
-    def __init__(self, placer, model, params, design, lr0, use_graphs):
+    def __init__(self, placer, model, params, design, lr0, use_graphs, resume=None):
         self.model, self.params, self.design = model, params, design
         pos = placer.data_collections.pos[0]
         ep = model.ops.density_op
@@ -105,6 +105,11 @@ class _EngineStepper(object):
         if ov.initial_density_map is None:
             ov.compute_initial_density_map(pos.data)
         self.eng = GPEngine(params, design, placer.data_collections, placer.op_collections, model, use_graphs)
+        if resume is not None:
+            # the optimizer is already set up: its state comes from the checkpoint
+            self.lr = resume["lr"]
+            self.eng.load_state_dict(resume["engine"])
+            return
         if params.gp_noise_ratio > 0.0:
             model.ops.noise_op(self.eng.V[0], params.gp_noise_ratio)
         self.lr = self.eng.initial_learning_rate(lr0)
@@ -160,19 +165,29 @@ class NonLinearPlace(nn.Module):
         self.data_collections = PlaceDataCollection(self.pos, params, design, self.device)
         self.op_collections = build_ops(params, design, self.data_collections)
 
-    def __call__(self, params=None, design=None, max_iterations=None, callback=None):
-        gen = self.run_gen(params, design, max_iterations, callback)
+    def __call__(self, params=None, design=None, max_iterations=None, callback=None, checkpoint_every=0,
+                 checkpoint_fn=None, resume=None):
+        gen = self.run_gen(params, design, max_iterations, callback, checkpoint_every, checkpoint_fn, resume)
         try:
             while True:
                 next(gen)
         except StopIteration as stop:
             return stop.value
 
-    def run_gen(self, params=None, design=None, max_iterations=None, callback=None):
+    def run_gen(self, params=None, design=None, max_iterations=None, callback=None, checkpoint_every=0,
+                checkpoint_fn=None, resume=None):
         """The GP loop as a generator: with the graph engine it yields once per
         iteration, after enqueuing the iteration's first trial, so that a batch
         driver can interleave several designs (each on its own stream); the
-        return value is __call__'s."""
+        return value is __call__'s.
+
+        Checkpoint / resume (graph engine, the default schedule): with
+        checkpoint_every = N, checkpoint_fn(state) receives, at the start of
+        every N-th iteration, the loop's and the engine's state (host tensors
+        and plain values, torch.save-able); resume=state continues a run from
+        such a state with the same trajectory.  The state plays the role of the
+        reference's dumped placement plus optimizer state
+        (dreamplace/BasicPlace.py:1174-1248, NonLinearPlace.py:273)."""
         params = params or self.params
         design = design or self.design
         torch.manual_seed(params.random_seed)
@@ -187,10 +202,14 @@ class NonLinearPlace(nn.Module):
         model = PlaceObj(0.0, params, design, self.data_collections, self.op_collections, gp).to(self.device)
         self.model = model
         mode = getattr(params, "gp_engine", "graph")
+        if (checkpoint_every or resume is not None) and mode != "graph":
+            raise ValueError("checkpoint / resume runs on the graph engine (gp_engine='graph')")
+        if resume is not None:
+            self._restore_model(model, resume)
         if mode == "autograd":
             stepper = _AutogradStepper(self, model, params, design, gp["learning_rate"])
         else:
-            stepper = _EngineStepper(self, model, params, design, gp["learning_rate"], mode == "graph")
+            stepper = _EngineStepper(self, model, params, design, gp["learning_rate"], mode == "graph", resume)
         self.stepper = stepper
         # the graph engine applies the density-weight and gamma updates itself,
         # on the device at the start of the next iteration (the same formulas)
@@ -206,8 +225,42 @@ class NonLinearPlace(nn.Module):
         stop_placement = False
         iteration = 0
         flat_llambda = 0
+        start_step = 0
         self.iteration_times = []
         self.divergence_iteration = None  # the iteration whose divergence check rolled back, if any
+        if resume is not None:
+            L = resume["loop"]
+            iteration = start_step = int(L["iteration"])
+            flat_llambda = int(L["flat_llambda"])
+            last_perturb_iter = int(L["last_perturb_iter"])
+            overflow_list = list(L["overflow_list"])
+            divergence_list = [list(x) for x in L["divergence_list"]]
+            all_metrics = [[[EvalMetrics(*row)]] for row in L["metrics"]]
+            bm = L["best_metric"]
+            best = {"metric": EvalMetrics(*bm) if bm is not None else None,
+                    "pos": L["best_pos"].to(self.device) if L["best_pos"] is not None else None}
+            noise_gen.set_state(L["noise_gen"])
+            self.iteration_times = list(L.get("iteration_times", []))
+
+        def checkpoint():
+            flat = [m for g in all_metrics for lam in g for m in lam]
+            eng_state = stepper.eng.state_dict()
+            best_pos = stepper.best_position() if best["metric"] is not None else None
+            return {"loop": {"iteration": iteration, "flat_llambda": flat_llambda,
+                             "last_perturb_iter": last_perturb_iter, "overflow_list": list(overflow_list),
+                             "divergence_list": [list(x) for x in divergence_list],
+                             "metrics": [(m.iteration, m.hpwl, m.overflow, m.max_density, m.objective)
+                                         for m in flat],
+                             "best_metric": None if best["metric"] is None else
+                             (best["metric"].iteration, best["metric"].hpwl, best["metric"].overflow,
+                              best["metric"].max_density, best["metric"].objective),
+                             "best_pos": None if best_pos is None else best_pos.detach().cpu().clone(),
+                             "noise_gen": noise_gen.get_state(), "iteration_times": list(self.iteration_times)},
+                    "model": {"density_factor": model.density_factor, "quad_penalty": model.quad_penalty,
+                              "init_density": None if model.init_density is None else model.init_density.cpu(),
+                              "density_weight": model.density_weight.detach().cpu(),
+                              "gamma": model.gamma.detach().cpu()},
+                    "engine": eng_state, "lr": stepper.lr}
 
         def divergence_numpy(xs, threshold):
             x = np.array(xs)
@@ -268,7 +321,10 @@ class NonLinearPlace(nn.Module):
                     return r < threshold
             return (np.max(x) - np.min(x)) / np.mean(x) < threshold
 
-        for Lgamma_step in range(model.Lgamma_iteration):
+        for Lgamma_step in range(start_step, model.Lgamma_iteration):
+            if checkpoint_every and checkpoint_fn is not None and iteration > start_step and \
+                    iteration % checkpoint_every == 0:
+                checkpoint_fn(checkpoint())
             all_metrics.append([])
             llam = all_metrics[-1]
             for Llambda_step in range(model.Llambda_density_weight_iteration):
@@ -343,6 +399,20 @@ class NonLinearPlace(nn.Module):
         self.metrics = all_metrics
         self.best = best
         return all_metrics
+
+    @staticmethod
+    def _restore_model(model, resume):
+        m = resume["model"]
+        dev = model.density_weight.device
+        model.density_factor = m["density_factor"]
+        model.quad_penalty = m["quad_penalty"]
+        model.density_weight = m["density_weight"].to(dev)
+        model.gamma.data.copy_(m["gamma"].to(dev))
+        if m["init_density"] is not None:
+            model.init_density = m["init_density"].to(dev)
+            model.density_weight_grad_precond = torch.where(model.init_density > 0, 1 / model.init_density,
+                                                            model.init_density)
+            model.quad_penalty_coeff = model.density_quad_coeff / 2 * model.density_weight_grad_precond
 
     @staticmethod
     def _entropy_injection(stepper, design, shrink_factor, noise_intensity, generator=None):
