@@ -665,6 +665,16 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("transform_gemm", &transform_gemm);
   m.def("prepare_operand", &prepare_operand);
   m.def("tc_status", &tc_status);
+  m.def("trial_metrics", [](at::Tensor hpwl, at::Tensor overflow2, at::Tensor state, at::Tensor obj, at::Tensor wl,
+                            at::Tensor energy, at::Tensor out8) {
+    TORCH_CHECK(out8.scalar_type() == at::kDouble && out8.numel() >= 8, "trial_metrics: out8 needs 8 doubles");
+    DP_CALL(dp_trial_metrics(ptr<double>(hpwl), ptr<double>(overflow2), ptr<double>(state), ptr<double>(obj),
+                             ptr<double>(wl), ptr<double>(energy), ptr<double>(out8), cur_stream()));
+  });
+  m.def("zero_", [](at::Tensor t) {
+    CHECK_CUDA_T(t); CHECK_CONTIG(t);
+    DP_CALL(dp_zero(t.data_ptr(), (size_t)t.numel() * t.element_size(), cur_stream()));
+  });
   m.def("tc_set_wait_budget", [](long long cycles) { DP_CALL(dp_tc_set_wait_budget(cycles)); });
   m.def("tc_set_skip_loads", [](int skip) { DP_CALL(dp_tc_set_skip_loads(skip)); });
   m.def("spectral_weights", &spectral_weights);

@@ -80,3 +80,14 @@ extern "C" int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t s
 }
 extern "C" int dp_version(void) { return 1; }
 extern "C" uint64_t dp_launch_count(void) { return dpb::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int dp_zero(void* ptr, size_t bytes, dp_stream_t stream) {
+  DP_REQUIRE(ptr || bytes == 0, "dp_zero: null pointer");
+  if (bytes == 0) return DP_OK;
+  cudaError_t e = cudaMemsetAsync(ptr, 0, bytes, dpb::as_stream(stream));
+  if (e != cudaSuccess) {
+    dpb::set_error("dp_zero: %s", cudaGetErrorString(e));
+    return DP_ERR_CUDA;
+  }
+  return DP_OK;
+}

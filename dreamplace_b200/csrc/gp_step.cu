@@ -256,9 +256,31 @@ __global__ void objective_finish_kernel(const double* wl, const double* energy, 
   if (grad_scale) grad_scale[0] = (float)(lam * dd);
 }
 
+// the metrics a trial's host read-back needs, gathered into one 8-double row:
+// HPWL and (overflow, max density) of v_k, the accept flag and step size of
+// the trial, its objective, wirelength and energy
+__global__ void trial_metrics_kernel(const double* hpwl, const double* overflow2, const double* state,
+                                     const double* obj, const double* wl, const double* energy, double* out) {
+  out[0] = hpwl[0];
+  out[1] = overflow2[0];
+  out[2] = overflow2[1];
+  out[3] = state[NS_ACCEPT];
+  out[4] = state[NS_ALPHA];
+  out[5] = obj[0];
+  out[6] = wl[0];
+  out[7] = energy[0];
+}
+
 }  // namespace dpb
 
 using namespace dpb;
+
+extern "C" int dp_trial_metrics(const double* hpwl, const double* overflow2, const double* state, const double* obj,
+                                const double* wl, const double* energy, double* out8, dp_stream_t stream) {
+  DP_REQUIRE(hpwl && overflow2 && state && obj && wl && energy && out8, "dp_trial_metrics: null pointer");
+  trial_metrics_kernel<<<1, 1, 0, as_stream(stream)>>>(hpwl, overflow2, state, obj, wl, energy, out8);
+  return check_launch("dp_trial_metrics");
+}
 
 extern "C" int dp_objective_finish(const double* wl, const double* energy, const float* density_weight,
                                    const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream) {

@@ -154,7 +154,8 @@ def poisson_solve(rho, bin_size_x, bin_size_y, precision, fast_mode=False, rho_s
     _, chN, shN = transform_matrices(N, prec, dev)
     if ws is not None:
         ws.check(M, N, prec)
-        energy = ws.energy.zero_()
+        energy = ws.energy
+        C.zero_(energy)
     else:
         energy = torch.zeros(1, dtype=torch.float64, device=dev)
     spec = _poisson_spectral(rho, bin_size_x, bin_size_y, prec, None if fast_mode else energy, rho_scale, ws)

@@ -549,8 +549,7 @@ class GPEngine(object):
         self._mark("nesterov_trial", 1)
         energy = self.objective_and_step(v, g, vn, gn, s)
         # HPWL / overflow of v_k (computed when v_k was the trial point), then the trial's scalars
-        torch.cat([self.H[s][0:1], self.O[s][0:2], st[NS_ACCEPT:NS_ACCEPT + 1], st[NS_ALPHA:NS_ALPHA + 1],
-                   self.obj64, self.wl64, energy.reshape(1)], out=self.metrics[s])
+        C.trial_metrics(self.H[s], self.O[s], st, self.obj64, self.wl64, energy, self.metrics[s])
 
     def nesterov_trial_only(self, s):
         """The trial-point kernel alone (used for per-kernel timing)."""

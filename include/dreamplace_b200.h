@@ -468,6 +468,15 @@ int dp_gather_order_pos(const float* pos, int num_nodes, const int* order, int c
 int dp_scatter_pairs_to_nodes(const float* vals_o, const int* order, int count, int num_nodes, float* out,
                               dp_stream_t stream);
 
+/* out8 = {hpwl[0], overflow2[0], overflow2[1], state accept flag, state step
+ * size, obj[0], wl[0], energy[0]}: a GP trial's metrics gathered into the one
+ * row the host reads back (the engine's own bookkeeping, no reference
+ * counterpart). */
+int dp_trial_metrics(const double* hpwl, const double* overflow2, const double* state, const double* obj,
+                     const double* wl, const double* energy, double* out8, dp_stream_t stream);
+/* Zeroes bytes at ptr on the stream (a memset, no kernel). */
+int dp_zero(void* ptr, size_t bytes, dp_stream_t stream);
+
 /* obj = wl + lambda_eff * D (1 + c D), lambda_eff = factor_quad[0] *
  * density_weight, c = factor_quad[1] (0: no quadratic penalty);
  * grad_scale = d obj / d D.  All operands live on the device, so a captured

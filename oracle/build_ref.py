@@ -22,7 +22,8 @@ each linked with utility/src/msg.cpp (the reference's ``utility_cxx``).
 Only ``tests/``, ``__graft_entry__`` and ``bench.py``'s CPU-baseline leg load
 these modules; nothing in ``dreamplace_b200`` does.
 
-Usage:  python oracle/build_ref.py [--ref /root/reference] [--jobs 8]
+Usage:  python oracle/build_ref.py [--ref PATH] [--jobs 8]
+(PATH defaults to $DREAMPLACE_REFERENCE, else /root/reference.)
 """
 import argparse
 import concurrent.futures as cf
@@ -80,8 +81,18 @@ def build_one(name, srcs, ref, cflags, ldflags, cxx):
     return target
 
 
-def build(ref="/root/reference", jobs=8, quiet=False):
-    if not os.path.isdir(os.path.join(ref, "dreamplace", "ops")):
+# where the reference checkout is read from: $DREAMPLACE_REFERENCE, else the
+# checkout this recipe was written against
+DEFAULT_REF = os.environ.get("DREAMPLACE_REFERENCE", "/root/reference")
+
+
+def available(ref=None):
+    return os.path.isdir(os.path.join(ref or DEFAULT_REF, "dreamplace", "ops"))
+
+
+def build(ref=None, jobs=8, quiet=False):
+    ref = ref or DEFAULT_REF
+    if not available(ref):
         raise FileNotFoundError(f"reference checkout not found at {ref}")
     os.makedirs(OUT, exist_ok=True)
     cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
@@ -98,7 +109,7 @@ def build(ref="/root/reference", jobs=8, quiet=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=DEFAULT_REF)
     ap.add_argument("--jobs", type=int, default=8)
     a = ap.parse_args()
     build(a.ref, a.jobs)
