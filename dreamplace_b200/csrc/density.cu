@@ -20,7 +20,6 @@
 #include <mutex>
 #include <cuda.h>
 #include <type_traits>
-#include <cub/block/block_radix_sort.cuh>
 #include "reduce.cuh"
 
 namespace dpb {
@@ -109,137 +108,139 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
   }
 }
 
-// ---------------------------------------------------------------- window scatter
+// ---------------------------------------------------------------- tile scatter
 // Cells are visited in the caller's order (a spatial order refreshed every few
-// iterations, grouping cells whose stretched footprint starts in the same
-// bin), read from per-cell records (stretched width, height, offsets,
-// ratio) and positions stored in the same order (written there by the
-// Nesterov trial kernel), so every read of the scatter is contiguous.
+// iterations: cells sorted by the bin where their stretched footprint starts,
+// see dp_order_cells_by_bin), read from per-cell records (stretched width,
+// height, offsets, ratio) and positions stored in the same order, so every
+// read of the scatter is contiguous.
 //
-// A stretched cell is at least sqrt(2) bins wide, and a standard cell covers
-// at most kWin x kWin bins.  Each lane computes its cell's kWin px and kWin py
-// overlaps once and forms the kWin x kWin window of bin contributions in
-// registers (fp32, or int64 fixed point converted per contribution as the CPU
-// op does).  A lane keeps one running window while its successive cells start
-// at the same bin.  At the end, a run of lanes whose windows start at the same
-// bin is summed with a segmented shuffle reduction (only as many steps as the
-// longest run needs), and the run's first lane adds the window to the block's
-// shared-memory tile over its bin bounding box (or to global memory when the
-// box does not fit).  The tile is flushed with one global atomic per touched
-// bin.  Cells wider than the window take a plain per-bin loop.  In the
-// clustered start of GP, tens of thousands of cells share a bin, so one warp
-// issues kWin*kWin adds for its 128 cells; when cells are spread each cell
-// flushes its own window and adds only its own bins.  The fixed-point map is
-// independent of the summation order, so the deterministic result does not
-// depend on the visiting order or the tiling.
-constexpr int kWin = 3;
-constexpr int kWsThreads = 256;
-constexpr int kWsCellsPerLane = 4;
-constexpr int kWsWarpCells = 32 * kWsCellsPerLane;
-constexpr int kWsCells = kWsThreads * kWsCellsPerLane;
-constexpr int kWsSmemBytes = 24 * 1024;
+// One block takes kTsCells consecutive cells of the order.  It reduces their
+// bin bounding box (redux.sync per warp, then across the warps) and adds the
+// cells into a shared-memory tile over that box; the tile is flushed with one
+// global atomic per non-zero bin.  When the box exceeds the tile (cells that
+// moved far since the order was refreshed), the tile becomes a window of
+// kWinRows x kWinCols bins placed on the block's median cell, and the cells
+// outside it add straight to the global map.  A stretched cell is at least
+// sqrt(2) bins wide, so a standard cell covers 2 or 3 bins per axis: each
+// thread forms a cell's 3 x 3 window (entries beyond the footprint are zero
+// and land on a valid slot) and adds all nine, with no branch; cells wider
+// than 3 bins take a per-bin loop of global atomics.
+//
+// The tile accumulates in int32 words, because shared-memory int32 atomics
+// are single instructions while fp32 and int64 ones are compare-and-swap
+// loops that serialise on contended bins:
+//   * deterministic: the contribution's fixed-point value v = trunc(area * 2^f)
+//     (the CPU op's `long(area * scale)`) is split exactly with float
+//     arithmetic into hi = trunc(v / 2^22) and lo = v - hi * 2^22 (y = area *
+//     2^(f-22) is exact; y - trunc(y) is its exact fraction), summed in two
+//     planes, and recombined into one int64 at the flush.  512 contributions
+//     of |lo| < 2^22 and |hi| < 2^22 stay inside int32, so the map equals the
+//     CPU op's int64 sum bit for bit; a contribution with |hi| >= 2^22 (a bin
+//     far larger than the die's share) adds its int64 value to the global map
+//     directly;
+//   * fp32: one plane of round(area * S), S = 2^s with 512 * bin area * S <
+//     2^31 (a resolution of at most 2^-21 of the bin area), converted back
+//     and added to the fp32 map with one float atomic per bin.
+// The fixed-point map is independent of the summation order, so the
+// deterministic result does not depend on the visiting order or the tiling.
+//
+// Contended bins are what limits the tile's atomics: lanes of one warp that
+// add to the same word are serialised.  The visiting order therefore places
+// the cells of each kTsCells block so that the 32 lanes of a warp hold cells
+// kTsCells / 32 apart in sort order (different bins), while the block as a
+// whole keeps its compact bin box.
+constexpr int kTsThreads = 256;
+constexpr int kTsCellsPerThread = 2;
+constexpr int kTsCells = kTsThreads * kTsCellsPerThread;  // 512: the int32 plane bound above
+constexpr int kTsTab = 128;                                // longest box side with a bin-edge table
+constexpr int kTsSmemBytes = 16 * 1024;
+constexpr float kTsLoSpan = 4194304.0f;                    // 2^22
 
-template <typename Acc>
-__device__ __forceinline__ void add_to(Acc* tile, float* map_f32, unsigned long long* map_fx, bool use_tile, int slot,
-                                       int bin, Acc v) {
-  if (use_tile) {
-    atomicAdd(tile + slot, v);
-  } else if (sizeof(Acc) == 8) {
-    atomicAdd(map_fx + bin, (unsigned long long)v);
-  } else {
-    atomicAdd(map_f32 + bin, (float)v);
-  }
-}
-
-// adds the non-zero entries of a window starting at bin (k0, h0)
-template <typename Acc>
-__device__ __forceinline__ void flush_window(const Acc (&w)[kWin][kWin], int k0, int h0, int bk0, int bh0, int H,
-                                             int nby, bool use_tile, Acc* tile, float* map_f32,
-                                             unsigned long long* map_fx) {
-#pragma unroll
-  for (int kk = 0; kk < kWin; ++kk)
-#pragma unroll
-    for (int hh = 0; hh < kWin; ++hh)
-      if (w[kk][hh] != (Acc)0) {
-        const int k = k0 + kk, h = h0 + hh;
-        add_to<Acc>(tile, map_f32, map_fx, use_tile, (k - bk0) * H + (h - bh0), k * nby + h, w[kk][hh]);
-      }
-}
-
-// Cells [b0, b1) of the visiting order (blocked-sorted when sort0, added to
-// map0) and [b1, b2) (sorted when sort1, added to map1) in one launch: the
-// first ceil((b1 - b0) / kWsCells) blocks take the first range, so the
-// second range's blocks fill the first's last wave.
+// Cells [b0, b1) of the visiting order, added to map0, and [b1, b2), added to
+// map1, in one launch: the first ceil((b1 - b0) / kTsCells) blocks take the
+// first range, so the second range's blocks fill the first's last wave.
 struct WsRanges {
   int b0, b1, b2;
-  int sort0, sort1;
   float* map0_f32;
   float* map1_f32;
   unsigned long long* map0_fx;
   unsigned long long* map1_fx;
 };
 
-template <bool kFixed, int kRadixBits>
-__global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_kernel(TriangleArgs a, WsRanges rg,
-                                                                        const float2* __restrict__ xy_o,
-                                                                        const int* __restrict__ order,
-                                                                        const float4* __restrict__ rec4,
-                                                                        const float* __restrict__ ratio_o,
-                                                                        float fx_scale,
-                                                                        const int* __restrict__ gate) {
+template <bool kFixed>
+__global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a, WsRanges rg,
+                                                                  const float2* __restrict__ xy_o,
+                                                                  const int* __restrict__ order,
+                                                                  const float4* __restrict__ rec4,
+                                                                  const float* __restrict__ ratio_o,
+                                                                  float fx_scale, float plane_scale,
+                                                                  float plane_unit, const int* __restrict__ gate) {
   if (gate_closed(gate)) return;
-  const int nb0 = (rg.b1 - rg.b0 + kWsCells - 1) / kWsCells;
+  constexpr int kPlanes = kFixed ? 2 : 1;
+  constexpr int kCap = kTsSmemBytes / (4 * kPlanes);  // tile bins
+  constexpr int kWinRows = 32;
+  constexpr int kWinCols0 = kCap / kWinRows < kTsTab ? kCap / kWinRows : kTsTab;
+  constexpr int kWinCols = (kWinCols0 & 1) ? kWinCols0 : kWinCols0 - 1;  // odd, so kWinRows * kWinCols <= kCap
+  const int nb0 = (rg.b1 - rg.b0 + kTsCells - 1) / kTsCells;
   const bool second = (int)blockIdx.x >= nb0;
   const int begin = second ? rg.b1 : rg.b0;
-  const int count = second ? rg.b2 : rg.b1;  // end of this block's range
-  const int sort_cells = second ? rg.sort1 : rg.sort0;
+  const int end = second ? rg.b2 : rg.b1;
   float* const map_f32 = second ? rg.map1_f32 : rg.map0_f32;
   unsigned long long* const map_fx = second ? rg.map1_fx : rg.map0_fx;
   const int bid = second ? (int)blockIdx.x - nb0 : (int)blockIdx.x;
   extern __shared__ __align__(16) unsigned char tile_raw[];
-  using Acc = typename std::conditional<kFixed, unsigned long long, float>::type;
-  Acc* tile = reinterpret_cast<Acc*>(tile_raw);
-  constexpr int kCap = kWsSmemBytes / sizeof(Acc);
-  __shared__ int red[4][kWsThreads / 32];
+  int* const plane0 = reinterpret_cast<int*>(tile_raw);
+  __shared__ int red[4][kTsThreads / 32];
+  __shared__ int anchor[2];
+  __shared__ float2 tabx[kTsTab], taby[kTsTab];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // each warp takes kWsWarpCells consecutive cells, each lane kWsCellsPerLane
-  // consecutive ones, so cells of one window start bin (sorted together) meet
-  // in one lane's running window and then in neighbouring lanes
-  const int wbase = begin + bid * kWsCells + warp * kWsWarpCells;
-  float nx[kWsCellsPerLane], ny[kWsCellsPerLane], sxs[kWsCellsPerLane], sys[kWsCellsPerLane], rr[kWsCellsPerLane];
+
+  // a thread's cells are adjacent in the order (one 16-byte position load)
+  float nx[kTsCellsPerThread], ny[kTsCellsPerThread], sx[kTsCellsPerThread], sy[kTsCellsPerThread],
+      rr[kTsCellsPerThread];
+  int k0[kTsCellsPerThread], h0[kTsCellsPerThread], nk[kTsCellsPerThread], nh[kTsCellsPerThread];
   int bk0 = INT_MAX, bk1 = INT_MIN, bh0 = INT_MAX, bh1 = INT_MIN;
-  unsigned live = 0;
 #pragma unroll
-  for (int c = 0; c < kWsCellsPerLane; ++c) {
-    const int idx = wbase + lane * kWsCellsPerLane + c;
-    nx[c] = ny[c] = sxs[c] = sys[c] = rr[c] = 0.f;
-    if (idx < count) {
+  for (int c = 0; c < kTsCellsPerThread; ++c) {
+    const int li = threadIdx.x * kTsCellsPerThread + c;
+    const int idx = begin + bid * kTsCells + li;
+    nk[c] = nh[c] = k0[c] = h0[c] = 0;
+    nx[c] = ny[c] = sx[c] = sy[c] = rr[c] = 0.f;
+    if (idx < end) {
       const float4 r4 = __ldg(rec4 + idx);
       // positions in visiting order, or in node order read through the order
       const float2 p = order ? __ldg(xy_o + __ldg(order + idx)) : __ldg(xy_o + idx);
-      sxs[c] = r4.x;
-      sys[c] = r4.y;
+      sx[c] = r4.x;
+      sy[c] = r4.y;
       nx[c] = fadd(p.x, r4.z);
       ny[c] = fadd(p.y, r4.w);
       rr[c] = __ldg(ratio_o + idx);
-      int k0, k1, h0, h1;
-      triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
-      triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
-      if (k1 > k0 && h1 > h0) {
-        live |= 1u << c;
-        bk0 = min(bk0, k0);
-        bk1 = max(bk1, k1);
-        bh0 = min(bh0, h0);
-        bh1 = max(bh1, h1);
+      int ka, kb, ha, hb;
+      triangle_bin_range(nx[c], sx[c], a.xl, a.inv_bsx, a.num_bins_x, ka, kb);
+      triangle_bin_range(ny[c], sy[c], a.yl, a.inv_bsy, a.num_bins_y, ha, hb);
+      if (kb > ka && hb > ha) {
+        k0[c] = ka;
+        h0[c] = ha;
+        nk[c] = kb - ka;
+        nh[c] = hb - ha;
+        bk0 = min(bk0, ka);
+        bk1 = max(bk1, kb);
+        bh0 = min(bh0, ha);
+        bh1 = max(bh1, hb);
       }
     }
+    // the window anchor: slot 32 holds the block's median cell in the
+    // block-spread order (any cell otherwise)
+    if (li == 32) {
+      anchor[0] = nk[c] ? k0[c] : INT_MIN;
+      anchor[1] = h0[c];
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    bk0 = min(bk0, __shfl_xor_sync(0xffffffffu, bk0, o));
-    bk1 = max(bk1, __shfl_xor_sync(0xffffffffu, bk1, o));
-    bh0 = min(bh0, __shfl_xor_sync(0xffffffffu, bh0, o));
-    bh1 = max(bh1, __shfl_xor_sync(0xffffffffu, bh1, o));
-  }
+  bk0 = __reduce_min_sync(0xffffffffu, bk0);
+  bk1 = __reduce_max_sync(0xffffffffu, bk1);
+  bh0 = __reduce_min_sync(0xffffffffu, bh0);
+  bh1 = __reduce_max_sync(0xffffffffu, bh1);
   if (lane == 0) {
     red[0][warp] = bk0;
     red[1][warp] = bk1;
@@ -247,167 +248,123 @@ __global__ void __launch_bounds__(kWsThreads, kFixed ? 2 : 4) window_scatter_ker
     red[3][warp] = bh1;
   }
   __syncthreads();
-  bk0 = INT_MAX; bk1 = INT_MIN; bh0 = INT_MAX; bh1 = INT_MIN;
-#pragma unroll
-  for (int i = 0; i < kWsThreads / 32; ++i) {
-    bk0 = min(bk0, red[0][i]);
-    bk1 = max(bk1, red[1][i]);
-    bh0 = min(bh0, red[2][i]);
-    bh1 = max(bh1, red[3][i]);
+  {
+    const bool w = lane < kTsThreads / 32;
+    bk0 = __reduce_min_sync(0xffffffffu, w ? red[0][lane] : INT_MAX);
+    bk1 = __reduce_max_sync(0xffffffffu, w ? red[1][lane] : INT_MIN);
+    bh0 = __reduce_min_sync(0xffffffffu, w ? red[2][lane] : INT_MAX);
+    bh1 = __reduce_max_sync(0xffffffffu, w ? red[3][lane] : INT_MIN);
   }
   if (bk1 <= bk0) return;  // nothing to scatter (uniform across the block)
-  const int H = bh1 - bh0;
-  const long long box = (long long)(bk1 - bk0) * H;
-  if (sort_cells && box < (1 << 16)) {
-    // Block-local order: the visiting order is refreshed only every few
-    // iterations, while cells keep moving; sorting the block's cells by the
-    // bin where their window starts (relative to the block's bounding box)
-    // restores the runs that the lane windows and the warp reduction rely on.
-    using BlockSort = cub::BlockRadixSort<unsigned, kWsThreads, kWsCellsPerLane, int, kRadixBits>;
-    __shared__ typename BlockSort::TempStorage sort_tmp;
-    __shared__ float s_cell[5][kWsCells];
-    unsigned keys[kWsCellsPerLane];
-    int vals[kWsCellsPerLane];
-#pragma unroll
-    for (int c = 0; c < kWsCellsPerLane; ++c) {
-      const int li = warp * kWsWarpCells + lane * kWsCellsPerLane + c;
-      keys[c] = (unsigned)box;  // empty cells sort last
-      if (live & (1u << c)) {
-        int k0, k1, h0, h1;
-        triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
-        triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
-        keys[c] = (unsigned)((k0 - bk0) * H + (h0 - bh0));
-      }
-      vals[c] = li;
-      s_cell[0][li] = nx[c];
-      s_cell[1][li] = ny[c];
-      s_cell[2][li] = sxs[c];
-      s_cell[3][li] = sys[c];
-      s_cell[4][li] = rr[c];
+  if ((long long)(bk1 - bk0) * ((bh1 - bh0) | 1) > kCap || bk1 - bk0 > kTsTab || bh1 - bh0 > kTsTab) {
+    int km = anchor[0], hm = anchor[1];
+    if (km == INT_MIN) {
+      km = bk0;
+      hm = bh0;
     }
-    BlockSort(sort_tmp).Sort(keys, vals, 0, 32 - __clz((unsigned)box));
-    __syncthreads();
-    live = 0;
-#pragma unroll
-    for (int c = 0; c < kWsCellsPerLane; ++c) {
-      const int li = vals[c];
-      nx[c] = s_cell[0][li];
-      ny[c] = s_cell[1][li];
-      sxs[c] = s_cell[2][li];
-      sys[c] = s_cell[3][li];
-      rr[c] = s_cell[4][li];
-      if (keys[c] < (unsigned)box) live |= 1u << c;
+    const int wk0 = max(bk0, min(km - kWinRows / 2, bk1 - kWinRows));
+    const int wh0 = max(bh0, min(hm - kWinCols / 2, bh1 - kWinCols));
+    bk1 = min(bk1, wk0 + kWinRows);
+    bh1 = min(bh1, wh0 + kWinCols);
+    bk0 = wk0;
+    bh0 = wh0;
+  }
+  const int K = bk1 - bk0, H = bh1 - bh0;
+  const int P = H | 1;  // odd row pitch: the bins of a tile column fall in different banks
+  const int box = K * P;
+  for (int t = threadIdx.x; t < kPlanes * box; t += kTsThreads) plane0[t] = 0;
+  // bin edges of the box, in the reference's arithmetic (bin_xl = xl + k * bs)
+  for (int t = threadIdx.x; t < K + H; t += kTsThreads) {
+    if (t < K) {
+      const float lo = fadd(a.xl, fmul((float)(bk0 + t), a.bsx));
+      tabx[t] = make_float2(lo, fadd(lo, a.bsx));
+    } else {
+      const float lo = fadd(a.yl, fmul((float)(bh0 + t - K), a.bsy));
+      taby[t - K] = make_float2(lo, fadd(lo, a.bsy));
     }
   }
-  const bool use_tile = box <= kCap;
-  if (use_tile) {
-    for (int t = threadIdx.x; t < (int)box; t += kWsThreads) tile[t] = (Acc)0;
-    __syncthreads();
-  }
+  __syncthreads();
+  int* const plane1 = plane0 + box;
   const int nby = a.num_bins_y;
-  unsigned wide = 0;
-  // Running window of this lane: consecutive cells of the lane whose windows
-  // start at the same bin accumulate in registers; a new start bin flushes the
-  // previous window with direct adds.
-  Acc acc[kWin][kWin];
 #pragma unroll
-  for (int kk = 0; kk < kWin; ++kk)
+  for (int c = 0; c < kTsCellsPerThread; ++c) {
+    if (nk[c] == 0) continue;
+    const int rk = k0[c] - bk0, rh = h0[c] - bh0;
+    if (rk >= 0 && rh >= 0 && rk + nk[c] <= K && rh + nh[c] <= H && nk[c] <= 3 && nh[c] <= 3) {
+      const float xh = fadd(nx[c], sx[c]), yh = fadd(ny[c], sy[c]);
+      float pxr[3], py[3];
+      int row[3], col[3];
 #pragma unroll
-    for (int hh = 0; hh < kWin; ++hh) acc[kk][hh] = (Acc)0;
-  int run_key = -1 - lane;  // no window yet: a key no other lane holds
-  int run_k0 = 0, run_h0 = 0;
+      for (int j = 0; j < 3; ++j) {
+        const bool okx = j < nk[c], oky = j < nh[c];
+        const float2 ex = tabx[okx ? rk + j : rk];
+        const float2 ey = taby[oky ? rh + j : rh];
+        // triangle_overlap: min(x + size, bin_xh) - max(x, bin_xl)
+        pxr[j] = okx ? fmul(fsub(fminf(xh, ex.y), fmaxf(nx[c], ex.x)), rr[c]) : 0.f;
+        py[j] = oky ? fsub(fminf(yh, ey.y), fmaxf(ny[c], ey.x)) : 0.f;
+        row[j] = (okx ? rk + j : rk) * P + rh;
+        col[j] = oky ? j : 0;
+      }
 #pragma unroll
-  for (int c = 0; c < kWsCellsPerLane; ++c) {
-    if (!(live & (1u << c))) continue;
-    int k0, k1, h0, h1;
-    triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
-    triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
-    const int nk = k1 - k0, nh = h1 - h0;
-    if (nk > kWin || nh > kWin) {
-      wide |= 1u << c;
-      continue;
-    }
-    const int key = k0 * nby + h0;
-    if (key != run_key) {
-      if (run_key >= 0) flush_window<Acc>(acc, run_k0, run_h0, bk0, bh0, H, nby, use_tile, tile, map_f32, map_fx);
+      for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int kk = 0; kk < kWin; ++kk)
-#pragma unroll
-        for (int hh = 0; hh < kWin; ++hh) acc[kk][hh] = (Acc)0;
-      run_key = key;
-      run_k0 = k0;
-      run_h0 = h0;
-    }
-    float py[kWin];
-#pragma unroll
-    for (int hh = 0; hh < kWin; ++hh) py[hh] = hh < nh ? triangle_overlap(ny[c], sys[c], a.yl, h0 + hh, a.bsy) : 0.f;
-#pragma unroll
-    for (int kk = 0; kk < kWin; ++kk) {
-      if (kk < nk) {
-        const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k0 + kk, a.bsx), rr[c]);
-#pragma unroll
-        for (int hh = 0; hh < kWin; ++hh) {
-          if (hh < nh) {
-            const float area = fmul(pxr, py[hh]);
-            acc[kk][hh] += kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area;
+        for (int j = 0; j < 3; ++j) {
+          const float area = fmul(pxr[i], py[j]);
+          const int slot = row[i] + col[j];
+          const float y = fmul(area, plane_scale);
+          if (kFixed) {
+            const float hf = truncf(y);
+            if (fabsf(hf) < kTsLoSpan) {
+              atomicAdd(plane0 + slot, (int)hf);
+              atomicAdd(plane1 + slot, (int)fmul(fsub(y, hf), kTsLoSpan));
+            } else {
+              atomicAdd(map_fx + (bk0 + rk + i) * nby + bh0 + rh + j, (unsigned long long)to_fixed(area, fx_scale));
+            }
+          } else {
+            if (fabsf(y) < kTsLoSpan - 1.0f) {  // |round(y)| < 2^22
+              atomicAdd(plane0 + slot, __float2int_rn(y));
+            } else {
+              atomicAdd(map_f32 + (bk0 + rk + i) * nby + bh0 + rh + j, area);
+            }
           }
         }
-      }
-    }
-  }
-  // runs of lanes whose windows start at the same bin are summed into the
-  // run's first lane; lanes without a window hold unique keys
-  {
-    const int prev = __shfl_up_sync(0xffffffffu, run_key, 1);
-    const bool head = lane == 0 || prev != run_key;
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const unsigned later = lane == 31 ? 0u : heads & (0xfffffffeu << lane);
-    const int seg_end = later ? __ffs(later) - 2 : 31;
-    const int run = head ? seg_end - lane + 1 : 0;
-    const int longest = (int)__reduce_max_sync(0xffffffffu, (unsigned)run);
-    for (int o = 1; o < longest; o <<= 1) {
-      const bool take = lane + o <= seg_end;
-#pragma unroll
-      for (int kk = 0; kk < kWin; ++kk)
-#pragma unroll
-        for (int hh = 0; hh < kWin; ++hh) {
-          const Acc t = __shfl_down_sync(0xffffffffu, acc[kk][hh], o);
-          if (take) acc[kk][hh] += t;
-        }
-    }
-    if (head && run_key >= 0) flush_window<Acc>(acc, run_k0, run_h0, bk0, bh0, H, nby, use_tile, tile, map_f32, map_fx);
-  }
-  // cells wider than the window: one add per bin
-#pragma unroll
-  for (int c = 0; c < kWsCellsPerLane; ++c) {
-    if (!(wide & (1u << c))) continue;
-    int k0, k1, h0, h1;
-    triangle_bin_range(nx[c], sxs[c], a.xl, a.inv_bsx, a.num_bins_x, k0, k1);
-    triangle_bin_range(ny[c], sys[c], a.yl, a.inv_bsy, a.num_bins_y, h0, h1);
-    for (int k = k0; k < k1; ++k) {
-      const float pxr = fmul(triangle_overlap(nx[c], sxs[c], a.xl, k, a.bsx), rr[c]);
-      for (int h = h0; h < h1; ++h) {
-        const float area = fmul(pxr, triangle_overlap(ny[c], sys[c], a.yl, h, a.bsy));
-        add_to<Acc>(tile, map_f32, map_fx, use_tile, (k - bk0) * H + (h - bh0), k * nby + h,
-                    kFixed ? (Acc)to_fixed(area, fx_scale) : (Acc)area);
-      }
-    }
-  }
-  if (use_tile) {
-    __syncthreads();
-    // one warp per box row, lanes along the row (no index division)
-    for (int k = warp; k < bk1 - bk0; k += kWsThreads / 32) {
-      const Acc* row = tile + k * H;
-      const int gbase = (bk0 + k) * nby + bh0;
-      for (int h = lane; h < H; h += 32) {
-        const Acc v = row[h];
-        if (v != (Acc)0) {
+    } else {
+      // outside the tile, or wider than 3 bins: one global add per bin
+      for (int k = k0[c]; k < k0[c] + nk[c]; ++k) {
+        const float pxr = fmul(triangle_overlap(nx[c], sx[c], a.xl, k, a.bsx), rr[c]);
+        for (int h = h0[c]; h < h0[c] + nh[c]; ++h) {
+          const float area = fmul(pxr, triangle_overlap(ny[c], sy[c], a.yl, h, a.bsy));
           if (kFixed)
-            atomicAdd(map_fx + gbase + h, (unsigned long long)v);
+            atomicAdd(map_fx + k * nby + h, (unsigned long long)to_fixed(area, fx_scale));
           else
-            atomicAdd(map_f32 + gbase + h, (float)v);
+            atomicAdd(map_f32 + k * nby + h, area);
         }
       }
+    }
+  }
+  __syncthreads();
+  // flush: tile slot t is row t / P, column t % P (stepped without division
+  // after the first; the pad column holds zeros)
+  const float inv_p = __frcp_rn((float)P);
+  int k = (int)((float)threadIdx.x * inv_p), h = (int)threadIdx.x - k * P;
+  if (h < 0) { --k; h += P; } else if (h >= P) { ++k; h -= P; }
+  int dk = (int)((float)kTsThreads * inv_p), dh = kTsThreads - dk * P;
+  if (dh < 0) { --dk; dh += P; } else if (dh >= P) { ++dk; dh -= P; }
+  for (int t = threadIdx.x; t < box; t += kTsThreads) {
+    const int g = (bk0 + k) * nby + bh0 + h;
+    if (kFixed) {
+      const int hi = plane0[t], lo = plane1[t];
+      if ((hi | lo) != 0)
+        atomicAdd(map_fx + g, (unsigned long long)(((long long)hi << 22) + (long long)lo));
+    } else {
+      const int v = plane0[t];
+      if (v != 0) atomicAdd(map_f32 + g, (float)v * plane_unit);
+    }
+    k += dk;
+    h += dh;
+    if (h >= P) {
+      h -= P;
+      ++k;
     }
   }
 }
@@ -803,7 +760,7 @@ extern "C" int dp_build_cell_records(const float* sx, const float* sy, const flo
   return check_launch("dp_build_cell_records");
 }
 
-// Order-driven scatter (see window_scatter_kernel): the cells order[0..count)
+// Order-driven scatter (see tile_scatter_kernel): the cells order[0..count)
 // with their records, positions interleaved in xy.
 namespace {
 
@@ -818,34 +775,40 @@ struct OrderedScatter {
 
 // adds the cells of rg's two ranges of the visiting order onto their maps
 // (fp32, or the fixed-point scratch maps), in one launch
-template <int kRadixBits>
-int scatter_ranges_r(const OrderedScatter& o, const WsRanges& rg, int deterministic, int fraction_bits) {
-  int rc = deterministic ? opt_in_smem(window_scatter_kernel<true, kRadixBits>, kWsSmemBytes, "density scatter")
-                         : opt_in_smem(window_scatter_kernel<false, kRadixBits>, kWsSmemBytes, "density scatter");
+int scatter_ranges(const OrderedScatter& o, const WsRanges& rg, int deterministic, int fraction_bits) {
+  int rc = deterministic ? opt_in_smem(tile_scatter_kernel<true>, kTsSmemBytes, "density scatter")
+                         : opt_in_smem(tile_scatter_kernel<false>, kTsSmemBytes, "density scatter");
   if (rc) return rc;
-  const int blocks = ceil_div(rg.b1 - rg.b0, kWsCells) + ceil_div(rg.b2 - rg.b1, kWsCells);
+  const int blocks = ceil_div(rg.b1 - rg.b0, kTsCells) + ceil_div(rg.b2 - rg.b1, kTsCells);
   if (blocks <= 0) return DP_OK;
-  if (deterministic)
-    window_scatter_kernel<true, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, ldexpf(1.0f, fraction_bits), trial_gate());
-  else
-    window_scatter_kernel<false, kRadixBits><<<blocks, kWsThreads, kWsSmemBytes, o.s>>>(
-        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, 0.f, trial_gate());
+  if (deterministic) {
+    // plane scale 2^(f - 22): hi = trunc(v / 2^22) of v = trunc(area * 2^f)
+    const float fx_scale = ldexpf(1.0f, fraction_bits);
+    tile_scatter_kernel<true><<<blocks, kTsThreads, kTsSmemBytes, o.s>>>(
+        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, fx_scale, ldexpf(1.0f, fraction_bits - 22), 0.f,
+        trial_gate());
+  } else {
+    // S = 2^s with (bin area) * S < 2^22 - 1: a block's 512 contributions of
+    // at most one bin area each sum below 2^31
+    const double bin_area = (double)o.a.bsx * (double)o.a.bsy;
+    const int s = (int)floor(log2((4194302.0 / 1.0001) / bin_area));
+    tile_scatter_kernel<false><<<blocks, kTsThreads, kTsSmemBytes, o.s>>>(
+        o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, 0.f, ldexpf(1.0f, s), ldexpf(1.0f, -s), trial_gate());
+  }
   return check_launch("dp_density_map_ordered scatter");
 }
 
 // adds cells [begin, end) of the visiting order onto out (fp32) or scratch (fixed)
 int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic, int fraction_bits, int64_t* scratch,
-                  float* out, int sort_cells = 1) {
+                  float* out) {
   if (end <= begin) return DP_OK;
   WsRanges rg;
   memset(&rg, 0, sizeof(rg));
   rg.b0 = begin;
   rg.b1 = rg.b2 = end;
-  rg.sort0 = sort_cells;
   rg.map0_f32 = out;
   rg.map0_fx = reinterpret_cast<unsigned long long*>(scratch);
-  return scatter_ranges_r<4>(o, rg, deterministic, fraction_bits);
+  return scatter_ranges(o, rg, deterministic, fraction_bits);
 }
 
 int convert_fixed(const int64_t* scratch, const float* init, int fraction_bits, float* out, int nbins,
@@ -888,7 +851,7 @@ int ordered_setup(const char* who, const float* xy_o, const int* order, const fl
 
 }  // namespace
 
-// Order-driven scatter (see window_scatter_kernel): cells 0..count of the
+// Order-driven scatter (see tile_scatter_kernel): cells 0..count of the
 // visiting order, positions (xy_o) and attributes (rec4, ratio_o) in that order.
 extern "C" int dp_density_map_ordered(const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
                                       int count,
@@ -955,7 +918,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
       rc = convert_fixed(scratch, init, fraction_bits, out_first, nbins, o.s);
     }
     if (rc) return rc;
-    rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr, 0);
+    rc = scatter_range(o, num_first, count, 1, fraction_bits, scratch, nullptr);
     if (rc) return rc;
     return convert_fixed(scratch, init, fraction_bits, out_all, nbins, o.s);
   }
@@ -974,11 +937,9 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
   rg.b0 = 0;
   rg.b1 = num_first;
   rg.b2 = count;
-  rg.sort0 = 1;  // the movable cells: block-local sort (their order goes stale)
-  rg.sort1 = 0;  // the fillers: about one per bin, runs stay short
   rg.map0_f32 = out_first;
   rg.map1_f32 = out_all;
-  rc = scatter_ranges_r<4>(o, rg, 0, 0);
+  rc = scatter_ranges(o, rg, 0, 0);
   if (rc) return rc;
   if (overflow_out) cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
   first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, 1, nbins, target_area,
@@ -1098,7 +1059,8 @@ extern "C" int dp_density_map_fx64_noalloc(const float* pos, int num_nodes, cons
 // computes each cell's bucket and counts the buckets, an exclusive scan turns
 // counts into starts, a second pass places the cells (the order inside a
 // bucket is whatever the atomics give: every visiting order is valid for the
-// scatter and the field gather).
+// scatter and the field gather).  The sorted ranks are then placed block by
+// block for the tile scatter (block_spread_slot).
 namespace dpb {
 
 constexpr int kScanThreads = 1024;
@@ -1187,12 +1149,32 @@ __global__ void add_block_offsets_kernel(unsigned* data, int n, const unsigned* 
   if (i < n) data[i] += block_offsets[blockIdx.x];
 }
 
+// Position of sorted rank `slot` of the range [b, e) (the movable cells or
+// the fillers): inside each full block of kTsCells cells (the tile scatter's
+// block), rank r goes to the slot read by lane r / (kTsCells / 32) of warp
+// (r % (kTsCells / 32)) / kTsCellsPerThread, so the 32 lanes of a warp hold
+// cells kTsCells / 32 apart in sort order while the block keeps its cells.
+// A partial last block keeps the sorted order.
+__device__ __forceinline__ int block_spread_slot(int slot, int b, int e) {
+  constexpr int kStride = kTsCells / 32;
+  const int q = slot - b;
+  const int j = q / kTsCells;
+  if ((j + 1) * kTsCells > e - b) return slot;
+  const int r = q - j * kTsCells;
+  const int lane = r / kStride, rem = r - lane * kStride;
+  const int warp = rem / kTsCellsPerThread, c = rem - warp * kTsCellsPerThread;
+  return b + j * kTsCells + (warp * 32 + lane) * kTsCellsPerThread + c;
+}
+
 __global__ void order_place_kernel(const unsigned* __restrict__ keys, int num_nodes, int nm, int nf,
                                    unsigned* __restrict__ starts, int* __restrict__ order) {
   const int count = nm + nf;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const unsigned slot = atomicAdd(starts + keys[i], 1u);
-    order[slot] = i < nm ? i : num_nodes - nf + (i - nm);
+    const int slot = (int)atomicAdd(starts + keys[i], 1u);
+    if (i < nm)
+      order[block_spread_slot(slot, 0, nm)] = i;
+    else
+      order[block_spread_slot(slot, nm, count)] = num_nodes - nf + (i - nm);
   }
 }
 

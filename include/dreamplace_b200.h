@@ -128,12 +128,14 @@ int dp_gather_order_xy(const float* xy, const int* order, int count, float* xy_o
 
 /* Order-driven triangle scatter of the cells 0..count of a visiting order onto
  * initial_density_map (NULL = zeros); positions (xy_o, interleaved) and
- * records (rec4, ratio_o) are both stored in that order.  Same
- * arithmetic as dp_density_map_f32 / _fx64.  Blocks of consecutive cells
- * accumulate in registers (3 x 3-bin windows) or a shared-memory tile over
- * their bin box before touching global memory, so a spatial order turns most
- * global atomics into local ones.  deterministic != 0: int64 fixed point
- * (scratch_fixed [num_bins] required).  order (optional): the visiting order
+ * records (rec4, ratio_o) are both stored in that order.  Same per-bin
+ * contributions as dp_density_map_f32 / _fx64.  Blocks of 512 consecutive
+ * cells accumulate in a shared-memory tile over their bin box (int32 words)
+ * before touching global memory, so a spatial order turns most global atomics
+ * into local ones.  deterministic != 0: int64 fixed point, bit-exact with the
+ * CPU op (scratch_fixed [num_bins] required); otherwise the tile sums each
+ * block's contributions at a resolution of at most 2^-21 of the bin area and
+ * adds them to the fp32 map with float atomics.  order (optional): the visiting order
  * itself; then xy_o holds the positions in node order and cell idx is read at
  * xy_o[order[idx]], so no visiting-order copy of the positions is needed. */
 int dp_density_map_ordered(const float* xy_o, const int* order, const float* rec4, const float* ratio_o,
@@ -450,8 +452,10 @@ int dp_wa_pins_backward(const float* grad_lane, const int* lane_of_pin, const un
  * movable cells and order[num_movable..) the fillers, each bucketed by the bin
  * where the stretched footprint starts (pos + offset; 16 x 16-bin tiles in
  * serpentine order, then the bin inside the tile) by a counting sort; inside
- * a bucket the order is arbitrary.  scratch: dp_order_cells_scratch_bytes
- * bytes, 4-byte aligned. */
+ * a bucket the order is arbitrary.  Each full block of 512 cells of either
+ * range is then laid out for the ordered scatter: slot (32 w + l) * 2 + c
+ * holds sorted rank 16 l + 2 w + c, so the 32 lanes of a warp take cells 16
+ * ranks apart.  scratch: dp_order_cells_scratch_bytes bytes, 4-byte aligned. */
 size_t dp_order_cells_scratch_bytes(int num_movable, int num_filler, int num_bins_x, int num_bins_y);
 int dp_order_cells_by_bin(const float* pos, int num_nodes, const float* offset_x, const float* offset_y,
                           int num_movable, int num_filler, float xl, float yl, float inv_bin_size_x,
