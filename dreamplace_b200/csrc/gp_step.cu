@@ -485,11 +485,18 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
 // net's pins in registers and runs the reference's per-net loops in pin order
 // (so the sums are formed in the CPU op's order), and the per-net terms (the
 // fp64 a terms, the divisions) are issued once per 32 nets instead of once
-// per chunk of ~10 nets.  A larger net is a group of its own, handled by the
-// whole warp with strided loops and warp reductions.
+// per chunk of ~10 nets.  Nets of degree 9..32 go four of one degree to a
+// group, eight lanes each (pins in registers, segment reductions); a larger
+// net is a group of its own, handled by the whole warp with strided loops and
+// warp reductions.
 namespace dpb {
 
 constexpr int kLaneDeg = 8;
+// nets of degree kLaneDeg < d <= kSubDeg: four nets of one degree per group,
+// kSubLanes lanes per net (each lane up to kSubDeg / kSubLanes pins)
+constexpr int kSubDeg = 32;
+constexpr int kSubLanes = 8;
+constexpr int kSubPins = kSubDeg / kSubLanes;
 
 struct LaneArgs {
   const float2* xy;        // interleaved node positions, or nullptr: planar pin positions below
@@ -618,7 +625,118 @@ __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, 
   }
 }
 
-// a net of degree > kLaneDeg: pins base .. base + deg (contiguous), whole warp
+// reduction over the kSubLanes lanes of one net (aligned lane segment)
+__device__ __forceinline__ float sub_all(float v, int kind) {
+#pragma unroll
+  for (int o = kSubLanes / 2; o > 0; o >>= 1) {
+    const float u = __shfl_xor_sync(0xffffffffu, v, o);
+    v = kind == 0 ? fmaxf(v, u) : kind == 1 ? fminf(v, u) : fadd(v, u);
+  }
+  return v;
+}
+
+// a net of degree kLaneDeg < deg <= kSubDeg on kSubLanes lanes (four nets per
+// warp, net -1 on padding segments): its pins are contiguous from base, lane
+// s of the segment holds pins s, s + kSubLanes, ... in registers; maxima,
+// minima and the exponential sums are reduced across the segment.  Every lane
+// of the warp takes part in the shuffles.
+template <bool kGrad, bool kPins>
+__device__ void sub_net(const LaneArgs& A, float ig, int base, int deg, int lane, int net, bool hpwl,
+                        double& contrib, double& hcontrib) {
+  const int sl = lane & (kSubLanes - 1);
+  const bool live = net >= 0;
+  float x[kSubPins], y[kSubPins];
+  float x_max = -FLT_MAX, x_min = FLT_MAX, y_max = -FLT_MAX, y_min = FLT_MAX;
+#pragma unroll
+  for (int t = 0; t < kSubPins; ++t) {
+    const int j = sl + kSubLanes * t;
+    x[t] = y[t] = 0.f;
+    if (live && j < deg) {
+      const float2 q = lane_xy<kPins>(A, base + j);
+      x[t] = q.x;
+      y[t] = q.y;
+      x_max = fmaxf(x_max, q.x);
+      x_min = fminf(x_min, q.x);
+      y_max = fmaxf(y_max, q.y);
+      y_min = fminf(y_min, q.y);
+    }
+  }
+  x_max = sub_all(x_max, 0);
+  x_min = sub_all(x_min, 1);
+  y_max = sub_all(y_max, 0);
+  y_min = sub_all(y_min, 1);
+  // no early exit before the last shuffle: every lane runs the same sequence
+  const float w = live && A.net_weights ? A.net_weights[net] : 1.0f;
+  if (!kGrad) {
+    if (live && sl == 0 && A.net_mask[net]) {
+      float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+      if (A.net_weights) h = fmul(h, w);
+      contrib += (double)h;
+    }
+    return;
+  }
+  if (live && hpwl && sl == 0 && A.hpwl_mask[net]) {
+    float h = fsub(fadd(fsub(x_max, x_min), y_max), y_min);
+    if (A.net_weights) h = fmul(h, w);
+    hcontrib += (double)h;
+  }
+  const bool on = live && A.net_mask[net];
+  float e_p = 0.f, e_n = 0.f, xe_p = 0.f, xe_n = 0.f, f_p = 0.f, f_n = 0.f, ye_p = 0.f, ye_n = 0.f;
+  if (on) {
+#pragma unroll
+    for (int t = 0; t < kSubPins; ++t) {
+      if (sl + kSubLanes * t < deg) {
+        const float a1 = expf(fmul(fsub(x[t], x_max), ig));
+        const float a2 = expf(fmul(fsub(x_min, x[t]), ig));
+        const float a3 = expf(fmul(fsub(y[t], y_max), ig));
+        const float a4 = expf(fmul(fsub(y_min, y[t]), ig));
+        e_p = fadd(e_p, a1);
+        e_n = fadd(e_n, a2);
+        xe_p = fadd(xe_p, fmul(x[t], a1));
+        xe_n = fadd(xe_n, fmul(x[t], a2));
+        f_p = fadd(f_p, a3);
+        f_n = fadd(f_n, a4);
+        ye_p = fadd(ye_p, fmul(y[t], a3));
+        ye_n = fadd(ye_n, fmul(y[t], a4));
+      }
+    }
+  }
+  e_p = sub_all(e_p, 2); e_n = sub_all(e_n, 2); xe_p = sub_all(xe_p, 2); xe_n = sub_all(xe_n, 2);
+  f_p = sub_all(f_p, 2); f_n = sub_all(f_n, 2); ye_p = sub_all(ye_p, 2); ye_n = sub_all(ye_n, 2);
+  if (!live) return;
+  if (!on) {
+#pragma unroll
+    for (int t = 0; t < kSubPins; ++t)
+      if (sl + kSubLanes * t < deg) __stcs(A.gnode + grad_slot(A, base + sl + kSubLanes * t), make_float2(0.f, 0.f));
+    return;
+  }
+  if (sl == 0) {
+    const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
+                          __fdiv_rn(ye_n, f_n));
+    contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
+  }
+  const float b_x = __fdiv_rn(ig, e_p), a_x = wa_a_term(b_x, xe_p, e_p);
+  const float b_nx = __fdiv_rn(-ig, e_n), a_nx = wa_a_term(b_nx, xe_n, e_n);
+  const float b_y = __fdiv_rn(ig, f_p), a_y = wa_a_term(b_y, ye_p, f_p);
+  const float b_ny = __fdiv_rn(-ig, f_n), a_ny = wa_a_term(b_ny, ye_n, f_n);
+#pragma unroll
+  for (int t = 0; t < kSubPins; ++t) {
+    const int j = sl + kSubLanes * t;
+    if (j < deg) {
+      const float a1 = expf(fmul(fsub(x[t], x_max), ig)), a2 = expf(fmul(fsub(x_min, x[t]), ig));
+      const float a3 = expf(fmul(fsub(y[t], y_max), ig)), a4 = expf(fmul(fsub(y_min, y[t]), ig));
+      float gx = fsub(fmul(fadd(a_x, fmul(b_x, x[t])), a1), fmul(fadd(a_nx, fmul(b_nx, x[t])), a2));
+      float gy = fsub(fmul(fadd(a_y, fmul(b_y, y[t])), a3), fmul(fadd(a_ny, fmul(b_ny, y[t])), a4));
+      if (A.net_weights) {
+        gx = fmul(gx, w);
+        gy = fmul(gy, w);
+      }
+      __stcs(A.gnode + grad_slot(A, base + j), make_float2(gx, gy));
+    }
+  }
+}
+
+// a net of degree > kSubDeg: pins base .. base + deg (contiguous), whole warp
 template <bool kGrad, bool kPins>
 __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lane, int net, bool hpwl,
                          double& contrib, double& hcontrib) {
@@ -711,8 +829,13 @@ __global__ void __launch_bounds__(256, 4) wa_lane_kernel(LaneArgs A, double* __r
   double contrib = 0.0, hcontrib = 0.0;
   for (int g = warp; g < A.num_groups; g += nwarps) {
     const int deg = A.group_deg[g], base = A.group_base[g];
-    if (deg > kLaneDeg) {
+    if (deg > kSubDeg) {
       warp_net<kGrad, kPins>(A, ig, base, deg, lane, A.group_net[32 * g], hpwl, contrib, hcontrib);
+      continue;
+    }
+    if (deg > kLaneDeg) {
+      const int s = lane / kSubLanes;
+      sub_net<kGrad, kPins>(A, ig, base + s * deg, deg, lane, A.group_net[32 * g + s], hpwl, contrib, hcontrib);
       continue;
     }
     const int net = A.group_net[32 * g + lane];
@@ -780,10 +903,40 @@ extern "C" int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, con
       base += 32 * d;
     }
   }
+  // degrees kLaneDeg + 1 .. kSubDeg: 32 / kSubLanes nets of one degree per
+  // group, net s's pins contiguous from group_base + s * d
+  constexpr int kSubNets = 32 / kSubLanes;
+  for (int d = kLaneDeg + 1; d <= kSubDeg; ++d) {
+    int in_group = 0;
+    for (int t = 0; t < num_nets; ++t) {
+      const int e = net_order_host ? net_order_host[t] : t;
+      const int s0 = netpin_start_host[e];
+      if (netpin_start_host[e + 1] - s0 != d) continue;
+      if (in_group == 0 && fill) {
+        group_deg[g] = d;
+        group_base[g] = (int)base;
+        for (int l = 0; l < 32; ++l) group_net[32 * g + l] = -1;
+        for (int i = 0; i < kSubNets * d; ++i) lane_slot[base + i] = -1;
+      }
+      if (fill) {
+        group_net[32 * g + in_group] = e;
+        for (int j = 0; j < d; ++j) lane_slot[base + in_group * d + j] = s0 + j;
+      }
+      if (++in_group == kSubNets) {
+        in_group = 0;
+        ++g;
+        base += kSubNets * d;
+      }
+    }
+    if (in_group) {
+      ++g;
+      base += kSubNets * d;
+    }
+  }
   for (int t = 0; t < num_nets; ++t) {
     const int e = net_order_host ? net_order_host[t] : t;
     const int s0 = netpin_start_host[e], d = netpin_start_host[e + 1] - s0;
-    if (d <= kLaneDeg) continue;
+    if (d <= kSubDeg) continue;
     if (fill) {
       group_deg[g] = d;
       group_base[g] = (int)base;

@@ -393,21 +393,24 @@ int dp_set_trial_gate(const int* gate);
 int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t stream);
 /* Lane-per-net plan (host): nets of degree 1..8 grouped 32 at a time by degree,
  * in the order net_order_host gives (a permutation of the nets; NULL: net
- * index order) within a degree; each larger net a group of its own.  The
+ * index order) within a degree; nets of degree 9..32 four of one degree per
+ * group; each larger net a group of its own.  The
  * order only places the nets in memory: ordering nets by where their pins
  * live in the node arrays makes the pin-position gathers and the gradient
  * gather of the assembly local.  Call with
  * NULL group_deg / group_base / group_net / lane_slot to get *num_groups and
  * *num_lane_slots, then with buffers of those sizes (group_net: 32 per group).
  * Group g of degree d <= 8 stores pin j of lane l at lane slot
- * group_base[g] + 32 j + l; a larger net stores its pins contiguously from
- * group_base[g].  lane_slot maps lane slots to pin slots (flat_netpin order),
- * -1 for padding; group_net holds net ids, -1 for padding lanes. */
+ * group_base[g] + 32 j + l; a group of degree 9..32 stores pin j of its net s
+ * (s < 4, net id group_net[32 g + s]) at group_base[g] + s d + j; a larger net
+ * stores its pins contiguously from group_base[g].  lane_slot maps lane slots
+ * to pin slots (flat_netpin order), -1 for padding; group_net holds net ids,
+ * -1 for padding lanes. */
 int dp_plan_net_lanes(const int* netpin_start_host, int num_nets, const int* net_order_host, int* num_groups,
                       int* num_lane_slots, int* group_deg, int* group_base, int* group_net, int* lane_slot);
 /* WA forward over a lane plan: one warp per group, one lane per net (degree
- * <= 8, pins in registers, the reference's per-net loops in pin order) or the
- * whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the
+ * <= 8, pins in registers, the reference's per-net loops in pin order), eight
+ * lanes per net (degree 9..32) or the whole warp for a larger net.  ln_node / ln_offx / ln_offy / ln_csr are the
  * pin arrays gathered to lane-slot order (ln_csr: the pin's position in
  * node-CSR order, where its gradient is written; NULL writes the gradient of
  * lane slot p at p).  The per-pin gradient, times the net weight, is written
