@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, i
 // add to the same word are serialised.  The visiting order therefore places
 // the cells of each kTsCells block so that the 32 lanes of a warp hold cells
 // kTsCells / 32 apart in sort order (different bins), while the block as a
-// whole keeps its compact bin box.
+// whole keeps its compact bin box; and a thread's two cells, adjacent in sort
+// order, that start at the same bin add one merged window (fp32 mode).
 constexpr int kTsThreads = 256;
 constexpr int kTsCellsPerThread = 2;
 constexpr int kTsCells = kTsThreads * kTsCellsPerThread;  // 512: the int32 plane bound above
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
   __syncthreads();
   int* const plane1 = plane0 + box;
   const int nby = a.num_bins_y;
+  if (kFixed) {
 #pragma unroll
   for (int c = 0; c < kTsCellsPerThread; ++c) {
     if (nk[c] == 0) continue;
@@ -312,20 +314,12 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
           const float area = fmul(pxr[i], py[j]);
           const int slot = row[i] + col[j];
           const float y = fmul(area, plane_scale);
-          if (kFixed) {
-            const float hf = truncf(y);
-            if (fabsf(hf) < kTsLoSpan) {
-              atomicAdd(plane0 + slot, (int)hf);
-              atomicAdd(plane1 + slot, (int)fmul(fsub(y, hf), kTsLoSpan));
-            } else {
-              atomicAdd(map_fx + (bk0 + rk + i) * nby + bh0 + rh + j, (unsigned long long)to_fixed(area, fx_scale));
-            }
+          const float hf = truncf(y);
+          if (fabsf(hf) < kTsLoSpan) {
+            atomicAdd(plane0 + slot, (int)hf);
+            atomicAdd(plane1 + slot, (int)fmul(fsub(y, hf), kTsLoSpan));
           } else {
-            if (fabsf(y) < kTsLoSpan - 1.0f) {  // |round(y)| < 2^22
-              atomicAdd(plane0 + slot, __float2int_rn(y));
-            } else {
-              atomicAdd(map_f32 + (bk0 + rk + i) * nby + bh0 + rh + j, area);
-            }
+            atomicAdd(map_fx + (bk0 + rk + i) * nby + bh0 + rh + j, (unsigned long long)to_fixed(area, fx_scale));
           }
         }
     } else {
@@ -334,10 +328,77 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
         const float pxr = fmul(triangle_overlap(nx[c], sx[c], a.xl, k, a.bsx), rr[c]);
         for (int h = h0[c]; h < h0[c] + nh[c]; ++h) {
           const float area = fmul(pxr, triangle_overlap(ny[c], sy[c], a.yl, h, a.bsy));
-          if (kFixed)
-            atomicAdd(map_fx + k * nby + h, (unsigned long long)to_fixed(area, fx_scale));
-          else
-            atomicAdd(map_f32 + k * nby + h, area);
+          atomicAdd(map_fx + k * nby + h, (unsigned long long)to_fixed(area, fx_scale));
+        }
+      }
+    }
+  }
+  } else {
+    // fp32: each cell's nine rounded contributions are formed first; a
+    // thread's two cells (adjacent in sort order) that start at the same bin
+    // add one merged window, halving the atomics where cells crowd
+    int vals[kTsCellsPerThread][9];
+    bool ok[kTsCellsPerThread];
+#pragma unroll
+    for (int c = 0; c < kTsCellsPerThread; ++c) {
+      const int rk = k0[c] - bk0, rh = h0[c] - bh0;
+      ok[c] = nk[c] && rk >= 0 && rh >= 0 && rk + nk[c] <= K && rh + nh[c] <= H && nk[c] <= 3 && nh[c] <= 3;
+      const float xh = fadd(nx[c], sx[c]), yh = fadd(ny[c], sy[c]);
+      float pxr[3], py[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const bool okx = j < nk[c], oky = j < nh[c];
+        // (table indices clamped into the tables: a cell outside the tile
+        // computes values it does not use)
+        const float2 ex = tabx[min(max(okx ? rk + j : rk, 0), kTsTab - 1)];
+        const float2 ey = taby[min(max(oky ? rh + j : rh, 0), kTsTab - 1)];
+        // triangle_overlap: min(x + size, bin_xh) - max(x, bin_xl)
+        pxr[j] = okx ? fmul(fsub(fminf(xh, ex.y), fmaxf(nx[c], ex.x)), rr[c]) : 0.f;
+        py[j] = oky ? fsub(fminf(yh, ey.y), fmaxf(ny[c], ey.x)) : 0.f;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const float y = fmul(fmul(pxr[i], py[j]), plane_scale);
+          ok[c] = ok[c] && fabsf(y) < kTsLoSpan - 1.0f;  // |round(y)| < 2^22
+          vals[c][3 * i + j] = __float2int_rn(y);
+        }
+    }
+    // tile slot of window entry (i, j) of a cell at (rk, rh) with nk x nh
+    // bins; entries beyond the footprint (value 0) land on the window's
+    // first row / column
+    auto slot_of = [P](int rk, int rh, int nk_, int nh_, int i, int j) {
+      return (i < nk_ ? rk + i : rk) * P + rh + (j < nh_ ? j : 0);
+    };
+    bool merged = false;
+    if (ok[0] && ok[1] && k0[0] == k0[1] && h0[0] == h0[1]) {
+      merged = true;
+      const int mk = max(nk[0], nk[1]), mh = max(nh[0], nh[1]);
+      const int rk = k0[0] - bk0, rh = h0[0] - bh0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          atomicAdd(plane0 + slot_of(rk, rh, mk, mh, i, j),
+                    (i < mk && j < mh) ? vals[0][3 * i + j] + vals[1][3 * i + j] : 0);
+    }
+#pragma unroll
+    for (int c = 0; c < kTsCellsPerThread; ++c) {
+      if (merged || nk[c] == 0) continue;
+      if (ok[c]) {
+        const int rk = k0[c] - bk0, rh = h0[c] - bh0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) atomicAdd(plane0 + slot_of(rk, rh, nk[c], nh[c], i, j), vals[c][3 * i + j]);
+      } else {
+        // outside the tile, wider than 3 bins, or beyond the plane's range:
+        // one global add per bin
+        for (int k = k0[c]; k < k0[c] + nk[c]; ++k) {
+          const float pxr = fmul(triangle_overlap(nx[c], sx[c], a.xl, k, a.bsx), rr[c]);
+          for (int h = h0[c]; h < h0[c] + nh[c]; ++h)
+            atomicAdd(map_f32 + k * nby + h, fmul(pxr, triangle_overlap(ny[c], sy[c], a.yl, h, a.bsy)));
         }
       }
     }
