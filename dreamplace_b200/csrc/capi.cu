@@ -15,6 +15,7 @@ static const int* g_trial_gate = nullptr;
 const int* trial_gate() { return g_trial_gate; }
 
 __global__ void trial_gate_kernel(int* gate, const double* accept_prev) {
+  grid_dep_sync();
   *gate = accept_prev ? (*accept_prev == 0.0 ? 1 : 0) : 0;
 }
 
@@ -39,6 +40,7 @@ void smem_opt_in_mark(const void* kernel, int device) {
 }
 
 __global__ void finish_sum_kernel(double* buf, int count, float* out_f32) {
+  grid_dep_sync();
   double r = finish_sum(buf + 1, count);
   if (threadIdx.x == 0) {
     buf[0] = r;
@@ -47,12 +49,13 @@ __global__ void finish_sum_kernel(double* buf, int count, float* out_f32) {
 }
 
 int launch_finish_sum(double* buf, int count, float* out_f32, cudaStream_t s) {
-  finish_sum_kernel<<<1, kReduceThreads, 0, s>>>(buf, count, out_f32);
+  launch_kernel(finish_sum_kernel, 1, kReduceThreads, 0, s, buf, count, out_f32);
   return check_launch("finish_sum");
 }
 
 // two independent fixed-order reductions of `count` partials in one launch
 __global__ void finish_sum2_kernel(double* a, double* b, int count) {
+  grid_dep_sync();
   double ra = finish_sum(a + 1, count);
   double rb = finish_sum(b + 1, count);
   if (threadIdx.x == 0) {
@@ -62,7 +65,7 @@ __global__ void finish_sum2_kernel(double* a, double* b, int count) {
 }
 
 int launch_finish_sum2(double* a, double* b, int count, cudaStream_t s) {
-  finish_sum2_kernel<<<1, kReduceThreads, 0, s>>>(a, b, count);
+  launch_kernel(finish_sum2_kernel, 1, kReduceThreads, 0, s, a, b, count);
   return check_launch("finish_sum2");
 }
 
@@ -75,7 +78,7 @@ extern "C" int dp_set_trial_gate(const int* gate) {
 }
 extern "C" int dp_trial_gate(int* gate, const double* accept_prev, dp_stream_t stream) {
   DP_REQUIRE(gate, "dp_trial_gate: null gate");
-  dpb::trial_gate_kernel<<<1, 1, 0, dpb::as_stream(stream)>>>(gate, accept_prev);
+  dpb::launch_kernel(dpb::trial_gate_kernel, 1, 1, 0, dpb::as_stream(stream), gate, accept_prev);
   return dpb::check_launch("dp_trial_gate");
 }
 extern "C" int dp_version(void) { return 1; }

@@ -10,6 +10,7 @@
 #include <stdio.h>
 #include <atomic>
 #include <string>
+#include <utility>
 
 #include "dreamplace_b200.h"
 
@@ -40,6 +41,36 @@ inline int check_launch(const char* what) {
 }
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Programmatic dependent launch.  Every kernel of this library is launched
+// with programmatic stream serialisation allowed, and starts with
+// grid_dep_sync(): it waits there until the kernels before it in the stream
+// have completed and their writes are visible (griddepcontrol.wait), then lets
+// the next kernel be scheduled (griddepcontrol.launch_dependents).  The next
+// kernel's launch and block scheduling thus overlap this kernel's run instead
+// of following its last block; no kernel reads data before its wait.  A kernel
+// launched without the attribute (or after a copy or memset) waits as usual.
+__device__ __forceinline__ void grid_dep_sync() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                          Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // a failed launch is reported by the caller's check_launch (cudaGetLastError)
+  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Raises a kernel's dynamic shared-memory limit once per device: the
 // attribute applies to the device current when it is set, so a process that

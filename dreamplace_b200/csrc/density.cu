@@ -61,6 +61,7 @@ template <bool kFixed>
 __global__ void __launch_bounds__(256) triangle_scatter_kernel(TriangleArgs a, int total,
                                                                float fx_scale, float* map_f32,
                                                                unsigned long long* map_fx) {
+  grid_dep_sync();
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
     int idx = base + threadIdx.x;
@@ -177,6 +178,7 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
                                                                   const float* __restrict__ ratio_o,
                                                                   float fx_scale, float plane_scale,
                                                                   float plane_unit, const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   constexpr int kPlanes = kFixed ? 2 : 1;
   constexpr int kCap = kTsSmemBytes / (4 * kPlanes);  // tile bins
@@ -432,6 +434,7 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
 
 __global__ void gather_order_xy_kernel(const float2* __restrict__ xy, const int* __restrict__ order, int count,
                                        float2* __restrict__ xy_o, const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
     xy_o[idx] = xy[order[idx]];
@@ -442,6 +445,7 @@ __global__ void build_records_kernel(const float* __restrict__ sx, const float* 
                                      const float* __restrict__ ratio, const int* __restrict__ order, int count,
                                      float4* __restrict__ rec4, float* __restrict__ ratio_o,
                                      int* __restrict__ inv_order) {
+  grid_dep_sync();
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
     const int i = order[idx];
     rec4[idx] = make_float4(sx[i], sy[i], ox[i], oy[i]);
@@ -453,6 +457,7 @@ __global__ void build_records_kernel(const float* __restrict__ sx, const float* 
 // out = (float)((double)init + (double)fixed * 2^-f)  (utility/src/atomic_ops.h:48-54)
 __global__ void fixed_to_float_kernel(const long long* fixed, const float* init, double inv_scale,
                                       float* out, int n) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double base = init ? (double)init[i] : 0.0;
     out[i] = (float)(base + (double)fixed[i] * inv_scale);
@@ -461,6 +466,7 @@ __global__ void fixed_to_float_kernel(const long long* fixed, const float* init,
 
 __global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__ dst, int n4,
                             const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x)
     dst[i] = src[i];
@@ -469,7 +475,7 @@ __global__ void copy_kernel(const float4* __restrict__ src, float4* __restrict__
 static int copy_map(const float* src, float* dst, int n, cudaStream_t s) {
   if (src == dst) return DP_OK;
   if ((n & 3) == 0 && ((uintptr_t)src & 15) == 0 && ((uintptr_t)dst & 15) == 0) {
-    copy_kernel<<<grid_for(n / 4, 256), 256, 0, s>>>((const float4*)src, (float4*)dst, n / 4, trial_gate());
+    launch_kernel(copy_kernel, grid_for(n / 4, 256), 256, 0, s, (const float4*)src, (float4*)dst, n / 4, trial_gate());
     return check_launch("copy_map");
   }
   cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
@@ -513,6 +519,7 @@ __global__ void exact_scatter_kernel(const float* x, const float* y, const float
                                      float xl, float yl, float xh, float yh, float bsx, float bsy,
                                      int nbx, int nby, bool fixed_node_flag, bool use_centers,
                                      float fx_scale, float* map_f32, unsigned long long* map_fx) {
+  grid_dep_sync();
   for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
     float bxl = x[i], byl = y[i];
     float bxh = fadd(bxl, sx[i]), byh = fadd(byl, sy[i]);
@@ -545,6 +552,7 @@ template <bool kFixed>
 __global__ void box_scatter_kernel(const float* x, const float* y, const float* sx, const float* sy, int begin,
                                    int end, float xl, float yl, float xh, float yh, int nbx, int nby,
                                    float fx_scale, float* map_f32, unsigned long long* map_fx) {
+  grid_dep_sync();
   const float bsx = __fdiv_rn(fsub(xh, xl), (float)nbx);
   const float bsy = __fdiv_rn(fsub(yh, yl), (float)nby);
   for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
@@ -577,6 +585,7 @@ __global__ void box_scatter_kernel(const float* x, const float* y, const float* 
 }
 
 __global__ void clamp_max_kernel(float* map, int n, float vmax) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     map[i] = fminf(map[i], vmax);
 }
@@ -593,6 +602,7 @@ __device__ __forceinline__ float key_float(unsigned k) {
 
 __global__ void overflow_kernel(const float* __restrict__ map, int n, double target_area,
                                 double* partials, unsigned* maxkey) {
+  grid_dep_sync();
   double s = 0.0;
   float m = -INFINITY;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -617,6 +627,7 @@ __global__ void first_map_kernel(const long long* __restrict__ fixed, const floa
                                  double inv_scale, float* first, float* __restrict__ copy_to, int add_to_copy,
                                  int n, double target_area, double* partials, unsigned* maxkey,
                                  const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   double s = 0.0;
   float m = -INFINITY;
@@ -641,6 +652,7 @@ __global__ void first_map_kernel(const long long* __restrict__ fixed, const floa
 
 __global__ void overflow_finish_kernel(double* out2, const unsigned* maxkey, double bin_area,
                                        float* out2_f32, const double* partials, int count) {
+  grid_dep_sync();
   double total = finish_sum(partials, count);
   if (threadIdx.x != 0) return;
   out2[0] = total;
@@ -675,7 +687,7 @@ extern "C" int dp_density_map_f32(const float* pos, int num_nodes, const float* 
   int total = nm + nf;
   if (total == 0) return DP_OK;
   TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, nm, nf, nbx, nby, sorted);
-  triangle_scatter_kernel<false><<<grid_for(total, 256, 16), 256, 0, s>>>(a, total, 0.f, out, nullptr);
+  launch_kernel(triangle_scatter_kernel<false>, grid_for(total, 256, 16), 256, 0, s, a, total, 0.f, out, nullptr);
   return check_launch("dp_density_map_f32");
 }
 
@@ -696,12 +708,12 @@ extern "C" int dp_density_map_fx64(const float* pos, int num_nodes, const float*
   float scale = ldexpf(1.0f, fraction_bits);
   if (total > 0) {
     TriangleArgs a = make_args(pos, num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx, iby, nm, nf, nbx, nby, sorted);
-    triangle_scatter_kernel<true><<<grid_for(total, 256, 16), 256, 0, s>>>(
+    launch_kernel(triangle_scatter_kernel<true>, grid_for(total, 256, 16), 256, 0, s, 
         a, total, scale, nullptr, reinterpret_cast<unsigned long long*>(scratch));
     rc = check_launch("dp_density_map_fx64 scatter");
     if (rc) return rc;
   }
-  fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
+  launch_kernel(fixed_to_float_kernel, grid_for(nbins, 256), 256, 0, s, (const long long*)scratch, init,
                                                             ldexp(1.0, -fraction_bits), out, nbins);
   return check_launch("dp_density_map_fx64 convert");
 }
@@ -724,24 +736,24 @@ extern "C" int dp_fixed_density_map(const float* pos, int num_nodes, const float
   int blocks = grid_for(nt, 128, 8);
   if (deterministic) {
     cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
-    exact_scatter_kernel<true><<<blocks, 128, 0, s>>>(x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
+    launch_kernel(exact_scatter_kernel<true>, blocks, 128, 0, s, x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
                                                       bsx, bsy, nbx, nby, true, true,
                                                       ldexpf(1.0f, fraction_bits), nullptr,
                                                       reinterpret_cast<unsigned long long*>(scratch));
     int rc = check_launch("dp_fixed_density_map scatter");
     if (rc) return rc;
-    fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, nullptr,
+    launch_kernel(fixed_to_float_kernel, grid_for(nbins, 256), 256, 0, s, (const long long*)scratch, nullptr,
                                                               ldexp(1.0, -fraction_bits), out, nbins);
     rc = check_launch("dp_fixed_density_map convert");
     if (rc) return rc;
   } else {
-    exact_scatter_kernel<false><<<blocks, 128, 0, s>>>(x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
+    launch_kernel(exact_scatter_kernel<false>, blocks, 128, 0, s, x, y, sx, sy, bcx, bcy, nm, nm + nt, xl, yl, xh, yh,
                                                        bsx, bsy, nbx, nby, true, true, 0.f, out, nullptr);
     int rc = check_launch("dp_fixed_density_map scatter");
     if (rc) return rc;
   }
   float vmax = (float)((double)bsx * (double)bsy);
-  clamp_max_kernel<<<grid_for(nbins, 256), 256, 0, s>>>(out, nbins, vmax);
+  launch_kernel(clamp_max_kernel, grid_for(nbins, 256), 256, 0, s, out, nbins, vmax);
   return check_launch("dp_fixed_density_map clamp");
 }
 
@@ -764,17 +776,17 @@ extern "C" int dp_density_map_exact(const float* pos, int num_nodes, const float
     if (deterministic) {
       // each range is converted onto the running map on its own, as the reference does
       cudaMemsetAsync(scratch, 0, sizeof(int64_t) * nbins, s);
-      box_scatter_kernel<true><<<grid_for(n, 128, 8), 128, 0, s>>>(
+      launch_kernel(box_scatter_kernel<true>, grid_for(n, 128, 8), 128, 0, s, 
           x, y, sx, sy, rb[r], re[r], xl, yl, xh, yh, nbx, nby, ldexpf(1.0f, fraction_bits), nullptr,
           reinterpret_cast<unsigned long long*>(scratch));
       int rc = check_launch("dp_density_map_exact scatter");
       if (rc) return rc;
-      fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, out,
+      launch_kernel(fixed_to_float_kernel, grid_for(nbins, 256), 256, 0, s, (const long long*)scratch, out,
                                                                 ldexp(1.0, -fraction_bits), out, nbins);
       rc = check_launch("dp_density_map_exact convert");
       if (rc) return rc;
     } else {
-      box_scatter_kernel<false><<<grid_for(n, 128, 8), 128, 0, s>>>(x, y, sx, sy, rb[r], re[r], xl, yl, xh, yh,
+      launch_kernel(box_scatter_kernel<false>, grid_for(n, 128, 8), 128, 0, s, x, y, sx, sy, rb[r], re[r], xl, yl, xh, yh,
                                                                     nbx, nby, 0.f, out, nullptr);
       int rc = check_launch("dp_density_map_exact scatter");
       if (rc) return rc;
@@ -791,10 +803,10 @@ extern "C" int dp_density_overflow(const float* map, int nbins, double target_ar
   int blocks = grid_for(nbins, 256, 4);
   unsigned* maxslot = reinterpret_cast<unsigned*>(out2 + 2);
   cudaMemsetAsync(maxslot, 0, sizeof(double), s);
-  overflow_kernel<<<blocks, 256, 0, s>>>(map, nbins, target_area, out2 + 3, maxslot);
+  launch_kernel(overflow_kernel, blocks, 256, 0, s, map, nbins, target_area, out2 + 3, maxslot);
   int rc = check_launch("dp_density_overflow");
   if (rc) return rc;
-  overflow_finish_kernel<<<1, kReduceThreads, 0, s>>>(out2, maxslot, bin_area, out2_f32, out2 + 3, blocks);
+  launch_kernel(overflow_finish_kernel, 1, kReduceThreads, 0, s, out2, maxslot, bin_area, out2_f32, out2 + 3, blocks);
   return check_launch("dp_density_overflow finish");
 }
 
@@ -803,7 +815,7 @@ extern "C" int dp_gather_order_xy(const float* xy, const int* order, int count, 
   DP_REQUIRE(xy && xy_o && (count == 0 || order), "dp_gather_order_xy: null pointer");
   DP_REQUIRE(((uintptr_t)xy & 7) == 0 && ((uintptr_t)xy_o & 7) == 0, "dp_gather_order_xy: misaligned xy / xy_o");
   if (count == 0) return DP_OK;
-  gather_order_xy_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(gather_order_xy_kernel, grid_for(count, 256, 8), 256, 0, as_stream(stream), 
       reinterpret_cast<const float2*>(xy), order, count, reinterpret_cast<float2*>(xy_o), trial_gate());
   return check_launch("dp_gather_order_xy");
 }
@@ -816,7 +828,7 @@ extern "C" int dp_build_cell_records(const float* sx, const float* sy, const flo
   DP_REQUIRE(sx && sy && ox && oy && ratio && order && rec4 && ratio_o, "dp_build_cell_records: null pointer");
   DP_REQUIRE(((uintptr_t)rec4 & 15) == 0, "dp_build_cell_records: rec4 must be 16-byte aligned");
   if (count == 0) return DP_OK;
-  build_records_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(build_records_kernel, grid_for(count, 256, 8), 256, 0, as_stream(stream), 
       sx, sy, ox, oy, ratio, order, count, reinterpret_cast<float4*>(rec4), ratio_o, inv_order);
   return check_launch("dp_build_cell_records");
 }
@@ -845,7 +857,7 @@ int scatter_ranges(const OrderedScatter& o, const WsRanges& rg, int deterministi
   if (deterministic) {
     // plane scale 2^(f - 22): hi = trunc(v / 2^22) of v = trunc(area * 2^f)
     const float fx_scale = ldexpf(1.0f, fraction_bits);
-    tile_scatter_kernel<true><<<blocks, kTsThreads, kTsSmemBytes, o.s>>>(
+    launch_kernel(tile_scatter_kernel<true>, blocks, kTsThreads, kTsSmemBytes, o.s, 
         o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, fx_scale, ldexpf(1.0f, fraction_bits - 22), 0.f,
         trial_gate());
   } else {
@@ -853,7 +865,7 @@ int scatter_ranges(const OrderedScatter& o, const WsRanges& rg, int deterministi
     // at most one bin area each sum below 2^31
     const double bin_area = (double)o.a.bsx * (double)o.a.bsy;
     const int s = (int)floor(log2((4194302.0 / 1.0001) / bin_area));
-    tile_scatter_kernel<false><<<blocks, kTsThreads, kTsSmemBytes, o.s>>>(
+    launch_kernel(tile_scatter_kernel<false>, blocks, kTsThreads, kTsSmemBytes, o.s, 
         o.a, rg, o.xy_o, o.order, o.rec4, o.ratio_o, 0.f, ldexpf(1.0f, s), ldexpf(1.0f, -s), trial_gate());
   }
   return check_launch("dp_density_map_ordered scatter");
@@ -874,7 +886,7 @@ int scatter_range(const OrderedScatter& o, int begin, int end, int deterministic
 
 int convert_fixed(const int64_t* scratch, const float* init, int fraction_bits, float* out, int nbins,
                   cudaStream_t s) {
-  fixed_to_float_kernel<<<grid_for(nbins, 256), 256, 0, s>>>((const long long*)scratch, init,
+  launch_kernel(fixed_to_float_kernel, grid_for(nbins, 256), 256, 0, s, (const long long*)scratch, init,
                                                             ldexp(1.0, -fraction_bits), out, nbins);
   return check_launch("dp_density_map_ordered convert");
 }
@@ -967,12 +979,12 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
     if (rc) return rc;
     if (overflow_out) {
       cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
-      first_map_kernel<<<blocks, 256, 0, o.s>>>((const long long*)scratch, init, ldexp(1.0, -fraction_bits),
+      launch_kernel(first_map_kernel, blocks, 256, 0, o.s, (const long long*)scratch, init, ldexp(1.0, -fraction_bits),
                                                  out_first, nullptr, 0, nbins, target_area, overflow_out + 3, maxslot,
                                                  trial_gate());
       rc = check_launch("dp_density_map_ordered_split first map");
       if (rc) return rc;
-      overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
+      launch_kernel(overflow_finish_kernel, 1, kReduceThreads, 0, o.s, overflow_out, maxslot, bin_area, nullptr,
                                                             overflow_out + 3, blocks);
       rc = check_launch("dp_density_map_ordered_split overflow");
     } else {
@@ -1003,11 +1015,11 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
   rc = scatter_ranges(o, rg, 0, 0);
   if (rc) return rc;
   if (overflow_out) cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
-  first_map_kernel<<<blocks, 256, 0, o.s>>>(nullptr, nullptr, 0.0, out_first, out_all, 1, nbins, target_area,
+  launch_kernel(first_map_kernel, blocks, 256, 0, o.s, nullptr, nullptr, 0.0, out_first, out_all, 1, nbins, target_area,
                                              overflow_out ? overflow_out + 3 : nullptr, maxslot, trial_gate());
   rc = check_launch("dp_density_map_ordered_split first map");
   if (rc || !overflow_out) return rc;
-  overflow_finish_kernel<<<1, kReduceThreads, 0, o.s>>>(overflow_out, maxslot, bin_area, nullptr,
+  launch_kernel(overflow_finish_kernel, 1, kReduceThreads, 0, o.s, overflow_out, maxslot, bin_area, nullptr,
                                                         overflow_out + 3, blocks);
   return check_launch("dp_density_map_ordered_split overflow");
 }
@@ -1135,6 +1147,7 @@ __global__ void order_keys_kernel(const float* __restrict__ pos, int num_nodes, 
                                   const float* __restrict__ oy, int nm, int nf, float xl, float yl, float ibx,
                                   float iby, int nbx, int nby, unsigned tile_buckets, unsigned* __restrict__ keys,
                                   unsigned* __restrict__ hist) {
+  grid_dep_sync();
   const int count = nm + nf;
   const int tiles_y = (nby + 15) >> 4;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -1178,6 +1191,7 @@ __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* w
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(unsigned* data, int n, unsigned* block_totals) {
+  grid_dep_sync();
   __shared__ unsigned warp_sums[32];
   const int i = blockIdx.x * kScanThreads + threadIdx.x;
   const unsigned v = i < n ? data[i] : 0u;
@@ -1189,6 +1203,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_blocks_kernel(unsigned* dat
 
 // one block scans the block totals (at most kScanThreads * kScanThreads blocks)
 __global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(unsigned* totals, int nblocks) {
+  grid_dep_sync();
   __shared__ unsigned warp_sums[32];
   __shared__ unsigned carry;
   if (threadIdx.x == 0) carry = 0u;
@@ -1206,6 +1221,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(unsigned* tot
 }
 
 __global__ void add_block_offsets_kernel(unsigned* data, int n, const unsigned* block_offsets) {
+  grid_dep_sync();
   const int i = blockIdx.x * kScanThreads + threadIdx.x;
   if (i < n) data[i] += block_offsets[blockIdx.x];
 }
@@ -1229,6 +1245,7 @@ __device__ __forceinline__ int block_spread_slot(int slot, int b, int e) {
 
 __global__ void order_place_kernel(const unsigned* __restrict__ keys, int num_nodes, int nm, int nf,
                                    unsigned* __restrict__ starts, int* __restrict__ order) {
+  grid_dep_sync();
   const int count = nm + nf;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const int slot = (int)atomicAdd(starts + keys[i], 1u);
@@ -1242,6 +1259,7 @@ __global__ void order_place_kernel(const unsigned* __restrict__ keys, int num_no
 // xy_o[idx] = (x, y) of node order[idx], from planar positions [x(n) | y(n)]
 __global__ void gather_order_pos_kernel(const float* __restrict__ pos, int num_nodes, const int* __restrict__ order,
                                         int count, float2* __restrict__ xy_o) {
+  grid_dep_sync();
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
     const int i = __ldg(order + idx);
     xy_o[idx] = make_float2(__ldg(pos + i), __ldg(pos + num_nodes + i));
@@ -1289,21 +1307,21 @@ extern "C" int dp_order_cells_by_bin(const float* pos, int num_nodes, const floa
     set_error("dp_order_cells_by_bin: cudaMemsetAsync: %s", cudaGetErrorString(e));
     return DP_ERR_CUDA;
   }
-  order_keys_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(pos, num_nodes, offset_x, offset_y, num_movable,
+  launch_kernel(order_keys_kernel, grid_for(count, 256, 8), 256, 0, s, pos, num_nodes, offset_x, offset_y, num_movable,
                                                             num_filler, xl, yl, inv_bin_size_x, inv_bin_size_y,
                                                             num_bins_x, num_bins_y, tile_buckets, keys, hist);
   int rc = check_launch("dp_order_cells_by_bin keys");
   if (rc) return rc;
-  scan_blocks_kernel<<<blocks, kScanThreads, 0, s>>>(hist, buckets, totals);
+  launch_kernel(scan_blocks_kernel, blocks, kScanThreads, 0, s, hist, buckets, totals);
   rc = check_launch("dp_order_cells_by_bin scan");
   if (rc) return rc;
-  scan_totals_kernel<<<1, kScanThreads, 0, s>>>(totals, blocks);
+  launch_kernel(scan_totals_kernel, 1, kScanThreads, 0, s, totals, blocks);
   rc = check_launch("dp_order_cells_by_bin scan totals");
   if (rc) return rc;
-  add_block_offsets_kernel<<<blocks, kScanThreads, 0, s>>>(hist, buckets, totals);
+  launch_kernel(add_block_offsets_kernel, blocks, kScanThreads, 0, s, hist, buckets, totals);
   rc = check_launch("dp_order_cells_by_bin offsets");
   if (rc) return rc;
-  order_place_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(keys, num_nodes, num_movable, num_filler, hist, order);
+  launch_kernel(order_place_kernel, grid_for(count, 256, 8), 256, 0, s, keys, num_nodes, num_movable, num_filler, hist, order);
   return check_launch("dp_order_cells_by_bin place");
 }
 
@@ -1313,7 +1331,7 @@ extern "C" int dp_gather_order_pos(const float* pos, int num_nodes, const int* o
   DP_REQUIRE(pos && xy_o && (count == 0 || order), "dp_gather_order_pos: null pointer argument");
   DP_REQUIRE(((uintptr_t)xy_o & 7) == 0, "dp_gather_order_pos: xy_o must be 8-byte aligned");
   if (count == 0) return DP_OK;
-  gather_order_pos_kernel<<<grid_for(count, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(gather_order_pos_kernel, grid_for(count, 256, 8), 256, 0, as_stream(stream), 
       pos, num_nodes, order, count, reinterpret_cast<float2*>(xy_o));
   return check_launch("dp_gather_order_pos");
 }

@@ -20,6 +20,7 @@ __global__ void __launch_bounds__(256) electric_force_kernel(
     float bsy, float ibx, float iby, int num_movable, int filler_begin, int total,
     const int* __restrict__ sorted, float scale, float* __restrict__ gx_out,
     float* __restrict__ gy_out) {
+  grid_dep_sync();
   const float g = grad_pos[0];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     int i = idx < num_movable ? (sorted ? sorted[idx] : idx) : filler_begin + (idx - num_movable);
@@ -50,6 +51,7 @@ __global__ void __launch_bounds__(256) electric_force_kernel(
 }
 
 __global__ void zero_range_kernel(float* a, int begin, int end, float* b) {
+  grid_dep_sync();
   for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
     a[i] = 0.f;
     b[i] = 0.f;
@@ -68,6 +70,7 @@ __global__ void __launch_bounds__(256) electric_force_records_kernel(
     const float2* __restrict__ xy_o, const int* __restrict__ order, const float4* __restrict__ rec4,
     const float* __restrict__ ratio_o, int count, float xl, float yl, float bsx, float bsy, float ibx, float iby,
     float scale, float2* __restrict__ force_o, const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   const float g = grad_pos[0];
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
@@ -134,7 +137,7 @@ extern "C" int dp_electric_force_ordered(const float* grad_pos, int nbx, int nby
   DP_REQUIRE(((uintptr_t)xy_o & 7) == 0 && ((uintptr_t)rec4 & 15) == 0 && ((uintptr_t)force_o & 7) == 0,
              "dp_electric_force_ordered: misaligned xy_o / rec4 / force_o");
   if (count == 0) return DP_OK;
-  electric_force_records_kernel<<<grid_for(count, 256, 16), 256, 0, as_stream(stream)>>>(
+  launch_kernel(electric_force_records_kernel, grid_for(count, 256, 16), 256, 0, as_stream(stream), 
       grad_pos, nbx, nby, ex, ey, reinterpret_cast<const float2*>(xy_o), order, reinterpret_cast<const float4*>(rec4),
       ratio_o, count, xl, yl, bsx, bsy, ibx, iby, scale, reinterpret_cast<float2*>(force_o), trial_gate());
   return check_launch("dp_electric_force_ordered");
@@ -155,13 +158,13 @@ extern "C" int dp_electric_force(const float* grad_pos, int nbx, int nby, const 
   float* gy = out + num_nodes;
   int fixed_begin = nm, fixed_end = num_nodes - nf;
   if (fixed_end > fixed_begin) {
-    zero_range_kernel<<<grid_for(fixed_end - fixed_begin, 256), 256, 0, s>>>(gx, fixed_begin, fixed_end, gy);
+    launch_kernel(zero_range_kernel, grid_for(fixed_end - fixed_begin, 256), 256, 0, s, gx, fixed_begin, fixed_end, gy);
     int rc = check_launch("dp_electric_force zero");
     if (rc) return rc;
   }
   int total = nm + nf;
   if (total == 0) return DP_OK;
-  electric_force_kernel<<<grid_for(total, 256, 16), 256, 0, s>>>(
+  launch_kernel(electric_force_kernel, grid_for(total, 256, 16), 256, 0, s, 
       grad_pos, nbx, nby, ex, ey, pos, pos + num_nodes, sx, sy, ox, oy, ratio, xl, yl, bsx, bsy, ibx,
       iby, nm, num_nodes - nf, total, sorted, scale, gx, gy);
   return check_launch("dp_electric_force");
@@ -172,6 +175,7 @@ namespace dpb {
 // visiting order put back in node order
 __global__ void scatter_pairs_kernel(const float2* __restrict__ vals_o, const int* __restrict__ order, int count,
                                      int num_nodes, float* __restrict__ out) {
+  grid_dep_sync();
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
     const int i = __ldg(order + idx);
     const float2 v = __ldcs(vals_o + idx);
@@ -193,7 +197,7 @@ extern "C" int dp_scatter_pairs_to_nodes(const float* vals_o, const int* order, 
     return DP_ERR_CUDA;
   }
   if (count == 0) return DP_OK;
-  scatter_pairs_kernel<<<grid_for(count, 256, 8), 256, 0, s>>>(reinterpret_cast<const float2*>(vals_o), order, count,
+  launch_kernel(scatter_pairs_kernel, grid_for(count, 256, 8), 256, 0, s, reinterpret_cast<const float2*>(vals_o), order, count,
                                                                num_nodes, out);
   return check_launch("dp_scatter_pairs_to_nodes");
 }

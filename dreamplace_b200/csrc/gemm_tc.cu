@@ -167,6 +167,7 @@ struct TcConfig {
 template <int PREC, int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcBatch batch, int M,
                                                                  int N, int K, const int* __restrict__ gate) {
+  grid_dep_sync();
   // a closed trial gate (dp_set_trial_gate): every thread of every CTA returns
   // before any barrier, TMEM allocation or copy is set up
   if (gate_closed(gate)) return;
@@ -366,7 +367,7 @@ static int run_tc(int M, int N, int K, const dp_gemm_problem* probs, int count, 
   int rc_smem = opt_in_smem(kern, Cfg::kSmemBytes, "dp_transform_gemm");
   if (rc_smem) return rc_smem;
   dim3 grid(ceil_div(N, BN), ceil_div(M, TC_BM), count);
-  kern<<<grid, TC_THREADS, Cfg::kSmemBytes, s>>>(batch, M, N, K, trial_gate());
+  launch_kernel(kern, grid, TC_THREADS, Cfg::kSmemBytes, s, batch, M, N, K, trial_gate());
   return check_launch("dp_transform_gemm(tcgen05)");
 }
 

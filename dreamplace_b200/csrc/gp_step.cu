@@ -64,6 +64,7 @@ __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* 
                                       int num_nodes, int num_movable, int num_filler,
                                       const int* __restrict__ inv_order, float2* __restrict__ xy_o,
                                       const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   const float alpha = (float)st[NS_ALPHA];
   const float coef = (float)st[NS_COEF];
@@ -88,6 +89,7 @@ __global__ void nesterov_trial_kernel(const float* __restrict__ v, const float* 
 }
 
 __global__ void pack_xy_kernel(const float* __restrict__ v, float2* __restrict__ xy, int num_nodes) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x)
     xy[i] = make_float2(v[i], v[i + num_nodes]);
 }
@@ -98,6 +100,7 @@ __global__ void __launch_bounds__(256) precondition_norms_kernel(
     float* __restrict__ g_new, const float* __restrict__ g, const float* __restrict__ v_new,
     const float* __restrict__ v, const float* __restrict__ pws, const float* __restrict__ area,
     const float* __restrict__ lam_p, int num_nodes, double* __restrict__ partials) {
+  grid_dep_sync();
   const float lam = *lam_p;
   const int n2 = 2 * num_nodes;
   double dv = 0.0, dg = 0.0;
@@ -135,6 +138,7 @@ __global__ void __launch_bounds__(kAsmThreads, 4) assemble_precondition_kernel(
     const float* __restrict__ v_new, const float* __restrict__ v, const float* __restrict__ g,
     float* __restrict__ g_new, double* __restrict__ partials, const int* __restrict__ grad_index,
     const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   __shared__ float2 s_q[kAsmThreads / 32][kAsmWarpPins];
   const float lam = *lam_p;
@@ -220,6 +224,7 @@ __global__ void __launch_bounds__(kAsmThreads, 4) assemble_precondition_kernel(
 }
 
 __global__ void nesterov_finish_kernel(double* st, const double* partials, int count) {
+  grid_dep_sync();
   double dv = finish_sum(partials, count);
   double dg = finish_sum(partials + count, count);
   if (threadIdx.x != 0) return;
@@ -233,6 +238,7 @@ __global__ void nesterov_finish_kernel(double* st, const double* partials, int c
 }
 
 __global__ void nesterov_init_kernel(double* st, double alpha) {
+  grid_dep_sync();
   st[NS_ALPHA] = alpha;
   st[NS_A] = 1.0;
   double an = (1.0 + sqrt(5.0)) / 2.0;
@@ -247,6 +253,7 @@ __global__ void nesterov_init_kernel(double* st, double alpha) {
 // (dreamplace/PlaceObj.py:293-320).
 __global__ void objective_finish_kernel(const double* wl, const double* energy, const float* density_weight,
                                         const float* factor_quad, double* obj, float* grad_scale) {
+  grid_dep_sync();
   const float density_factor = factor_quad[0], quad_c = factor_quad[1];
   double lam = (double)density_factor * (double)density_weight[0];
   double d = energy[0];
@@ -261,6 +268,7 @@ __global__ void objective_finish_kernel(const double* wl, const double* energy, 
 // the trial, its objective, wirelength and energy
 __global__ void trial_metrics_kernel(const double* hpwl, const double* overflow2, const double* state,
                                      const double* obj, const double* wl, const double* energy, double* out) {
+  grid_dep_sync();
   out[0] = hpwl[0];
   out[1] = overflow2[0];
   out[2] = overflow2[1];
@@ -278,7 +286,7 @@ using namespace dpb;
 extern "C" int dp_trial_metrics(const double* hpwl, const double* overflow2, const double* state, const double* obj,
                                 const double* wl, const double* energy, double* out8, dp_stream_t stream) {
   DP_REQUIRE(hpwl && overflow2 && state && obj && wl && energy && out8, "dp_trial_metrics: null pointer");
-  trial_metrics_kernel<<<1, 1, 0, as_stream(stream)>>>(hpwl, overflow2, state, obj, wl, energy, out8);
+  launch_kernel(trial_metrics_kernel, 1, 1, 0, as_stream(stream), hpwl, overflow2, state, obj, wl, energy, out8);
   return check_launch("dp_trial_metrics");
 }
 
@@ -286,13 +294,13 @@ extern "C" int dp_objective_finish(const double* wl, const double* energy, const
                                    const float* factor_quad, double* obj, float* grad_scale, dp_stream_t stream) {
   DP_REQUIRE(energy && density_weight && factor_quad && (obj || grad_scale) && (!obj || wl),
              "dp_objective_finish: null pointer");
-  objective_finish_kernel<<<1, 1, 0, as_stream(stream)>>>(wl, energy, density_weight, factor_quad, obj, grad_scale);
+  launch_kernel(objective_finish_kernel, 1, 1, 0, as_stream(stream), wl, energy, density_weight, factor_quad, obj, grad_scale);
   return check_launch("dp_objective_finish");
 }
 
 extern "C" int dp_nesterov_init(double* state, double alpha, dp_stream_t stream) {
   DP_REQUIRE(state, "dp_nesterov_init: null state");
-  nesterov_init_kernel<<<1, 1, 0, as_stream(stream)>>>(state, alpha);
+  launch_kernel(nesterov_init_kernel, 1, 1, 0, as_stream(stream), state, alpha);
   return check_launch("dp_nesterov_init");
 }
 
@@ -305,7 +313,7 @@ extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u,
              "dp_nesterov_trial: xy_new / xy_order must be 8-byte aligned");
   DP_REQUIRE(!xy_order || inv_order, "dp_nesterov_trial: xy_order needs inv_order");
   if (num_nodes == 0) return DP_OK;
-  nesterov_trial_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(nesterov_trial_kernel, grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream), 
       v, g, u, u_new, v_new, reinterpret_cast<float2*>(xy_new), state, sx, sy, xl, yl, xh, yh, num_nodes, num_movable,
       num_filler, inv_order, reinterpret_cast<float2*>(xy_order), trial_gate());
   return check_launch("dp_nesterov_trial");
@@ -314,7 +322,7 @@ extern "C" int dp_nesterov_trial(const float* v, const float* g, const float* u,
 extern "C" int dp_pack_xy(const float* pos, int num_nodes, float* xy, dp_stream_t stream) {
   DP_REQUIRE(pos && xy && ((uintptr_t)xy & 7) == 0, "dp_pack_xy: bad arguments");
   if (num_nodes == 0) return DP_OK;
-  pack_xy_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(pos, reinterpret_cast<float2*>(xy),
+  launch_kernel(pack_xy_kernel, grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream), pos, reinterpret_cast<float2*>(xy),
                                                                             num_nodes);
   return check_launch("dp_pack_xy");
 }
@@ -327,10 +335,10 @@ extern "C" int dp_precondition_step_size(float* g_new, const float* g, const flo
   int blocks = grid_for(2ll * num_nodes, 256, 4);
   if (2 * blocks > 2 * DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
-  precondition_norms_kernel<<<blocks, 256, 0, s>>>(g_new, g, v_new, v, pws, area, lambda_, num_nodes, partials);
+  launch_kernel(precondition_norms_kernel, blocks, 256, 0, s, g_new, g, v_new, v, pws, area, lambda_, num_nodes, partials);
   int rc = check_launch("dp_precondition_step_size");
   if (rc) return rc;
-  nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
+  launch_kernel(nesterov_finish_kernel, 1, 256, 0, s, state, partials, blocks);
   return check_launch("dp_precondition_step_size finish");
 }
 
@@ -353,6 +361,7 @@ __global__ void iteration_head_kernel(const double* __restrict__ st_prev, double
                                       const double* __restrict__ hpwl_k, const double* __restrict__ ovf_k,
                                       const float* __restrict__ w_prev, float* __restrict__ w_new, double base_gamma,
                                       double total_area, double ref_hpwl, double lower, double upper, int* gate) {
+  grid_dep_sync();
   // the previous trial was rejected: this iteration was enqueued ahead and is
   // void; its gated kernels return at once
   if (gate) *gate = st_prev[NS_ACCEPT] == 0.0 ? 1 : 0;
@@ -393,7 +402,7 @@ extern "C" int dp_iteration_head(const double* state_prev, double* state_new, co
   DP_REQUIRE(state_prev != state_new && sched_prev != sched_new && weights_prev != weights_new,
              "dp_iteration_head: the previous and the new iteration need separate buffers");
   DP_REQUIRE(total_area > 0.0 && ref_hpwl > 0.0, "dp_iteration_head: total_area and ref_hpwl must be positive");
-  iteration_head_kernel<<<1, 1, 0, as_stream(stream)>>>(state_prev, state_new, sched_prev, sched_new, hpwl_k,
+  launch_kernel(iteration_head_kernel, 1, 1, 0, as_stream(stream), state_prev, state_new, sched_prev, sched_new, hpwl_k,
                                                         overflow_k, weights_prev, weights_new, base_gamma,
                                                         total_area, ref_hpwl, lower, upper, gate);
   return check_launch("dp_iteration_head");
@@ -416,6 +425,7 @@ __device__ __forceinline__ float warp_all(float v, int kind) {
 __global__ void node_sum_kernel(const float2* __restrict__ gnode, const int* __restrict__ node_start,
                                 const float* __restrict__ grad_p, int num_movable, int num_nodes, int accumulate,
                                 float* __restrict__ out_x, float* __restrict__ out_y) {
+  grid_dep_sync();
   const float g = *grad_p;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
     float sx = 0.f, sy = 0.f;
@@ -445,7 +455,7 @@ extern "C" int dp_node_pin_sum(const float* grad_node_order, int num_slots, cons
   DP_REQUIRE(grad_node_order && node_start && grad_pos && grad_out, "dp_node_pin_sum: null pointer argument");
   if (num_nodes == 0) return DP_OK;
   DP_REQUIRE(((uintptr_t)grad_node_order & 7) == 0, "dp_node_pin_sum: grad_node_order must be 8-byte aligned");
-  dpb::node_sum_kernel<<<dpb::grid_for(num_nodes, 256, 8), 256, 0, dpb::as_stream(stream)>>>(
+  launch_kernel(dpb::node_sum_kernel, dpb::grid_for(num_nodes, 256, 8), 256, 0, dpb::as_stream(stream), 
       reinterpret_cast<const float2*>(grad_node_order), node_start, grad_pos, num_movable, num_nodes, accumulate,
       grad_out, grad_out + num_nodes);
   return dpb::check_launch("dp_node_pin_sum");
@@ -467,13 +477,13 @@ extern "C" int dp_assemble_precondition_step(const float* grad_node_order, const
   int blocks = grid_for(num_nodes, kAsmThreads, 4);
   if (blocks > DP_REDUCE_DOUBLES) blocks = DP_REDUCE_DOUBLES;
   double* partials = state + DP_NESTEROV_STATE_DOUBLES;
-  assemble_precondition_kernel<<<blocks, kAsmThreads, 0, s>>>(
+  launch_kernel(assemble_precondition_kernel, blocks, kAsmThreads, 0, s, 
       reinterpret_cast<const float2*>(grad_node_order), node_start, wl_scale, reinterpret_cast<const float2*>(force_o),
       inv_order, num_movable, num_filler, pws, area, lambda_, num_nodes, v_new, v, g, g_new, partials, grad_index,
       trial_gate());
   int rc = check_launch("dp_assemble_precondition_step");
   if (rc) return rc;
-  nesterov_finish_kernel<<<1, 256, 0, s>>>(state, partials, blocks);
+  launch_kernel(nesterov_finish_kernel, 1, 256, 0, s, state, partials, blocks);
   return check_launch("dp_assemble_precondition_step finish");
 }
 
@@ -820,6 +830,7 @@ template <bool kGrad, bool kPins>
 __global__ void __launch_bounds__(256, 4) wa_lane_kernel(LaneArgs A, double* __restrict__ partials,
                                                       double* __restrict__ hpwl_partials,
                                                       const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -962,12 +973,12 @@ static int launch_lanes(bool grad, const dpb::LaneArgs& A, double* out_f64, doub
   if (blocks > kNumSMs * 4) blocks = kNumSMs * 4;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
   if (grad && A.px)
-    wa_lane_kernel<true, true><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
+    launch_kernel(wa_lane_kernel<true, true>, blocks, 256, 0, s, A, out_f64 + 1, nullptr, trial_gate());
   else if (grad)
-    wa_lane_kernel<true, false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr,
+    launch_kernel(wa_lane_kernel<true, false>, blocks, 256, 0, s, A, out_f64 + 1, hpwl_f64 ? hpwl_f64 + 1 : nullptr,
                                                        trial_gate());
   else
-    wa_lane_kernel<false, false><<<blocks, 256, 0, s>>>(A, out_f64 + 1, nullptr, trial_gate());
+    launch_kernel(wa_lane_kernel<false, false>, blocks, 256, 0, s, A, out_f64 + 1, nullptr, trial_gate());
   int rc = check_launch(grad ? "dp_wa_lanes_forward" : "dp_hpwl_lanes");
   if (rc) return rc;
   // the WA total and the HPWL (same fixed-order reduction each) in one launch
@@ -1052,6 +1063,7 @@ namespace dpb {
 __global__ void wa_pins_backward_kernel(const float2* __restrict__ grad_lane, const int* __restrict__ lane_of_pin,
                                         const unsigned char* __restrict__ pin_mask, const float* __restrict__ grad_out,
                                         int num_pins, float* __restrict__ gx, float* __restrict__ gy) {
+  grid_dep_sync();
   const float g = grad_out[0];
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < num_pins; p += gridDim.x * blockDim.x) {
     float x = 0.f, y = 0.f;
@@ -1072,7 +1084,7 @@ extern "C" int dp_wa_pins_backward(const float* grad_lane, const int* lane_of_pi
   DP_REQUIRE(grad_lane && lane_of_pin && grad_out && grad_pin_pos, "dp_wa_pins_backward: null pointer argument");
   DP_REQUIRE(((uintptr_t)grad_lane & 7) == 0, "dp_wa_pins_backward: grad_lane must be 8-byte aligned");
   if (num_pins == 0) return DP_OK;
-  wa_pins_backward_kernel<<<grid_for(num_pins, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(wa_pins_backward_kernel, grid_for(num_pins, 256, 8), 256, 0, as_stream(stream), 
       reinterpret_cast<const float2*>(grad_lane), lane_of_pin, pin_mask, grad_out, num_pins, grad_pin_pos,
       grad_pin_pos + num_pins);
   return check_launch("dp_wa_pins_backward");

@@ -33,6 +33,7 @@ constexpr int SBM = 128, SBN = 64, SBK = 16;
 
 __global__ void __launch_bounds__(256) simt_gemm_kernel(SimtBatch batch, int M, int N, int K,
                                                         const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   const SimtProblem& P = batch.p[blockIdx.z];
   __shared__ float As[2][SBK][SBM + 4];
@@ -149,6 +150,7 @@ template <int FMT>
 __global__ void prepare_operand_kernel(const float* __restrict__ x, size_t n, float scale,
                                        float* __restrict__ f32, __nv_bfloat16* __restrict__ hi,
                                        __nv_bfloat16* __restrict__ lo, const int* __restrict__ gate) {
+  grid_dep_sync();
   if (gate_closed(gate)) return;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     float v = __fmul_rn(x[i], scale);
@@ -184,7 +186,7 @@ extern "C" int dp_transform_gemm(int precision, int M, int N, int K, const dp_ge
                "dp_transform_gemm: fp32 operands need 16-byte aligned rows");
   }
   dim3 grid(ceil_div(N, SBN), ceil_div(M, SBM), count);
-  simt_gemm_kernel<<<grid, 256, 0, s>>>(b, M, N, K, trial_gate());
+  launch_kernel(simt_gemm_kernel, grid, 256, 0, s, b, M, N, K, trial_gate());
   return check_launch("dp_transform_gemm(fp32)");
 }
 
@@ -198,18 +200,19 @@ extern "C" int dp_prepare_operand(int precision, const float* x, size_t n, float
   cudaStream_t s = as_stream(stream);
   int g = grid_for((long long)n, 256, 8);
   if (fmt == kFmtF32)
-    prepare_operand_kernel<kFmtF32><<<g, 256, 0, s>>>(x, n, scale, out_f32, nullptr, nullptr, trial_gate());
+    launch_kernel(prepare_operand_kernel<kFmtF32>, g, 256, 0, s, x, n, scale, out_f32, nullptr, nullptr, trial_gate());
   else if (fmt == kFmtBF16)
-    prepare_operand_kernel<kFmtBF16><<<g, 256, 0, s>>>(x, n, scale, nullptr, (__nv_bfloat16*)out_hi, nullptr,
+    launch_kernel(prepare_operand_kernel<kFmtBF16>, g, 256, 0, s, x, n, scale, nullptr, (__nv_bfloat16*)out_hi, nullptr,
                                                        trial_gate());
   else
-    prepare_operand_kernel<kFmtSplit><<<g, 256, 0, s>>>(x, n, scale, nullptr, (__nv_bfloat16*)out_hi,
+    launch_kernel(prepare_operand_kernel<kFmtSplit>, g, 256, 0, s, x, n, scale, nullptr, (__nv_bfloat16*)out_hi,
                                                         (__nv_bfloat16*)out_lo, trial_gate());
   return check_launch("dp_prepare_operand");
 }
 
 namespace dpb {
 __global__ void spectral_table_kernel(EpiParams p, float* out) {
+  grid_dep_sync();
   const size_t mn = (size_t)p.M * p.N;
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < mn; t += (size_t)gridDim.x * blockDim.x) {
     float wx, wy, wi;
@@ -228,6 +231,6 @@ extern "C" int dp_spectral_weights(int M, int N, float wv_scale, float* out, dp_
   q.epilogue = DP_EPI_SPECTRAL;
   q.wv_scale = wv_scale;
   EpiParams e = make_epi(q, DP_PREC_FP32, M, N);
-  spectral_table_kernel<<<grid_for((long long)M * N, 256, 8), 256, 0, as_stream(stream)>>>(e, out);
+  launch_kernel(spectral_table_kernel, grid_for((long long)M * N, 256, 8), 256, 0, as_stream(stream), e, out);
   return check_launch("dp_spectral_weights");
 }

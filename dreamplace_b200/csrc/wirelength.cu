@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(256) wa_merged_forward_kernel(
     const unsigned char* __restrict__ net_mask, const float* __restrict__ inv_gamma_p,
     float* __restrict__ partial_wl, double* __restrict__ partials, float* __restrict__ gx,
     float* __restrict__ gy) {
+  grid_dep_sync();
   const float inv_gamma = *inv_gamma_p;
   double contrib = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
@@ -101,6 +102,7 @@ __global__ void wa_merged_backward_kernel(const float* __restrict__ grad_pos,
                                           const unsigned char* __restrict__ net_mask,
                                           const unsigned char* __restrict__ pin_mask, int num_pins,
                                           float* __restrict__ gx, float* __restrict__ gy) {
+  grid_dep_sync();
   const float g = grad_pos[0];
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < num_pins; p += gridDim.x * blockDim.x) {
     float vx = fmul(gx[p], g), vy = fmul(gy[p], g);
@@ -125,6 +127,7 @@ __global__ void pin_pos_forward_kernel(const float* __restrict__ x, const float*
                                        const float* __restrict__ offx, const float* __restrict__ offy,
                                        const int* __restrict__ pin2node, int num_pins,
                                        float* __restrict__ pin_x, float* __restrict__ pin_y) {
+  grid_dep_sync();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < num_pins; p += gridDim.x * blockDim.x) {
     int n = pin2node[p];
     pin_x[p] = fadd(offx[p], x[n]);
@@ -136,6 +139,7 @@ __global__ void pin_pos_backward_kernel(const float* __restrict__ gpx, const flo
                                         const int* __restrict__ flat_node2pin,
                                         const int* __restrict__ node_start, int num_physical,
                                         int num_nodes, float* __restrict__ gx, float* __restrict__ gy) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
     float sx = 0.f, sy = 0.f;
     if (i < num_physical) {
@@ -157,6 +161,7 @@ __global__ void __launch_bounds__(256) hpwl_kernel(const float* __restrict__ px,
                                                    const float* __restrict__ net_weights,
                                                    const unsigned char* __restrict__ net_mask,
                                                    double* __restrict__ partials) {
+  grid_dep_sync();
   double c = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nets; i += gridDim.x * blockDim.x) {
     if (net_mask[i]) {
@@ -181,6 +186,7 @@ __global__ void move_boundary_kernel(float* __restrict__ x, float* __restrict__ 
                                      const float* __restrict__ sx, const float* __restrict__ sy,
                                      float xl, float yl, float xh, float yh, int num_nodes,
                                      int num_movable, int num_filler) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
     if (i < num_movable || i >= num_nodes - num_filler) {
       float vx = fmaxf(x[i], xl);
@@ -196,6 +202,7 @@ __global__ void move_boundary_kernel(float* __restrict__ x, float* __restrict__ 
 __global__ void pws_kernel(const float* __restrict__ w, const int* __restrict__ flat_nodepin,
                            const int* __restrict__ node_start, const int* __restrict__ pin2net,
                            int num_physical, int num_nodes, float* __restrict__ out) {
+  grid_dep_sync();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < num_nodes; i += gridDim.x * blockDim.x) {
     float s = 0.f;
     if (i < num_physical)
@@ -219,7 +226,7 @@ extern "C" int dp_wa_merged_forward(const float* pin_pos, int num_pins, const in
   cudaStream_t s = as_stream(stream);
   int blocks = num_nets > 0 ? grid_for(num_nets, 256, 8) : 1;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  wa_merged_forward_kernel<<<blocks, 256, 0, s>>>(pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets,
+  launch_kernel(wa_merged_forward_kernel, blocks, 256, 0, s, pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets,
                                                  net_weights, net_mask, inv_gamma, partial_wl, wl_f64 + 1,
                                                  grad_intermediate, grad_intermediate + num_pins);
   int rc = check_launch("dp_wa_merged_forward");
@@ -235,7 +242,7 @@ extern "C" int dp_wa_merged_backward(const float* grad_pos, const int* pin2net_m
   DP_REQUIRE(!net_weights || (pin2net_map && net_mask), "dp_wa_merged_backward: net weights need pin2net_map and net_mask");
   if (num_pins == 0) return DP_OK;
   cudaStream_t s = as_stream(stream);
-  wa_merged_backward_kernel<<<grid_for(num_pins, 256, 8), 256, 0, s>>>(
+  launch_kernel(wa_merged_backward_kernel, grid_for(num_pins, 256, 8), 256, 0, s, 
       grad_pos, pin2net_map, net_weights, net_mask, pin_mask, num_pins, grad_intermediate,
       grad_intermediate + num_pins);
   return check_launch("dp_wa_merged_backward");
@@ -246,7 +253,7 @@ extern "C" int dp_pin_pos_forward(const float* pos, int num_nodes, const float* 
                                   float* pin_pos, dp_stream_t stream) {
   DP_REQUIRE(pos && offx && offy && pin2node && pin_pos, "dp_pin_pos_forward: null pointer argument");
   if (num_pins == 0) return DP_OK;
-  pin_pos_forward_kernel<<<grid_for(num_pins, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(pin_pos_forward_kernel, grid_for(num_pins, 256, 8), 256, 0, as_stream(stream), 
       pos, pos + num_nodes, offx, offy, pin2node, num_pins, pin_pos, pin_pos + num_pins);
   return check_launch("dp_pin_pos_forward");
 }
@@ -257,7 +264,7 @@ extern "C" int dp_pin_pos_backward(const float* grad_pin, int num_pins, const in
   DP_REQUIRE(grad_pin && flat_node2pin && node_start && grad_pos, "dp_pin_pos_backward: null pointer argument");
   DP_REQUIRE(num_physical <= num_nodes, "dp_pin_pos_backward: num_physical_nodes > num_nodes");
   if (num_nodes == 0) return DP_OK;
-  pin_pos_backward_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(pin_pos_backward_kernel, grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream), 
       grad_pin, grad_pin + num_pins, flat_node2pin, node_start, num_physical, num_nodes, grad_pos,
       grad_pos + num_nodes);
   return check_launch("dp_pin_pos_backward");
@@ -271,7 +278,7 @@ extern "C" int dp_hpwl(const float* pin_pos, int num_pins, const int* flat_netpi
   cudaStream_t s = as_stream(stream);
   int blocks = num_nets > 0 ? grid_for(num_nets, 256, 8) : 1;
   if (blocks > kMaxReduceBlocks) blocks = kMaxReduceBlocks;
-  hpwl_kernel<<<blocks, 256, 0, s>>>(pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets, net_weights,
+  launch_kernel(hpwl_kernel, blocks, 256, 0, s, pin_pos, pin_pos + num_pins, flat_netpin, netpin_start, num_nets, net_weights,
                                     net_mask, out_f64 + 1);
   int rc = check_launch("dp_hpwl");
   if (rc) return rc;
@@ -282,7 +289,7 @@ extern "C" int dp_move_boundary(float* pos, int num_nodes, const float* sx, cons
                                 float yl, float xh, float yh, int nm, int nf, dp_stream_t stream) {
   DP_REQUIRE(pos && sx && sy, "dp_move_boundary: null pointer argument");
   if (num_nodes == 0) return DP_OK;
-  move_boundary_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(
+  launch_kernel(move_boundary_kernel, grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream), 
       pos, pos + num_nodes, sx, sy, xl, yl, xh, yh, num_nodes, nm, nf);
   return check_launch("dp_move_boundary");
 }
@@ -292,7 +299,7 @@ extern "C" int dp_pin_weight_sum(const float* w, const int* flat_nodepin, const 
                                  dp_stream_t stream) {
   DP_REQUIRE(w && flat_nodepin && node_start && pin2net && out, "dp_pin_weight_sum: null pointer argument");
   if (num_nodes == 0) return DP_OK;
-  pws_kernel<<<grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream)>>>(w, flat_nodepin, node_start,
+  launch_kernel(pws_kernel, grid_for(num_nodes, 256, 8), 256, 0, as_stream(stream), w, flat_nodepin, node_start,
                                                                         pin2net, num_physical, num_nodes, out);
   return check_launch("dp_pin_weight_sum");
 }
