@@ -650,6 +650,58 @@ __global__ void first_map_kernel(const long long* __restrict__ fixed, const floa
   block_partial(s, partials);
 }
 
+// fp32 split scatter, second pass: first = init + first (the movable cells
+// were scattered onto a zeroed map), all += first (all held the fillers), and
+// the overflow sum and maximum of first as overflow_kernel does.  float4
+// accesses when the three maps are 16-byte aligned.
+__device__ __forceinline__ void finish_map_bin(float f, float in, float& first_out, float& all_io, double target_area,
+                                               double& s, float& m) {
+  const float d = fadd(in, f);
+  first_out = d;
+  all_io = fadd(d, all_io);
+  const double over = (double)d - target_area;
+  s += over > 0.0 ? over : 0.0;
+  m = fmaxf(m, d);
+}
+
+__global__ void finish_maps_kernel(const float* __restrict__ init, float* __restrict__ first, float* __restrict__ all,
+                                   int n, double target_area, double* partials, unsigned* maxkey,
+                                   const int* __restrict__ gate) {
+  grid_dep_sync();
+  if (gate_closed(gate)) return;
+  double s = 0.0;
+  float m = -INFINITY;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const bool vec = (((uintptr_t)first | (uintptr_t)all | (uintptr_t)init) & 15) == 0;
+  int done = 0;
+  if (vec) {
+    const int n4 = n >> 2;
+    for (int i = tid; i < n4; i += stride) {
+      const float4 f = reinterpret_cast<const float4*>(first)[i];
+      const float4 in = init ? reinterpret_cast<const float4*>(init)[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 a = reinterpret_cast<const float4*>(all)[i];
+      float4 o;
+      finish_map_bin(f.x, in.x, o.x, a.x, target_area, s, m);
+      finish_map_bin(f.y, in.y, o.y, a.y, target_area, s, m);
+      finish_map_bin(f.z, in.z, o.z, a.z, target_area, s, m);
+      finish_map_bin(f.w, in.w, o.w, a.w, target_area, s, m);
+      reinterpret_cast<float4*>(first)[i] = o;
+      reinterpret_cast<float4*>(all)[i] = a;
+    }
+    done = n4 << 2;
+  }
+  for (int i = done + tid; i < n; i += stride) {
+    float o, a = all[i];
+    finish_map_bin(first[i], init ? init[i] : 0.f, o, a, target_area, s, m);
+    first[i] = o;
+    all[i] = a;
+  }
+  if (!partials) return;  // uniform: no overflow wanted
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxkey, float_key(m));
+  block_partial(s, partials);
+}
+
 __global__ void overflow_finish_kernel(double* out2, const unsigned* maxkey, double bin_area,
                                        float* out2_f32, const double* partials, int count) {
   grid_dep_sync();
@@ -996,11 +1048,11 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
     return convert_fixed(scratch, init, fraction_bits, out_all, nbins, o.s);
   }
   // fp32: both ranges in one launch (the second range's blocks fill the
-  // first's last wave), the first onto out_first = init, the second onto
-  // out_all = 0; then out_all += out_first, with the overflow of out_first
-  rc = start_map(init, out_first, nbins, o.s);
-  if (rc) return rc;
-  cudaError_t e = cudaMemsetAsync(out_all, 0, sizeof(float) * nbins, o.s);
+  // first's last wave), the first onto out_first = 0, the second onto
+  // out_all = 0; then out_first += init and out_all += out_first, with the
+  // overflow of out_first
+  cudaError_t e = cudaMemsetAsync(out_first, 0, sizeof(float) * nbins, o.s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(out_all, 0, sizeof(float) * nbins, o.s);
   if (e != cudaSuccess) {
     set_error("dp_density_map_ordered_split: cudaMemsetAsync: %s", cudaGetErrorString(e));
     return DP_ERR_CUDA;
@@ -1015,7 +1067,7 @@ extern "C" int dp_density_map_ordered_split(const float* xy_o, const int* order,
   rc = scatter_ranges(o, rg, 0, 0);
   if (rc) return rc;
   if (overflow_out) cudaMemsetAsync(maxslot, 0, sizeof(double), o.s);
-  launch_kernel(first_map_kernel, blocks, 256, 0, o.s, nullptr, nullptr, 0.0, out_first, out_all, 1, nbins, target_area,
+  launch_kernel(finish_maps_kernel, blocks, 256, 0, o.s, init, out_first, out_all, nbins, target_area,
                                              overflow_out ? overflow_out + 3 : nullptr, maxslot, trial_gate());
   rc = check_launch("dp_density_map_ordered_split first map");
   if (rc || !overflow_out) return rc;

@@ -30,17 +30,19 @@ __device__ __forceinline__ void block_partial(double a, double* partials) {
   __syncthreads();
 }
 
+// every thread returns the same total: strided per-thread sums, an xor
+// butterfly per warp (identical in every lane), then the warp totals in warp
+// order; a fixed order, two block barriers
 __device__ __forceinline__ double finish_sum(const double* partials, int count) {
-  __shared__ double sh[kReduceThreads];
+  __shared__ double sh[kReduceThreads / 32];
   double v = 0.0;
   for (int i = threadIdx.x; i < count; i += kReduceThreads) v += partials[i];
-  sh[threadIdx.x] = v;
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
-  for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-    __syncthreads();
-  }
-  double r = sh[0];
+  double r = 0.0;
+#pragma unroll
+  for (int w = 0; w < kReduceThreads / 32; ++w) r += sh[w];
   __syncthreads();
   return r;
 }
