@@ -231,7 +231,8 @@ class TimedRun(object):
                     means = eng.piece_means()
                     if means:
                         self.dominant = max(means, key=means.get)
-                        eng.reset_piece_times([self.dominant])
+                        # the timed trials carry the dominant piece's two events only
+                        eng.time_only([self.dominant])
                 torch.cuda.synchronize()
                 barrier(self.world)
                 torch.cuda.synchronize()

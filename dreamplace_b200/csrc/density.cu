@@ -1212,7 +1212,11 @@ __global__ void order_keys_kernel(const float* __restrict__ pos, int num_nodes, 
     const unsigned key = (((tx * (unsigned)tiles_y + ty) << 8) | ((kx & 15u) << 4) | (hy & 15u)) +
                          (i < nm ? 0u : tile_buckets);
     keys[i] = key;
-    atomicAdd(hist + key, 1u);
+    // one atomic per distinct bucket of the warp (clustered cells share a few
+    // buckets early in GP)
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, key);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + key, (unsigned)__popc(peers));
   }
 }
 
@@ -1300,7 +1304,16 @@ __global__ void order_place_kernel(const unsigned* __restrict__ keys, int num_no
   grid_dep_sync();
   const int count = nm + nf;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const int slot = (int)atomicAdd(starts + keys[i], 1u);
+    // warp-aggregated bucket slots: the leader of each group of lanes with one
+    // key takes them all, each lane its rank among the group
+    const unsigned key = keys[i];
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, key);
+    const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(starts + key, (unsigned)__popc(peers));
+    base = __shfl_sync(active, base, leader);
+    const int slot = (int)(base + (unsigned)__popc(peers & ((1u << lane) - 1u)));
     if (i < nm)
       order[block_spread_slot(slot, 0, nm)] = i;
     else

@@ -181,6 +181,7 @@ class GPEngine(object):
         self.piece_events = None
         self._mark_slot = 0
         self.piece_query = set(PIECES)
+        self.piece_record = set(PIECES)  # pieces whose events the captured trials record
         self.piece_ms = {k: 0.0 for k in PIECES}
         self.piece_n = {k: 0 for k in PIECES}
         if getattr(params, "time_pieces", False):
@@ -421,7 +422,7 @@ class GPEngine(object):
         return energy
 
     def _mark(self, piece, which):
-        if self.piece_events is not None:
+        if self.piece_events is not None and piece in self.piece_record:
             self.piece_events[self._mark_slot][piece][which].record()
 
     def _collect_pieces(self, s):
@@ -434,6 +435,28 @@ class GPEngine(object):
         self.piece_query = set(PIECES) if query is None else set(query)
         self.piece_ms = {k: 0.0 for k in PIECES}
         self.piece_n = {k: 0 for k in PIECES}
+
+    def time_only(self, pieces):
+        """Keep the in-graph timing events of `pieces` only and capture the
+        trial graphs again now (each event is a graph node that also breaks
+        the programmatic launch overlap of the kernels around it, ~10% of a
+        trial for all pieces).  Call between iterations, outside a timed
+        window; the engine's lazy resources are initialised by then, so the
+        graphs are captured without a warm-up run."""
+        self.reset_piece_times(pieces)
+        self.piece_record = set(pieces)
+        if not self.use_graphs or not self.graphs:
+            return
+        torch.cuda.synchronize(self.dev)
+        # the old graphs keep the shared memory pool alive until the new ones
+        # are captured into it
+        old = (self.graphs, self.graph_exec, self.graph_kernels)
+        self.graphs, self.graph_exec, self.graph_kernels = {}, {}, {}
+        for q in range(NSLOT):
+            for head in (False, True):
+                self._graph(q, head, warm=False)
+        torch.cuda.synchronize(self.dev)
+        del old
 
     def piece_means(self):
         """Mean device ms per trial of each timed piece."""

@@ -49,6 +49,33 @@ def test_gp_converges_and_split_bf16_matches_plain(design):
     assert abs(split["hpwl"] - plain["hpwl"]) <= 1e-3 * plain["hpwl"], (split, plain)
 
 
+def test_recapture_with_one_timed_piece_keeps_the_trajectory(design):
+    """GPEngine.time_only (the bench's timed window): the trial graphs,
+    captured again mid-GP with one piece's events, follow the run that kept
+    its first graphs bit for bit (deterministic mode), and the piece is timed."""
+    p = lambda **kw: Params(target_density=design.target_density, stop_overflow=0.07,  # noqa: E731
+                            dct_precision="split_bf16", deterministic_flag=1, **kw)
+    t1, t2 = [], []
+    place(design, p(time_pieces=True), max_iterations=40, callback=lambda it, m: t1.append((m.hpwl, m.overflow)))
+    holder = {}
+
+    def cb(it, m):
+        t2.append((m.hpwl, m.overflow))
+        if it == 12:
+            eng = holder["placer"].stepper.eng
+            eng.time_only(["wa_forward"])
+            holder["eng"] = eng
+
+    from dreamplace_b200.nonlinear_place import NonLinearPlace
+    params = p(time_pieces=True)
+    placer = NonLinearPlace(params, design, "cuda")
+    holder["placer"] = placer
+    placer(params, design, max_iterations=40, callback=cb)
+    assert t1 == t2
+    means = holder["eng"].piece_means()
+    assert set(means) == {"wa_forward"} and means["wa_forward"] > 0
+
+
 def test_gp_deterministic_mode_is_reproducible(design):
     p = lambda: Params(target_density=design.target_density, stop_overflow=0.07, dct_precision="fp32",  # noqa: E731
                        deterministic_flag=1)
