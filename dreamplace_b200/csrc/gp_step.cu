@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) precondition_norms_kernel(
 // shared buffer; each lane then folds its own node's staged pins in pin order,
 // so the sums are those of the sequential per-node loop.
 constexpr int kAsmThreads = 256;
-constexpr int kAsmWarpPins = 256;
+constexpr int kAsmWarpPins = 128;
 
 __global__ void __launch_bounds__(kAsmThreads, 4) assemble_precondition_kernel(
     const float2* __restrict__ gnode, const int* __restrict__ node_start, const float* __restrict__ wl_scale_p,
