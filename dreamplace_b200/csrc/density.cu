@@ -367,41 +367,46 @@ __global__ void __launch_bounds__(kTsThreads) tile_scatter_kernel(TriangleArgs a
           vals[c][3 * i + j] = __float2int_rn(y);
         }
     }
-    // tile slot of window entry (i, j) of a cell at (rk, rh) with nk x nh
-    // bins; entries beyond the footprint (value 0) land on the window's
-    // first row / column
-    auto slot_of = [P](int rk, int rh, int nk_, int nh_, int i, int j) {
-      return (i < nk_ ? rk + i : rk) * P + rh + (j < nh_ ? j : 0);
-    };
-    bool merged = false;
+    // same start bin: cell 0 takes the merged window (the larger extents;
+    // each cell's entries beyond its footprint are zero) and cell 1 adds none
+    bool add1 = ok[1];
+    int mk = nk[0], mh = nh[0];
     if (ok[0] && ok[1] && k0[0] == k0[1] && h0[0] == h0[1]) {
-      merged = true;
-      const int mk = max(nk[0], nk[1]), mh = max(nh[0], nh[1]);
-      const int rk = k0[0] - bk0, rh = h0[0] - bh0;
+      add1 = false;
+      mk = max(nk[0], nk[1]);
+      mh = max(nh[0], nh[1]);
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          atomicAdd(plane0 + slot_of(rk, rh, mk, mh, i, j),
-                    (i < mk && j < mh) ? vals[0][3 * i + j] + vals[1][3 * i + j] : 0);
+      for (int t = 0; t < 9; ++t) vals[0][t] += vals[1][t];
     }
+    // one predicated pass per cell: a warp whose lanes all merged skips the second
 #pragma unroll
     for (int c = 0; c < kTsCellsPerThread; ++c) {
-      if (merged || nk[c] == 0) continue;
-      if (ok[c]) {
-        const int rk = k0[c] - bk0, rh = h0[c] - bh0;
+      const bool add = c == 0 ? ok[0] : add1;
+      if (!__any_sync(0xffffffffu, add)) continue;
+      const int ek = c == 0 ? mk : nk[1], eh = c == 0 ? mh : nh[1];
+      const int rk = k0[c] - bk0, rh = h0[c] - bh0;
+      int row[3], col[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        row[j] = (j < ek ? rk + j : rk) * P + rh;
+        col[j] = j < eh ? j : 0;
+      }
+      if (add) {
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int j = 0; j < 3; ++j) atomicAdd(plane0 + slot_of(rk, rh, nk[c], nh[c], i, j), vals[c][3 * i + j]);
-      } else {
-        // outside the tile, wider than 3 bins, or beyond the plane's range:
-        // one global add per bin
-        for (int k = k0[c]; k < k0[c] + nk[c]; ++k) {
-          const float pxr = fmul(triangle_overlap(nx[c], sx[c], a.xl, k, a.bsx), rr[c]);
-          for (int h = h0[c]; h < h0[c] + nh[c]; ++h)
-            atomicAdd(map_f32 + k * nby + h, fmul(pxr, triangle_overlap(ny[c], sy[c], a.yl, h, a.bsy)));
-        }
+          for (int j = 0; j < 3; ++j) atomicAdd(plane0 + row[i] + col[j], vals[c][3 * i + j]);
+      }
+    }
+    // outside the tile, wider than 3 bins, or beyond the plane's range: one
+    // global add per bin
+#pragma unroll
+    for (int c = 0; c < kTsCellsPerThread; ++c) {
+      if (nk[c] == 0 || ok[c]) continue;
+      for (int k = k0[c]; k < k0[c] + nk[c]; ++k) {
+        const float pxr = fmul(triangle_overlap(nx[c], sx[c], a.xl, k, a.bsx), rr[c]);
+        for (int h = h0[c]; h < h0[c] + nh[c]; ++h)
+          atomicAdd(map_f32 + k * nby + h, fmul(pxr, triangle_overlap(ny[c], sy[c], a.yl, h, a.bsy)));
       }
     }
   }
