@@ -55,6 +55,8 @@ def parse():
                     help="skip the runs of both Poisson-solve forms to the 0.07 overflow stop")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host round-trip run (profiling)")
+    ap.add_argument("--no-dropin", action="store_true",
+                    help="skip timing the reference-facing modules (ElectricPotential, WeightedAverageWirelength)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the per-kernel timing (profiling)")
     ap.add_argument("--skip-to", type=int, default=0,
                     help="run this many GP iterations untimed before the warm-up (times a later GP stage; "
@@ -350,6 +352,84 @@ def kernel_roofline(placer, design, peaks, reps=20):
     return {k: (t[k],) + work[k] for k in t}
 
 
+def dropin_ops(placer, design, peaks, precision, reps=10):
+    """The reference-facing modules timed alone at the current GP position:
+    ElectricPotential forward + backward (density map, Poisson solve, field
+    gather) in fp32-atomic and deterministic (int64) scatter modes, and PinPos
+    + WeightedAverageWirelength forward + backward.  CUDA events around reps
+    eager calls after one warm call.  Algorithmic bytes: the electric potential
+    reads 28 B per scattered cell twice (scatter, gather) and writes 8 B of
+    force, plus the bin maps (4 B init read, two 4 B maps written, two 4 B
+    field maps read); the Poisson GEMMs are counted as flops.  WA: pin_pos
+    reads 8 B per node and 12 B per pin (node id, offsets) and writes 8 B per
+    pin; WA reads 8 B and writes 8 B per pin gradient, plus 10 B per net;
+    the backward sums 8 B per pin into 8 B per node."""
+    import numpy as np
+    from dreamplace_b200.electric_potential import ElectricPotential, poisson_flops
+    from dreamplace_b200.placement_ops import PinPos
+    from dreamplace_b200.weighted_average_wirelength import WeightedAverageWirelength
+    from dreamplace_b200._native import precision_code
+    d = design
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    pos0 = placer.stepper.position().detach().clone()
+    m, n = d.num_movable_nodes, d.num_nodes
+    n_s = m + d.num_filler_nodes
+    M, N = d.num_bins_x, d.num_bins_y
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out = {}
+
+    def time_fn(fn):
+        fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    bcx = t(d.bin_centers(d.xl, d.xh, d.bin_size_x))
+    bcy = t(d.bin_centers(d.yl, d.yh, d.bin_size_y))
+    sorted_map = t(np.argsort(d.node_size_x[:m], kind="stable").astype(np.int32))
+    ep_bytes = 2 * 28.0 * n_s + 8.0 * n_s + 4.0 * M * N * 5
+    for det in (0, 1):
+        ep = ElectricPotential(t(d.node_size_x), t(d.node_size_y), bcx, bcy, d.target_density, d.xl, d.yl, d.xh,
+                               d.yh, d.bin_size_x, d.bin_size_y, m, d.num_terminals, d.num_filler_nodes, 0,
+                               bool(det), sorted_map, precision=precision)
+        pos = pos0.clone().requires_grad_(True)
+
+        def ep_step():
+            pos.grad = None
+            ep(pos).backward()
+        ms = time_fn(ep_step)
+        out["electric_potential_" + ("deterministic" if det else "fp32_atomic")] = {
+            "ms": round(ms, 4), "hbm_bytes": ep_bytes, "gemm_flop": poisson_flops(M, N, precision_code(precision)),
+            "achieved_gbs_if_hbm_only": round(ep_bytes / (ms * 1e-3) / 1e9, 1)}
+        del ep
+    deg = np.diff(d.flat_net2pin_start_map)
+    mask = ((deg >= 2) & (deg < 100)).astype(np.uint8)
+    pin_pos = PinPos(t(d.pin_offset_x), t(d.pin_offset_y), t(d.pin2node_map), t(d.flat_node2pin_map),
+                     t(d.flat_node2pin_start_map), d.num_physical_nodes)
+    gamma = torch.tensor(4.0 * (d.bin_size_x + d.bin_size_y), device=dev)
+    wa = WeightedAverageWirelength(t(d.flat_net2pin_map), t(d.flat_net2pin_start_map), t(d.pin2net_map),
+                                   t(d.net_weights), t(mask), t(d.pin2node_map >= m), gamma, algorithm="merged")
+    pos = pos0.clone().requires_grad_(True)
+
+    def wa_step():
+        pos.grad = None
+        wa(pin_pos(pos)).backward()
+    ms = time_fn(wa_step)
+    P, E = d.num_pins, d.num_nets
+    wa_bytes = 8.0 * n + 12.0 * P + 8.0 * P + 16.0 * P + 10.0 * E + 8.0 * P + 8.0 * n
+    out["weighted_average_wirelength"] = {"ms": round(ms, 4), "hbm_bytes": wa_bytes,
+                                          "achieved_gbs": round(wa_bytes / (ms * 1e-3) / 1e9, 1),
+                                          "frac": round(wa_bytes / (ms * 1e-3) / 1e9 / hbm, 4)}
+    out["timing"] = "CUDA events around %d eager forward + backward calls at the GP position of the timed run" % reps
+    return out
+
+
 def full_gp(design, precision, deterministic, max_iterations=3000):
     """Global placement of the design to the 0.07 overflow stop through the
     public placer; final metrics and wall time.  The 2.1M-cell design needs
@@ -613,6 +693,7 @@ def main():
         e2e = {"value": round(replica_value(K, world, ms_e2e), 3), "unit": UNIT,
                "h2d_bytes_per_step": run_e2e.h2d, "d2h_bytes_per_step": run_e2e.d2h}
     pieces = {} if args.no_roofline else kernel_roofline(run.placer, design, peaks)
+    dropin = None if args.no_dropin else dropin_ops(run.placer, design, peaks, args.precision)
     roof = None
     if run.dominant is not None and run.dominant_ms:
         work, bound = piece_work(design, run.placer.stepper.eng)[run.dominant]
@@ -667,6 +748,7 @@ def main():
                 "trials_per_step": round(run.trials / max(K, 1), 3),
                 "voided_speculative_trials": int(run.trials - K),
                 "plain_fp32": plain,
+                "dropin_ops": dropin,
                 "full_gp_to_overflow_0.07": convergence,
                 "hpwl_rel_diff_final": (convergence["fp32_atomic"]["hpwl_rel_diff_final"]
                                         if convergence else None)}

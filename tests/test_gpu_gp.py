@@ -249,3 +249,10 @@ def test_best_position_copied_before_its_slot_is_reused(design):
     eng.set_position(buf)  # completes the pending copy, then restores from it
     torch.cuda.synchronize()
     assert torch.equal(buf, third) and torch.equal(eng.current_position(), third)
+
+
+def test_profile_piece_runs_every_piece():
+    """The profiling entry point runs each piece of the trial on a GP state."""
+    from dreamplace_b200 import profile_piece
+    for piece in profile_piece.PIECES:
+        profile_piece.main(["--piece", piece, "--design", "cells_10k", "--iterations", "3", "--repeat", "1"])
