@@ -55,6 +55,8 @@ def parse():
                     help="skip the runs of both Poisson-solve forms to the 0.07 overflow stop")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host round-trip run (profiling)")
+    ap.add_argument("--process-warmup", type=int, default=50,
+                    help="GP iterations of an untimed run of the same design before the timed run (0: none)")
     ap.add_argument("--no-dropin", action="store_true",
                     help="skip timing the reference-facing modules (ElectricPotential, WeightedAverageWirelength)")
     ap.add_argument("--no-roofline", action="store_true", help="skip the per-kernel timing (profiling)")
@@ -679,6 +681,14 @@ def main():
     W, K = max(args.warmup, 3), args.steps
     clocks = ClockSampler(local) if rank == 0 else None
     spec = not args.no_speculate
+    if args.process_warmup > 0:
+        # an untimed GP run of the same design first: the timed run then starts
+        # with the process's one-time costs (lazy kernel loading, allocator
+        # growth, first-call host paths) behind it, as every later run does
+        pre = TimedRun(design, args.precision, world, speculate=spec)
+        pre.run(3, args.process_warmup)
+        del pre
+        torch.cuda.empty_cache()
     run = TimedRun(design, args.precision, world, time_pieces=not args.no_roofline, speculate=spec)
     ms = run.run(W, K, clocks=clocks, skip=args.skip_to)
     clk = clocks.stop() if clocks else None
@@ -739,7 +749,9 @@ def main():
                            % (design.name, design.num_movable_nodes, design.num_terminals, design.num_filler_nodes,
                               design.num_nets, design.num_pins, design.num_bins_x, design.num_bins_y),
                            "dct_precision": args.precision, "parallelism": "replicas%d" % world,
-                           "l2": "per-iteration working set > 126 MB L2, no flush"},
+                           "l2": "per-iteration working set > 126 MB L2, no flush",
+                           "process_warmup": "%d untimed GP iterations of the same design in a separate run "
+                                             "before the timed run" % args.process_warmup},
                 "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "kernel_ms": {k: round(v[0], 4) for k, v in pieces.items()},
