@@ -312,8 +312,10 @@ def piece_work(design, eng):
     * assemble_precondition: per pin 8 B gradient read; per node 4 B pin
       start + 4 B inverse order + 8 B force + 4 B pin weight sum + 4 B area +
       3 x 8 B (v_new, v, g) read + 8 B written;
-    * nesterov_trial: per node 3 x 8 B read (v, g, u), 2 x 8 B written (u, v)
-      + 8 B interleaved copy + 8 B cell size."""
+    * nesterov_trial: per node 3 x 8 B read (v, g, u) + 8 B cell size, 2 x 8 B
+      written (u, v) + 8 B interleaved copy; per scattered cell 4 B order
+      index + 8 B visiting-order copy written (the gather's re-read of the
+      interleaved copy is not counted)."""
     from dreamplace_b200.electric_potential import poisson_flops
     d, ep = design, eng.ep
     n_s = d.num_movable_nodes + d.num_filler_nodes
@@ -324,7 +326,7 @@ def piece_work(design, eng):
             "field_gather": (36.0 * n_s + 8.0 * M * N, "hbm"),
             "wa_forward": (20.0 * P + 10.0 * E + 8.0 * n, "hbm"),
             "assemble_precondition": (8.0 * P + 64.0 * n, "hbm"),
-            "nesterov_trial": (64.0 * n, "hbm")}
+            "nesterov_trial": (56.0 * n + 12.0 * n_s, "hbm")}
 
 
 def kernel_roofline(placer, design, peaks, reps=20):

@@ -441,8 +441,21 @@ __global__ void gather_order_xy_kernel(const float2* __restrict__ xy, const int*
                                        float2* __restrict__ xy_o, const int* __restrict__ gate) {
   grid_dep_sync();
   if (gate_closed(gate)) return;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
-    xy_o[idx] = xy[order[idx]];
+  // four independent gathers in flight per thread: the random 8-byte reads
+  // are latency-bound, not bandwidth-bound
+  const int stride = gridDim.x * blockDim.x;
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; (long long)idx + 3ll * stride < count; idx += 4 * stride) {
+    int o[4];
+    float2 q[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) o[u] = order[idx + u * stride];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) q[u] = xy[o[u]];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xy_o[idx + u * stride] = q[u];
+  }
+  for (; idx < count; idx += stride) xy_o[idx] = xy[order[idx]];
 }
 
 __global__ void build_records_kernel(const float* __restrict__ sx, const float* __restrict__ sy,

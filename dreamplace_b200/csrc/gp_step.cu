@@ -541,10 +541,52 @@ __device__ __forceinline__ float2 lane_xy(const LaneArgs& A, int p) {
 // itself (lane-slot order, gathered by the assembly through grad_index)
 __device__ __forceinline__ int grad_slot(const LaneArgs& A, int p) { return A.ln_csr ? __ldcs(A.ln_csr + p) : p; }
 
-// a = (1 - b * xe) / e evaluated as the reference does (the literal 1.0
-// promotes the expression to double), rounded to float
-__device__ __forceinline__ float wa_a_term(float b, float xe, float e) {
-  return (float)((1.0 - (double)fmul(b, xe)) / (double)e);
+// Quotients of the WA sums.  Every exponential sum e is >= 1 (the extreme pin
+// of a net contributes exp(0) = 1), so 1/e comes from one rcp.approx (within
+// one ulp; no denormal or special operand can occur) and x / e from
+// q = x * (1/e) with one FMA-residual correction (Markstein, IBM J. Res. Dev.
+// 34(1), 1990): the residual x - q e is exact in one fma, and
+// q + (x - q e) / e is the correctly rounded quotient -- the value of the
+// reference's fp32 division -- in all but near-tie cases.
+__device__ __forceinline__ float sum_rcp(float e) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
+  return r;
+}
+
+__device__ __forceinline__ float sum_quot(float x, float e, float r) {
+  const float q = fmul(x, r);
+  return __fmaf_rn(__fmaf_rn(-q, e, x), r, q);
+}
+
+// a = (1 - b xe) / e.  The reference forms 1 - b xe in double (the literal
+// 1.0 promotes it; weighted_average_wirelength_merged.cpp) and rounds the
+// double quotient to float.  Here 1 - p (p = b xe rounded to float) is carried
+// exactly as the float pair s + t (Knuth's TwoSum, TAOCP vol. 2, 4.2.2) and
+// (s + t) / e is corrected as in sum_quot: the same float in all but near-tie
+// cases, with no fp64 arithmetic.
+__device__ __forceinline__ float wa_a_term(float b, float xe, float e, float r) {
+  const float p = fmul(b, xe);
+  const float s = fsub(1.f, p);
+  const float bb = fsub(s, 1.f);
+  const float t = fadd(fsub(1.f, fsub(s, bb)), fsub(-p, bb));
+  const float q = fmul(s, r);
+  return __fmaf_rn(fadd(__fmaf_rn(-q, e, s), t), r, q);
+}
+
+// b = ig / e and a = (1 - b xe) / e of one direction of a net
+__device__ __forceinline__ void wa_terms(float ig, float e, float xe, float& b, float& a) {
+  const float r = sum_rcp(e);
+  b = sum_quot(ig, e, r);
+  a = wa_a_term(b, xe, e, r);
+}
+
+// the WA value of a net from its eight sums
+__device__ __forceinline__ float wa_value(float xe_p, float e_p, float xe_n, float e_n, float ye_p, float f_p,
+                                          float ye_n, float f_n) {
+  return fsub(fadd(fsub(sum_quot(xe_p, e_p, sum_rcp(e_p)), sum_quot(xe_n, e_n, sum_rcp(e_n))),
+                   sum_quot(ye_p, f_p, sum_rcp(f_p))),
+              sum_quot(ye_n, f_n, sum_rcp(f_n)));
 }
 
 template <int D, bool kGrad, bool kPins>
@@ -612,13 +654,13 @@ __device__ __forceinline__ void lane_net(const LaneArgs& A, float ig, int base, 
     ye_p = fadd(ye_p, fmul(y[j], a3));
     ye_n = fadd(ye_n, fmul(y[j], a4));
   }
-  const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                        __fdiv_rn(ye_n, f_n));
+  const float wl = wa_value(xe_p, e_p, xe_n, e_n, ye_p, f_p, ye_n, f_n);
   contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
-  const float b_x = __fdiv_rn(ig, e_p), a_x = wa_a_term(b_x, xe_p, e_p);
-  const float b_nx = __fdiv_rn(-ig, e_n), a_nx = wa_a_term(b_nx, xe_n, e_n);
-  const float b_y = __fdiv_rn(ig, f_p), a_y = wa_a_term(b_y, ye_p, f_p);
-  const float b_ny = __fdiv_rn(-ig, f_n), a_ny = wa_a_term(b_ny, ye_n, f_n);
+  float b_x, a_x, b_nx, a_nx, b_y, a_y, b_ny, a_ny;
+  wa_terms(ig, e_p, xe_p, b_x, a_x);
+  wa_terms(-ig, e_n, xe_n, b_nx, a_nx);
+  wa_terms(ig, f_p, ye_p, b_y, a_y);
+  wa_terms(-ig, f_n, ye_n, b_ny, a_ny);
 #pragma unroll
   for (int j = 0; j < D; ++j) {
     const float a1 = kKeep ? ex[kKeep ? j : 0] : expf(fmul(fsub(x[j], x_max), ig));
@@ -721,14 +763,14 @@ __device__ void sub_net(const LaneArgs& A, float ig, int base, int deg, int lane
     return;
   }
   if (sl == 0) {
-    const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                          __fdiv_rn(ye_n, f_n));
+    const float wl = wa_value(xe_p, e_p, xe_n, e_n, ye_p, f_p, ye_n, f_n);
     contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
   }
-  const float b_x = __fdiv_rn(ig, e_p), a_x = wa_a_term(b_x, xe_p, e_p);
-  const float b_nx = __fdiv_rn(-ig, e_n), a_nx = wa_a_term(b_nx, xe_n, e_n);
-  const float b_y = __fdiv_rn(ig, f_p), a_y = wa_a_term(b_y, ye_p, f_p);
-  const float b_ny = __fdiv_rn(-ig, f_n), a_ny = wa_a_term(b_ny, ye_n, f_n);
+  float b_x, a_x, b_nx, a_nx, b_y, a_y, b_ny, a_ny;
+  wa_terms(ig, e_p, xe_p, b_x, a_x);
+  wa_terms(-ig, e_n, xe_n, b_nx, a_nx);
+  wa_terms(ig, f_p, ye_p, b_y, a_y);
+  wa_terms(-ig, f_n, ye_n, b_ny, a_ny);
 #pragma unroll
   for (int t = 0; t < kSubPins; ++t) {
     const int j = sl + kSubLanes * t;
@@ -797,15 +839,17 @@ __device__ void warp_net(const LaneArgs& A, float ig, int base, int deg, int lan
     xe_p = warp_all(xe_p, 2); xe_n = warp_all(xe_n, 2); e_p = warp_all(e_p, 2); e_n = warp_all(e_n, 2);
     ye_p = warp_all(ye_p, 2); ye_n = warp_all(ye_n, 2); f_p = warp_all(f_p, 2); f_n = warp_all(f_n, 2);
     if (lane == 0) {
-      const float wl = fsub(fadd(fsub(__fdiv_rn(xe_p, e_p), __fdiv_rn(xe_n, e_n)), __fdiv_rn(ye_p, f_p)),
-                            __fdiv_rn(ye_n, f_n));
+      const float wl = wa_value(xe_p, e_p, xe_n, e_n, ye_p, f_p, ye_n, f_n);
       contrib += (double)(A.net_weights ? fmul(wl, w) : wl);
     }
   }
-  const float b_x = on ? __fdiv_rn(ig, e_p) : 0.f, a_x = on ? wa_a_term(b_x, xe_p, e_p) : 0.f;
-  const float b_nx = on ? __fdiv_rn(-ig, e_n) : 0.f, a_nx = on ? wa_a_term(b_nx, xe_n, e_n) : 0.f;
-  const float b_y = on ? __fdiv_rn(ig, f_p) : 0.f, a_y = on ? wa_a_term(b_y, ye_p, f_p) : 0.f;
-  const float b_ny = on ? __fdiv_rn(-ig, f_n) : 0.f, a_ny = on ? wa_a_term(b_ny, ye_n, f_n) : 0.f;
+  float b_x = 0.f, a_x = 0.f, b_nx = 0.f, a_nx = 0.f, b_y = 0.f, a_y = 0.f, b_ny = 0.f, a_ny = 0.f;
+  if (on) {
+    wa_terms(ig, e_p, xe_p, b_x, a_x);
+    wa_terms(-ig, e_n, xe_n, b_nx, a_nx);
+    wa_terms(ig, f_p, ye_p, b_y, a_y);
+    wa_terms(-ig, f_n, ye_n, b_ny, a_ny);
+  }
   for (int j = lane; j < deg; j += 32) {
     float gx = 0.f, gy = 0.f;
     if (on) {

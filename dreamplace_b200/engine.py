@@ -554,7 +554,6 @@ class GPEngine(object):
         """One Nesterov trial from slot s into slot s + 1.  head: the first trial
         of an iteration k >= 1, preceded by the loop's between-iteration work on
         the device (advance, density weight, gamma from slot s - 1)."""
-        d = self.design
         t = (s + 1) % NSLOT
         self._mark_slot = s
         gate = self.gate if self.use_graphs else None
@@ -564,28 +563,29 @@ class GPEngine(object):
                              self.weights[r], self.weights[s], *self.head_scalars, gate=gate)
         elif gate is not None:
             C.trial_gate(gate)
-        v, g, u = self.V[s], self.G[s], self.U[s]
-        vn, gn, un = self.V[t], self.G[t], self.U[t]
+        v, g = self.V[s], self.G[s]
+        vn, gn = self.V[t], self.G[t]
         st = self.S[s]
         self._mark("nesterov_trial", 0)
-        scatter_write = self.xyo_mode == "trial"
-        C.nesterov_trial(v, g, u, un, vn, self.XY[t], st, self.data.node_size_x, self.data.node_size_y,
-                         float(d.xl), float(d.yl), float(d.xh), float(d.yh), d.num_movable_nodes, d.num_filler_nodes,
-                         self.inv_order if scatter_write else None, self.XYO[t] if scatter_write else None)
-        if self.xyo_mode == "gather":
-            C.gather_order_xy(self.XY[t], self.order, self.order.numel(), self.XYO[t])
+        self.nesterov_trial_only(s)
         self._mark("nesterov_trial", 1)
         energy = self.objective_and_step(v, g, vn, gn, s)
         # HPWL / overflow of v_k (computed when v_k was the trial point), then the trial's scalars
         C.trial_metrics(self.H[s], self.O[s], st, self.obj64, self.wl64, energy, self.metrics[s])
 
     def nesterov_trial_only(self, s):
-        """The trial-point kernel alone (used for per-kernel timing)."""
+        """The trial point from slot s into slot s + 1, and its visiting-order
+        copy for the scatter (xyo_mode "trial": written by the trial kernel
+        through inv_order; "gather": gathered through order after it)."""
         d = self.design
         t = (s + 1) % NSLOT
+        scatter_write = self.xyo_mode == "trial"
         C.nesterov_trial(self.V[s], self.G[s], self.U[s], self.U[t], self.V[t], self.XY[t], self.S[s],
                          self.data.node_size_x, self.data.node_size_y, float(d.xl), float(d.yl), float(d.xh),
-                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes, self.inv_order, self.XYO[t])
+                         float(d.yh), d.num_movable_nodes, d.num_filler_nodes,
+                         self.inv_order if scatter_write else None, self.XYO[t] if scatter_write else None)
+        if self.xyo_mode == "gather":
+            C.gather_order_xy(self.XY[t], self.order, self.order.numel(), self.XYO[t])
 
     def _body(self, s, head):
         # v_k was clamped into the die when it was produced (trial kernel, or
