@@ -204,6 +204,10 @@ class TimedRun(object):
         self.world = world
         self.placer = NonLinearPlace(self.params, design, "cuda")
         self.e2e = e2e
+        # the host round trip runs in E2E_CHUNKS pieces on two copy streams:
+        # the upload of piece i overlaps the download of piece i + 1 (PCIe is
+        # full duplex and each direction has its own copy engine)
+        self.copy_streams = (torch.cuda.Stream(), torch.cuda.Stream()) if e2e else None
 
     def run(self, warmup, steps, clocks=None, skip=0):
         """skip: GP iterations run (untimed) before the warm-up, to time a
@@ -249,8 +253,7 @@ class TimedRun(object):
                 if self.e2e:
                     # host round trip of the step's state: positions out and back in, metrics out
                     cur = self.placer.stepper.position()
-                    host_pos.copy_(cur, non_blocking=True)
-                    cur.copy_(host_pos, non_blocking=True)
+                    host_round_trip(cur, host_pos, self.copy_streams)
                     self.h2d = host_pos.numel() * 4
                     self.d2h = host_pos.numel() * 4 + 3 * 8
                 if it == warmup + steps - 1:
@@ -274,6 +277,32 @@ class TimedRun(object):
         self.trials = state.get("trials1", 0) - state.get("trials0", 0)
         self.wall = wall
         return ms
+
+
+E2E_CHUNKS = 8
+
+
+def host_round_trip(dev, host, streams, chunks=E2E_CHUNKS):
+    """dev -> pinned host -> dev, in order with the current stream: the
+    download starts after the work already enqueued on it, and work enqueued
+    after this call starts after the upload.  The buffer goes in `chunks`
+    pieces on two copy streams, piece i's upload waiting only for piece i's
+    download."""
+    main = torch.cuda.current_stream()
+    down, up = streams
+    down.wait_stream(main)
+    n = dev.numel()
+    step = (n + chunks - 1) // chunks
+    for a in range(0, n, step):
+        b = min(a + step, n)
+        with torch.cuda.stream(down):
+            host[a:b].copy_(dev[a:b], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(down)
+        up.wait_event(done)
+        with torch.cuda.stream(up):
+            dev[a:b].copy_(host[a:b], non_blocking=True)
+    main.wait_stream(up)
 
 
 def _graph_time(fn, reps=20):
