@@ -440,8 +440,90 @@ def ep_options():
     np.savez_compressed(os.path.join(HERE, "ep_options.npz"), **res)
 
 
+def _unwrap_arrays(node):
+    """np.array(x, ...) / x.astype(...) -> x, recursively, so nested array
+    literals (lists of index arrays) evaluate with ast.literal_eval."""
+    class Strip(ast.NodeTransformer):
+        def visit_Call(self, call):
+            self.generic_visit(call)
+            f = call.func
+            if isinstance(f, ast.Attribute) and f.attr == "array" and call.args:
+                return call.args[0]
+            if isinstance(f, ast.Attribute) and f.attr == "astype":
+                return f.value
+            return call
+    return Strip().visit(node)
+
+
+def reference_test_values(relpath, func):
+    """Like reference_test_literals, with nested np.array literals unwrapped."""
+    tree = ast.parse(open(os.path.join(REF, relpath)).read())
+    fn = next(n for n in ast.walk(tree) if isinstance(n, ast.FunctionDef) and n.name == func)
+    out = {}
+    for st in fn.body:
+        if isinstance(st, ast.Assign) and len(st.targets) == 1 and isinstance(st.targets[0], ast.Name):
+            try:
+                out[st.targets[0].id] = ast.literal_eval(_unwrap_arrays(st.value))
+            except ValueError:
+                pass
+    return out
+
+
+def ops_unit():
+    """The reference's unit-test cases of the ops beside the hot path, through
+    its CPU ops: hpwl (unittest/ops/hpwl_unittest.py, test_hpwlRandom: 5 pins,
+    2 weighted nets), pin_pos (unittest/ops/pin_pos_unittest.py,
+    test_pin_pos_random: 2 physical nodes, 5 pins; the test flattens its 3 x 2
+    position array row-major, so x = (1, 10, 2), y = (20, 3, 30)) forward and
+    the backward of sum(pin_pos), and move_boundary
+    (unittest/ops/move_boundary_unittest.py: 2 movable cells, one outside the
+    die)."""
+    hp, pp, mb = need("hpwl_cpp"), need("pin_pos_cpp"), need("move_boundary_cpp")
+    res = {}
+    a = reference_test_values("unittest/ops/hpwl_unittest.py", "test_hpwlRandom")
+    pin = np.array(a["pin_pos"], np.float32)
+    nets = a["net2pin_map"]
+    flat = np.array([q for n in nets for q in n], np.int32)
+    start = np.r_[0, np.cumsum([len(n) for n in nets])].astype(np.int32)
+    weights = np.array(a["net_weights"], np.float32)
+    mask = np.ones(len(nets), np.uint8)  # the test's mask: degree <= max degree
+    pos = np.concatenate([pin[:, 0], pin[:, 1]]).astype(np.float32)
+    res.update(hpwl_pin_pos=pos, hpwl_flat_netpin=flat, hpwl_netpin_start=start, hpwl_net_weights=weights,
+               hpwl_net_mask=mask,
+               hpwl=np.float32(hp.forward(t(pos), t(flat), t(start), t(weights), t(mask)).item()))
+    a = reference_test_values("unittest/ops/pin_pos_unittest.py", "test_pin_pos_random")
+    pos = np.array(a["pos"], np.float32).reshape(-1)
+    node2pin = a["node2pin_map"]
+    num_pins = sum(len(q) for q in node2pin)
+    p2n = np.zeros(num_pins, np.int32)
+    for node, pins in enumerate(node2pin):
+        p2n[list(pins)] = node
+    fn2p = np.array([q for pins in node2pin for q in pins], np.int32)
+    nstart = np.r_[0, np.cumsum([len(q) for q in node2pin])].astype(np.int32)
+    offx, offy = np.array(a["pin_offset_x"], np.float32), np.array(a["pin_offset_y"], np.float32)
+    tp = t(pos)
+    out = pp.forward(tp, t(offx), t(offy), t(p2n.astype(np.int64)), t(fn2p), t(nstart))
+    back = pp.backward(torch.ones(2 * num_pins), tp, t(offx), t(offy), t(p2n.astype(np.int64)), t(fn2p), t(nstart),
+                       len(node2pin))
+    res.update(pp_pos=pos, pp_offset_x=offx, pp_offset_y=offy, pp_pin2node=p2n, pp_flat_node2pin=fn2p,
+               pp_node_start=nstart, pp_num_physical=np.int32(len(node2pin)), pin_pos=out.numpy().copy(),
+               pin_pos_backward=back.numpy().copy())
+    a = reference_test_values("unittest/ops/move_boundary_unittest.py", "test_densityOverflowRandom")
+    xx, yy = np.array(a["xx"], np.float32), np.array(a["yy"], np.float32)
+    sx, sy = np.array(a["node_size_x"], np.float32), np.array(a["node_size_y"], np.float32)
+    box = np.array([a["xl"], a["yl"], a["xh"], a["yh"]], np.float64)
+    mpos = np.concatenate([xx, yy])
+    num_movable = len(xx)  # the test's num_movable_nodes = len(xx)
+    moved = mb.forward(t(mpos.copy()), t(sx), t(sy), *[float(v) for v in box], num_movable,
+                       int(a["num_filler_nodes"]))
+    res.update(mb_pos=mpos, mb_node_size_x=sx, mb_node_size_y=sy, mb_box=box,
+               mb_num_movable=np.int32(num_movable), mb_num_filler=np.int32(a["num_filler_nodes"]),
+               move_boundary=moved.numpy().copy())
+    np.savez_compressed(os.path.join(HERE, "ops_unit.npz"), **res)
+
+
 FIXTURES = {"wa_unit": wa_unit, "dct_small": dct_small, "design_small": design_small, "ep_unit": ep_unit,
-            "dct_unit": dct_unit, "wa_edge": wa_edge, "ep_options": ep_options}
+            "dct_unit": dct_unit, "wa_edge": wa_edge, "ep_options": ep_options, "ops_unit": ops_unit}
 
 if __name__ == "__main__":
     torch.set_num_threads(1)

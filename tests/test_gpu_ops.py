@@ -180,6 +180,27 @@ def test_wa_unit_golden(C, golden):
     np.testing.assert_allclose(out.cpu().numpy(), g["grad"], rtol=1e-6, atol=1e-7)
 
 
+def test_ops_unit_cases(C, golden):
+    """The reference's own unit-test cases of hpwl, pin_pos and move_boundary
+    (unittest/ops/{hpwl,pin_pos,move_boundary}_unittest.py) through the CUDA
+    ops: pin_pos forward / backward and move_boundary bit for bit against the
+    reference's CPU ops, the HPWL to the float32 total they return."""
+    g = golden("ops_unit.npz")
+    h = C.hpwl_forward(dev(g["hpwl_pin_pos"]), dev(g["hpwl_flat_netpin"]), dev(g["hpwl_netpin_start"]),
+                       dev(g["hpwl_net_weights"]), dev(g["hpwl_net_mask"]))
+    assert math.isclose(float(h.item()), float(g["hpwl"]), rel_tol=1e-6)
+    pos = dev(g["pp_pos"])
+    pin = C.pin_pos_forward(pos, dev(g["pp_offset_x"]), dev(g["pp_offset_y"]), dev(g["pp_pin2node"]))
+    assert np.array_equal(pin.cpu().numpy(), g["pin_pos"])
+    back = C.pin_pos_backward(torch.ones(2 * len(g["pp_pin2node"]), device="cuda"), pos, dev(g["pp_flat_node2pin"]),
+                              dev(g["pp_node_start"]), int(g["pp_num_physical"]))
+    assert np.array_equal(back.cpu().numpy(), g["pin_pos_backward"])
+    moved = dev(g["mb_pos"])
+    C.move_boundary_forward(moved, dev(g["mb_node_size_x"]), dev(g["mb_node_size_y"]), *[float(v) for v in g["mb_box"]],
+                            int(g["mb_num_movable"]), int(g["mb_num_filler"]))
+    assert np.array_equal(moved.cpu().numpy(), g["move_boundary"])
+
+
 def test_move_boundary_and_pws(C):
     d = synthetic.cells_10k()
     pos = d.initial_positions()

@@ -189,3 +189,24 @@ def test_ep_options_oracle(golden):
     ba = d.bin_size_x * d.bin_size_y
     assert math.isclose(np.clip(om - target * ba, 0, None).sum(), float(g["overflow"]), rel_tol=1e-5)
     assert math.isclose(om.max() / ba, float(g["max_density"]), rel_tol=1e-6)
+
+
+def test_ops_unit_golden(golden):
+    """The reference's own unit-test cases of hpwl, pin_pos and move_boundary
+    (unittest/ops/{hpwl,pin_pos,move_boundary}_unittest.py) as its CPU ops
+    computed them: the oracle agrees bit for bit (HPWL: to the float32 the
+    reference returns)."""
+    g = golden("ops_unit.npz")
+    h = oracle.hpwl(g["hpwl_pin_pos"], g["hpwl_flat_netpin"], g["hpwl_netpin_start"], g["hpwl_net_mask"],
+                    g["hpwl_net_weights"])
+    # the reference returns its total as float32; the oracle sums in fp64
+    assert math.isclose(h, float(g["hpwl"]), rel_tol=1e-6)
+    n = len(g["pp_pos"]) // 2
+    pin = oracle.pin_pos(g["pp_pos"], g["pp_offset_x"], g["pp_offset_y"], g["pp_pin2node"], n)
+    assert np.array_equal(pin, g["pin_pos"])
+    back = oracle.pin_pos_backward(np.ones(2 * len(g["pp_pin2node"]), np.float32), g["pp_flat_node2pin"],
+                                   g["pp_node_start"], int(g["pp_num_physical"]), n)
+    assert np.array_equal(back, g["pin_pos_backward"])
+    moved = oracle.move_boundary(g["mb_pos"], g["mb_node_size_x"], g["mb_node_size_y"], *g["mb_box"],
+                                 int(g["mb_num_movable"]), int(g["mb_num_filler"]))
+    assert np.array_equal(moved, g["move_boundary"])
